@@ -1,0 +1,307 @@
+"""Benchmark: the plain photon-mapping frame at 10M photons, 1920x1080.
+
+One step = one full frame of the plain method on the ``cornell_hf_1080p``
+workload: trace 10M global photons (max 10 bounces), build the photon grid,
+render 1920x1080 (kNN k = 64, r = 0.05, eye depth 4).  ``value`` is Mphotons/s
+of the whole frame pipeline (photons / step time) summed over ranks;
+``ms_per_step`` is ms/frame.  Inputs (scene, photon maps ~0.5 GB) are larger
+than L2.  Multi-GPU: independent replicas (weak scaling, no collective on the
+data path; the photon maps do not exchange).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cuda-photon-mapping_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Mphotons/s + ms/frame @10M,1080p"
+WORKLOAD = "cornell_hf_1080p"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- CPU leg
+def cpu_reference_estimate(sc, w, rows=8, trace_photons=3000, threads=None):
+    """The reference's CPU path on the host cores, on a bounded sample, scaled
+    to one full frame of the workload.
+
+    * photon pass: the reference has no CPU tracer (emit is __device__); its
+      algorithm is timed as the oracle's restatement (brute-force closest hit,
+      OpenMP over the host cores) on ``trace_photons`` photons and scaled to
+      the workload's photon count;
+    * grid: the oracle's grid build on those photons, scaled linearly;
+    * frame: the reference's own Raytracer::render_trace (oracle/_ref, its CPU
+      mode) on ``rows`` full image rows, one process per host core, over a map
+      with the workload's photon density (the traced sample replicated with a
+      1e-4 jitter up to the workload's photon count), scaled to all rows.
+    """
+    import multiprocessing as mp
+    from oracle import Oracle
+    orc = Oracle()
+    s = orc.scene(sc)
+    threads = threads or os.cpu_count() or 1
+    t0 = time.perf_counter()
+    tr = s.trace_photons(w["seed"], w["max_bounces"], trace_photons)
+    t_trace = (time.perf_counter() - t0) * (w["photons"] / trace_photons)
+    t0 = time.perf_counter()
+    orc.grid_build(tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    t_grid = (time.perf_counter() - t0) * (w["photons"] / trace_photons)
+    n = w["photons"]
+    rep = int(np.ceil(n / trace_photons))
+    rng = np.random.default_rng(1)
+    pos = (np.tile(tr["g_pos"], (rep, 1))[:n] + rng.normal(scale=1e-4, size=(n, 3))).astype(np.float32)
+    dirs = np.tile(tr["g_dir"], (rep, 1))[:n]
+    pw = np.tile(tr["g_pow"], (rep, 1))[:n]
+    g = orc.grid_build(pos, pw, dirs, s.aabb())
+    H = w["height"]
+    ys = np.linspace(0, H - 1, rows).astype(int)
+    ctx = mp.get_context("spawn")
+    args = [(sc, w, g, int(y)) for y in ys]
+    t0 = time.perf_counter()
+    with ctx.Pool(min(threads, rows)) as pool:
+        per_row = pool.map(_ref_row, args)
+    wall = time.perf_counter() - t0
+    t_row = float(np.mean(per_row))
+    t_frame = t_row * H / threads
+    total = t_trace + t_grid + t_frame
+    return dict(step_s=total, trace_s=t_trace, grid_s=t_grid, frame_s=t_frame, row_s=t_row, cores=threads,
+                sample=f"{trace_photons} photons traced (scaled to {n}); {rows} of {H} rows rendered by the "
+                       f"reference's render_trace over a {n}-photon map (sample replicated), {threads} processes",
+                wall_s=wall)
+
+
+def _ref_row(arg):
+    sc, w, g, y = arg
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefHost
+    from photonmap import scenes
+    ref = RefHost()
+    rs = ref.scene(sc)
+    cam = scenes.default_camera(w["width"], w["height"])
+    t0 = time.perf_counter()
+    rs.render(cam, g, w["k"], w["radius"], w["max_depth"], y0=y, y1=y + 1)
+    return time.perf_counter() - t0
+
+
+# ----------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import photonmap
+    from photonmap import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sc, cs, w = scenes.workload(args.workload)
+    ctx = photonmap.Context(local)
+    ctx.set_scene(sc)
+    cam = photonmap.camera_setup(cs.position, cs.direction, cs.up, cs.fov_deg, cs.width, cs.height)
+    W, H = cs.width, cs.height
+    rgb = torch.empty(W * H * 3, dtype=torch.uint8, device="cuda")
+    host_rgb = torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True)
+
+    def step(i, e2e=False):
+        ctx.trace_photons(w["seed"] + 1000 * rank + i, w["max_bounces"], w["photons"])
+        ctx.build_grid(0)
+        ctx.render(cam, w["k"], w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb)
+        if e2e:
+            host_rgb.copy_(rgb, non_blocking=True)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    stage_sum = np.zeros(5)
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for i in range(args.steps):
+        step(args.warmup + i)
+        st = ctx.stage_times()
+        stage_sum += np.array([st["trace_ms"], st["grid_ms"], st["eye_ms"], st["gather_ms"], st["resolve_ms"]])
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # end to end through the public API with the frame read back to pinned host memory
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(10_000 + i, e2e=True)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1000 / args.steps
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    stages = stage_sum / args.steps
+
+    # gather kernel roofline: compulsory bytes per query = k neighbours x (16 B position
+    # + 12 B direction + 12 B power) + 32 B request (point, normal) + 12 B estimate
+    ph = ctx.photons(0, sorted_=False)  # noqa: F841  (map still resident)
+    hbm, src = peaks()
+    line = None
+    if rank == 0:
+        nreq = W * H   # lower bound: one gather per primary hit pixel
+        gather_bytes = nreq * (w["k"] * 40 + 44)
+        gather_ms = stages[3]
+        achieved = gather_bytes / (gather_ms * 1e-3) / 1e9 if gather_ms > 0 else 0.0
+        cpu = None
+        if not args.no_cpu_baseline:
+            est = cpu_reference_estimate(sc, w)
+            cpu = {"value": w["photons"] / est["step_s"] / 1e6, "unit": "Mphotons/s", "cores": est["cores"],
+                   "kind": "reference", "sample": est["sample"],
+                   "ms_per_frame": est["step_s"] * 1000, "stages_s": {k: est[k] for k in ("trace_s", "grid_s", "frame_s")}}
+        line = {
+            "metric": METRIC, "value": world * w["photons"] / (ms * 1e-3) / 1e6, "unit": "Mphotons/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene, seeded Philox photon streams)",
+            "config": {"workload": args.workload, "photons": w["photons"], "max_bounces": w["max_bounces"],
+                       "image": f"{W}x{H}", "k": w["k"], "radius": w["radius"], "eye_depth": w["max_depth"],
+                       "triangles": sc.ntri, "l2": "inputs larger than L2 (photon map ~0.5 GB)",
+                       "parallelism": f"replicas{world}"},
+            "stages_ms": {"trace": stages[0], "grid": stages[1], "eye": stages[2], "gather": stages[3],
+                          "resolve": stages[4]},
+            "roofline": {"kernel": "k_gather (kNN + estimate)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": None,
+                         "algorithmic_bytes_per_launch": gather_bytes},
+            "e2e": {"value": world * w["photons"] / (e2e_ms * 1e-3) / 1e6, "unit": "Mphotons/s",
+                    "ms_per_step": e2e_ms, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3},
+            "gpu_launches": None,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return line
+
+
+def run_reference(args):
+    from photonmap import scenes
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    sc, cs, w = scenes.workload(args.workload)
+    times = []
+    for i in range(args.warmup + args.steps):
+        est = cpu_reference_estimate(sc, w, rows=8, trace_photons=1500)
+        if i >= args.warmup:
+            times.append(est["step_s"])
+    step_s = float(np.mean(times))
+    v = w["photons"] / step_s / 1e6
+    return {"metric": METRIC, "value": v, "unit": "Mphotons/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1000, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "photons": w["photons"], "image": f"{w['width']}x{w['height']}"},
+            "cpu_baseline": {"value": v, "unit": "Mphotons/s", "cores": est["cores"], "kind": "reference",
+                             "sample": est["sample"]},
+            "e2e": {"value": v, "unit": "Mphotons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,758 @@
+// pm_api.cu -- context, device memory and the C ABI of include/pm_api.h.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pm_api.h"
+#include "pm_device.cuh"
+#include "pm_gather.cuh"
+#include "pm_grid.cuh"
+#include "pm_render.cuh"
+#include "pm_scan.cuh"
+#include "pm_scene.cuh"
+#include "pm_trace.cuh"
+
+namespace pm {
+void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& nodes_out, std::vector<int>& prim);
+}
+
+using namespace pm;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct MapState {
+    int64_t n = 0;                       // photons in the list
+    DevBuf pos, dir, pow;                // traced-order list (3 floats per photon)
+    bool built = false;
+    int dims[3] = {0, 0, 0};
+    float cell = 0.f;
+    int64_t cells = 0;
+    float aabb[6] = {0, 0, 0, 0, 0, 0};
+    DevBuf starts, sizes, gpos, gdir, gpow;
+    DevBuf cid, keys0, keys1, vals0, vals1, hist, scan_ws, small;
+};
+
+}  // namespace
+
+struct pm_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int sm_count = 148;
+    // scene
+    bool has_scene = false;
+    int ntri = 0, nmodel = 0, light_model = 0, light_first = 0, light_count = 0, nca = 0;
+    float light_intensity[3] = {1, 1, 1};
+    float default_ior = 1.f;
+    float aabb[6] = {0, 0, 0, 0, 0, 0};
+    bool has_tri_diffuse = false;
+    DevBuf tri, tri_pos, tri_nrm, tri_diffuse, nodes, prim, maabb, mats, ca;
+    MapState maps[2];
+    // photon-pass scratch
+    DevBuf counter, stage_pos, stage_dir, cnt_g, cnt_c, scan_g, scan_c, totals, trace_ws, scratch_pow;
+    // render scratch
+    DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, est_c;
+    DevBuf status, gws;
+    cudaEvent_t ev[12] = {};
+    float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+namespace {
+
+int fail(pm_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+int cuda_fail(pm_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, e == cudaErrorMemoryAllocation ? PM_ERR_OOM : PM_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(expr)                                                        \
+    do {                                                                \
+        cudaError_t e_ = (expr);                                        \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #expr);        \
+    } while (0)
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e == cudaSuccess) b.bytes = bytes;
+    return e;
+}
+void release(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+template <class T> T* P(DevBuf& b) { return (T*)b.p; }
+
+#define ENSURE(buf, bytes) CK(ensure(buf, bytes))
+
+DevScene dev_scene(pm_ctx* c) {
+    DevScene S;
+    S.tri = P<float4>(c->tri);
+    S.tri_pos = P<float>(c->tri_pos);
+    S.tri_nrm = P<float>(c->tri_nrm);
+    S.tri_diffuse = c->has_tri_diffuse ? P<float>(c->tri_diffuse) : nullptr;
+    S.nodes = P<float4>(c->nodes);
+    S.prim = P<int>(c->prim);
+    S.maabb = P<float>(c->maabb);
+    S.mats = P<float>(c->mats);
+    S.ca = P<float>(c->ca);
+    S.nca = c->nca;
+    S.ntri = c->ntri;
+    S.nmodel = c->nmodel;
+    S.light_first = c->light_first;
+    S.light_count = c->light_count;
+    S.default_ior = c->default_ior;
+    return S;
+}
+
+int check_status(pm_ctx* ctx, const char* what) {
+    uint32_t bits = 0;
+    CK(cudaMemcpyAsync(&bits, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (bits) {
+        CK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->st));
+        char buf[160];
+        snprintf(buf, sizeof buf, "%s: device status 0x%x (1 timeout, 2 overflow, 4 stack, 8 bad input)", what, bits);
+        return fail(ctx, (bits & ST_TIMEOUT) ? PM_ERR_TIMEOUT : PM_ERR_OVERFLOW, buf);
+    }
+    return PM_OK;
+}
+
+// critical-angle table as the reference builds it (PhotonTracing.cu:71-125)
+void add_angle(std::vector<float>& t, float e1, float e2) {
+    float eta = e2 / e1;
+    if (!(eta < 1.f)) return;
+    for (size_t i = 0; i < t.size(); i += 3) {
+        uint32_t a, b, x, y;
+        std::memcpy(&a, &t[i], 4); std::memcpy(&b, &t[i + 1], 4);
+        std::memcpy(&x, &e1, 4); std::memcpy(&y, &e2, 4);
+        if (a == x && b == y) return;
+    }
+    float ca = std::cos(std::asin(eta));
+    t.push_back(e1); t.push_back(e2); t.push_back(ca);
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return -1.f;
+    return ms;
+}
+
+int valid_map(pm_ctx* ctx, int map) {
+    if (map != PM_MAP_GLOBAL && map != PM_MAP_CAUSTIC) return fail(ctx, PM_ERR_INVALID, "map must be 0 (global) or 1 (caustic)");
+    return PM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pm_create(pm_ctx** out, const pm_device_opts* opts) {
+    if (!out) return PM_ERR_INVALID;
+    *out = nullptr;
+    pm_ctx* ctx = new pm_ctx();
+    ctx->device = opts ? opts->device : 0;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) { delete ctx; return PM_ERR_CUDA; }
+    if (opts && opts->stream) {
+        ctx->st = (cudaStream_t)opts->stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete ctx; return PM_ERR_CUDA; }
+        ctx->own_stream = true;
+    }
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    for (auto& ev : ctx->ev) {
+        if (cudaEventCreate(&ev) != cudaSuccess) { pm_destroy(ctx); return PM_ERR_CUDA; }
+    }
+    if (ensure(ctx->status, 16) != cudaSuccess || cudaMemsetAsync(ctx->status.p, 0, 16, ctx->st) != cudaSuccess) {
+        pm_destroy(ctx);
+        return PM_ERR_OOM;
+    }
+    *out = ctx;
+    return PM_OK;
+}
+
+void pm_destroy(pm_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    DevBuf* bufs[] = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
+                      &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage_pos, &ctx->stage_dir,
+                      &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
+                      &ctx->scratch_pow, &ctx->req_a, &ctx->req_b, &ctx->req_c, &ctx->req_counter, &ctx->px_base,
+                      &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws};
+    for (DevBuf* b : bufs) release(*b);
+    for (auto& m : ctx->maps) {
+        DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
+                        &m.keys0, &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small};
+        for (DevBuf* b : mb) release(*b);
+    }
+    for (auto& ev : ctx->ev) if (ev) cudaEventDestroy(ev);
+    if (ctx->own_stream && ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+const char* pm_last_error(const pm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pm_sync(pm_ctx* ctx) {
+    if (!ctx) return PM_ERR_INVALID;
+    CK(cudaStreamSynchronize(ctx->st));
+    return PM_OK;
+}
+
+int pm_status(pm_ctx* ctx, uint32_t* out_bits) {
+    if (!ctx || !out_bits) return PM_ERR_INVALID;
+    CK(cudaMemcpyAsync(out_bits, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return PM_OK;
+}
+
+int pm_stage_times(pm_ctx* ctx, float out_ms[8]) {
+    if (!ctx || !out_ms) return PM_ERR_INVALID;
+    for (int i = 0; i < 8; i++) out_ms[i] = ctx->stage_ms[i];
+    return PM_OK;
+}
+
+int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
+    if (!ctx || !sd) return PM_ERR_INVALID;
+    if (sd->ntri <= 0 || !sd->tri_pos || !sd->tri_nrm || !sd->tri_model || sd->nmodel <= 0 || !sd->materials)
+        return fail(ctx, PM_ERR_INVALID, "scene: empty or missing arrays");
+    if (sd->light_model < 0 || sd->light_model >= sd->nmodel) return fail(ctx, PM_ERR_INVALID, "scene: light_model out of range");
+    const int T = sd->ntri, M = sd->nmodel;
+    std::vector<int> first(M, -1), count(M, 0);
+    for (int t = 0; t < T; t++) {
+        int m = sd->tri_model[t];
+        if (m < 0 || m >= M) return fail(ctx, PM_ERR_INVALID, "scene: tri_model out of range");
+        if (t > 0 && m < sd->tri_model[t - 1]) return fail(ctx, PM_ERR_INVALID, "scene: triangles must be sorted by model");
+        if (first[m] < 0) first[m] = t;
+        count[m]++;
+    }
+    if (count[sd->light_model] == 0) return fail(ctx, PM_ERR_INVALID, "scene: the light model has no triangles");
+    CK(cudaSetDevice(ctx->device));
+
+    // per-triangle records (same operations as the reference's triangle test)
+    std::vector<float> rec(20 * (size_t)T);
+    for (int t = 0; t < T; t++) {
+        const float* p = sd->tri_pos + 9 * (size_t)t;
+        float v0[3] = {p[0], p[1], p[2]}, v1[3] = {p[3], p[4], p[5]}, v2[3] = {p[6], p[7], p[8]};
+        float e1[3] = {v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2]};
+        float e2[3] = {v2[0] - v0[0], v2[1] - v0[1], v2[2] - v0[2]};
+        float n[3] = {e1[1] * e2[2] - e1[2] * e2[1], -(e1[0] * e2[2] - e1[2] * e2[0]), e1[0] * e2[1] - e1[1] * e2[0]};
+        float nn = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+        float denom = 1.0f / nn;
+        float nd0 = n[0] * v0[0] + n[1] * v0[1] + n[2] * v0[2];
+        float f[3] = {v0[0] - v2[0], v0[1] - v2[1], v0[2] - v2[2]};
+        float* r = &rec[20 * (size_t)t];
+        int m = sd->tri_model[t];
+        r[0] = v0[0]; r[1] = v0[1]; r[2] = v0[2]; r[3] = nd0;
+        r[4] = e1[0]; r[5] = e1[1]; r[6] = e1[2]; r[7] = denom;
+        r[8] = v2[0]; r[9] = v2[1]; r[10] = v2[2]; std::memcpy(&r[11], &m, 4);
+        r[12] = f[0]; r[13] = f[1]; r[14] = f[2]; r[15] = 0.f;
+        r[16] = n[0]; r[17] = n[1]; r[18] = n[2]; r[19] = 0.f;
+    }
+    // model AABBs (first vertex, then grow) and the scene AABB (their union)
+    std::vector<float> maabb(6 * (size_t)M, 0.f);
+    for (int m = 0; m < M; m++) {
+        if (count[m] == 0) continue;
+        float* b = &maabb[6 * (size_t)m];
+        const float* p0 = sd->tri_pos + 9 * (size_t)first[m];
+        for (int a = 0; a < 3; a++) { b[a] = p0[a]; b[a + 3] = p0[a]; }
+        for (int t = first[m]; t < first[m] + count[m]; t++)
+            for (int v = 0; v < 3; v++) {
+                const float* q = sd->tri_pos + 9 * (size_t)t + 3 * v;
+                for (int a = 0; a < 3; a++) {
+                    if (q[a] > b[a + 3]) b[a + 3] = q[a];
+                    if (q[a] < b[a]) b[a] = q[a];
+                }
+            }
+    }
+    float aabb[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int m = 0; m < M; m++) {
+        if (count[m] == 0) continue;
+        for (int a = 0; a < 3; a++) {
+            aabb[a] = std::min(aabb[a], maabb[6 * m + a]);
+            aabb[a + 3] = std::max(aabb[a + 3], maabb[6 * m + a + 3]);
+        }
+    }
+    std::vector<float> ca;
+    for (int i = 0; i < M - 1; i++)
+        for (int j = i + 1; j < M; j++) {
+            add_angle(ca, sd->materials[12 * i + 9], sd->materials[12 * j + 9]);
+            add_angle(ca, sd->materials[12 * j + 9], sd->materials[12 * i + 9]);
+        }
+    for (int i = 0; i < M; i++) {
+        add_angle(ca, sd->default_ior, sd->materials[12 * i + 9]);
+        add_angle(ca, sd->materials[12 * i + 9], sd->default_ior);
+    }
+    float ext = std::max(std::max(aabb[3] - aabb[0], aabb[4] - aabb[1]), aabb[5] - aabb[2]);
+    std::vector<float> nodes;
+    std::vector<int> prim;
+    build_bvh(sd->tri_pos, T, 1e-4f * std::max(ext, 1.0f), nodes, prim);
+
+    ENSURE(ctx->tri, rec.size() * 4);
+    ENSURE(ctx->tri_pos, 9 * (size_t)T * 4);
+    ENSURE(ctx->tri_nrm, 9 * (size_t)T * 4);
+    ENSURE(ctx->nodes, nodes.size() * 4);
+    ENSURE(ctx->prim, prim.size() * 4);
+    ENSURE(ctx->maabb, maabb.size() * 4);
+    ENSURE(ctx->mats, 12 * (size_t)M * 4);
+    ENSURE(ctx->ca, std::max<size_t>(ca.size(), 3) * 4);
+    CK(cudaMemcpyAsync(ctx->tri.p, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->tri_pos.p, sd->tri_pos, 9 * (size_t)T * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->tri_nrm.p, sd->tri_nrm, 9 * (size_t)T * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->nodes.p, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->prim.p, prim.data(), prim.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->maabb.p, maabb.data(), maabb.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->mats.p, sd->materials, 12 * (size_t)M * 4, cudaMemcpyHostToDevice, ctx->st));
+    if (!ca.empty()) CK(cudaMemcpyAsync(ctx->ca.p, ca.data(), ca.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    ctx->has_tri_diffuse = sd->tri_diffuse != nullptr;
+    if (sd->tri_diffuse) {
+        ENSURE(ctx->tri_diffuse, 3 * (size_t)T * 4);
+        CK(cudaMemcpyAsync(ctx->tri_diffuse.p, sd->tri_diffuse, 3 * (size_t)T * 4, cudaMemcpyHostToDevice, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));   // host vectors go out of scope
+    ctx->ntri = T;
+    ctx->nmodel = M;
+    ctx->light_model = sd->light_model;
+    ctx->light_first = first[sd->light_model];
+    ctx->light_count = count[sd->light_model];
+    ctx->nca = (int)(ca.size() / 3);
+    for (int a = 0; a < 3; a++) ctx->light_intensity[a] = sd->light_intensity[a];
+    ctx->default_ior = sd->default_ior;
+    std::memcpy(ctx->aabb, aabb, sizeof aabb);
+    ctx->has_scene = true;
+    for (auto& m : ctx->maps) { m.built = false; m.n = 0; }
+    return PM_OK;
+}
+
+int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]) {
+    if (!ctx || !out_aabb) return PM_ERR_INVALID;
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
+    std::memcpy(out_aabb, ctx->aabb, 24);
+    return PM_OK;
+}
+
+static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, TraceBatch& B) {
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "pm_set_scene first");
+    if (o->max_bounces < 1 || o->max_bounces > 32) return fail(ctx, PM_ERR_INVALID, "max_bounces must be 1..32");
+    const size_t stage = (size_t)o->max_bounces * (size_t)npaths * 16;
+    ENSURE(ctx->counter, 8);
+    ENSURE(ctx->stage_pos, stage);
+    ENSURE(ctx->stage_dir, stage);
+    ENSURE(ctx->cnt_g, (size_t)npaths * 4);
+    ENSURE(ctx->cnt_c, (size_t)npaths * 4);
+    ENSURE(ctx->scan_g, (size_t)npaths * 4);
+    ENSURE(ctx->scan_c, (size_t)npaths * 4);
+    ENSURE(ctx->totals, 16);
+    ENSURE(ctx->trace_ws, scan_workspace_bytes(npaths));
+    B.S = dev_scene(ctx);
+    B.seed = o->seed;
+    B.tag = o->stream_tag;
+    B.max_bounces = o->max_bounces;
+    B.path_counter = P<unsigned long long>(ctx->counter);
+    B.stage_pos = P<float4>(ctx->stage_pos);
+    B.stage_dir = P<float4>(ctx->stage_dir);
+    B.cnt_g = P<uint32_t>(ctx->cnt_g);
+    B.cnt_c = P<uint32_t>(ctx->cnt_c);
+    B.scan_g = P<uint32_t>(ctx->scan_g);
+    B.scan_c = P<uint32_t>(ctx->scan_c);
+    B.totals = P<uint32_t>(ctx->totals);
+    B.scan_ws = ctx->trace_ws.p;
+    B.status = P<unsigned>(ctx->status);
+    B.sm_count = ctx->sm_count;
+    return PM_OK;
+}
+
+int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
+    if (!ctx || !o) return PM_ERR_INVALID;
+    if (o->global_capacity < 0 || o->caustic_capacity < 0) return fail(ctx, PM_ERR_INVALID, "negative capacity");
+    CK(cudaSetDevice(ctx->device));
+    const int64_t cg = o->global_capacity, cc = o->caustic_capacity;
+    const int64_t max_paths = o->max_paths > 0 ? o->max_paths : 64 * std::max<int64_t>(std::max(cg, cc), 1);
+    MapState& G = ctx->maps[PM_MAP_GLOBAL];
+    MapState& C = ctx->maps[PM_MAP_CAUSTIC];
+    ENSURE(G.pos, std::max<int64_t>(cg, 1) * 12); ENSURE(G.dir, std::max<int64_t>(cg, 1) * 12); ENSURE(G.pow, std::max<int64_t>(cg, 1) * 12);
+    ENSURE(C.pos, std::max<int64_t>(cc, 1) * 12); ENSURE(C.dir, std::max<int64_t>(cc, 1) * 12); ENSURE(C.pow, std::max<int64_t>(cc, 1) * 12);
+    G.built = C.built = false;
+    G.n = C.n = 0;
+    float power[3];
+    for (int a = 0; a < 3; a++) power[a] = ctx->light_intensity[a] / (float)cg;
+    const int64_t MAX_BATCH = (int64_t)1 << 23;
+    int64_t nb = std::min<int64_t>(std::max<int64_t>(cg + cc, 4096), MAX_BATCH);
+    int64_t fg = 0, fc = 0, p0 = 0;
+    double yg = 0.0, yc = 0.0;   // photons per path so far
+    int64_t got_g = 0, got_c = 0;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    while ((fg < cg || fc < cc) && p0 < max_paths) {
+        nb = std::min(nb, max_paths - p0);
+        TraceBatch B;
+        int rc = prepare_trace(ctx, o, nb, B);
+        if (rc) return rc;
+        B.p0 = p0;
+        B.npaths = nb;
+        for (int a = 0; a < 3; a++) B.power[a] = power[a];
+        PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg};
+        PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc};
+        CK(trace_batch(B, LG, LC, ctx->st));
+        uint32_t tot[2] = {0, 0};
+        CK(cudaMemcpyAsync(tot, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        got_g += tot[0];
+        got_c += tot[1];
+        fg = std::min(cg, fg + (int64_t)tot[0]);
+        fc = std::min(cc, fc + (int64_t)tot[1]);
+        p0 += nb;
+        yg = (double)got_g / (double)p0;
+        yc = (double)got_c / (double)p0;
+        double need = 0.0;
+        if (fg < cg) need = std::max(need, yg > 0 ? (double)(cg - fg) / yg : (double)MAX_BATCH);
+        if (fc < cc) need = std::max(need, yc > 0 ? (double)(cc - fc) / yc : (double)MAX_BATCH);
+        nb = std::min<int64_t>(MAX_BATCH, std::max<int64_t>(4096, (int64_t)(need * 1.02) + 1024));
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[1]));
+    ctx->stage_ms[0] = elapsed(ctx->ev[0], ctx->ev[1]);
+    G.n = fg;
+    C.n = fc;
+    if (out_paths) *out_paths = p0;
+    int rc = check_status(ctx, "trace");
+    if (rc) return rc;
+    if (fg < cg || fc < cc) return fail(ctx, PM_ERR_INVALID, "photon maps not filled within max_paths");
+    return PM_OK;
+}
+
+int pm_trace_paths(pm_ctx* ctx, const pm_trace_opts* o, int64_t p0, int64_t p1, int64_t power_capacity,
+                   float* g_pos, float* g_dir, float* c_pos, float* c_dir, uint32_t* counts,
+                   int64_t* out_ng, int64_t* out_nc) {
+    if (!ctx || !o || p1 <= p0 || !g_pos || !g_dir || !c_pos || !c_dir) return PM_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    const int64_t n = p1 - p0;
+    TraceBatch B;
+    int rc = prepare_trace(ctx, o, n, B);
+    if (rc) return rc;
+    B.p0 = p0;
+    B.npaths = n;
+    for (int a = 0; a < 3; a++) B.power[a] = ctx->light_intensity[a] / (float)power_capacity;
+    const int64_t cap = n * o->max_bounces;
+    ENSURE(ctx->scratch_pow, (size_t)cap * 24);
+    float* pw = P<float>(ctx->scratch_pow);
+    PhotonList LG{g_pos, g_dir, pw, cap, 0};
+    PhotonList LC{c_pos, c_dir, pw + 3 * cap, cap, 0};
+    CK(trace_batch(B, LG, LC, ctx->st));
+    if (counts) {
+        CK(cudaMemcpy2DAsync(counts, 8, B.cnt_g, 4, 4, (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpy2DAsync(counts + 1, 8, B.cnt_c, 4, 4, (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
+    }
+    uint32_t tot[2] = {0, 0};
+    CK(cudaMemcpyAsync(tot, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (out_ng) *out_ng = tot[0];
+    if (out_nc) *out_nc = tot[1];
+    return check_status(ctx, "trace_paths");
+}
+
+int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const float* power, const float* dir) {
+    if (!ctx || n < 0 || (n > 0 && (!pos || !power || !dir))) return PM_ERR_INVALID;
+    if (int rc = valid_map(ctx, map)) return rc;
+    CK(cudaSetDevice(ctx->device));
+    MapState& m = ctx->maps[map];
+    ENSURE(m.pos, std::max<int64_t>(n, 1) * 12);
+    ENSURE(m.dir, std::max<int64_t>(n, 1) * 12);
+    ENSURE(m.pow, std::max<int64_t>(n, 1) * 12);
+    if (n > 0) {
+        CK(cudaMemcpyAsync(m.pos.p, pos, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(m.dir.p, dir, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(m.pow.p, power, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    m.n = n;
+    m.built = false;
+    return PM_OK;
+}
+
+int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb) {
+    if (!ctx) return PM_ERR_INVALID;
+    if (int rc = valid_map(ctx, map)) return rc;
+    pm_grid_opts d = {1000, 5, 5};
+    if (!o) o = &d;
+    if (o->desired_per_cell < 1 || o->regrid_div < 1 || o->regrid_mult < 1) return fail(ctx, PM_ERR_INVALID, "grid options must be >= 1");
+    const float* box = aabb ? aabb : ctx->aabb;
+    if (!aabb && !ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene and no aabb");
+    CK(cudaSetDevice(ctx->device));
+    MapState& m = ctx->maps[map];
+    const int64_t n = m.n;
+    if (n == 0) return fail(ctx, PM_ERR_INVALID, "map has no photons");
+    int d1[3], d2[3];
+    float c1, c2;
+    grid_dims(box, n, o->desired_per_cell, d1, &c1);
+    int desired2 = std::max(o->desired_per_cell / o->regrid_div, 1);
+    grid_dims(box, n, desired2, d2, &c2);
+    const int64_t cells_max = std::max<int64_t>((int64_t)d1[0] * d1[1] * d1[2], (int64_t)d2[0] * d2[1] * d2[2]);
+    if (cells_max <= 0 || cells_max > ((int64_t)1 << 31)) return fail(ctx, PM_ERR_INVALID, "grid: cell count out of range");
+    size_t hist_elems = 0, scan_ws = 0;
+    grid_scratch_sizes(n, cells_max, &hist_elems, &scan_ws);
+    ENSURE(m.starts, (size_t)cells_max * 4);
+    ENSURE(m.sizes, (size_t)cells_max * 4);
+    ENSURE(m.gpos, (size_t)n * 16);
+    ENSURE(m.gdir, (size_t)n * 12);
+    ENSURE(m.gpow, (size_t)n * 12);
+    ENSURE(m.cid, (size_t)n * 4);
+    ENSURE(m.keys0, (size_t)n * 4);
+    ENSURE(m.keys1, (size_t)n * 4);
+    ENSURE(m.vals0, (size_t)n * 4);
+    ENSURE(m.vals1, (size_t)n * 4);
+    ENSURE(m.hist, hist_elems * 4);
+    ENSURE(m.scan_ws, scan_ws);
+    ENSURE(m.small, 64);
+    GridBuffers B;
+    B.pos = P<float>(m.pos); B.dir = P<float>(m.dir); B.pow = P<float>(m.pow); B.n = n;
+    B.cell_starts = P<uint32_t>(m.starts); B.cell_sizes = P<uint32_t>(m.sizes);
+    B.gpos = P<float4>(m.gpos); B.gdir = P<float>(m.gdir); B.gpow = P<float>(m.gpow);
+    B.cid = P<uint32_t>(m.cid);
+    B.keys[0] = P<uint32_t>(m.keys0); B.keys[1] = P<uint32_t>(m.keys1);
+    B.vals[0] = P<uint32_t>(m.vals0); B.vals[1] = P<uint32_t>(m.vals1);
+    B.hist = P<uint32_t>(m.hist);
+    B.scan_ws = m.scan_ws.p;
+    B.small = P<uint32_t>(m.small);
+    B.status = P<unsigned>(ctx->status);
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(grid_build(B, box, o->desired_per_cell, o->regrid_mult, o->regrid_div, m.dims, &m.cell, &m.cells, ctx->st));
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[3]));
+    if (map == PM_MAP_GLOBAL) ctx->stage_ms[1] = elapsed(ctx->ev[2], ctx->ev[3]);
+    std::memcpy(m.aabb, box, 24);
+    int rc = check_status(ctx, "grid build");
+    if (rc) return rc;
+    m.built = true;
+    return PM_OK;
+}
+
+int pm_get_photons(pm_ctx* ctx, int map, pm_photon_view* out) {
+    if (!ctx || !out) return PM_ERR_INVALID;
+    if (int rc = valid_map(ctx, map)) return rc;
+    MapState& m = ctx->maps[map];
+    std::memset(out, 0, sizeof *out);
+    out->count = m.n;
+    out->list_pos = P<float>(m.pos);
+    out->list_dir = P<float>(m.dir);
+    out->list_power = P<float>(m.pow);
+    if (m.built) {
+        out->cells = m.cells;
+        for (int a = 0; a < 3; a++) out->dims[a] = m.dims[a];
+        out->cell_size = m.cell;
+        std::memcpy(out->aabb, m.aabb, 24);
+        out->cell_starts = P<uint32_t>(m.starts);
+        out->cell_sizes = P<uint32_t>(m.sizes);
+        out->sorted_pos = P<float>(m.gpos);
+        out->sorted_dir = P<float>(m.gdir);
+        out->sorted_power = P<float>(m.gpow);
+    }
+    return PM_OK;
+}
+
+int pm_save_photons(pm_ctx* ctx, int map, const char* path) {
+    if (!ctx || !path) return PM_ERR_INVALID;
+    if (int rc = valid_map(ctx, map)) return rc;
+    MapState& m = ctx->maps[map];
+    const int64_t n = m.n;
+    std::vector<float> pos(3 * n), pw(3 * n), dir(3 * n);
+    if (n > 0) {
+        CK(cudaMemcpyAsync(pos.data(), m.pos.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(pw.data(), m.pow.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(dir.data(), m.dir.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(ctx, PM_ERR_IO, std::string("cannot open ") + path);
+    uint64_t cnt = (uint64_t)n;
+    bool ok = fwrite(&cnt, 8, 1, f) == 1;
+    std::vector<float> rec(9 * 4096);
+    for (int64_t i = 0; ok && i < n; i += 4096) {
+        int64_t k = std::min<int64_t>(4096, n - i);
+        for (int64_t j = 0; j < k; j++) {
+            std::memcpy(&rec[9 * j], &pos[3 * (i + j)], 12);
+            std::memcpy(&rec[9 * j + 3], &pw[3 * (i + j)], 12);
+            std::memcpy(&rec[9 * j + 6], &dir[3 * (i + j)], 12);
+        }
+        ok = fwrite(rec.data(), 36, (size_t)k, f) == (size_t)k;
+    }
+    if (fclose(f) != 0) ok = false;
+    return ok ? PM_OK : fail(ctx, PM_ERR_IO, std::string("write failed: ") + path);
+}
+
+int pm_load_photons(pm_ctx* ctx, int map, const char* path) {
+    if (!ctx || !path) return PM_ERR_INVALID;
+    if (int rc = valid_map(ctx, map)) return rc;
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(ctx, PM_ERR_IO, std::string("cannot open ") + path);
+    uint64_t cnt = 0;
+    if (fread(&cnt, 8, 1, f) != 1 || cnt > ((uint64_t)1 << 32)) { fclose(f); return fail(ctx, PM_ERR_IO, "bad photon count"); }
+    std::vector<float> rec(9 * (size_t)cnt);
+    size_t got = cnt ? fread(rec.data(), 36, (size_t)cnt, f) : 0;
+    fclose(f);
+    if (got != cnt) return fail(ctx, PM_ERR_IO, "truncated photon file");
+    std::vector<float> pos(3 * cnt), pw(3 * cnt), dir(3 * cnt);
+    for (size_t i = 0; i < cnt; i++) {
+        std::memcpy(&pos[3 * i], &rec[9 * i], 12);
+        std::memcpy(&pw[3 * i], &rec[9 * i + 3], 12);
+        std::memcpy(&dir[3 * i], &rec[9 * i + 6], 12);
+    }
+    return pm_set_photons(ctx, map, (int64_t)cnt, pos.data(), pw.data(), dir.data());
+}
+
+static GatherGrid grid_of(MapState& m, MapState& est_src) {
+    GatherGrid G;
+    G.gpos = P<float4>(m.gpos);
+    G.gdir = P<float>(est_src.gdir);
+    G.gpow = P<float>(est_src.gpow);
+    G.starts = P<uint32_t>(m.starts);
+    G.sizes = P<uint32_t>(m.sizes);
+    G.mn[0] = m.aabb[0]; G.mn[1] = m.aabb[1]; G.mn[2] = m.aabb[2];
+    G.gx = m.dims[0]; G.gy = m.dims[1]; G.gz = m.dims[2];
+    G.cell = m.cell;
+    return G;
+}
+
+int pm_gather(pm_ctx* ctx, int map, int64_t n, const float* qpos, const float* qnrm, int k, float radius,
+              float* out_rad, uint32_t* out_ids, int32_t* out_cnt) {
+    if (!ctx || n < 0 || (n > 0 && (!qpos || !qnrm || !out_rad))) return PM_ERR_INVALID;
+    if (int rc = valid_map(ctx, map)) return rc;
+    if (k < 0 || k > 256) return fail(ctx, PM_ERR_INVALID, "k must be 0..256");
+    MapState& m = ctx->maps[map];
+    if (!m.built) return fail(ctx, PM_ERR_INVALID, "map grid not built");
+    CK(cudaSetDevice(ctx->device));
+    GatherQueries Q{};
+    Q.n = n; Q.pos3 = qpos; Q.nrm3 = qnrm;
+    GatherOut O{out_rad, out_ids, out_cnt, nullptr};
+    CK(gather(grid_of(m, m), Q, radius, k, 0, O, P<unsigned>(ctx->status), ctx->st));
+    return check_status(ctx, "gather");
+}
+
+int pm_camera_setup(const float position[3], const float direction[3], const float upv[3], float fov, int32_t W,
+                    int32_t H, pm_camera* out) {
+    if (!position || !direction || !upv || !out || W <= 0 || H <= 0) return PM_ERR_INVALID;
+    const float pi = 3.141592653589793f;
+    float aspect = (float)W / (float)H;
+    float theta = fov * pi / 180.0f;
+    float h = std::tan(theta / 2);
+    out->viewport_h = 2.0f * h;
+    out->viewport_w = aspect * out->viewport_h;
+    out->focal = 1.0f;
+    auto norm_div = [](const float* v, float* o) {
+        if (v[0] == 0.f && v[1] == 0.f && v[2] == 0.f) { o[0] = v[0]; o[1] = v[1]; o[2] = v[2]; return; }
+        float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        o[0] = v[0] / l; o[1] = v[1] / l; o[2] = v[2] / l;
+    };
+    auto cross = [](const float* a, const float* b, float* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = -(a[0] * b[2] - a[2] * b[0]);
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    for (int a = 0; a < 3; a++) out->position[a] = position[a];
+    norm_div(direction, out->forward);
+    float rc[3];
+    cross(out->forward, upv, rc);
+    norm_div(rc, out->right);
+    cross(out->right, out->forward, out->up);
+    out->width = W;
+    out->height = H;
+    return PM_OK;
+}
+
+int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance) {
+    if (!ctx || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
+    if (o->max_depth < 0 || o->max_depth > RENDER_MAX_DEPTH) return fail(ctx, PM_ERR_INVALID, "max_depth must be 0..5");
+    if (o->k_global < 0 || o->k_global > 256 || o->k_caustic < 0 || o->k_caustic > 256)
+        return fail(ctx, PM_ERR_INVALID, "k must be 0..256");
+    if (cam->width <= 0 || cam->height <= 0) return fail(ctx, PM_ERR_INVALID, "bad camera size");
+    MapState& G = ctx->maps[PM_MAP_GLOBAL];
+    MapState& C = ctx->maps[PM_MAP_CAUSTIC];
+    if (!G.built) return fail(ctx, PM_ERR_INVALID, "global map grid not built");
+    CK(cudaSetDevice(ctx->device));
+    const int64_t npx = (int64_t)cam->width * cam->height;
+    const int64_t per_px = ((int64_t)1 << std::max(o->max_depth, 1)) - 1;
+    const int64_t cap = npx * per_px;
+    ENSURE(ctx->req_a, (size_t)cap * 16);
+    ENSURE(ctx->req_b, (size_t)cap * 16);
+    ENSURE(ctx->req_c, (size_t)cap * 16);
+    ENSURE(ctx->req_counter, 8);
+    ENSURE(ctx->px_base, (size_t)npx * 4);
+    ENSURE(ctx->px_count, (size_t)npx * 4);
+    ENSURE(ctx->est_g, (size_t)cap * 12);
+    const bool caustic = C.built;
+    if (caustic && o->faithful_caustic && C.n > G.n)
+        return fail(ctx, PM_ERR_INVALID, "faithful caustic estimate reads the global map with caustic indices: "
+                                         "the caustic map must not be larger than the global map");
+    if (caustic) ENSURE(ctx->est_c, (size_t)cap * 12);
+    DevScene S = dev_scene(ctx);
+    CameraDev cd;
+    for (int a = 0; a < 3; a++) {
+        cd.pos[a] = cam->position[a]; cd.fwd[a] = cam->forward[a]; cd.right[a] = cam->right[a]; cd.up[a] = cam->up[a];
+    }
+    cd.vw = cam->viewport_w; cd.vh = cam->viewport_h; cd.focal = cam->focal;
+    cd.W = cam->width; cd.H = cam->height;
+    Requests R;
+    R.a = P<float4>(ctx->req_a); R.b = P<float4>(ctx->req_b); R.c = P<float4>(ctx->req_c);
+    R.cap = cap;
+    R.counter = P<unsigned long long>(ctx->req_counter);
+    R.px_base = P<uint32_t>(ctx->px_base);
+    R.px_count = P<uint32_t>(ctx->px_count);
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    CK(eye_pass(S, cd, o->max_depth, R, P<unsigned>(ctx->status), ctx->st));
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    unsigned long long nreq = 0;
+    CK(cudaMemcpyAsync(&nreq, R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    nreq = std::min<unsigned long long>(nreq, (unsigned long long)cap);
+    GatherQueries Q{};
+    Q.n = (int64_t)nreq; Q.pos4 = R.a; Q.nrm4 = R.b; Q.flag_mask = 1u;
+    GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OG, P<unsigned>(ctx->status), ctx->st));
+    if (caustic) {
+        Q.flag_mask = 2u;
+        GatherOut OC{P<float>(ctx->est_c), nullptr, nullptr, nullptr};
+        CK(gather(grid_of(C, o->faithful_caustic ? G : C), Q, o->r_caustic, o->k_caustic, 1, OC,
+                  P<unsigned>(ctx->status), ctx->st));
+    }
+    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    const float tone_t = (float)std::pow((double)0.6f, -1);
+    CK(resolve(S, cd, R, P<float>(ctx->est_g), caustic ? P<float>(ctx->est_c) : nullptr, tone_t, out_rgb8,
+               out_radiance, ctx->st));
+    CK(cudaEventRecord(ctx->ev[8], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[8]));
+    ctx->stage_ms[2] = elapsed(ctx->ev[4], ctx->ev[5]);
+    ctx->stage_ms[3] = elapsed(ctx->ev[6], ctx->ev[7]);
+    ctx->stage_ms[4] = elapsed(ctx->ev[7], ctx->ev[8]);
+    return check_status(ctx, "render");
+}
+
+int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive) {
+    if (!ctx || n < 0 || (n > 0 && (!in || !out))) return PM_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    ENSURE(ctx->gws, scan_workspace_bytes(n));
+    CK(scan_u32(in, out, n, inclusive, nullptr, ctx->gws.p, P<unsigned>(ctx->status), ctx->st));
+    return check_status(ctx, "scan");
+}
+
+}  // extern "C"

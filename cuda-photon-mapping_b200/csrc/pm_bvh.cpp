@@ -1,0 +1,139 @@
+// pm_bvh.cpp -- host BVH builder for the closest-hit queries of pm_scene.cuh.
+//
+// The reference has no acceleration structure: every ray tests every triangle
+// of every model whose box it meets (CudaPhotonMapping/Model.cuh:366-446); its
+// kd-tree code only reduces a model's triangles to one AABB
+// (KdTree.cu:395-464).  This is a binary BVH built with binned SAH (16 bins on
+// the widest centroid axis, leaves of <= 4 triangles, depth <= 60).  Node boxes
+// are padded so that culling is conservative with respect to the exact
+// triangle test; the traversal (pm_scene.cuh) keeps the reference's answer.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace pm {
+
+namespace {
+
+struct Box {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    void grow(const float* p) {
+        for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], p[a]); hi[a] = std::max(hi[a], p[a]); }
+    }
+    void grow(const Box& b) {
+        for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], b.lo[a]); hi[a] = std::max(hi[a], b.hi[a]); }
+    }
+    float area() const {
+        if (lo[0] > hi[0]) return 0.f;
+        float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        return 2.f * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct Node {
+    Box box;
+    int first = 0;
+    int count = 0;
+};
+
+struct Task { int node, b, e, depth; };
+
+}  // namespace
+
+// nodes_out: 8 floats per node = lo.xyz, bits(left child | first prim), hi.xyz, bits(count)
+// (count > 0: leaf over prim[first, first + count); count == 0: children left, left + 1)
+void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& nodes_out, std::vector<int>& prim) {
+    std::vector<Box> pb(ntri);
+    std::vector<float> cen(3 * (size_t)ntri);
+    for (int t = 0; t < ntri; t++) {
+        for (int v = 0; v < 3; v++) pb[t].grow(tri_pos + 9 * (size_t)t + 3 * v);
+        for (int a = 0; a < 3; a++) cen[3 * (size_t)t + a] = 0.5f * (pb[t].lo[a] + pb[t].hi[a]);
+    }
+    prim.resize(ntri);
+    for (int t = 0; t < ntri; t++) prim[t] = t;
+    std::vector<Node> nodes(1);
+    std::vector<Task> stack;
+    stack.push_back(Task{0, 0, ntri, 0});
+    const int BINS = 16;
+    while (!stack.empty()) {
+        Task tk = stack.back();
+        stack.pop_back();
+        Box nb, cb;
+        for (int i = tk.b; i < tk.e; i++) { nb.grow(pb[prim[i]]); cb.grow(&cen[3 * (size_t)prim[i]]); }
+        nodes[tk.node].box = nb;
+        const int n = tk.e - tk.b;
+        auto make_leaf = [&]() { nodes[tk.node].first = tk.b; nodes[tk.node].count = n; };
+        if (n <= 4 || tk.depth >= 60) { make_leaf(); continue; }
+        int axis = 0;
+        float ext[3];
+        for (int a = 0; a < 3; a++) ext[a] = cb.hi[a] - cb.lo[a];
+        if (ext[1] > ext[axis]) axis = 1;
+        if (ext[2] > ext[axis]) axis = 2;
+        int mid;
+        if (!(ext[axis] > 0.f)) {
+            mid = tk.b + n / 2;
+        } else {
+            Box bb[BINS];
+            int bc[BINS] = {0};
+            auto bin_of = [&](int t) {
+                int k = (int)((cen[3 * (size_t)t + axis] - cb.lo[axis]) / ext[axis] * BINS);
+                return std::min(std::max(k, 0), BINS - 1);
+            };
+            for (int i = tk.b; i < tk.e; i++) { int k = bin_of(prim[i]); bc[k]++; bb[k].grow(pb[prim[i]]); }
+            float best = FLT_MAX;
+            int bsplit = -1;
+            Box left[BINS];
+            int lc[BINS];
+            Box acc; int ac = 0;
+            for (int k = 0; k < BINS; k++) { acc.grow(bb[k]); ac += bc[k]; left[k] = acc; lc[k] = ac; }
+            Box racc; int rc = 0;
+            for (int k = BINS - 1; k > 0; k--) {
+                racc.grow(bb[k]); rc += bc[k];
+                if (lc[k - 1] == 0 || rc == 0) continue;
+                float c = left[k - 1].area() * lc[k - 1] + racc.area() * rc;
+                if (c < best) { best = c; bsplit = k; }
+            }
+            if (bsplit < 0) {
+                mid = tk.b + n / 2;
+            } else {
+                int* it = std::partition(prim.data() + tk.b, prim.data() + tk.e,
+                                         [&](int t) { return bin_of(t) < bsplit; });
+                mid = (int)(it - prim.data());
+                if (mid == tk.b || mid == tk.e) mid = tk.b + n / 2;
+            }
+        }
+        if (mid == tk.b + n / 2 && !(ext[axis] > 0.f)) {
+            // all centroids coincide: keep order, split by count
+        } else if (mid == tk.b + n / 2) {
+            std::nth_element(prim.data() + tk.b, prim.data() + mid, prim.data() + tk.e, [&](int x, int y) {
+                return cen[3 * (size_t)x + axis] < cen[3 * (size_t)y + axis];
+            });
+        }
+        int left_idx = (int)nodes.size();
+        nodes.resize(nodes.size() + 2);
+        nodes[tk.node].first = left_idx;
+        nodes[tk.node].count = 0;
+        stack.push_back(Task{left_idx + 1, mid, tk.e, tk.depth + 1});
+        stack.push_back(Task{left_idx, tk.b, mid, tk.depth + 1});
+    }
+    nodes_out.resize(8 * nodes.size());
+    for (size_t i = 0; i < nodes.size(); i++) {
+        float* o = &nodes_out[8 * i];
+        const Node& nd = nodes[i];
+        for (int a = 0; a < 3; a++) {
+            float span = std::max(std::fabs(nd.box.lo[a]), std::fabs(nd.box.hi[a]));
+            float p = pad + span * 1e-5f;
+            o[a] = nd.box.lo[a] - p;
+            o[4 + a] = nd.box.hi[a] + p;
+        }
+        int f = nd.first, c = nd.count;
+        std::memcpy(&o[3], &f, 4);
+        std::memcpy(&o[7], &c, 4);
+    }
+}
+
+}  // namespace pm

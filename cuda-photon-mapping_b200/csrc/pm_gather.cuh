@@ -1,0 +1,43 @@
+// pm_gather.cuh -- kNN photon gather + radiance estimate.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pm {
+
+struct GatherGrid {
+    const float4* gpos;        // sorted photons: xyz + source id bits
+    const float* gdir;         // direction / power arrays the estimate reads (3 floats per slot)
+    const float* gpow;
+    const uint32_t* starts;
+    const uint32_t* sizes;
+    float mn[3];               // grid origin (scene AABB min)
+    int gx, gy, gz;
+    float cell;
+};
+
+struct GatherQueries {
+    int64_t n;
+    // either packed 3-float arrays ...
+    const float* pos3;
+    const float* nrm3;
+    // ... or float4 records (xyz; flag bits in w of nrm4): a record is gathered
+    // when (flags & flag_mask) != 0, otherwise its estimate is zero
+    const float4* pos4;
+    const float4* nrm4;
+    uint32_t flag_mask;
+};
+
+struct GatherOut {
+    float* rad;               // 3 floats per query (required)
+    uint32_t* ids;            // k per query, ascending (distance, id); UINT_MAX padding (optional)
+    int* cnt;                 // neighbours found (optional)
+    float* rk;                // largest selected distance (optional)
+};
+
+// k <= 256.  require_full: the estimate is written only when k neighbours were
+// found (the caustic rule of CudaPhotonMapping/Raytracer.cuh:200), zero otherwise.
+cudaError_t gather(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full,
+                   const GatherOut& O, unsigned* status, cudaStream_t st);
+
+}  // namespace pm

@@ -1,0 +1,264 @@
+// pm_render.cu -- eye pass and per-pixel resolve.
+//
+// Reference: CudaPhotonMapping/Raytracer.cuh:140-241 (render_trace),
+// RaytracePlanner.cuh:30-69, MediumManager.cuh:17-79, MMInnerStack.cuh:131,
+// MMOuterStack.cuh:269, RayPlanStack.cuh:13-88, Camera.cuh:67-81,
+// Raytracer.cuh:95-107 (tone map), 277 (quantisation).
+//
+// The reference computes each pixel in one thread, interleaving ray steps and
+// kNN gathers.  The ray steps never depend on gathered values, so the pass is
+// split: k_eye follows every eye path (closest hits, refraction plans, mirror
+// bounces) and records one gather request per hit; the gather kernel then
+// estimates all requests in one launch; k_resolve combines each pixel's
+// requests in hit order (clamp <= 1, path weight), tone-maps and quantises.
+// The refraction planner and medium bookkeeping are restated with the
+// reference's index arithmetic and per-pixel storage that starts zeroed
+// (the reference's GPU path zeroes it once with cudaMemset and lets threads
+// share slots across pixels; per-pixel zeroed storage is the deterministic
+// reading of that).
+#include "pm_render.cuh"
+
+namespace pm {
+
+namespace {
+
+constexpr int EYE_THREADS = 128;
+constexpr int MD = RENDER_MAX_DEPTH;
+constexpr int DCMAX = (MD + 1) / 2;
+constexpr int SLOTS = MD + 2;
+
+struct Plan { Ray ray; int depth; V3 coef; int in_obj; };
+
+struct MediumState {
+    int D, DC;
+    int outer_size;
+    int cont[SLOTS];
+    float dior[SLOTS * DCMAX];
+    int did[SLOTS * DCMAX];
+    int nplans;
+    Plan plans[MD];
+    bool overflow;
+    __device__ void init(int d) {
+        D = d; DC = (d + 1) / 2; outer_size = 0; nplans = 0; overflow = false;
+        for (int i = 0; i < SLOTS; i++) cont[i] = 0;
+        for (int i = 0; i < SLOTS * DCMAX; i++) { dior[i] = 0.f; did[i] = 0; }
+    }
+    __device__ int idx(int slot, int depth) {
+        if (slot < 0 || slot > D + 1 || depth < 0 || depth >= DC) { overflow = true; return -1; }
+        return slot * DCMAX + depth;
+    }
+    __device__ float ior_at(int slot, int depth) { int k = idx(slot, depth); return k < 0 ? 0.f : dior[k]; }
+    __device__ int id_at(int slot, int depth) { int k = idx(slot, depth); return k < 0 ? 0 : did[k]; }
+    __device__ void set_at(int slot, int depth, float ior, int id) {
+        int k = idx(slot, depth);
+        if (k >= 0) { dior[k] = ior; did[k] = id; }
+    }
+};
+
+struct Rgi { float n1, n2; bool in_obj; };
+
+__device__ Rgi get_refractive_indices(MediumState& M, float def, int model_id, float ior) {
+    int L = M.outer_size;
+    if (L == 0) return Rgi{def, ior, true};
+    int s = M.cont[L - 1];
+    if (s == 0) return Rgi{def, ior, true};
+    if (M.id_at(L, s - 1) == model_id) {
+        bool in_obj = s > 1;
+        return Rgi{ior, in_obj ? M.ior_at(L, s - 2) : def, in_obj};
+    }
+    return Rgi{M.ior_at(L, s - 1), ior, true};
+}
+__device__ void increase_depth(MediumState& M, bool& max_level) {
+    int L = M.outer_size;
+    if (L == 0) { M.outer_size = 1; L = 1; }
+    if (L < M.D) {
+        int count = (M.D + 1) / 2;
+        int other = M.cont[L - 1];
+        if (!(M.outer_size > M.D - 1)) {
+            int to = max(other, 0);
+            int from = max(to - count, 0);
+            for (int i = from; i < to; i++) M.set_at(L, i, M.ior_at(L - 1, i), M.id_at(L - 1, i));
+            M.cont[M.outer_size] = to - from;
+            M.outer_size++;
+        }
+        max_level = false;
+    } else {
+        max_level = true;
+    }
+}
+__device__ void reduce_depth(MediumState& M, bool& max_level) {
+    if (!max_level && M.outer_size > 0) M.outer_size--;
+    max_level = false;
+}
+__device__ void inform(MediumState& M, int model_id, float ior, bool max_level) {
+    int pos = M.outer_size - 1 - (max_level ? 0 : 1);
+    if (pos < 0 || pos >= SLOTS) { M.overflow = true; return; }
+    int s = M.cont[pos];
+    if (s != 0) {
+        if (M.id_at(s, s - 1) == model_id) M.cont[pos] = s - 1;
+    } else if (!(M.DC == 0 || s > M.DC - 1)) {
+        M.set_at(s, s, ior, model_id);
+        M.cont[pos] = s + 1;
+    }
+}
+__device__ void push_refraction(MediumState& M, bool& max_level, const Ray& r, int depth, V3 coef, int model_id,
+                                float ior, float opaque, bool in_obj) {
+    increase_depth(M, max_level);
+    inform(M, model_id, ior, max_level);
+    if (!(M.D == 0 || M.nplans > M.D - 1)) {
+        Plan& p = M.plans[M.nplans++];
+        p.ray = r; p.depth = depth + 1; p.coef = vscale(coef, 1.f - opaque); p.in_obj = in_obj;
+    }
+}
+__device__ bool pop_refraction(MediumState& M, bool& max_level, Ray& r, int& depth, V3& coef, bool& in_obj) {
+    reduce_depth(M, max_level);
+    if (M.nplans == 0) return false;
+    const Plan& p = M.plans[--M.nplans];
+    r = p.ray; depth = p.depth; coef = p.coef; in_obj = p.in_obj != 0;
+    return true;
+}
+
+__device__ __forceinline__ V3 camera_dir(const CameraDev& c, int x, int y) {
+    float u = ((float)x + 0.5f) / (float)c.W;
+    float v = ((float)y + 0.5f) / (float)c.H;
+    V3 pos = ld3(c.pos);
+    V3 hor = vscale(ld3(c.right), c.vw);
+    V3 ver = vscale(ld3(c.up), c.vh);
+    V3 llc = vsub(vsub(vscale(vadd(pos, ld3(c.fwd)), c.focal), vscale(hor, 0.5f)), vscale(ver, 0.5f));
+    return vsub(vadd(vadd(llc, vscale(hor, u)), vscale(ver, v)), pos);
+}
+
+__global__ void __launch_bounds__(EYE_THREADS)
+k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
+    const int64_t npx = (int64_t)cam.W * cam.H;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < npx;
+    float4 ha[RENDER_MAX_HITS], hb[RENDER_MAX_HITS], hc[RENDER_MAX_HITS];
+    int nh = 0;
+    if (valid) {
+        const int x = (int)(i % cam.W), y = (int)(i / cam.W);
+        Ray ray;
+        ray.o = ld3(cam.pos);
+        ray.d = vnorm_div(camera_dir(cam, x, y));
+        MediumState M;
+        M.init(D);
+        int new_depth = 0, cur = -1;
+        V3 coef = v3(1.f, 1.f, 1.f);
+        bool max_level = false, in_obj = false;
+        while ((cur < D && cur != new_depth) || pop_refraction(M, max_level, ray, new_depth, coef, in_obj)) {
+            cur = new_depth;
+            Hit h;
+            if (!intersect(S, ray.o, ray.d, h)) continue;
+            const int model = hit_model(S, h.tri);
+            const Material m = load_mat(S, model);
+            V3 n = shading_normal(S, h);
+            V3 ip = vadd(vscale(ray.d, h.t), ray.o);
+            if (in_obj && vdot(ray.d, n) > 0) n = vscale(n, -1.f);
+            V3 mdiff = tri_albedo(S, h.tri, m);
+            uint32_t flags = 2u | ((!in_obj && !vnull(mdiff)) ? 1u : 0u);
+            if (nh < RENDER_MAX_HITS) {
+                ha[nh] = make_float4(ip.x, ip.y, ip.z, __int_as_float(h.tri));
+                hb[nh] = make_float4(n.x, n.y, n.z, __uint_as_float(flags));
+                hc[nh] = make_float4(coef.x, coef.y, coef.z, __uint_as_float((uint32_t)i));
+                nh++;
+            } else {
+                raise_status(status, ST_OVERFLOW);
+            }
+            if (m.opaque < 1.f && cur != D - 1) {
+                Rgi ri = get_refractive_indices(M, S.default_ior, model, m.ior);
+                Ray nr;
+                if (ray_refract(ray, ip, n, ri.n1, ri.n2, nr))
+                    push_refraction(M, max_level, nr, cur, coef, model, m.ior, m.opaque, ri.in_obj);
+            }
+            if (!in_obj && !vnull(m.specular) && cur != D - 1) {
+                Ray nr = ray_reflect(ray, ip, n);
+                float c = powf(fmaxf(vdot(nr.d, vneg(ray.d)), 0.0f), m.shininess);
+                coef = vmul(coef, vscale(vscale(m.specular, m.opaque), c));
+                ray = nr;
+                new_depth = cur + 1;
+            }
+        }
+        if (M.overflow) raise_status(status, ST_STACK);
+    }
+    // reserve nh consecutive request slots: one atomic per warp
+    const int lane = threadIdx.x & 31;
+    unsigned incl = (unsigned)nh;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    unsigned long long base = 0;
+    unsigned wtotal = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 31 && wtotal) base = atomicAdd(R.counter, (unsigned long long)wtotal);
+    base = __shfl_sync(0xffffffffu, base, 31) + (incl - (unsigned)nh);
+    if (!valid) return;
+    if ((int64_t)(base + nh) > R.cap) {
+        raise_status(status, ST_OVERFLOW);
+        R.px_base[i] = 0;
+        R.px_count[i] = 0;
+        return;
+    }
+    for (int k = 0; k < nh; k++) {
+        R.a[base + k] = ha[k];
+        R.b[base + k] = hb[k];
+        R.c[base + k] = hc[k];
+    }
+    R.px_base[i] = (uint32_t)base;
+    R.px_count[i] = (uint32_t)nh;
+}
+
+__global__ void k_resolve(DevScene S, int64_t npx, Requests R, const float* __restrict__ est_g,
+                          const float* __restrict__ est_c, float tone_t, uint8_t* __restrict__ rgb8,
+                          float* __restrict__ radiance) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npx) return;
+    const uint32_t base = R.px_base[i], cnt = R.px_count[i];
+    V3 acc = v3(0.f, 0.f, 0.f);
+    for (uint32_t r = 0; r < cnt; r++) {
+        const size_t q = (size_t)base + r;
+        float4 a = R.a[q], b = R.b[q], c = R.c[q];
+        const int tri = __float_as_int(a.w);
+        const int model = hit_model(S, tri);
+        const Material m = load_mat(S, model);
+        const uint32_t flags = __float_as_uint(b.w);
+        V3 color = v3(0.f, 0.f, 0.f);
+        if (flags & 1u) {
+            V3 di_op = vscale(tri_albedo(S, tri, m), m.opaque);
+            color = vadd(color, vscale(vmul(ld3(est_g + 3 * q), di_op), 4.f));
+        }
+        color = vadd(color, m.emission);
+        if (est_c) color = vadd(color, vscale(ld3(est_c + 3 * q), m.opaque));
+        color = vmin1(color, 1.f);
+        acc = vadd(acc, vmul(color, xyz(c)));
+    }
+    if (radiance) st3(radiance + 3 * i, acc);
+    V3 e = v3(expf(-tone_t * acc.x), expf(-tone_t * acc.y), expf(-tone_t * acc.z));
+    V3 mp = vsub(v3(1.f, 1.f, 1.f), e);
+    const float rg = 1.0f / 2.2f;
+    V3 l = vmin1(v3(powf(mp.x, rg), powf(mp.y, rg), powf(mp.z, rg)), 1.f);
+    rgb8[3 * i] = (uint8_t)(l.x * 255);
+    rgb8[3 * i + 1] = (uint8_t)(l.y * 255);
+    rgb8[3 * i + 2] = (uint8_t)(l.z * 255);
+}
+
+}  // namespace
+
+cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
+                     cudaStream_t st) {
+    if (max_depth < 0 || max_depth > RENDER_MAX_DEPTH) return cudaErrorInvalidValue;
+    const int64_t npx = (int64_t)cam.W * cam.H;
+    cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
+    if (e != cudaSuccess) return e;
+    k_eye<<<(unsigned)((npx + EYE_THREADS - 1) / EYE_THREADS), EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status);
+    return cudaGetLastError();
+}
+
+cudaError_t resolve(const DevScene& S, const CameraDev& cam, Requests R, const float* est_g, const float* est_c,
+                    float tone_t, uint8_t* rgb8, float* radiance, cudaStream_t st) {
+    const int64_t npx = (int64_t)cam.W * cam.H;
+    k_resolve<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(S, npx, R, est_g, est_c, tone_t, rgb8, radiance);
+    return cudaGetLastError();
+}
+
+}  // namespace pm

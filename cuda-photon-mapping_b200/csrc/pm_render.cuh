@@ -1,0 +1,41 @@
+// pm_render.cuh -- eye pass (gather requests) and per-pixel resolve.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "pm_scene.cuh"
+
+namespace pm {
+
+constexpr int RENDER_MAX_DEPTH = 5;                          // eye-path depth limit of this build
+constexpr int RENDER_MAX_HITS = (1 << RENDER_MAX_DEPTH) - 1; // binary hit tree
+
+struct CameraDev {
+    float pos[3], fwd[3], right[3], up[3];
+    float vw, vh, focal;
+    int W, H;
+};
+
+// Gather request of one eye-path hit (3 float4):
+//   a = (hit point, triangle bits)  b = (shading normal, flags bits)  c = (path weight, pixel bits)
+// flags bit 0: the global-map estimate is needed (not inside an object, albedo non-zero)
+struct Requests {
+    float4* a;
+    float4* b;
+    float4* c;
+    int64_t cap;
+    unsigned long long* counter;   // requests written
+    uint32_t* px_base;             // first request of each pixel
+    uint32_t* px_count;            // requests of each pixel (hit order)
+};
+
+cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
+                     cudaStream_t st);
+
+// Combines the estimates of each pixel's requests in hit order, tone-maps and
+// quantises (CudaPhotonMapping/Raytracer.cuh:187-211, 238-240, 277).
+// est_c may be null (no caustic map).  rgb8: 3 bytes per pixel; radiance: 3
+// floats per pixel (optional).  tone_t = 1 / exposure as the reference computes it.
+cudaError_t resolve(const DevScene& S, const CameraDev& cam, Requests R, const float* est_g, const float* est_c,
+                    float tone_t, uint8_t* rgb8, float* radiance, cudaStream_t st);
+
+}  // namespace pm

@@ -1,0 +1,219 @@
+// pm_scene.cuh -- device scene layout and closest-hit query (BVH traversal).
+//
+// The reference intersects every ray with every triangle of every model whose
+// AABB the ray meets (CudaPhotonMapping/Model.cuh:366-446, AABB.cuh:103-111,
+// PhotonTracing.cu:178-213).  Here a binary BVH over all triangles culls the
+// search; the answer is kept identical to the reference's:
+//   * each triangle is tested with the reference's edge-function test
+//     (Model.cuh:69-120); the per-triangle terms that do not depend on the ray
+//     (v1-v0, v0-v2, the plane normal, 1/|n|^2, n.v0) are precomputed with the
+//     same operations, so every tested value is bit-identical;
+//   * the winner is the smallest (t, triangle index) pair.  Triangles are
+//     sorted by model, so this is the reference's order: models in index
+//     order with strict '<', triangles in index order with strict '<';
+//   * a triangle may only win if the reference's slab test of its model's
+//     AABB passes for the ray (evaluated lazily, once per model per ray);
+//   * BVH node boxes are padded, and a node is skipped only when its entry
+//     distance is strictly larger than the best t, so no candidate that could
+//     win (including exact ties) is culled.
+#pragma once
+#include "pm_device.cuh"
+
+namespace pm {
+
+// Triangle record: 5 float4 = 80 bytes
+//   q0 = (v0, n.v0)   q1 = (v1 - v0, 1/(n.n))   q2 = (v2, model bits)
+//   q3 = (v0 - v2, 0) q4 = (n, 0)             n = cross(v1 - v0, v2 - v0)
+struct DevScene {
+    const float4* tri;        // 5 per triangle
+    const float* tri_pos;     // 9 per triangle (vertex positions, as given)
+    const float* tri_nrm;     // 9 per triangle (vertex normals)
+    const float* tri_diffuse; // 3 per triangle or null
+    const float4* nodes;      // 2 per node: (lo, left|first), (hi, count)
+    const int* prim;          // leaf triangle indices
+    const float* maabb;       // 6 per model (min xyz, max xyz)
+    const float* mats;        // 12 per model
+    const float* ca;          // critical angle table: (n1, n2, cos) triples
+    int nca;
+    int ntri, nmodel;
+    int light_first, light_count;
+    float default_ior;
+};
+
+struct Material {
+    V3 diffuse, specular, emission;
+    float ior, opaque, shininess;
+};
+__device__ __forceinline__ Material load_mat(const DevScene& S, int m) {
+    const float* q = S.mats + 12 * m;
+    Material r;
+    r.diffuse = ld3(q); r.specular = ld3(q + 3); r.emission = ld3(q + 6);
+    r.ior = q[9]; r.opaque = q[10]; r.shininess = q[11];
+    return r;
+}
+__device__ __forceinline__ V3 tri_albedo(const DevScene& S, int tri, const Material& m) {
+    return S.tri_diffuse ? ld3(S.tri_diffuse + 3 * (size_t)tri) : m.diffuse;
+}
+__device__ __forceinline__ bool critical_angle(const DevScene& S, float n1, float n2, float& out) {
+    for (int i = 0; i < S.nca; i++) {
+        if (__float_as_uint(S.ca[3 * i]) == __float_as_uint(n1) && __float_as_uint(S.ca[3 * i + 1]) == __float_as_uint(n2)) {
+            out = S.ca[3 * i + 2];
+            return true;
+        }
+    }
+    return false;
+}
+
+// the reference's model AABB test: division, signbit corner choice, fmaxf/fminf
+__device__ __forceinline__ bool model_gate(const float* c, V3 o, V3 d) {
+    float tmin = 0.0f, tmax = __int_as_float(0x7f800000);
+    const float oo[3] = {o.x, o.y, o.z};
+    const float dd[3] = {d.x, d.y, d.z};
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        int s = signbit(dd[i]) ? 1 : 0;
+        float bmin = c[s * 3 + i];
+        float bmax = c[(1 - s) * 3 + i];
+        float dmin = (bmin - oo[i]) / dd[i];
+        float dmax = (bmax - oo[i]) / dd[i];
+        tmin = fmaxf(dmin, tmin);
+        tmax = fminf(dmax, tmax);
+    }
+    return tmin <= tmax;
+}
+
+struct Hit {
+    float t;
+    int tri;
+    V3 uvw;
+};
+
+// edge-function test with precomputed terms; returns false when the triangle
+// cannot be a better (t, index) candidate than (best_t, best_tri)
+__device__ __forceinline__ bool tri_test(const float4* T, V3 o, V3 d, float best_t, int tri, int best_tri,
+                                         float& t_out, V3& uvw) {
+    float4 q0 = T[0], q4 = T[4];
+    V3 n = xyz(q4);
+    float ndd = vdot(n, d);
+    if (fabsf(ndd) < 1e-6f) return false;
+    float t = (q0.w - vdot(n, o)) / ndd;
+    if (t < 0) return false;
+    if (t > best_t || (t == best_t && tri > best_tri)) return false;
+    float4 q1 = T[1], q2 = T[2], q3 = T[3];
+    V3 v0 = xyz(q0);
+    V3 P = vadd(o, vscale(d, t));
+    float w = vdot(n, vcross(xyz(q1), vsub(P, v0)));
+    if (w < 0) return false;
+    float v = vdot(n, vcross(xyz(q3), vsub(P, xyz(q2))));
+    if (v < 0) return false;
+    w = w * q1.w;
+    v = v * q1.w;
+    float u = 1.f - v - w;
+    if (u < 0) return false;
+    t_out = t;
+    uvw = v3(u, v, w);
+    return true;
+}
+
+__device__ __forceinline__ float safe_inv(float x) { return 1.0f / (x == 0.0f ? 1e-30f : x); }
+
+// closest hit; h.tri = -1 on a miss
+static __device__ __noinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit& h) {
+    float best_t = __int_as_float(0x7f800000);
+    int best_tri = 0x7fffffff;
+    V3 best_uvw = v3(0.f, 0.f, 0.f);
+    unsigned long long gate_known = 0ull, gate_pass = 0ull;
+    const float ix = safe_inv(d.x), iy = safe_inv(d.y), iz = safe_inv(d.z);
+    int stack[64];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        float4 a = __ldg(S.nodes + 2 * node);
+        float4 b = __ldg(S.nodes + 2 * node + 1);
+        float tx0 = (a.x - o.x) * ix, tx1 = (b.x - o.x) * ix;
+        float ty0 = (a.y - o.y) * iy, ty1 = (b.y - o.y) * iy;
+        float tz0 = (a.z - o.z) * iz, tz1 = (b.z - o.z) * iz;
+        float tmin = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+        float tmax = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+        bool visit = tmin <= tmax && tmin <= best_t;
+        if (visit) {
+            int count = __float_as_int(b.w);
+            int first = __float_as_int(a.w);
+            if (count > 0) {
+                for (int i = 0; i < count; i++) {
+                    int tri = __ldg(S.prim + first + i);
+                    float t; V3 uvw;
+                    const float4* T = S.tri + 5 * (size_t)tri;
+                    if (tri_test(T, o, d, best_t, tri, best_tri, t, uvw)) {
+                        int m = __float_as_int(__ldg(&T[2].w));
+                        bool pass;
+                        if (m < 64) {
+                            unsigned long long bit = 1ull << m;
+                            if (!(gate_known & bit)) {
+                                gate_known |= bit;
+                                if (model_gate(S.maabb + 6 * m, o, d)) gate_pass |= bit;
+                            }
+                            pass = (gate_pass & bit) != 0ull;
+                        } else {
+                            pass = model_gate(S.maabb + 6 * m, o, d);
+                        }
+                        if (pass) { best_t = t; best_tri = tri; best_uvw = uvw; }
+                    }
+                }
+            } else {
+                // interior: children first and first + 1; nearer child first
+                int c0 = first, c1 = first + 1;
+                float4 a0 = __ldg(S.nodes + 2 * c0), b0 = __ldg(S.nodes + 2 * c0 + 1);
+                float4 a1 = __ldg(S.nodes + 2 * c1), b1 = __ldg(S.nodes + 2 * c1 + 1);
+                float e0 = fmaxf(fmaxf(fminf((a0.x - o.x) * ix, (b0.x - o.x) * ix), fminf((a0.y - o.y) * iy, (b0.y - o.y) * iy)),
+                                 fminf((a0.z - o.z) * iz, (b0.z - o.z) * iz));
+                float e1 = fmaxf(fmaxf(fminf((a1.x - o.x) * ix, (b1.x - o.x) * ix), fminf((a1.y - o.y) * iy, (b1.y - o.y) * iy)),
+                                 fminf((a1.z - o.z) * iz, (b1.z - o.z) * iz));
+                int nearc = e0 <= e1 ? c0 : c1;
+                int farc = e0 <= e1 ? c1 : c0;
+                if (sp < 64) stack[sp++] = farc;
+                node = nearc;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    if (best_tri == 0x7fffffff) { h.tri = -1; return false; }
+    h.t = best_t; h.tri = best_tri; h.uvw = best_uvw;
+    return true;
+}
+
+// interpolated vertex normal, reciprocal-normalised (Model.cuh:436-443)
+__device__ __forceinline__ V3 shading_normal(const DevScene& S, const Hit& h) {
+    const float* n = S.tri_nrm + 9 * (size_t)h.tri;
+    V3 n0 = vscale(ld3(n), h.uvw.x), n1 = vscale(ld3(n + 3), h.uvw.y), n2 = vscale(ld3(n + 6), h.uvw.z);
+    return vnorm_recip(vadd(vadd(n0, n1), n2));
+}
+__device__ __forceinline__ int hit_model(const DevScene& S, int tri) {
+    return __float_as_int(__ldg(&S.tri[5 * (size_t)tri + 2].w));
+}
+
+// ----------------------------------------------------------- ray helpers --
+struct Ray { V3 o, d; };
+
+__device__ __forceinline__ Ray ray_reflect(const Ray& r, V3 from, V3 n) {   // Ray.cuh:64-71
+    float dnd = vdot(r.d, n);
+    V3 refl = vsub(r.d, vscale(vscale(n, 2.f), dnd));
+    Ray o;
+    o.d = vnorm_div(refl);
+    o.o = vadd(from, vscale(n, 0.01f));
+    return o;
+}
+__device__ __forceinline__ bool ray_refract(const Ray& r, V3 from, V3 n, float r1, float r2, Ray& out) {   // Ray.cuh:85-96
+    float eta = r1 / r2;
+    float c1 = -vdot(r.d, n);
+    float w = eta * c1;
+    float c2m = (w - eta) * (w + eta);
+    if (c2m < -1.f) return false;
+    out.d = vadd(vscale(r.d, eta), vscale(n, w - sqrtf(1.f + c2m)));
+    out.o = vadd(from, vscale(vneg(n), 0.01f));
+    return true;
+}
+
+}  // namespace pm

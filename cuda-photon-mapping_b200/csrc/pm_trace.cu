@@ -1,0 +1,305 @@
+// pm_trace.cu -- photon tracing.
+//
+// Reference: CudaPhotonMapping/PhotonTracing.cu:127-375 (emit / trace / destiny),
+// Model.cuh:202-243 (light point), Ray.cuh:16-96, PathOperator.cuh:7-42,
+// PhotonTraceStack.cuh:40-116, PhotonArray.cuh:31-42.
+//
+// Layout and scheduling differ from the reference on purpose:
+//  * every photon path p draws from its own counter-based stream (Philox,
+//    counter = (draw, p, tag)), so a path's photons do not depend on which
+//    thread traces it or when;
+//  * a persistent grid traces the paths [p0, p0 + npaths) of one batch.  Lanes
+//    whose path ended take the next path indices together (one atomic per
+//    warp, ballot ranks), so SIMD lanes stay busy however long paths are;
+//  * the k-th photon a path stores goes to stage slot [k][path] as two 16-byte
+//    vector stores: (position, map flag) and (direction, 0);
+//  * k_compact writes the batch's photons into the global / caustic lists in
+//    canonical order (path, then bounce) after exclusive scans of the per-path
+//    counts, and cuts each list exactly at its capacity.
+// A path that misses all geometry ends there and stores nothing (the reference
+// returns an undefined value from trace() in that case); a refraction that
+// yields no ray also ends the path.
+#include "pm_trace.cuh"
+#include "pm_scan.cuh"
+
+namespace pm {
+
+namespace {
+
+constexpr int TRACE_THREADS = 128;
+constexpr int MAX_STACK = 32;
+constexpr int REJECT_LIMIT = 1 << 16;   // emission rejection loop bound (acceptance ~1/2 on valid lights)
+
+enum { DIF = 0, SPEC = 1, ABSORB = 2, REFR = 3, NONE = 4 };
+
+struct Lane {
+    Stream st;
+    Ray ray;
+    int bounce;
+    int ng, nc;             // photons stored so far (global / caustic)
+    int diffuse_surfs;
+    int last;
+    int sn;                 // medium stack size
+};
+
+struct KParams {
+    DevScene S;
+    uint64_t seed;
+    uint32_t tag;
+    int max_bounces;
+    int64_t p0, npaths;
+    V3 power;
+    unsigned long long* counter;
+    float4* stage_pos;
+    float4* stage_dir;
+    uint32_t* cnt_g;
+    uint32_t* cnt_c;
+    unsigned* status;
+};
+
+// light point + cosine-weighted direction by rejection (PhotonTracing.cu:345-369)
+__device__ __forceinline__ void start_path(const KParams& P, Lane& L, int64_t path) {
+    const DevScene& S = P.S;
+    L.st.init(P.seed, (uint64_t)path, P.tag);
+    int k = (int)roundf(0 + L.st.next() * (float)(S.light_count - 1));
+    int tri = S.light_first + k;
+    float bx = L.st.next();
+    float by = 0.f + L.st.next() * ((1.f - bx) - 0.f);
+    float bz = 1.f - bx - by;
+    const float* tp = S.tri_pos + 9 * (size_t)tri;
+    const float* tn = S.tri_nrm + 9 * (size_t)tri;
+    V3 point = vadd(vadd(vscale(ld3(tp), bx), vscale(ld3(tp + 3), by)), vscale(ld3(tp + 6), bz));
+    V3 lnorm = vadd(vadd(vscale(ld3(tn), bx), vscale(ld3(tn + 3), by)), vscale(ld3(tn + 6), bz));
+    L.ray.o = vadd(point, vscale(lnorm, 0.0001f));
+    float prob, dt;
+    V3 d;
+    int tries = 0;
+    do {
+        if (++tries > REJECT_LIMIT) {   // a light without a usable normal: end the path
+            raise_status(P.status, ST_BAD_INPUT);
+            L.ray.d = v3(0.f, 0.f, 0.f);
+            break;
+        }
+        d.x = -1.f + L.st.next() * 2.f;
+        d.y = -1.f + L.st.next() * 2.f;
+        d.z = -1.f + L.st.next() * 2.f;
+        d = vnorm_recip(d);
+        prob = L.st.next();
+        dt = vdot(d, lnorm);
+        if (dt < 0) { dt = -dt; d = vscale(d, -1.f); }
+    } while (prob > dt);
+    if (tries <= REJECT_LIMIT) L.ray.d = d;
+    L.bounce = 0;
+    L.ng = L.nc = 0;
+    L.diffuse_surfs = 0;
+    L.last = NONE;
+    L.sn = 0;
+}
+
+// Marsaglia disc, rejected into the hemisphere of n (Ray.cuh:16-56)
+__device__ __forceinline__ Ray diffuse_bounce(V3 from, V3 n, Stream& st) {
+    V3 d;
+    do {
+        float x1, x2, s1, s2;
+        do {
+            x1 = -1.f + st.next() * 2.f;
+            x2 = -1.f + st.next() * 2.f;
+            s1 = x1 * x1;
+            s2 = x2 * x2;
+        } while (s1 + s2 >= 1);
+        float f = sqrtf(1.f - s1 - s2);
+        d = v3(2.f * x1 * f, 2.f * x2 * f, 1.f - 2.f * (s1 + s2));
+    } while (vdot(d, n) < 0);
+    Ray r;
+    r.d = vnorm_div(d);
+    r.o = vadd(from, vscale(r.d, 0.0001f));
+    return r;
+}
+
+// Fresnel-Schlick with the integer powers written as products (PhotonTracing.cu:215-218)
+__device__ __forceinline__ float schlick(float cosNL, float n1, float n2) {
+    float q = (n1 - n2) / (n1 + n2);
+    float f0 = q * q;
+    float c = 1.f - cosNL;
+    float c2 = c * c;
+    float c5 = c2 * c2 * c;
+    return f0 + (1.f - f0) * c5;
+}
+
+// one bounce of lane L (PhotonTracing.cu:278-326); returns false when the path ends
+__device__ __forceinline__ bool bounce(const KParams& P, Lane& L, float* sior, int* sid, int64_t j) {
+    const DevScene& S = P.S;
+    Hit h;
+    if (!intersect(S, L.ray.o, L.ray.d, h)) return false;
+    const int model = hit_model(S, h.tri);
+    const Material m = load_mat(S, model);
+    V3 n = shading_normal(S, h);
+    V3 ip = vadd(vscale(L.ray.d, h.t), L.ray.o);
+    if (vdot(L.ray.d, n) > 0) n = vscale(n, -1.f);
+    float cosNL = vdot(vneg(L.ray.d), n);
+    V3 mdiff = tri_albedo(S, h.tri, m);
+
+    int dest;
+    bool refr = false;
+    if (m.opaque != 1.f) {
+        float n1, n2;
+        if (L.sn == 0) { n1 = S.default_ior; n2 = m.ior; }
+        else if (sid[L.sn - 1] == model) { n1 = sior[L.sn - 1]; n2 = L.sn == 1 ? S.default_ior : sior[L.sn - 2]; }
+        else { n1 = sior[L.sn - 1]; n2 = m.ior; }
+        float cang;
+        bool tir = critical_angle(S, n1, n2, cang) && cosNL <= cang;
+        if (!tir) {
+            float pr = 1.f - schlick(cosNL, n1, n2);
+            float e = L.st.next();
+            refr = !(e > pr);
+        }
+    }
+    if (refr) {
+        dest = REFR;
+    } else {
+        float max_lp = vmax3(P.power);
+        float e = 0.f + L.st.next() * (2.f - 0.f);
+        float pd = vmax3(vmul(mdiff, P.power)) / max_lp;
+        if (e <= pd) dest = DIF;
+        else {
+            float ps = vmax3(vmul(m.specular, P.power)) / max_lp;
+            dest = (e <= pd + ps) ? SPEC : ABSORB;
+        }
+    }
+
+    Ray nr;
+    nr.o = v3(0.f, 0.f, 0.f); nr.d = v3(0.f, 0.f, 0.f);
+    bool alive = true;
+    if (dest == REFR) {
+        float n1, n2;
+        if (L.sn != 0 && sid[L.sn - 1] == model) {
+            n1 = sior[L.sn - 1];
+            n2 = L.sn == 1 ? S.default_ior : sior[L.sn - 2];
+            L.sn--;
+        } else {
+            bool was_empty = L.sn == 0;
+            float top_ior = was_empty ? 0.f : sior[L.sn - 1];
+            if (L.sn < P.max_bounces && L.sn < MAX_STACK) { sior[L.sn] = m.ior; sid[L.sn] = model; L.sn++; }
+            else raise_status(P.status, ST_STACK);
+            n1 = was_empty ? S.default_ior : top_ior;
+            n2 = m.ior;
+        }
+        if (!ray_refract(L.ray, ip, n, n1, n2, nr)) alive = false;
+    } else if (dest == DIF || (dest == ABSORB && !vnear(m.specular, v3(1.f, 1.f, 1.f)))) {
+        bool caustic = (L.last == SPEC || L.last == REFR) && L.diffuse_surfs == 0;
+        int slot = L.ng + L.nc;
+        size_t o = (size_t)slot * (size_t)P.npaths + (size_t)j;
+        P.stage_pos[o] = make_float4(ip.x, ip.y, ip.z, __int_as_float(caustic ? 2 : 1));
+        P.stage_dir[o] = make_float4(L.ray.d.x, L.ray.d.y, L.ray.d.z, 0.f);
+        if (caustic) L.nc++; else L.ng++;
+    } else if (dest == SPEC) {
+        nr = ray_reflect(L.ray, ip, n);
+    }
+    if (dest == DIF) {
+        nr = diffuse_bounce(ip, n, L.st);
+        L.diffuse_surfs++;
+    }
+    L.last = dest;
+    if (dest == ABSORB || !alive) return false;
+    L.ray = nr;
+    return true;
+}
+
+__global__ void __launch_bounds__(TRACE_THREADS)
+k_trace(KParams P) {
+    const int lane = threadIdx.x & 31;
+    Lane L;
+    float sior[MAX_STACK];
+    int sid[MAX_STACK];
+    int64_t j = -1;          // batch-local path index of this lane, -1: idle
+    bool done = false;
+    while (true) {
+        bool need = !done && j < 0;
+        unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(P.counter, (unsigned long long)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                unsigned long long mine = base + (unsigned long long)__popc(m & lanemask_lt());
+                if ((int64_t)mine < P.npaths) {
+                    j = (int64_t)mine;
+                    start_path(P, L, P.p0 + j);
+                } else {
+                    done = true;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+        if (j >= 0) {
+            bool alive = bounce(P, L, sior, sid, j);
+            L.bounce++;
+            if (!alive || L.bounce > P.max_bounces - 1) {
+                P.cnt_g[j] = (uint32_t)L.ng;
+                P.cnt_c[j] = (uint32_t)L.nc;
+                j = -1;
+            }
+        }
+    }
+}
+
+// canonical-order append of one batch into the two photon lists
+__global__ void k_compact(int64_t npaths, const float4* __restrict__ stage_pos, const float4* __restrict__ stage_dir,
+                          const uint32_t* __restrict__ cnt_g, const uint32_t* __restrict__ cnt_c,
+                          const uint32_t* __restrict__ scan_g, const uint32_t* __restrict__ scan_c, V3 power,
+                          float* gpos, float* gdir, float* gpow, int64_t gcap, int64_t gfilled,
+                          float* cpos, float* cdir, float* cpow, int64_t ccap, int64_t cfilled) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= npaths) return;
+    int ng = (int)cnt_g[j], nc = (int)cnt_c[j];
+    int64_t og = gfilled + scan_g[j], oc = cfilled + scan_c[j];
+    for (int k = 0; k < ng + nc; k++) {
+        size_t o = (size_t)k * (size_t)npaths + (size_t)j;
+        float4 p = stage_pos[o];
+        float4 d = stage_dir[o];
+        bool caustic = __float_as_int(p.w) == 2;
+        float *dp, *dd, *dw;
+        int64_t idx;
+        if (caustic) {
+            if (oc >= ccap) { oc++; continue; }
+            idx = oc++; dp = cpos; dd = cdir; dw = cpow;
+        } else {
+            if (og >= gcap) { og++; continue; }
+            idx = og++; dp = gpos; dd = gdir; dw = gpow;
+        }
+        dp[3 * idx] = p.x; dp[3 * idx + 1] = p.y; dp[3 * idx + 2] = p.z;
+        dd[3 * idx] = d.x; dd[3 * idx + 1] = d.y; dd[3 * idx + 2] = d.z;
+        dw[3 * idx] = power.x; dw[3 * idx + 1] = power.y; dw[3 * idx + 2] = power.z;
+    }
+}
+
+}  // namespace
+
+cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_t st) {
+    cudaError_t e;
+    if (B.npaths <= 0) return cudaSuccess;
+    if ((e = cudaMemsetAsync(B.path_counter, 0, 8, st)) != cudaSuccess) return e;
+    KParams P;
+    P.S = B.S; P.seed = B.seed; P.tag = B.tag; P.max_bounces = B.max_bounces;
+    P.p0 = B.p0; P.npaths = B.npaths;
+    P.power = v3(B.power[0], B.power[1], B.power[2]);
+    P.counter = B.path_counter;
+    P.stage_pos = B.stage_pos; P.stage_dir = B.stage_dir;
+    P.cnt_g = B.cnt_g; P.cnt_c = B.cnt_c;
+    P.status = B.status;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace, TRACE_THREADS, 0)) != cudaSuccess) return e;
+    int64_t want = (B.npaths + TRACE_THREADS - 1) / TRACE_THREADS;
+    int64_t grid = std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * B.sm_count);
+    k_trace<<<(unsigned)grid, TRACE_THREADS, 0, st>>>(P);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = scan_u32(B.cnt_g, B.scan_g, B.npaths, 0, B.totals, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+    if ((e = scan_u32(B.cnt_c, B.scan_c, B.npaths, 0, B.totals + 1, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+    k_compact<<<(unsigned)((B.npaths + 255) / 256), 256, 0, st>>>(
+        B.npaths, B.stage_pos, B.stage_dir, B.cnt_g, B.cnt_c, B.scan_g, B.scan_c, P.power,
+        G.pos, G.dir, G.pow, G.cap, G.filled, C.pos, C.dir, C.pow, C.cap, C.filled);
+    return cudaGetLastError();
+}
+
+}  // namespace pm

@@ -1,0 +1,305 @@
+"""Python host side of the B200 photon-mapping core: ctypes over the C ABI.
+
+Every method is one call into ``lib/libpm_b200.so`` (declared in
+include/pm_api.h).  PyTorch supplies device memory (tensors are passed by
+``data_ptr()``); no computation happens in Python.  The library must be built
+(``make -C cuda-photon-mapping_b200/csrc``): there is no fallback path, and a
+missing library or CUDA device raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libpm_b200.so")
+
+PM_MAP_GLOBAL = 0
+PM_MAP_CAUSTIC = 1
+
+ERRORS = {-1: "PM_ERR_INVALID", -2: "PM_ERR_CUDA", -3: "PM_ERR_OOM", -4: "PM_ERR_TIMEOUT",
+          -5: "PM_ERR_OVERFLOW", -6: "PM_ERR_IO"}
+
+
+class PMError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _DeviceOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("stream", C.c_void_p)]
+
+
+class _SceneDesc(C.Structure):
+    _fields_ = [("ntri", C.c_int32), ("tri_pos", C.c_void_p), ("tri_nrm", C.c_void_p), ("tri_model", C.c_void_p),
+                ("tri_diffuse", C.c_void_p), ("nmodel", C.c_int32), ("materials", C.c_void_p),
+                ("light_model", C.c_int32), ("light_intensity", C.c_float * 3), ("default_ior", C.c_float)]
+
+
+class _TraceOpts(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("stream_tag", C.c_uint32), ("max_bounces", C.c_int32),
+                ("global_capacity", C.c_int64), ("caustic_capacity", C.c_int64), ("max_paths", C.c_int64)]
+
+
+class _GridOpts(C.Structure):
+    _fields_ = [("desired_per_cell", C.c_int32), ("regrid_mult", C.c_int32), ("regrid_div", C.c_int32)]
+
+
+class Camera(C.Structure):
+    """The reference Camera's fields (CudaPhotonMapping/Camera.cuh:11-33)."""
+    _fields_ = [("position", C.c_float * 3), ("forward", C.c_float * 3), ("right", C.c_float * 3),
+                ("up", C.c_float * 3), ("viewport_w", C.c_float), ("viewport_h", C.c_float), ("focal", C.c_float),
+                ("width", C.c_int32), ("height", C.c_int32)]
+
+    def as_vector(self):
+        return np.array(list(self.position) + list(self.forward) + list(self.right) + list(self.up) +
+                        [self.viewport_w, self.viewport_h, self.focal], np.float32)
+
+
+class _RenderOpts(C.Structure):
+    _fields_ = [("max_depth", C.c_int32), ("k_global", C.c_int32), ("r_global", C.c_float),
+                ("k_caustic", C.c_int32), ("r_caustic", C.c_float), ("faithful_caustic", C.c_int32)]
+
+
+class _PhotonView(C.Structure):
+    _fields_ = [("count", C.c_int64), ("cells", C.c_int64), ("dims", C.c_int32 * 3), ("cell_size", C.c_float),
+                ("aabb", C.c_float * 6), ("cell_starts", C.c_void_p), ("cell_sizes", C.c_void_p),
+                ("sorted_pos", C.c_void_p), ("sorted_dir", C.c_void_p), ("sorted_power", C.c_void_p),
+                ("list_pos", C.c_void_p), ("list_dir", C.c_void_p), ("list_power", C.c_void_p)]
+
+
+_LIB = None
+
+
+def library():
+    """Load libpm_b200.so (once).  Raises when it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `make -C cuda-photon-mapping_b200/csrc`")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, f32 = C.c_void_p, C.c_int32, C.c_int64, C.c_float
+    sig = {
+        "pm_create": ([C.POINTER(C.c_void_p), C.POINTER(_DeviceOpts)], C.c_int),
+        "pm_destroy": ([vp], None),
+        "pm_last_error": ([vp], C.c_char_p),
+        "pm_sync": ([vp], C.c_int),
+        "pm_set_scene": ([vp, C.POINTER(_SceneDesc)], C.c_int),
+        "pm_scene_aabb": ([vp, vp], C.c_int),
+        "pm_trace_photons": ([vp, C.POINTER(_TraceOpts), C.POINTER(C.c_int64)], C.c_int),
+        "pm_trace_paths": ([vp, C.POINTER(_TraceOpts), i64, i64, i64, vp, vp, vp, vp, vp,
+                            C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
+        "pm_set_photons": ([vp, C.c_int, i64, vp, vp, vp], C.c_int),
+        "pm_build_grid": ([vp, C.c_int, C.POINTER(_GridOpts), vp], C.c_int),
+        "pm_get_photons": ([vp, C.c_int, C.POINTER(_PhotonView)], C.c_int),
+        "pm_save_photons": ([vp, C.c_int, C.c_char_p], C.c_int),
+        "pm_load_photons": ([vp, C.c_int, C.c_char_p], C.c_int),
+        "pm_gather": ([vp, C.c_int, i64, vp, vp, C.c_int, f32, vp, vp, vp], C.c_int),
+        "pm_camera_setup": ([vp, vp, vp, f32, i32, i32, C.POINTER(Camera)], C.c_int),
+        "pm_render": ([vp, C.POINTER(Camera), C.POINTER(_RenderOpts), vp, vp], C.c_int),
+        "pm_scan_u32": ([vp, vp, vp, i64, C.c_int], C.c_int),
+        "pm_stage_times": ([vp, vp], C.c_int),
+        "pm_status": ([vp, vp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+def camera_setup(position, direction, up, fov_deg, width, height) -> Camera:
+    """Camera(position, direction, up, fov, W, H) as the reference constructs it."""
+    L = library()
+    cam = Camera()
+    p = np.asarray(position, np.float32); d = np.asarray(direction, np.float32); u = np.asarray(up, np.float32)
+    rc = L.pm_camera_setup(p.ctypes.data, d.ctypes.data, u.ctypes.data, float(fov_deg), int(width), int(height),
+                           C.byref(cam))
+    if rc:
+        raise PMError(rc, "pm_camera_setup")
+    return cam
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+class Context:
+    """One pm_ctx: a device, a stream, a scene, two photon maps."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+        self.torch = torch
+        self.L = library()
+        if not torch.cuda.is_available():
+            raise RuntimeError("photonmap needs a CUDA device")
+        self.device = torch.device("cuda", device)
+        h = C.c_void_p()
+        opts = _DeviceOpts(device, None if stream is None else C.c_void_p(stream.cuda_stream))
+        rc = self.L.pm_create(C.byref(h), C.byref(opts))
+        if rc:
+            raise PMError(rc, "pm_create")
+        self.h = h
+        self._scene = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            raise PMError(rc, f"{what}: {self.L.pm_last_error(self.h).decode()}")
+
+    # ------------------------------------------------------------ scene
+    def set_scene(self, sc):
+        pos = np.ascontiguousarray(sc.tri_pos, np.float32)
+        nrm = np.ascontiguousarray(sc.tri_nrm, np.float32)
+        tm = np.ascontiguousarray(sc.tri_model, np.int32)
+        mats = np.ascontiguousarray(sc.materials, np.float32)
+        td = None if sc.tri_diffuse is None else np.ascontiguousarray(sc.tri_diffuse, np.float32)
+        d = _SceneDesc(sc.ntri, pos.ctypes.data, nrm.ctypes.data, tm.ctypes.data,
+                       None if td is None else td.ctypes.data, sc.nmodel, mats.ctypes.data, int(sc.light_model),
+                       (C.c_float * 3)(*[float(x) for x in sc.light_intensity]), float(sc.default_ior))
+        self._check(self.L.pm_set_scene(self.h, C.byref(d)), "pm_set_scene")
+        self._scene = sc
+
+    def scene_aabb(self):
+        out = np.empty(6, np.float32)
+        self._check(self.L.pm_scene_aabb(self.h, out.ctypes.data), "pm_scene_aabb")
+        return out
+
+    # ----------------------------------------------------------- photons
+    def trace_photons(self, seed, max_bounces, global_capacity, caustic_capacity=0, tag=0, max_paths=0):
+        o = _TraceOpts(seed, tag, max_bounces, global_capacity, caustic_capacity, max_paths)
+        paths = C.c_int64()
+        self._check(self.L.pm_trace_photons(self.h, C.byref(o), C.byref(paths)), "pm_trace_photons")
+        return paths.value
+
+    def trace_paths(self, seed, max_bounces, power_capacity, p0, p1, tag=0):
+        torch = self.torch
+        n = p1 - p0
+        cap = n * max_bounces
+        gp = torch.empty((cap, 3), dtype=torch.float32, device=self.device)
+        gd = torch.empty_like(gp); cp = torch.empty_like(gp); cd = torch.empty_like(gp)
+        counts = torch.empty((n, 2), dtype=torch.int32, device=self.device)
+        o = _TraceOpts(seed, tag, max_bounces, 0, 0, 0)
+        ng, nc = C.c_int64(), C.c_int64()
+        self._check(self.L.pm_trace_paths(self.h, C.byref(o), p0, p1, power_capacity, _ptr(gp), _ptr(gd), _ptr(cp),
+                                          _ptr(cd), _ptr(counts), C.byref(ng), C.byref(nc)), "pm_trace_paths")
+        return dict(counts=counts, g_pos=gp[:ng.value], g_dir=gd[:ng.value], c_pos=cp[:nc.value], c_dir=cd[:nc.value])
+
+    def set_photons(self, map_id, pos, power, direction):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        pw = np.ascontiguousarray(power, np.float32).reshape(-1, 3)
+        dr = np.ascontiguousarray(direction, np.float32).reshape(-1, 3)
+        self._check(self.L.pm_set_photons(self.h, map_id, pos.shape[0], pos.ctypes.data, pw.ctypes.data,
+                                          dr.ctypes.data), "pm_set_photons")
+
+    def build_grid(self, map_id=PM_MAP_GLOBAL, desired=1000, regrid_mult=5, regrid_div=5, aabb=None):
+        o = _GridOpts(desired, regrid_mult, regrid_div)
+        box = None if aabb is None else np.ascontiguousarray(aabb, np.float32)
+        self._check(self.L.pm_build_grid(self.h, map_id, C.byref(o), None if box is None else box.ctypes.data),
+                    "pm_build_grid")
+
+    def view(self, map_id=PM_MAP_GLOBAL):
+        v = _PhotonView()
+        self._check(self.L.pm_get_photons(self.h, map_id, C.byref(v)), "pm_get_photons")
+        return v
+
+    def photons(self, map_id=PM_MAP_GLOBAL, sorted_=True):
+        """Copies of a map's device arrays as torch tensors."""
+        torch = self.torch
+        v = self.view(map_id)
+        n = v.count
+
+        def dev(ptr, count, dtype, shape):
+            if not count:
+                return torch.empty(shape, dtype=dtype, device=self.device)
+            return torch.as_tensor(_DeviceArray(ptr, shape, dtype), device=self.device).clone()
+
+        out = dict(count=n, list_pos=dev(v.list_pos, n, torch.float32, (n, 3)),
+                   list_dir=dev(v.list_dir, n, torch.float32, (n, 3)),
+                   list_power=dev(v.list_power, n, torch.float32, (n, 3)))
+        if sorted_ and v.cell_starts:
+            cells = v.cells
+            out.update(dims=tuple(v.dims), cell=v.cell_size, aabb=np.array(list(v.aabb), np.float32), cells=cells,
+                       cell_starts=dev(v.cell_starts, cells, torch.int32, (cells,)),
+                       cell_sizes=dev(v.cell_sizes, cells, torch.int32, (cells,)),
+                       sorted_pos=dev(v.sorted_pos, n, torch.float32, (n, 4)),
+                       sorted_dir=dev(v.sorted_dir, n, torch.float32, (n, 3)),
+                       sorted_power=dev(v.sorted_power, n, torch.float32, (n, 3)))
+        return out
+
+    def save_photons(self, map_id, path):
+        self._check(self.L.pm_save_photons(self.h, map_id, str(path).encode()), "pm_save_photons")
+
+    def load_photons(self, map_id, path):
+        self._check(self.L.pm_load_photons(self.h, map_id, str(path).encode()), "pm_load_photons")
+
+    # ------------------------------------------------------------ gather
+    def gather(self, qpos, qnrm, k, radius, map_id=PM_MAP_GLOBAL, want_ids=False):
+        torch = self.torch
+        qpos = qpos.to(self.device, torch.float32).contiguous()
+        qnrm = qnrm.to(self.device, torch.float32).contiguous()
+        n = qpos.shape[0]
+        rad = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        ids = torch.empty((n, k), dtype=torch.int32, device=self.device) if want_ids else None
+        cnt = torch.empty(n, dtype=torch.int32, device=self.device)
+        self._check(self.L.pm_gather(self.h, map_id, n, _ptr(qpos), _ptr(qnrm), int(k), float(radius), _ptr(rad),
+                                     _ptr(ids), _ptr(cnt)), "pm_gather")
+        return rad, ids, cnt
+
+    # ------------------------------------------------------------ render
+    def render(self, cam: Camera, k_global, r_global, max_depth=4, k_caustic=0, r_caustic=0.2,
+               faithful_caustic=True, radiance=True, out_rgb8=None, out_radiance=None):
+        torch = self.torch
+        W, H = cam.width, cam.height
+        rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
+        rad = out_radiance
+        if rad is None and radiance:
+            rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
+        o = _RenderOpts(max_depth, k_global, r_global, k_caustic, r_caustic, int(faithful_caustic))
+        self._check(self.L.pm_render(self.h, C.byref(cam), C.byref(o), _ptr(rgb), _ptr(rad)), "pm_render")
+        return rgb, rad
+
+    def scan_u32(self, x, inclusive):
+        torch = self.torch
+        x = x.to(self.device, torch.int32).contiguous()
+        out = torch.empty_like(x)
+        self._check(self.L.pm_scan_u32(self.h, _ptr(x), _ptr(out), x.numel(), int(inclusive)), "pm_scan_u32")
+        return out
+
+    def stage_times(self):
+        out = np.zeros(8, np.float32)
+        self._check(self.L.pm_stage_times(self.h, out.ctypes.data), "pm_stage_times")
+        return dict(trace_ms=float(out[0]), grid_ms=float(out[1]), eye_ms=float(out[2]), gather_ms=float(out[3]),
+                    resolve_ms=float(out[4]))
+
+    def status(self):
+        out = np.zeros(1, np.uint32)
+        self._check(self.L.pm_status(self.h, out.ctypes.data), "pm_status")
+        return int(out[0])
+
+    def sync(self):
+        self._check(self.L.pm_sync(self.h), "pm_sync")
+
+
+class _DeviceArray:
+    """Zero-copy view of a library-owned device array (CUDA array interface)."""
+    _TYPESTR = {"torch.float32": "<f4", "torch.int32": "<i4", "torch.uint8": "|u1"}
+
+    def __init__(self, ptr, shape, dtype):
+        self.__cuda_array_interface__ = {"shape": tuple(int(x) for x in shape), "typestr": self._TYPESTR[str(dtype)],
+                                         "data": (int(ptr), True), "version": 3, "strides": None}

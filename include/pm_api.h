@@ -1,0 +1,192 @@
+/* pm_api.h -- C ABI of the B200 photon-mapping core (libpm_b200.so).
+ *
+ * The reference (Alator-ux/Cuda-Photon-Mapping, paths relative to its
+ * CudaPhotonMapping/ directory) has no formal plugin API; its host calls C++
+ * functions at three seams.  Each entry point below names the seam it replaces.
+ *
+ * Conventions
+ *  - Every function returns PM_OK (0) or a negative PM_ERR_* code; the message
+ *    of the last failure is available from pm_last_error().  The library never
+ *    exits the process and never resets the device (the reference's check_cuda
+ *    does both, CudaUtils.cu:6-14).
+ *  - A pm_ctx belongs to one host thread at a time.  All device work is issued
+ *    on the context's stream; entry points that return host-visible results
+ *    synchronise that stream before returning.
+ *  - Device buffers the context allocates are owned by it and freed by
+ *    pm_destroy.  Output buffers passed in by the caller stay the caller's.
+ *  - Pointers documented as "device" must be device (or managed) memory of the
+ *    context's device; "host" pointers are read during the call only.
+ */
+#ifndef PM_API_H
+#define PM_API_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PM_OK 0
+#define PM_ERR_INVALID (-1)   /* bad argument or call order */
+#define PM_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define PM_ERR_OOM (-3)       /* device allocation failed */
+#define PM_ERR_TIMEOUT (-4)   /* a bounded device wait gave up (status word) */
+#define PM_ERR_OVERFLOW (-5)  /* a fixed-capacity device buffer would have overflowed */
+#define PM_ERR_IO (-6)        /* file read / write failed */
+
+#define PM_MAP_GLOBAL 0       /* the reference's diffuse_grid  */
+#define PM_MAP_CAUSTIC 1      /* the reference's specular_grid */
+
+typedef struct pm_ctx pm_ctx;
+
+typedef struct {
+    int device;        /* CUDA device ordinal */
+    void* stream;      /* cudaStream_t to issue work on; NULL: the context creates one */
+} pm_device_opts;
+
+/* Triangle soup sorted by model (tri_model non-decreasing).  materials: 12
+ * floats per model = diffuse[3] specular[3] emission[3] ior opaque shininess
+ * (Material.cuh:4-31).  tri_diffuse (optional, 3 floats per triangle)
+ * overrides the model's diffuse albedo per triangle.  Host pointers. */
+typedef struct {
+    int32_t ntri;
+    const float* tri_pos;       /* 9 floats per triangle: v0 v1 v2 */
+    const float* tri_nrm;       /* 9 floats per triangle: vertex normals */
+    const int32_t* tri_model;
+    const float* tri_diffuse;   /* may be NULL */
+    int32_t nmodel;
+    const float* materials;
+    int32_t light_model;        /* the model photons are emitted from (Initializer.cu:62-100) */
+    float light_intensity[3];   /* LightSource::intensity (Light.cuh:8) */
+    float default_ior;          /* GlobalParams::default_refractive_index */
+} pm_scene_desc;
+
+typedef struct {
+    uint64_t seed;              /* key of the per-path Philox streams */
+    uint32_t stream_tag;        /* fourth counter word (0 for photon paths) */
+    int32_t max_bounces;        /* PHOTON_BOUNCE_NUM (PhotonTracing.cu:20); 1..32 */
+    int64_t global_capacity;    /* diffuse_num of trace_photons */
+    int64_t caustic_capacity;   /* specular_num of trace_photons (0: no caustic map) */
+    int64_t max_paths;          /* give up (PM_ERR_INVALID) after this many paths; 0: 64 x capacity */
+} pm_trace_opts;
+
+typedef struct {
+    int32_t desired_per_cell;   /* 1000 in PhotonGrid::build */
+    int32_t regrid_mult;        /* re-grid when a cell holds > regrid_mult * desired (5) */
+    int32_t regrid_div;         /* ... at desired / regrid_div photons per cell (5) */
+} pm_grid_opts;
+
+/* The reference Camera's fields (Camera.cuh:11-33); pm_camera_setup fills them
+ * like Camera's constructor (Camera.cuh:43-65). */
+typedef struct {
+    float position[3], forward[3], right[3], up[3];
+    float viewport_w, viewport_h, focal;
+    int32_t width, height;
+} pm_camera;
+
+typedef struct {
+    int32_t max_depth;          /* GlobalParams::max_depth (kernel.cu:23): 0..5 */
+    int32_t k_global;           /* GlobalParams::global_photon_num: kNN k of the global map (<= 256) */
+    float r_global;             /* 0.1 in render_trace (Raytracer.cuh:187) */
+    int32_t k_caustic;          /* GlobalParams::caustic_photon_num (<= 256) */
+    float r_caustic;            /* 0.2 (Raytracer.cuh:200) */
+    int32_t faithful_caustic;   /* 1: the caustic estimate reads the global map's direction / power
+                                   arrays with caustic indices, as Raytracer.cuh:203-204 does */
+} pm_render_opts;
+
+/* Read-only device view of one photon map (valid until the map is rebuilt). */
+typedef struct {
+    int64_t count;              /* photons in the map */
+    int64_t cells;
+    int32_t dims[3];
+    float cell_size;
+    float aabb[6];
+    const uint32_t* cell_starts;    /* device, cells entries (exclusive scan of cell_sizes) */
+    const uint32_t* cell_sizes;     /* device, cells entries */
+    const float* sorted_pos;        /* device, 4 floats per photon: xyz + source index bits */
+    const float* sorted_dir;        /* device, 3 floats per photon */
+    const float* sorted_power;      /* device, 3 floats per photon */
+    const float* list_pos;          /* device, traced order (before the grid build), 3 floats */
+    const float* list_dir;
+    const float* list_power;
+} pm_photon_view;
+
+/* ------------------------------------------------------------- lifetime -- */
+int pm_create(pm_ctx** out, const pm_device_opts* opts);
+void pm_destroy(pm_ctx* ctx);
+const char* pm_last_error(const pm_ctx* ctx);
+int pm_sync(pm_ctx* ctx);
+
+/* Scene upload + BVH build.  Replaces the device half of
+ * initialize_scene_and_photon_maps (Initializer.cu:180-205): models, lights,
+ * scene AABB, critical-angle table (PhotonTracing.cu:79-125). */
+int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* scene);
+int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]);
+
+/* Photon pass.  Replaces trace_photons(gpu_scene, cpu_scene, diffuse_num,
+ * specular_num) (PhotonTracing.cu:379-422): fills both maps' photon lists to
+ * capacity in canonical order (path index, then bounce). out_paths (optional)
+ * receives the number of paths traced. */
+int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* opts, int64_t* out_paths);
+
+/* Photon output of paths [p0, p1) without a capacity cut (parity testing and
+ * path-range sharding).  Writes device arrays of capacity (p1-p0)*max_bounces
+ * photons per map: pos/dir (3 floats), and per path counts[2] (global,
+ * caustic).  power_capacity sets the photon power (intensity / power_capacity). */
+int pm_trace_paths(pm_ctx* ctx, const pm_trace_opts* opts, int64_t p0, int64_t p1, int64_t power_capacity,
+                   float* g_pos, float* g_dir, float* c_pos, float* c_dir, uint32_t* counts,
+                   int64_t* out_ng, int64_t* out_nc);
+
+/* Replace a map's photon list with caller data (host arrays, 3 floats per
+ * photon) -- the input side of PhotonGrid::build and of the photon-map
+ * reader load() (Initializer.cu:102-141). */
+int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const float* power, const float* dir);
+
+/* Grid build.  Replaces PhotonGrid(num_photons, aabb).build(photons, 1000,
+ * 5000) (PhotonGrid.cuh:44-66, PhotonGrid.cu:41-218).  aabb: NULL = scene AABB. */
+int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* opts, const float* aabb);
+int pm_get_photons(pm_ctx* ctx, int map, pm_photon_view* out);
+
+/* Photon-map file in the reference's layout: u64 count, then per photon
+ * pos[3] power[3] inc_dir[3] float32 (the reader is Initializer.cu:102-141).
+ * Save writes the map's traced-order list; load fills the list (build next). */
+int pm_save_photons(pm_ctx* ctx, int map, const char* path);
+int pm_load_photons(pm_ctx* ctx, int map, const char* path);
+
+/* kNN gather + radiance estimate over a built map.  Replaces
+ * PhotonGrid::find_nearests + Raytracer::get_color_from_photon_grid
+ * (PhotonGrid.cu:257-284, Raytracer.cuh:110-138) for n query points.
+ * Device arrays: qpos/qnrm 3 floats per query; out_rad 3 floats per query;
+ * out_ids (optional) k per query, source indices ascending by (distance, index),
+ * 0xffffffff padding; out_cnt (optional) neighbours found. */
+int pm_gather(pm_ctx* ctx, int map, int64_t n, const float* qpos, const float* qnrm, int k, float radius,
+              float* out_rad, uint32_t* out_ids, int32_t* out_cnt);
+
+/* Camera like Camera(position, direction, up, fov, W, H) (Camera.cuh:43-65). */
+int pm_camera_setup(const float position[3], const float direction[3], const float up[3], float vertical_fov_deg,
+                    int32_t width, int32_t height, pm_camera* out);
+
+/* One frame.  Replaces Drawer::draw_in_gpu / Raytracer::render_gpu
+ * (Drawer.cu:22-41, Raytracer.cuh:245-279): out_rgb8 is a device buffer of
+ * width*height*3 bytes (row 0 = bottom row, as the reference's canvas);
+ * out_radiance (optional) 3 floats per pixel, before tone mapping.
+ * The global map must be built; the caustic map is used when built. */
+int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, uint8_t* out_rgb8, float* out_radiance);
+
+/* Device prefix sum used by the grid build (exposed for known-answer tests):
+ * exclusive (inclusive = 0) or inclusive scan of n u32 device values. */
+int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive);
+
+/* Per-stage device times of the last pm_trace_photons / pm_build_grid /
+ * pm_render calls in milliseconds (CUDA events on the context stream):
+ * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather, [4] resolve. */
+int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
+
+/* Device status word (bits: 1 timeout, 2 overflow, 4 stack, 8 bad input); read + clear. */
+int pm_status(pm_ctx* ctx, uint32_t* out_bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PM_API_H */

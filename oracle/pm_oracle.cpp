@@ -344,7 +344,9 @@ static void trace_path(const Scene& s, const TraceOpts& o, int64_t p, V3 power,
     Ray ray;
     ray.o = vadd(point, vscale(lnorm, 0.0001f));
     float prob, dt;
+    int tries = 0;
     do {
+        if (++tries > (1 << 16)) { if (draws_out) *draws_out = (int)st.n; return; }   // light without a usable normal
         ray.d.x = -1.f + st.next() * 2.f;
         ray.d.y = -1.f + st.next() * 2.f;
         ray.d.z = -1.f + st.next() * 2.f;

@@ -1,0 +1,294 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and the
+reference-generated golden files.
+
+Tolerances: photon positions / directions / powers, grid arrays, kNN id sets:
+bit-exact.  Radiance: 1e-4 relative (the estimate and the tone map use CUDA's
+expf / powf, the oracle glibc's).  8-bit pixels: at most 1 level apart.
+"""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from photonmap import scenes  # noqa: E402
+
+RTOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import photonmap
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return photonmap.Context(0)
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+# ------------------------------------------------------------------- scan
+@pytest.mark.parametrize("n", [0, 1, 4095, 4096, 4097, 100_003, 1_000_000])
+def test_scan_matches_sequential_sum(ctx, n):
+    rng = np.random.default_rng(n)
+    a = rng.integers(0, 1000, n).astype(np.int32)
+    x = torch.from_numpy(a).cuda()
+    inc = _np(ctx.scan_u32(x, True)).astype(np.uint32)
+    exc = _np(ctx.scan_u32(x, False)).astype(np.uint32)
+    ref = np.cumsum(a.astype(np.uint64)).astype(np.uint32)
+    assert np.array_equal(inc, ref)
+    if n:
+        assert exc[0] == 0 and np.array_equal(exc[1:], ref[:-1])
+
+
+def test_scan_known_answer_of_reference(ctx):
+    # CudaPhotonMapping/DynamicArrayTest.cu:165-172 input, checked against a sequential sum
+    n = 1_000_000
+    i = np.arange(n)
+    a = np.where(i % 7 != 0, (i % 3 + 1) % 2, i % 2).astype(np.int32)
+    a[0] = 512 * 44
+    inc = _np(ctx.scan_u32(torch.from_numpy(a).cuda(), True)).astype(np.uint64)
+    assert np.array_equal(inc, np.cumsum(a.astype(np.uint64)))
+
+
+# ----------------------------------------------------------------- tracer
+@pytest.fixture(scope="module")
+def cornell(orc, ctx):
+    sc, cam, w = scenes.workload("cornell_small")
+    ctx.set_scene(sc)
+    s = orc.scene(sc)
+    return sc, cam, w, s
+
+
+def test_scene_aabb_and_tracer_matches_oracle(ctx, cornell):
+    sc, cam, w, s = cornell
+    assert np.array_equal(ctx.scene_aabb(), s.aabb())
+    n = w["photons"]
+    paths = ctx.trace_photons(w["seed"], w["max_bounces"], n)
+    tr = s.trace_photons(w["seed"], w["max_bounces"], n)
+    assert paths >= tr["paths"]
+    ph = ctx.photons(0, sorted_=False)
+    assert ph["count"] == n
+    assert np.array_equal(_np(ph["list_pos"]), tr["g_pos"])
+    assert np.array_equal(_np(ph["list_dir"]), tr["g_dir"])
+    assert np.array_equal(_np(ph["list_power"]), tr["g_pow"])
+
+
+def test_trace_with_caustic_map(ctx, cornell):
+    sc, cam, w, s = cornell
+    paths = ctx.trace_photons(3, 8, 20_000, 2_000)
+    tr = s.trace_photons(3, 8, 20_000, 2_000)
+    g = ctx.photons(0, sorted_=False)
+    c = ctx.photons(1, sorted_=False)
+    assert np.array_equal(_np(g["list_pos"]), tr["g_pos"])
+    assert np.array_equal(_np(c["list_pos"]), tr["c_pos"])
+    assert np.array_equal(_np(c["list_dir"]), tr["c_dir"])
+    assert np.array_equal(_np(c["list_power"]), tr["c_pow"])
+
+
+def test_trace_paths_heightfield_subset(ctx, orc):
+    # the 130k-triangle scene: the BVH must return the reference's closest hits
+    sc = scenes.cornell(sphere_level=3, heightfield_n=256, seed=0)
+    ctx.set_scene(sc)
+    s = orc.scene(sc)
+    p0, p1, B = 5000, 6500, 10
+    out = ctx.trace_paths(0, B, 10_000_000, p0, p1)
+    ref = s.trace_paths(0, B, 10_000_000, p0, p1)
+    assert np.array_equal(_np(out["counts"]), ref["counts"])
+    assert np.array_equal(_np(out["g_pos"]), ref["g_pos"])
+    assert np.array_equal(_np(out["g_dir"]), ref["g_dir"])
+    assert np.array_equal(_np(out["c_pos"]), ref["c_pos"])
+
+
+def test_heightfield_render_matches_oracle(ctx, orc):
+    # eye rays through the BVH of the 130k-triangle scene, small photon map
+    sc = scenes.cornell(sphere_level=3, heightfield_n=256, seed=0)
+    ctx.set_scene(sc)
+    s = orc.scene(sc)
+    ctx.trace_photons(0, 10, 30_000)
+    ctx.build_grid(0)
+    import photonmap
+    cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, 96, 54)
+    rgb, rad = ctx.render(cam, 64, 0.1, 4)
+    tr = s.trace_photons(0, 10, 30_000)
+    g = orc.grid_build(tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    out = s.render(cam.as_vector(), 96, 54, g, 64, 0.1, 4)
+    np.testing.assert_allclose(_np(rad), out["radiance"], rtol=RTOL, atol=1e-7)
+
+
+# ------------------------------------------------------------------- grid
+def _oracle_grid(orc, pos, pw, dr, aabb, desired=1000):
+    return orc.grid_build(pos, pw, dr, aabb, desired=desired)
+
+
+def _check_grid(ctx, g, map_id=0):
+    ph = ctx.photons(map_id)
+    assert tuple(ph["dims"]) == tuple(g.dims) and np.float32(ph["cell"]) == np.float32(g.cell)
+    assert np.array_equal(_np(ph["cell_sizes"]).astype(np.uint32), g.sizes)
+    assert np.array_equal(_np(ph["cell_starts"]).astype(np.uint32), g.starts)
+    sp = _np(ph["sorted_pos"])
+    assert np.array_equal(sp[:, :3], g.spos)
+    assert np.array_equal(sp[:, 3].view(np.uint32), g.sid)
+    assert np.array_equal(_np(ph["sorted_dir"]), g.sdir)
+    assert np.array_equal(_np(ph["sorted_power"]), g.spow)
+    return ph
+
+
+def test_grid_build_matches_oracle(ctx, orc, cornell):
+    sc, cam, w, s = cornell
+    ctx.set_scene(sc)
+    tr = s.trace_photons(w["seed"], w["max_bounces"], w["photons"])
+    ctx.set_photons(0, tr["g_pos"], tr["g_pow"], tr["g_dir"])
+    ctx.build_grid(0)
+    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    _check_grid(ctx, g)
+
+
+def test_grid_regrid_path_and_multi_pass_radix(ctx, orc):
+    # clustered photons force the re-grid (max cell > 5x desired) and > 256 cells (2 radix passes)
+    rng = np.random.default_rng(5)
+    n = 300_000
+    pos = np.concatenate([rng.normal(0.3, 0.02, (n // 2, 3)), rng.uniform(-1, 1, (n - n // 2, 3))]).astype(np.float32)
+    pos = np.clip(pos, -1, 1)
+    dr = rng.normal(size=(n, 3)).astype(np.float32)
+    pw = np.full((n, 3), 1e-5, np.float32)
+    aabb = np.array([-1, -1, -1, 1, 1, 1], np.float32)
+    ctx.set_photons(0, pos, pw, dr)
+    ctx.build_grid(0, desired=100, aabb=aabb)
+    g = _oracle_grid(orc, pos, pw, dr, aabb, desired=100)
+    assert g.sizes.size > 256 * 256   # three 8-bit passes
+    _check_grid(ctx, g)
+
+
+def test_grid_fixture100(ctx, orc, golden_dir):
+    f = np.load(os.path.join(golden_dir, "fixture100.npz"))
+    ctx.set_photons(0, f["pos"], f["power"], f["dir"])
+    ctx.build_grid(0, desired=int(f["desired"]), aabb=f["aabb"])
+    ph = ctx.photons(0)
+    assert tuple(ph["dims"]) == tuple(f["dims"])
+    assert np.array_equal(_np(ph["cell_starts"]).astype(np.uint32), f["starts"])
+    assert np.array_equal(_np(ph["cell_sizes"]).astype(np.uint32), f["sizes"])
+    # the reference's own find_nearests / get_color on this grid (golden)
+    k, r = int(f["k"]), float(f["r"])
+    rad, ids, cnt = ctx.gather(torch.from_numpy(f["q"]), torch.from_numpy(f["qn"]), k, r, want_ids=True)
+    assert np.array_equal(_np(cnt), f["ref_cnt"])
+    ids = _np(ids).astype(np.uint32)
+    for a, b, c in zip(ids, f["ref_ids"], f["ref_cnt"]):
+        assert set(a[:c]) == set(b[:c])
+    np.testing.assert_allclose(_np(rad), f["ref_rad"], rtol=RTOL, atol=1e-9)
+
+
+# ----------------------------------------------------------------- gather
+def test_gather_matches_oracle(ctx, orc, cornell):
+    sc, cam, w, s = cornell
+    ctx.set_scene(sc)
+    tr = s.trace_photons(w["seed"], w["max_bounces"], w["photons"])
+    ctx.set_photons(0, tr["g_pos"], tr["g_pow"], tr["g_dir"])
+    ctx.build_grid(0)
+    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    rng = np.random.default_rng(11)
+    q = (tr["g_pos"][rng.integers(0, len(tr["g_pos"]), 4000)] + rng.normal(scale=0.02, size=(4000, 3))).astype(np.float32)
+    qn = rng.normal(size=(4000, 3)).astype(np.float32)
+    qn /= np.linalg.norm(qn, axis=1, keepdims=True)
+    for k, r in [(100, 0.1), (1, 0.05), (16, 0.3), (256, 0.2)]:
+        ids_o, cnt_o, rk_o, rad_o = orc.gather(g, q, qn, r, k, heap_mode=False)
+        rad, ids, cnt = ctx.gather(torch.from_numpy(q), torch.from_numpy(qn), k, r, want_ids=True)
+        assert np.array_equal(_np(cnt), cnt_o)
+        assert np.array_equal(_np(ids).astype(np.uint32), ids_o)
+        np.testing.assert_allclose(_np(rad), rad_o, rtol=RTOL, atol=1e-8)
+
+
+# ----------------------------------------------------------------- render
+def test_render_matches_reference_golden(ctx, orc, golden_dir):
+    f = np.load(os.path.join(golden_dir, "cornell_ref.npz"))
+    sc, _, _ = scenes.workload("cornell_small")
+    ctx.set_scene(sc)
+    s = orc.scene(sc)
+    tr = s.trace_photons(int(f["seed"]), int(f["max_bounces"]), int(f["photons"]))
+    ctx.set_photons(0, tr["g_pos"], tr["g_pow"], tr["g_dir"])
+    ctx.build_grid(0)
+    import photonmap
+    W, H = int(f["render_w"]), int(f["render_h"])
+    cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, W, H)
+    assert np.array_equal(cam.as_vector(), f["cam_vecs"][0])
+    rgb, rad = ctx.render(cam, int(f["render_k"]), float(f["render_r"]), int(f["render_depth"]))
+    rgb = _np(rgb).reshape(-1, 3).astype(np.int32)
+    ref = f["ref_rgb8"].astype(np.int32)
+    assert np.abs(rgb - ref).max() <= 1
+    assert (rgb != ref).mean() < 0.01
+    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    out = s.render(orc.camera(scenes.default_camera(W, H)), W, H, g, int(f["render_k"]), float(f["render_r"]),
+                   int(f["render_depth"]), heap_mode=False)
+    np.testing.assert_allclose(_np(rad), out["radiance"], rtol=RTOL, atol=1e-7)
+
+
+def test_render_full_small_workload_matches_oracle(ctx, orc, cornell):
+    sc, _, w, s = cornell
+    ctx.set_scene(sc)
+    paths = ctx.trace_photons(w["seed"], w["max_bounces"], w["photons"])
+    ctx.build_grid(0)
+    import photonmap
+    cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, w["width"], w["height"])
+    rgb, rad = ctx.render(cam, w["k"], w["radius"], w["max_depth"])
+    tr = s.trace_photons(w["seed"], w["max_bounces"], w["photons"])
+    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    out = s.render(cam.as_vector(), w["width"], w["height"], g, w["k"], w["radius"], w["max_depth"])
+    np.testing.assert_allclose(_np(rad), out["radiance"], rtol=RTOL, atol=1e-7)
+    d = np.abs(_np(rgb).reshape(-1, 3).astype(np.int32) - out["rgb8"].astype(np.int32))
+    assert d.max() <= 1
+
+
+def test_render_with_caustic_map(ctx, orc, cornell):
+    sc, _, w, s = cornell
+    ctx.set_scene(sc)
+    ctx.trace_photons(1, 8, 40_000, 4_000)
+    ctx.build_grid(0)
+    ctx.build_grid(1)
+    import photonmap
+    cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, 64, 48)
+    rgb, rad = ctx.render(cam, 50, 0.1, 4, k_caustic=20, r_caustic=0.2, faithful_caustic=True)
+    tr = s.trace_photons(1, 8, 40_000, 4_000)
+    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+    c = _oracle_grid(orc, tr["c_pos"], tr["c_pow"], tr["c_dir"], s.aabb())
+    out = s.render(cam.as_vector(), 64, 48, g, 50, 0.1, 4, c=c, k_c=20, r_c=0.2, faithful_caustic=True)
+    np.testing.assert_allclose(_np(rad), out["radiance"], rtol=RTOL, atol=1e-7)
+
+
+# ------------------------------------------------------- full-size checks
+def test_full_size_photon_pass_properties(ctx):
+    """cornell_hf_1080p photon pass (10M photons): size-independent properties."""
+    sc, cam, w = scenes.workload("cornell_hf_1080p")
+    ctx.set_scene(sc)
+    n = w["photons"]
+    ctx.trace_photons(w["seed"], w["max_bounces"], n)
+    ctx.build_grid(0)
+    ph = ctx.photons(0)
+    aabb = ctx.scene_aabb()
+    lp = ph["list_pos"]
+    lo = torch.from_numpy(aabb[:3]).cuda() - 1e-4
+    hi = torch.from_numpy(aabb[3:]).cuda() + 1e-4
+    assert bool(((lp >= lo) & (lp <= hi)).all())
+    pw = ph["list_power"]
+    assert bool((pw == pw[0]).all()) and abs(float(pw[0, 0]) - 1.0 / n) < 1e-12
+    sizes = ph["cell_sizes"].long()
+    starts = ph["cell_starts"].long()
+    assert int(sizes.sum()) == n
+    assert bool((starts[1:] == torch.cumsum(sizes, 0)[:-1]).all()) and int(starts[0]) == 0
+    sp = ph["sorted_pos"]
+    ids = sp[:, 3].contiguous().view(torch.int32).long()
+    assert bool((torch.sort(ids).values == torch.arange(n, device=ids.device)).all())   # a permutation
+    # every photon sits in the cell its position hashes to, and cells keep trace order
+    gx, gy, gz = ph["dims"]
+    cell = ph["cell"]
+    mn = torch.from_numpy(aabb[:3]).cuda()
+    c3 = ((sp[:, :3] - mn) / cell).to(torch.int32)
+    c3 = torch.minimum(torch.maximum(c3, torch.zeros_like(c3)), torch.tensor([gx - 1, gy - 1, gz - 1], device=c3.device, dtype=torch.int32))
+    cid = (c3[:, 0] + c3[:, 1] * gx + c3[:, 2] * gx * gy).long()
+    slot_cell = torch.repeat_interleave(torch.arange(sizes.numel(), device=sizes.device), sizes)
+    assert bool((cid == slot_cell).all())
+    same = slot_cell[1:] == slot_cell[:-1]
+    assert bool((ids[1:][same] > ids[:-1][same]).all())
+    assert np.array_equal(_np(ph["list_pos"])[_np(ids)[:1000]], _np(sp[:1000, :3]))
