@@ -82,6 +82,10 @@ __device__ __forceinline__ bool model_gate(const float* c, V3 o, V3 d) {
     return tmin <= tmax;
 }
 
+__device__ __forceinline__ int hit_model_raw(const DevScene& S, int tri) {
+    return __float_as_int(__ldg(&S.tri[5 * (size_t)tri + 2].w));
+}
+
 struct Hit {
     float t;
     int tri;
@@ -117,11 +121,17 @@ __device__ __forceinline__ bool tri_test(const float4* T, V3 o, V3 d, float best
 
 __device__ __forceinline__ float safe_inv(float x) { return 1.0f / (x == 0.0f ? 1e-30f : x); }
 
-// closest hit; h.tri = -1 on a miss
-static __device__ __noinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit& h) {
+// One BVH traversal.  Returns the smallest (t, triangle) with t > 0 among the
+// triangles of models >= min_model whose model gate passes; also reports the
+// largest model index with a gated hit at exactly t == 0 (zmodel, -1 if none),
+// its lowest such triangle and that triangle's barycentrics.
+static __device__ __noinline__ bool traverse(const DevScene& S, V3 o, V3 d, int min_model, Hit& h, int& zmodel,
+                                             int& ztri, V3& zuvw) {
     float best_t = __int_as_float(0x7f800000);
     int best_tri = 0x7fffffff;
     V3 best_uvw = v3(0.f, 0.f, 0.f);
+    zmodel = -1;
+    ztri = 0x7fffffff;
     unsigned long long gate_known = 0ull, gate_pass = 0ull;
     const float ix = safe_inv(d.x), iy = safe_inv(d.y), iz = safe_inv(d.z);
     int stack[64];
@@ -142,23 +152,27 @@ static __device__ __noinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit
             if (count > 0) {
                 for (int i = 0; i < count; i++) {
                     int tri = __ldg(S.prim + first + i);
-                    float t; V3 uvw;
                     const float4* T = S.tri + 5 * (size_t)tri;
-                    if (tri_test(T, o, d, best_t, tri, best_tri, t, uvw)) {
-                        int m = __float_as_int(__ldg(&T[2].w));
-                        bool pass;
-                        if (m < 64) {
-                            unsigned long long bit = 1ull << m;
-                            if (!(gate_known & bit)) {
-                                gate_known |= bit;
-                                if (model_gate(S.maabb + 6 * m, o, d)) gate_pass |= bit;
-                            }
-                            pass = (gate_pass & bit) != 0ull;
-                        } else {
-                            pass = model_gate(S.maabb + 6 * m, o, d);
+                    int m = __float_as_int(__ldg(&T[2].w));
+                    if (m < min_model) continue;
+                    float t; V3 uvw;
+                    if (!tri_test(T, o, d, best_t, tri, best_tri, t, uvw)) continue;
+                    const bool zero = t == 0.0f;
+                    if (zero && (m < zmodel || (m == zmodel && tri > ztri))) continue;
+                    bool pass;
+                    if (m < 64) {
+                        unsigned long long bit = 1ull << m;
+                        if (!(gate_known & bit)) {
+                            gate_known |= bit;
+                            if (model_gate(S.maabb + 6 * m, o, d)) gate_pass |= bit;
                         }
-                        if (pass) { best_t = t; best_tri = tri; best_uvw = uvw; }
+                        pass = (gate_pass & bit) != 0ull;
+                    } else {
+                        pass = model_gate(S.maabb + 6 * m, o, d);
                     }
+                    if (!pass) continue;
+                    if (zero) { zmodel = m; ztri = tri; zuvw = uvw; }
+                    else { best_t = t; best_tri = tri; best_uvw = uvw; }
                 }
             } else {
                 // interior: children first and first + 1; nearer child first
@@ -181,6 +195,26 @@ static __device__ __noinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit
     }
     if (best_tri == 0x7fffffff) { h.tri = -1; return false; }
     h.t = best_t; h.tri = best_tri; h.uvw = best_uvw;
+    return true;
+}
+
+// Closest hit with the reference's model-loop semantics (PhotonTracing.cu:187-198,
+// Raytracer.cuh:73-84): a running "intersection" that starts at 0 means "no hit
+// yet", so a model whose nearest hit is at exactly t = 0 is taken only when no
+// later model is hit at all.  Hence: with z the last model hit at t = 0, the
+// answer is the nearest (t, triangle) hit among models after z, else z's hit.
+static __device__ __forceinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit& h) {
+    int zmodel, ztri;
+    V3 zuvw;
+    bool hit = traverse(S, o, d, 0, h, zmodel, ztri, zuvw);
+    if (zmodel < 0) return hit;
+    if (hit && hit_model_raw(S, h.tri) > zmodel) return true;
+    int z2, t2;
+    V3 u2;
+    if (traverse(S, o, d, zmodel + 1, h, z2, t2, u2)) return true;
+    h.t = 0.0f;
+    h.tri = ztri;
+    h.uvw = zuvw;
     return true;
 }
 

@@ -302,4 +302,4 @@ class _DeviceArray:
 
     def __init__(self, ptr, shape, dtype):
         self.__cuda_array_interface__ = {"shape": tuple(int(x) for x in shape), "typestr": self._TYPESTR[str(dtype)],
-                                         "data": (int(ptr), True), "version": 3, "strides": None}
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
