@@ -39,6 +39,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # size overrides (profiling captures run reduced cases of the same workload)
+    ap.add_argument("--photons", type=int, default=0)
+    ap.add_argument("--width", type=int, default=0)
+    ap.add_argument("--height", type=int, default=0)
     return ap.parse_args()
 
 
@@ -165,6 +169,19 @@ def _ref_row(arg):
     return time.perf_counter() - t0
 
 
+def override(w, cs, args):
+    w = dict(w)
+    if args.photons:
+        w["photons"] = args.photons
+    if args.width:
+        w["width"] = args.width
+    if args.height:
+        w["height"] = args.height
+    from photonmap import scenes
+    cs = scenes.CameraSpec(cs.position, cs.direction, cs.up, cs.fov_deg, w["width"], w["height"])
+    return w, cs
+
+
 # ----------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -185,6 +202,7 @@ def run_ours(args):
             dist.barrier()
 
     sc, cs, w = scenes.workload(args.workload)
+    w, cs = override(w, cs, args)
     ctx = photonmap.Context(local)
     ctx.set_scene(sc)
     cam = photonmap.camera_setup(cs.position, cs.direction, cs.up, cs.fov_deg, cs.width, cs.height)
@@ -208,6 +226,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.launch_count()
     ev0.record()
     for i in range(args.steps):
         step(args.warmup + i)
@@ -215,6 +234,7 @@ def run_ours(args):
         stage_sum += np.array([st["trace_ms"], st["grid_ms"], st["eye_ms"], st["gather_ms"], st["resolve_ms"]])
     ev1.record()
     torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
     barrier()
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -264,7 +284,7 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": gather_bytes},
             "e2e": {"value": world * w["photons"] / (e2e_ms * 1e-3) / 1e6, "unit": "Mphotons/s",
                     "ms_per_step": e2e_ms, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3},
-            "gpu_launches": None,
+            "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

@@ -37,7 +37,8 @@ struct MapState {
     float cell = 0.f;
     int64_t cells = 0;
     float aabb[6] = {0, 0, 0, 0, 0, 0};
-    DevBuf starts, sizes, gpos, gdir, gpow;
+    int S = 1;
+    DevBuf starts, sizes, gpos, gdir, gpow, key_counts, key_starts;
     DevBuf cid, keys0, keys1, vals0, vals1, hist, scan_ws, small;
 };
 
@@ -65,6 +66,7 @@ struct pm_ctx {
     DevBuf status, gws;
     cudaEvent_t ev[12] = {};
     float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;      // kernels this context has launched
 };
 
 namespace {
@@ -202,7 +204,8 @@ void pm_destroy(pm_ctx* ctx) {
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
-                        &m.keys0, &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small};
+                        &m.keys0, &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small,
+                        &m.key_counts, &m.key_starts};
         for (DevBuf* b : mb) release(*b);
     }
     for (auto& ev : ctx->ev) if (ev) cudaEventDestroy(ev);
@@ -223,6 +226,12 @@ int pm_status(pm_ctx* ctx, uint32_t* out_bits) {
     CK(cudaMemcpyAsync(out_bits, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    return PM_OK;
+}
+
+int pm_launch_count(pm_ctx* ctx, int64_t* out) {
+    if (!ctx || !out) return PM_ERR_INVALID;
+    *out = ctx->launches;
     return PM_OK;
 }
 
@@ -413,6 +422,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg};
         PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc};
         CK(trace_batch(B, LG, LC, ctx->st));
+        ctx->launches += 4;
         uint32_t tot[2] = {0, 0};
         CK(cudaMemcpyAsync(tot, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
@@ -458,6 +468,7 @@ int pm_trace_paths(pm_ctx* ctx, const pm_trace_opts* o, int64_t p0, int64_t p1, 
     PhotonList LG{g_pos, g_dir, pw, cap, 0};
     PhotonList LC{c_pos, c_dir, pw + 3 * cap, cap, 0};
     CK(trace_batch(B, LG, LC, ctx->st));
+    ctx->launches += 4;
     if (counts) {
         CK(cudaMemcpy2DAsync(counts, 8, B.cnt_g, 4, 4, (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
         CK(cudaMemcpy2DAsync(counts + 1, 8, B.cnt_c, 4, 4, (size_t)n, cudaMemcpyDeviceToDevice, ctx->st));
@@ -492,9 +503,11 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
 int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb) {
     if (!ctx) return PM_ERR_INVALID;
     if (int rc = valid_map(ctx, map)) return rc;
-    pm_grid_opts d = {1000, 5, 5};
+    pm_grid_opts d = {1000, 5, 5, 0, 0};
     if (!o) o = &d;
     if (o->desired_per_cell < 1 || o->regrid_div < 1 || o->regrid_mult < 1) return fail(ctx, PM_ERR_INVALID, "grid options must be >= 1");
+    if (!(o->sub_div == 0 || o->sub_div == 1 || o->sub_div == 2 || o->sub_div == 4 || o->sub_div == 8))
+        return fail(ctx, PM_ERR_INVALID, "sub_div must be 0, 1, 2, 4 or 8");
     const float* box = aabb ? aabb : ctx->aabb;
     if (!aabb && !ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene and no aabb");
     CK(cudaSetDevice(ctx->device));
@@ -504,12 +517,9 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     int d1[3], d2[3];
     float c1, c2;
     grid_dims(box, n, o->desired_per_cell, d1, &c1);
-    int desired2 = std::max(o->desired_per_cell / o->regrid_div, 1);
-    grid_dims(box, n, desired2, d2, &c2);
+    grid_dims(box, n, std::max(o->desired_per_cell / o->regrid_div, 1), d2, &c2);
     const int64_t cells_max = std::max<int64_t>((int64_t)d1[0] * d1[1] * d1[2], (int64_t)d2[0] * d2[1] * d2[2]);
-    if (cells_max <= 0 || cells_max > ((int64_t)1 << 31)) return fail(ctx, PM_ERR_INVALID, "grid: cell count out of range");
-    size_t hist_elems = 0, scan_ws = 0;
-    grid_scratch_sizes(n, cells_max, &hist_elems, &scan_ws);
+    if (cells_max <= 0 || cells_max > ((int64_t)1 << 26)) return fail(ctx, PM_ERR_INVALID, "grid: cell count out of range");
     ENSURE(m.starts, (size_t)cells_max * 4);
     ENSURE(m.sizes, (size_t)cells_max * 4);
     ENSURE(m.gpos, (size_t)n * 16);
@@ -520,8 +530,6 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     ENSURE(m.keys1, (size_t)n * 4);
     ENSURE(m.vals0, (size_t)n * 4);
     ENSURE(m.vals1, (size_t)n * 4);
-    ENSURE(m.hist, hist_elems * 4);
-    ENSURE(m.scan_ws, scan_ws);
     ENSURE(m.small, 64);
     GridBuffers B;
     B.pos = P<float>(m.pos); B.dir = P<float>(m.dir); B.pow = P<float>(m.pow); B.n = n;
@@ -530,15 +538,38 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     B.cid = P<uint32_t>(m.cid);
     B.keys[0] = P<uint32_t>(m.keys0); B.keys[1] = P<uint32_t>(m.keys1);
     B.vals[0] = P<uint32_t>(m.vals0); B.vals[1] = P<uint32_t>(m.vals1);
-    B.hist = P<uint32_t>(m.hist);
-    B.scan_ws = m.scan_ws.p;
     B.small = P<uint32_t>(m.small);
     B.status = P<unsigned>(ctx->status);
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
-    CK(grid_build(B, box, o->desired_per_cell, o->regrid_mult, o->regrid_div, m.dims, &m.cell, &m.cells, ctx->st));
+    GridPlan plan;
+    CK(grid_count(B, box, o->desired_per_cell, o->regrid_mult, o->regrid_div, &plan, ctx->st));
+    const int S = o->sub_div > 0 ? o->sub_div : grid_auto_subdiv(plan.max_count, o->k_hint > 0 ? o->k_hint : 64);
+    const int64_t keys = plan.cells * S * S * S;
+    if (keys > ((int64_t)1 << 31)) return fail(ctx, PM_ERR_INVALID, "grid: too many sub-cells");
+    size_t hist_elems = 0, scan_ws = 0;
+    grid_scratch_sizes(n, keys, &hist_elems, &scan_ws);
+    ENSURE(m.hist, hist_elems * 4);
+    ENSURE(m.scan_ws, scan_ws);
+    ENSURE(m.key_counts, (size_t)keys * 4);
+    ENSURE(m.key_starts, (size_t)(keys + 1) * 4);
+    B.hist = P<uint32_t>(m.hist);
+    B.scan_ws = m.scan_ws.p;
+    B.key_counts = P<uint32_t>(m.key_counts);
+    B.key_starts = P<uint32_t>(m.key_starts);
+    CK(grid_sort(B, box, plan, S, ctx->st));
+    {
+        int bits = 1;
+        while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)keys) bits++;
+        const int64_t regrid = (plan.cells == (int64_t)d1[0] * d1[1] * d1[2]) ? 0 : 1;
+        ctx->launches += 2 * (1 + regrid) + (S > 1 ? 3 : 1) + 3 * ((bits + 7) / 8) + 1;
+    }
     CK(cudaEventRecord(ctx->ev[3], ctx->st));
     CK(cudaEventSynchronize(ctx->ev[3]));
     if (map == PM_MAP_GLOBAL) ctx->stage_ms[1] = elapsed(ctx->ev[2], ctx->ev[3]);
+    for (int a = 0; a < 3; a++) m.dims[a] = plan.dims[a];
+    m.cell = plan.cell;
+    m.cells = plan.cells;
+    m.S = S;
     std::memcpy(m.aabb, box, 24);
     int rc = check_status(ctx, "grid build");
     if (rc) return rc;
@@ -565,6 +596,8 @@ int pm_get_photons(pm_ctx* ctx, int map, pm_photon_view* out) {
         out->sorted_pos = P<float>(m.gpos);
         out->sorted_dir = P<float>(m.gdir);
         out->sorted_power = P<float>(m.gpow);
+        out->sub_div = m.S;
+        out->key_starts = P<uint32_t>(m.key_starts);
     }
     return PM_OK;
 }
@@ -624,11 +657,11 @@ static GatherGrid grid_of(MapState& m, MapState& est_src) {
     G.gpos = P<float4>(m.gpos);
     G.gdir = P<float>(est_src.gdir);
     G.gpow = P<float>(est_src.gpow);
-    G.starts = P<uint32_t>(m.starts);
-    G.sizes = P<uint32_t>(m.sizes);
+    G.key_starts = P<uint32_t>(m.key_starts);
     G.mn[0] = m.aabb[0]; G.mn[1] = m.aabb[1]; G.mn[2] = m.aabb[2];
     G.gx = m.dims[0]; G.gy = m.dims[1]; G.gz = m.dims[2];
     G.cell = m.cell;
+    G.S = m.S;
     return G;
 }
 
@@ -644,6 +677,7 @@ int pm_gather(pm_ctx* ctx, int map, int64_t n, const float* qpos, const float* q
     Q.n = n; Q.pos3 = qpos; Q.nrm3 = qnrm;
     GatherOut O{out_rad, out_ids, out_cnt, nullptr};
     CK(gather(grid_of(m, m), Q, radius, k, 0, O, P<unsigned>(ctx->status), ctx->st));
+    ctx->launches += 1;
     return check_status(ctx, "gather");
 }
 
@@ -740,6 +774,7 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_
     CK(resolve(S, cd, R, P<float>(ctx->est_g), caustic ? P<float>(ctx->est_c) : nullptr, tone_t, out_rgb8,
                out_radiance, ctx->st));
     CK(cudaEventRecord(ctx->ev[8], ctx->st));
+    ctx->launches += 3 + (caustic ? 1 : 0);
     CK(cudaEventSynchronize(ctx->ev[8]));
     ctx->stage_ms[2] = elapsed(ctx->ev[4], ctx->ev[5]);
     ctx->stage_ms[3] = elapsed(ctx->ev[6], ctx->ev[7]);
@@ -752,6 +787,7 @@ int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int i
     CK(cudaSetDevice(ctx->device));
     ENSURE(ctx->gws, scan_workspace_bytes(n));
     CK(scan_u32(in, out, n, inclusive, nullptr, ctx->gws.p, P<unsigned>(ctx->status), ctx->st));
+    ctx->launches += 1;
     return check_status(ctx, "scan");
 }
 

@@ -9,11 +9,11 @@ struct GatherGrid {
     const float4* gpos;        // sorted photons: xyz + source id bits
     const float* gdir;         // direction / power arrays the estimate reads (3 floats per slot)
     const float* gpow;
-    const uint32_t* starts;
-    const uint32_t* sizes;
+    const uint32_t* key_starts;  // cells * S^3 + 1: photons of sub-cell key k are [key_starts[k], key_starts[k+1])
     float mn[3];               // grid origin (scene AABB min)
     int gx, gy, gz;
     float cell;
+    int S;                     // sub-cells per cell axis
 };
 
 struct GatherQueries {

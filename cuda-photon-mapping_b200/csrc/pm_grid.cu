@@ -3,14 +3,17 @@
 // Reference: CudaPhotonMapping/PhotonGrid.cu:41-218 (analyze_density,
 // count_photons_per_cell, prescan_per_cell_counts, assign_photons_to_cells).
 // The reference scatters with an atomic per-cell offset, so the order inside a
-// cell changes from run to run.  Here the scatter is stable: photons inside a
-// cell keep their trace order, which makes the sorted arrays a pure function of
-// the photon list.  Pipeline (one stream, no host round trip except the
+// cell changes from run to run.  Here the order inside a cell is defined: by
+// sub-cell (each cell split S x S x S, S chosen for the gather) and then by
+// trace order, which makes the sorted arrays a pure function of the photon
+// list; cell_starts / cell_sizes are the reference's exactly.  Pipeline (one stream, no host round trip except the
 // re-grid decision the reference also takes on the host):
 //   k_cell_count   cell id per photon (stored) + per-cell counts (atomics)
 //   k_max          the largest cell count -> host decides on the re-grid
-//   scan_u32       exclusive scan of counts -> cell_starts (decoupled look-back)
-//   LSD radix sort of the cell ids, 8 bits per pass, carrying the photon index:
+//   k_key_count    (sub-cell split S > 1) key = cell * S^3 + sub-cell + counts
+//   scan_u32       exclusive scan of key counts (decoupled look-back) ->
+//                  key_starts; cell_starts / cell_sizes follow exactly
+//   LSD radix sort of the keys, 8 bits per pass, carrying the photon index:
 //     k_radix_upsweep    per-tile digit histogram, digit-major
 //     scan_u32           offsets of every (digit, tile)
 //     k_radix_downsweep  stable in-tile ranks (warp match) + scatter
@@ -54,6 +57,39 @@ __global__ void k_cell_count(const float* __restrict__ pos, int64_t n, GridGeom 
     uint32_t c = cell_of(g, p[0], p[1], p[2]);
     cid[i] = c;
     atomicAdd(counts + c, 1u);
+}
+
+// sub-cell key: cell * S^3 + sub-cell, the sub-cell taken from the fractional
+// part of the same (p - min) / cell quotient that selects the cell
+__device__ __forceinline__ int sub_of(float u, int c, int S) {
+    float f = u - (float)c;
+    int s = (int)(f * (float)S);
+    return min(max(s, 0), S - 1);
+}
+
+__global__ void k_key_count(const float* __restrict__ pos, int64_t n, GridGeom g, int S, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ counts) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* p = pos + 3 * i;
+    float ux = (p[0] - g.mnx) / g.cell, uy = (p[1] - g.mny) / g.cell, uz = (p[2] - g.mnz) / g.cell;
+    int x = min(max((int)ux, 0), g.gx - 1);
+    int y = min(max((int)uy, 0), g.gy - 1);
+    int z = min(max((int)uz, 0), g.gz - 1);
+    uint32_t c = (uint32_t)(x + y * g.gx + z * g.gx * g.gy);
+    uint32_t sk = (uint32_t)(sub_of(ux, x, S) + S * (sub_of(uy, y, S) + S * sub_of(uz, z, S)));
+    uint32_t k = c * (uint32_t)(S * S * S) + sk;
+    key[i] = k;
+    atomicAdd(counts + k, 1u);
+}
+
+__global__ void k_cells_from_keys(const uint32_t* __restrict__ key_starts, int64_t cells, int S3,
+                                  uint32_t* __restrict__ starts, uint32_t* __restrict__ sizes) {
+    int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    uint32_t a = key_starts[c * S3], b = key_starts[(c + 1) * S3];
+    starts[c] = a;
+    sizes[c] = b - a;
 }
 
 __global__ void k_max(const uint32_t* __restrict__ a, int64_t n, uint32_t* out) {
@@ -174,44 +210,74 @@ void grid_dims(const float aabb[6], int64_t n, int desired, int dims[3], float* 
     *cell = c;
 }
 
-void grid_scratch_sizes(int64_t n, int64_t max_cells, size_t* hist_elems, size_t* scan_ws_bytes) {
+void grid_scratch_sizes(int64_t n, int64_t max_keys, size_t* hist_elems, size_t* scan_ws_bytes) {
     int64_t tiles = std::max<int64_t>(1, (n + RADIX_TILE - 1) / RADIX_TILE);
     *hist_elems = (size_t)256 * tiles;
-    *scan_ws_bytes = std::max(scan_workspace_bytes((int64_t)256 * tiles), scan_workspace_bytes(max_cells));
+    *scan_ws_bytes = std::max(scan_workspace_bytes((int64_t)256 * tiles), scan_workspace_bytes(max_keys + 1));
 }
 
-cudaError_t grid_build(GridBuffers& B, const float aabb[6], int desired, int regrid_mult, int regrid_div,
-                       int dims[3], float* cell, int64_t* cells_out, cudaStream_t st) {
+int grid_auto_subdiv(uint32_t max_count, int k_hint) {
+    double per = (double)max_count / (2.0 * std::max(k_hint, 1));
+    int S = 1;
+    while (S < 8 && (double)(2 * S) * (2 * S) <= per) S *= 2;
+    return S;
+}
+
+cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int regrid_mult, int regrid_div,
+                       GridPlan* plan, cudaStream_t st) {
     cudaError_t e;
     const int64_t n = B.n;
-    int64_t cells = 0;
     GridGeom g;
     g.mnx = aabb[0]; g.mny = aabb[1]; g.mnz = aabb[2];
     for (int pass = 0; pass < 2; pass++) {
         int want = pass == 0 ? desired : std::max(desired / regrid_div, 1);
-        grid_dims(aabb, n, want, dims, cell);
-        g.gx = dims[0]; g.gy = dims[1]; g.gz = dims[2]; g.cell = *cell;
-        cells = (int64_t)dims[0] * dims[1] * dims[2];
-        if ((e = cudaMemsetAsync(B.cell_sizes, 0, (size_t)cells * 4, st)) != cudaSuccess) return e;
+        grid_dims(aabb, n, want, plan->dims, &plan->cell);
+        g.gx = plan->dims[0]; g.gy = plan->dims[1]; g.gz = plan->dims[2]; g.cell = plan->cell;
+        plan->cells = (int64_t)g.gx * g.gy * g.gz;
+        if ((e = cudaMemsetAsync(B.cell_sizes, 0, (size_t)plan->cells * 4, st)) != cudaSuccess) return e;
         if (n > 0) {
             k_cell_count<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, g, B.cid, B.cell_sizes);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
-        if (pass == 1) break;
         if ((e = cudaMemsetAsync(B.small, 0, 4, st)) != cudaSuccess) return e;
-        k_max<<<std::min<int64_t>(blocks_for(cells, 256), 1184), 256, 0, st>>>(B.cell_sizes, cells, B.small);
+        k_max<<<std::min<int64_t>(blocks_for(plan->cells, 256), 1184), 256, 0, st>>>(B.cell_sizes, plan->cells, B.small);
         uint32_t mx = 0;
         if ((e = cudaMemcpyAsync(&mx, B.small, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
         if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-        if (!(mx > (uint32_t)(regrid_mult * desired))) break;
+        plan->max_count = mx;
+        if (pass == 0 && !(mx > (uint32_t)(regrid_mult * desired))) break;
     }
-    *cells_out = cells;
-    if ((e = scan_u32(B.cell_sizes, B.cell_starts, cells, 0, nullptr, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+cudaError_t grid_sort(GridBuffers& B, const float aabb[6], const GridPlan& plan, int S, cudaStream_t st) {
+    cudaError_t e;
+    const int64_t n = B.n;
+    const int64_t cells = plan.cells;
+    const int S3 = S * S * S;
+    const int64_t keys = cells * S3;
+    GridGeom g;
+    g.mnx = aabb[0]; g.mny = aabb[1]; g.mnz = aabb[2];
+    g.gx = plan.dims[0]; g.gy = plan.dims[1]; g.gz = plan.dims[2]; g.cell = plan.cell;
+    if (S == 1) {
+        // keys are the cell ids already in B.cid; counts are cell_sizes
+        if ((e = scan_u32(B.cell_sizes, B.key_starts, cells, 0, B.key_starts + cells, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(B.cell_starts, B.key_starts, (size_t)cells * 4, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+    } else {
+        if ((e = cudaMemsetAsync(B.key_counts, 0, (size_t)keys * 4, st)) != cudaSuccess) return e;
+        if (n > 0) {
+            k_key_count<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, g, S, B.cid, B.key_counts);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        if ((e = scan_u32(B.key_counts, B.key_starts, keys, 0, B.key_starts + keys, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+        k_cells_from_keys<<<blocks_for(cells, 256), 256, 0, st>>>(B.key_starts, cells, S3, B.cell_starts, B.cell_sizes);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (n == 0) return cudaSuccess;
 
-    // LSD radix sort of the cell ids (stable), carrying the photon index
+    // LSD radix sort of the keys (stable), carrying the photon index
     int bits = 1;
-    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)cells) bits++;
+    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)keys) bits++;
     const int passes = (bits + 7) / 8;
     const int tiles = (int)((n + RADIX_TILE - 1) / RADIX_TILE);
     const uint32_t* kin = B.cid;

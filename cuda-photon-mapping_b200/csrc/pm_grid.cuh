@@ -21,6 +21,8 @@ struct GridBuffers {
     float4* gpos;         // sorted: xyz + source index bits in w
     float* gdir;          // sorted: 3 floats per photon
     float* gpow;          // sorted: 3 floats per photon
+    uint32_t* key_counts; // cells * S^3 (sub-cell counts)
+    uint32_t* key_starts; // cells * S^3 + 1 (exclusive scan, total last)
     // scratch
     uint32_t* cid;        // n
     uint32_t* keys[2];    // n each
@@ -31,14 +33,32 @@ struct GridBuffers {
     unsigned* status;
 };
 
-// Build the grid of one photon map.  desired: photons per cell (1000 in the
-// reference); the grid is rebuilt at desired / regrid_div when a cell holds more
-// than regrid_mult * desired (5 and 5 in the reference).  Writes dims / cell /
-// cells.  Requires buffers sized for the larger of the two candidate grids.
-cudaError_t grid_build(GridBuffers& B, const float aabb[6], int desired, int regrid_mult, int regrid_div,
-                       int dims[3], float* cell, int64_t* cells, cudaStream_t st);
+struct GridPlan {
+    int dims[3];
+    float cell;
+    int64_t cells;
+    uint32_t max_count;   // photons in the fullest cell of the chosen grid
+};
 
-// scratch sizes for n photons and at most max_cells cells
-void grid_scratch_sizes(int64_t n, int64_t max_cells, size_t* hist_elems, size_t* scan_ws_bytes);
+// Phase 1: per-cell counts of the reference's grid, including its re-grid rule
+// (desired photons per cell, 1000 in the reference; rebuilt at desired /
+// regrid_div when a cell holds more than regrid_mult * desired, 5 and 5).
+// Writes cell ids (B.cid), cell_sizes and the plan.  Synchronises the stream
+// once (the re-grid decision is taken on the host, as in the reference).
+cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int regrid_mult, int regrid_div,
+                       GridPlan* plan, cudaStream_t st);
+
+// Phase 2: order the photons by (cell, sub-cell, trace index), where each cell
+// is split into S^3 sub-cells (S = 1, 2, 4 or 8), and write cell_starts /
+// cell_sizes (exactly the reference's), key_starts (sub-cell ranges) and the
+// sorted arrays.  Buffers: key arrays sized for cells * S^3 (+1).
+cudaError_t grid_sort(GridBuffers& B, const float aabb[6], const GridPlan& plan, int S, cudaStream_t st);
+
+// sub-cell division for a grid whose fullest cell holds max_count photons:
+// about 2k photons per sub-cell slab of a surface crossing the cell
+int grid_auto_subdiv(uint32_t max_count, int k_hint);
+
+// scratch sizes for n photons and at most max_keys sub-cells
+void grid_scratch_sizes(int64_t n, int64_t max_keys, size_t* hist_elems, size_t* scan_ws_bytes);
 
 }  // namespace pm

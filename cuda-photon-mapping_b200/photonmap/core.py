@@ -45,7 +45,8 @@ class _TraceOpts(C.Structure):
 
 
 class _GridOpts(C.Structure):
-    _fields_ = [("desired_per_cell", C.c_int32), ("regrid_mult", C.c_int32), ("regrid_div", C.c_int32)]
+    _fields_ = [("desired_per_cell", C.c_int32), ("regrid_mult", C.c_int32), ("regrid_div", C.c_int32),
+                ("sub_div", C.c_int32), ("k_hint", C.c_int32)]
 
 
 class Camera(C.Structure):
@@ -68,7 +69,8 @@ class _PhotonView(C.Structure):
     _fields_ = [("count", C.c_int64), ("cells", C.c_int64), ("dims", C.c_int32 * 3), ("cell_size", C.c_float),
                 ("aabb", C.c_float * 6), ("cell_starts", C.c_void_p), ("cell_sizes", C.c_void_p),
                 ("sorted_pos", C.c_void_p), ("sorted_dir", C.c_void_p), ("sorted_power", C.c_void_p),
-                ("list_pos", C.c_void_p), ("list_dir", C.c_void_p), ("list_power", C.c_void_p)]
+                ("list_pos", C.c_void_p), ("list_dir", C.c_void_p), ("list_power", C.c_void_p),
+                ("sub_div", C.c_int32), ("key_starts", C.c_void_p)]
 
 
 _LIB = None
@@ -104,6 +106,7 @@ def library():
         "pm_scan_u32": ([vp, vp, vp, i64, C.c_int], C.c_int),
         "pm_stage_times": ([vp, vp], C.c_int),
         "pm_status": ([vp, vp], C.c_int),
+        "pm_launch_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -207,8 +210,9 @@ class Context:
         self._check(self.L.pm_set_photons(self.h, map_id, pos.shape[0], pos.ctypes.data, pw.ctypes.data,
                                           dr.ctypes.data), "pm_set_photons")
 
-    def build_grid(self, map_id=PM_MAP_GLOBAL, desired=1000, regrid_mult=5, regrid_div=5, aabb=None):
-        o = _GridOpts(desired, regrid_mult, regrid_div)
+    def build_grid(self, map_id=PM_MAP_GLOBAL, desired=1000, regrid_mult=5, regrid_div=5, aabb=None, sub_div=0,
+                   k_hint=0):
+        o = _GridOpts(desired, regrid_mult, regrid_div, sub_div, k_hint)
         box = None if aabb is None else np.ascontiguousarray(aabb, np.float32)
         self._check(self.L.pm_build_grid(self.h, map_id, C.byref(o), None if box is None else box.ctypes.data),
                     "pm_build_grid")
@@ -234,7 +238,9 @@ class Context:
                    list_power=dev(v.list_power, n, torch.float32, (n, 3)))
         if sorted_ and v.cell_starts:
             cells = v.cells
+            S = v.sub_div
             out.update(dims=tuple(v.dims), cell=v.cell_size, aabb=np.array(list(v.aabb), np.float32), cells=cells,
+                       sub_div=S, key_starts=dev(v.key_starts, cells * S ** 3 + 1, torch.int32, (cells * S ** 3 + 1,)),
                        cell_starts=dev(v.cell_starts, cells, torch.int32, (cells,)),
                        cell_sizes=dev(v.cell_sizes, cells, torch.int32, (cells,)),
                        sorted_pos=dev(v.sorted_pos, n, torch.float32, (n, 4)),
@@ -286,6 +292,11 @@ class Context:
         self._check(self.L.pm_stage_times(self.h, out.ctypes.data), "pm_stage_times")
         return dict(trace_ms=float(out[0]), grid_ms=float(out[1]), eye_ms=float(out[2]), gather_ms=float(out[3]),
                     resolve_ms=float(out[4]))
+
+    def launch_count(self):
+        out = C.c_int64()
+        self._check(self.L.pm_launch_count(self.h, C.byref(out)), "pm_launch_count")
+        return out.value
 
     def status(self):
         out = np.zeros(1, np.uint32)

@@ -74,6 +74,10 @@ typedef struct {
     int32_t desired_per_cell;   /* 1000 in PhotonGrid::build */
     int32_t regrid_mult;        /* re-grid when a cell holds > regrid_mult * desired (5) */
     int32_t regrid_div;         /* ... at desired / regrid_div photons per cell (5) */
+    int32_t sub_div;            /* photons inside a cell are ordered by sub-cell, each cell split
+                                   sub_div^3 ways (1, 2, 4 or 8; 0 = chosen from the fullest cell);
+                                   the gather walks sub-cells.  The cells are the reference's. */
+    int32_t k_hint;             /* expected kNN k for the automatic sub_div (0 = 64) */
 } pm_grid_opts;
 
 /* The reference Camera's fields (Camera.cuh:11-33); pm_camera_setup fills them
@@ -109,6 +113,10 @@ typedef struct {
     const float* list_pos;          /* device, traced order (before the grid build), 3 floats */
     const float* list_dir;
     const float* list_power;
+    int32_t sub_div;                /* sub-cells per cell axis of the sorted order */
+    const uint32_t* key_starts;     /* device, cells * sub_div^3 + 1 entries: photons of sub-cell
+                                       key (cell * sub_div^3 + sx + sub_div * (sy + sub_div * sz))
+                                       are sorted slots [key_starts[key], key_starts[key + 1]) */
 } pm_photon_view;
 
 /* ------------------------------------------------------------- lifetime -- */
@@ -181,6 +189,9 @@ int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int i
  * pm_render calls in milliseconds (CUDA events on the context stream):
  * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather, [4] resolve. */
 int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
+
+/* Number of kernels this context has launched so far. */
+int pm_launch_count(pm_ctx* ctx, int64_t* out);
 
 /* Device status word (bits: 1 timeout, 2 overflow, 4 stack, 8 bad input); read + clear. */
 int pm_status(pm_ctx* ctx, uint32_t* out_bits);

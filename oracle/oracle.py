@@ -69,8 +69,8 @@ class Oracle:
         L.orc_trace_paths.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_int64, C.c_int64,
                                       C.c_int64] + [C.c_void_p] * 10
         L.orc_grid_build.restype = C.c_int64
-        L.orc_grid_build.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
-                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+        L.orc_grid_build.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
         L.orc_gather.argtypes = [C.c_void_p, C.c_void_p, C.c_float] + [C.c_void_p] * 6 + \
             [C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int] + [C.c_void_p] * 4
         L.orc_camera.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_void_p]
@@ -112,7 +112,7 @@ class Oracle:
                           _ptr(_c(cam.up, np.float32)), float(cam.fov_deg), cam.width, cam.height, _ptr(out))
         return out
 
-    def grid_build(self, pos, power, direction, aabb, desired=1000):
+    def grid_build(self, pos, power, direction, aabb, desired=1000, sub_div=1):
         pos = _c(pos, np.float32).reshape(-1, 3)
         n = pos.shape[0]
         aabb = _c(aabb, np.float32)
@@ -123,15 +123,18 @@ class Oracle:
             starts = np.empty(cap, np.uint32)
             sizes = np.empty(cap, np.uint32)
             order = np.empty(max(n, 1), np.uint32)
-            cells = self.L.orc_grid_build(_ptr(pos), n, _ptr(aabb), desired, _ptr(dims), _ptr(cell),
-                                          _ptr(starts), _ptr(sizes), _ptr(order), cap)
+            sub = np.zeros(1, np.int32)
+            cells = self.L.orc_grid_build(_ptr(pos), n, _ptr(aabb), desired, int(sub_div), _ptr(sub), _ptr(dims),
+                                          _ptr(cell), _ptr(starts), _ptr(sizes), _ptr(order), cap)
             if cells >= 0:
                 break
             cap = -cells
         order = order[:n]
-        return GridResult(aabb, dims.copy(), float(cell[0]), starts[:cells].copy(), sizes[:cells].copy(), order,
-                          pos[order], _c(direction, np.float32).reshape(-1, 3)[order],
-                          _c(power, np.float32).reshape(-1, 3)[order], order.copy())
+        g = GridResult(aabb, dims.copy(), float(cell[0]), starts[:cells].copy(), sizes[:cells].copy(), order,
+                       pos[order], _c(direction, np.float32).reshape(-1, 3)[order],
+                       _c(power, np.float32).reshape(-1, 3)[order], order.copy())
+        g.sub_div = int(sub[0])
+        return g
 
     def gather(self, g: GridResult, qpos, qnrm, radius, k, heap_mode=False):
         qpos = _c(qpos, np.float32).reshape(-1, 3)

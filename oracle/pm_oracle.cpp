@@ -469,8 +469,26 @@ static inline uint32_t cell_index(int x, int y, int z, int gx, int gy) {
     return (uint32_t)(x + y * gx + z * gx * gy);
 }
 
-// count -> (re-grid if a cell holds more than 5x desired) -> exclusive scan -> stable scatter
-static void grid_build(Grid& g, const float* pos, int n, const float* aabb, int desired) {
+// sub-cell of a point inside its cell: fractional part of the cell quotient
+static inline int sub_coord(float p, float mn, float cell, int c, int S) {
+    float u = (p - mn) / cell;
+    float f = u - (float)c;
+    int s = (int)(f * (float)S);
+    return std::min(std::max(s, 0), S - 1);
+}
+
+// Auto sub-division: about 2k photons per sub-cell slab of a surface crossing the fullest cell
+static int auto_subdiv(uint32_t max_count, int k_hint) {
+    double per = (double)max_count / (2.0 * std::max(k_hint, 1));
+    int S = 1;
+    while (S < 8 && (double)(2 * S) * (2 * S) <= per) S *= 2;
+    return S;
+}
+
+// count -> (re-grid if a cell holds more than 5x desired) -> exclusive scan -> stable scatter.
+// Inside a cell photons are ordered by sub-cell (S^3 per cell), then by index.
+static void grid_build(Grid& g, const float* pos, int n, const float* aabb, int desired, int S_req = 1,
+                       int* S_out = nullptr, uint32_t* max_out = nullptr) {
     std::memcpy(g.aabb, aabb, sizeof(g.aabb));
     std::vector<uint32_t> cid(n);
     for (int pass = 0; pass < 2; pass++) {
@@ -486,15 +504,34 @@ static void grid_build(Grid& g, const float* pos, int n, const float* aabb, int 
         }
         uint32_t mx = 0;
         for (auto c : g.sizes) mx = std::max(mx, c);
+        if (max_out) *max_out = mx;
         if (pass == 0 && !(mx > (uint32_t)(5 * desired))) break;
     }
+    const int S = S_req > 0 ? S_req : auto_subdiv(max_out ? *max_out : 0, 64);
+    if (S_out) *S_out = S;
     size_t cells = g.sizes.size();
     g.starts.assign(cells, 0);
     uint32_t acc = 0;
     for (size_t c = 0; c < cells; c++) { g.starts[c] = acc; acc += g.sizes[c]; }
+    // stable counting sort by key = cell * S^3 + sub-cell
+    const size_t S3 = (size_t)S * S * S;
+    std::vector<uint32_t> key(n);
+    std::vector<uint32_t> kcount(cells * S3 + 1, 0);
+    for (int i = 0; i < n; i++) {
+        const float* p = pos + 3 * (size_t)i;
+        int x, y, z;
+        cell_coords(aabb, ld3(p), g.gx, g.gy, g.gz, g.cell, x, y, z);
+        uint32_t sk = (uint32_t)(sub_coord(p[0], aabb[0], g.cell, x, S) +
+                                 S * (sub_coord(p[1], aabb[1], g.cell, y, S) + S * sub_coord(p[2], aabb[2], g.cell, z, S)));
+        key[i] = cid[i] * (uint32_t)S3 + sk;
+        kcount[key[i]]++;
+    }
+    std::vector<uint32_t> kstart(cells * S3 + 1, 0);
+    uint32_t a2 = 0;
+    for (size_t k = 0; k < cells * S3; k++) { kstart[k] = a2; a2 += kcount[k]; }
+    kstart[cells * S3] = a2;
     g.order.assign(n, 0);
-    std::vector<uint32_t> fill(cells, 0);
-    for (int i = 0; i < n; i++) g.order[g.starts[cid[i]] + fill[cid[i]]++] = (uint32_t)i;
+    for (int i = 0; i < n; i++) g.order[kstart[key[i]]++] = (uint32_t)i;
 }
 
 // --------------------------------------------------------------- kNN -------
@@ -964,14 +1001,17 @@ void orc_trace_paths(void* h, uint64_t seed, uint32_t tag, int max_bounces, int6
     *out_ng = ng; *out_nc = nc;
 }
 
-// Grid build.  out_dims = (gx, gy, gz); out_cell; starts/sizes must hold
+// Grid build.  sub_div: sub-cells per cell axis of the in-cell order (1, 2, 4, 8;
+// 0 = automatic as the product chooses it); out_sub receives it.
+// out_dims = (gx, gy, gz); out_cell; starts/sizes must hold
 // max_cells entries; order holds n.  Returns the cell count, or -(cells) if
 // max_cells was too small (nothing written but dims).
-int64_t orc_grid_build(const float* pos, int n, const float* aabb, int desired,
+int64_t orc_grid_build(const float* pos, int n, const float* aabb, int desired, int sub_div, int* out_sub,
                        int* out_dims, float* out_cell, uint32_t* starts, uint32_t* sizes,
                        uint32_t* order, int64_t max_cells) {
     Grid g;
-    grid_build(g, pos, n, aabb, desired);
+    uint32_t mx = 0;
+    grid_build(g, pos, n, aabb, desired, sub_div, out_sub, &mx);
     out_dims[0] = g.gx; out_dims[1] = g.gy; out_dims[2] = g.gz;
     *out_cell = g.cell;
     int64_t cells = (int64_t)g.sizes.size();

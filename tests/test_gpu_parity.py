@@ -120,12 +120,18 @@ def test_heightfield_render_matches_oracle(ctx, orc):
 
 
 # ------------------------------------------------------------------- grid
-def _oracle_grid(orc, pos, pw, dr, aabb, desired=1000):
-    return orc.grid_build(pos, pw, dr, aabb, desired=desired)
+def _oracle_grid(orc, pos, pw, dr, aabb, desired=1000, sub_div=1):
+    return orc.grid_build(pos, pw, dr, aabb, desired=desired, sub_div=sub_div)
 
 
-def _check_grid(ctx, g, map_id=0):
+def _check_grid(ctx, orc, pos, pw, dr, aabb, desired=1000, map_id=0, auto=False):
     ph = ctx.photons(map_id)
+    g = _oracle_grid(orc, pos, pw, dr, aabb, desired, sub_div=ph["sub_div"])
+    if auto:   # the automatic sub-division is the same rule on both sides
+        assert _oracle_grid(orc, pos, pw, dr, aabb, desired, sub_div=0).sub_div == ph["sub_div"]
+    ks = _np(ph["key_starts"]).astype(np.int64)
+    S3 = ph["sub_div"] ** 3
+    assert ks[-1] == len(pos) and np.array_equal(ks[:-1:S3][:len(g.starts)], g.starts.astype(np.int64))
     assert tuple(ph["dims"]) == tuple(g.dims) and np.float32(ph["cell"]) == np.float32(g.cell)
     assert np.array_equal(_np(ph["cell_sizes"]).astype(np.uint32), g.sizes)
     assert np.array_equal(_np(ph["cell_starts"]).astype(np.uint32), g.starts)
@@ -134,7 +140,7 @@ def _check_grid(ctx, g, map_id=0):
     assert np.array_equal(sp[:, 3].view(np.uint32), g.sid)
     assert np.array_equal(_np(ph["sorted_dir"]), g.sdir)
     assert np.array_equal(_np(ph["sorted_power"]), g.spow)
-    return ph
+    return g
 
 
 def test_grid_build_matches_oracle(ctx, orc, cornell):
@@ -142,9 +148,9 @@ def test_grid_build_matches_oracle(ctx, orc, cornell):
     ctx.set_scene(sc)
     tr = s.trace_photons(w["seed"], w["max_bounces"], w["photons"])
     ctx.set_photons(0, tr["g_pos"], tr["g_pow"], tr["g_dir"])
-    ctx.build_grid(0)
-    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
-    _check_grid(ctx, g)
+    for sub in (0, 1, 2, 8):
+        ctx.build_grid(0, sub_div=sub)
+        _check_grid(ctx, orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb(), auto=sub == 0)
 
 
 def test_grid_regrid_path_and_multi_pass_radix(ctx, orc):
@@ -157,10 +163,9 @@ def test_grid_regrid_path_and_multi_pass_radix(ctx, orc):
     pw = np.full((n, 3), 1e-5, np.float32)
     aabb = np.array([-1, -1, -1, 1, 1, 1], np.float32)
     ctx.set_photons(0, pos, pw, dr)
-    ctx.build_grid(0, desired=10, aabb=aabb)
-    g = _oracle_grid(orc, pos, pw, dr, aabb, desired=10)
+    ctx.build_grid(0, desired=10, aabb=aabb, sub_div=1)
+    g = _check_grid(ctx, orc, pos, pw, dr, aabb, desired=10)
     assert g.sizes.size > 256 * 256   # re-gridded; cell ids need three 8-bit passes
-    _check_grid(ctx, g)
 
 
 def test_grid_fixture100(ctx, orc, golden_dir):
@@ -193,12 +198,14 @@ def test_gather_matches_oracle(ctx, orc, cornell):
     q = (tr["g_pos"][rng.integers(0, len(tr["g_pos"]), 4000)] + rng.normal(scale=0.02, size=(4000, 3))).astype(np.float32)
     qn = rng.normal(size=(4000, 3)).astype(np.float32)
     qn /= np.linalg.norm(qn, axis=1, keepdims=True)
-    for k, r in [(100, 0.1), (1, 0.05), (16, 0.3), (256, 0.2)]:
-        ids_o, cnt_o, rk_o, rad_o = orc.gather(g, q, qn, r, k, heap_mode=False)
-        rad, ids, cnt = ctx.gather(torch.from_numpy(q), torch.from_numpy(qn), k, r, want_ids=True)
-        assert np.array_equal(_np(cnt), cnt_o)
-        assert np.array_equal(_np(ids).astype(np.uint32), ids_o)
-        np.testing.assert_allclose(_np(rad), rad_o, rtol=RTOL, atol=1e-8)
+    for sub in (1, 4, 8):
+        ctx.build_grid(0, sub_div=sub)
+        for k, r in [(100, 0.1), (1, 0.05), (16, 0.3), (256, 0.2)]:
+            ids_o, cnt_o, rk_o, rad_o = orc.gather(g, q, qn, r, k, heap_mode=False)
+            rad, ids, cnt = ctx.gather(torch.from_numpy(q), torch.from_numpy(qn), k, r, want_ids=True)
+            assert np.array_equal(_np(cnt), cnt_o)
+            assert np.array_equal(_np(ids).astype(np.uint32), ids_o)
+            np.testing.assert_allclose(_np(rad), rad_o, rtol=RTOL, atol=1e-8)
 
 
 # ----------------------------------------------------------------- render
@@ -280,16 +287,23 @@ def test_full_size_photon_pass_properties(ctx):
     sp = ph["sorted_pos"]
     ids = sp[:, 3].contiguous().view(torch.int32).long()
     assert bool((torch.sort(ids).values == torch.arange(n, device=ids.device)).all())   # a permutation
-    # every photon sits in the cell its position hashes to (IEEE float32 division on the
-    # host, as CudaPhotonMapping/PhotonGrid.cu:10-38 computes it), and cells keep trace order
+    # every photon sits in the cell / sub-cell its position hashes to (IEEE float32
+    # division on the host, as CudaPhotonMapping/PhotonGrid.cu:10-38 computes it), and
+    # photons of one sub-cell keep trace order
     gx, gy, gz = ph["dims"]
     cell = np.float32(ph["cell"])
+    S = ph["sub_div"]
     spn = _np(sp[:, :3])
-    c3 = ((spn - aabb[:3]) / cell).astype(np.int32)
-    c3 = np.minimum(np.maximum(c3, 0), np.array([gx - 1, gy - 1, gz - 1], np.int32))
-    cid = torch.from_numpy((c3[:, 0] + c3[:, 1] * gx + c3[:, 2] * gx * gy).astype(np.int64)).cuda()
-    slot_cell = torch.repeat_interleave(torch.arange(sizes.numel(), device=sizes.device), sizes)
-    assert bool((cid == slot_cell).all())
-    same = slot_cell[1:] == slot_cell[:-1]
+    u = (spn - aabb[:3]) / cell
+    c3 = np.minimum(np.maximum(u.astype(np.int32), 0), np.array([gx - 1, gy - 1, gz - 1], np.int32))
+    s3 = np.minimum(np.maximum(((u - c3.astype(np.float32)) * np.float32(S)).astype(np.int32), 0), S - 1)
+    key = ((c3[:, 0] + c3[:, 1] * gx + c3[:, 2] * gx * gy).astype(np.int64) * S ** 3 +
+           s3[:, 0] + S * (s3[:, 1] + S * s3[:, 2]))
+    ks = ph["key_starts"].long()
+    slot_key = torch.repeat_interleave(torch.arange(ks.numel() - 1, device=ks.device), ks[1:] - ks[:-1])
+    assert bool((torch.from_numpy(key).cuda() == slot_key).all())
+    slot_cell = torch.div(slot_key, S ** 3, rounding_mode="floor")
+    assert bool((torch.repeat_interleave(torch.arange(sizes.numel(), device=sizes.device), sizes) == slot_cell).all())
+    same = slot_key[1:] == slot_key[:-1]
     assert bool((ids[1:][same] > ids[:-1][same]).all())
     assert np.array_equal(_np(ph["list_pos"])[_np(ids)[:1000]], _np(sp[:1000, :3]))
