@@ -258,8 +258,10 @@ def test_render_with_caustic_map(ctx, orc, cornell):
     cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, 64, 48)
     rgb, rad = ctx.render(cam, 50, 0.1, 4, k_caustic=20, r_caustic=0.2, faithful_caustic=True)
     tr = s.trace_photons(1, 8, 40_000, 4_000)
-    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
-    c = _oracle_grid(orc, tr["c_pos"], tr["c_pow"], tr["c_dir"], s.aabb())
+    # the faithful caustic estimate reads the global map's arrays with caustic slot
+    # numbers, so both sides must use the same in-cell order (sub-division) per map
+    g = _oracle_grid(orc, tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb(), sub_div=ctx.photons(0)["sub_div"])
+    c = _oracle_grid(orc, tr["c_pos"], tr["c_pow"], tr["c_dir"], s.aabb(), sub_div=ctx.photons(1)["sub_div"])
     out = s.render(cam.as_vector(), 64, 48, g, 50, 0.1, 4, c=c, k_c=20, r_c=0.2, faithful_caustic=True)
     np.testing.assert_allclose(_np(rad), out["radiance"], rtol=RTOL, atol=1e-7)
 
