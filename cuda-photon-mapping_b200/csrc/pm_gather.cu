@@ -11,17 +11,19 @@
 // reference's heap keeps whichever the sift order leaves).  Distances are the
 // reference's length(p - q) in IEEE float, so the sets are bit-exact.
 //
-// One thread per query.  The candidate heap keeps 64-bit keys
-// (float bits of the distance << 32 | source id): non-negative float bits order
-// like the floats, so integer comparison is the lexicographic order.  Photons
-// are stored by (cell, sub-cell); the walk starts with the query's sub-cell,
-// and once k candidates are held, every (sub-)cell whose box lies farther than
-// the current k-th distance (with a relative margin far above float rounding)
-// is skipped.  A candidate is first tested on its squared distance against a
-// bound slightly above the threshold's square, so the correctly rounded sqrt
-// -- the reference's distance -- is only taken for candidates that can enter.
-// The answer is the exhaustive walk's.  The heap is finally sorted so the
-// estimate sums in ascending order.
+// One warp per query.  Photons are stored by (cell, sub-cell); the warp walks
+// the query's sub-cell first, then the other sub-cells of the reference's cube
+// of cells, skipping every (sub-)cell whose box lies farther than the current
+// k-th distance (with a margin far above float rounding).  Lanes read 32
+// consecutive photons at a time (one 16-byte load each), test the squared
+// distance against a bound slightly above the threshold's square, take the
+// correctly rounded sqrt only for survivors, and append the survivors' 64-bit
+// keys (distance bits << 32 | source id; non-negative float bits order like the
+// floats, so integer order is the lexicographic order) to a per-warp
+// shared-memory store by ballot.  When the store fills, an MSB-first radix
+// select (8-bit digits, finished by a 32-lane bitonic sort) finds the exact
+// k-th key, the store is compacted to the k best and the threshold tightens.
+// The answer is the exhaustive walk's.
 #include "pm_gather.cuh"
 #include "pm_device.cuh"
 
@@ -29,48 +31,113 @@ namespace pm {
 
 namespace {
 
-constexpr int GATHER_THREADS = 128;
+constexpr int WARPS = 8;   // queries per block
 
-template <int KCAP>
-struct TopK {
-    unsigned long long key[KCAP];
-    uint32_t slot[KCAP];
-    int size;
-    __device__ __forceinline__ void sift_down(int i, int n) {
-        while (true) {
-            int l = 2 * i + 1, r = l + 1, big = i;
-            if (l < n && key[l] > key[big]) big = l;
-            if (r < n && key[r] > key[big]) big = r;
-            if (big == i) break;
-            unsigned long long tk = key[i]; key[i] = key[big]; key[big] = tk;
-            uint32_t ts = slot[i]; slot[i] = slot[big]; slot[big] = ts;
-            i = big;
-        }
-    }
-    __device__ __forceinline__ void push(unsigned long long k, uint32_t s, int kmax) {
-        if (size < kmax) {
-            int i = size++;
-            key[i] = k; slot[i] = s;
-            while (i > 0) {
-                int p = (i - 1) >> 1;
-                if (key[p] >= key[i]) break;
-                unsigned long long tk = key[i]; key[i] = key[p]; key[p] = tk;
-                uint32_t ts = slot[i]; slot[i] = slot[p]; slot[p] = ts;
-                i = p;
-            }
-        } else if (k < key[0]) {
-            key[0] = k; slot[0] = s;
-            sift_down(0, size);
-        }
-    }
-    __device__ __forceinline__ void sort_ascending() {
-        for (int n = size; n > 1; n--) {
-            unsigned long long tk = key[0]; key[0] = key[n - 1]; key[n - 1] = tk;
-            uint32_t ts = slot[0]; slot[0] = slot[n - 1]; slot[n - 1] = ts;
-            sift_down(0, n - 1);
-        }
-    }
+template <int UCAP>
+struct WarpStore {
+    unsigned long long key[UCAP];
+    uint32_t slot[UCAP];
+    uint32_t hist[256];   // radix-select histogram; doubles as 32 x u64 scratch
 };
+
+__device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
+    return __shfl_sync(0xffffffffu, v, src);
+}
+__device__ __forceinline__ unsigned long long shfl_xor_u64(unsigned long long v, int m) {
+    return __shfl_xor_sync(0xffffffffu, v, m);
+}
+
+// ascending bitonic sort of one value per lane
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, int lane) {
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            unsigned long long o = shfl_xor_u64(v, stride);
+            bool ascending = (lane & size) == 0;
+            bool lower = (lane & stride) == 0;
+            unsigned long long lo = v < o ? v : o, hi = v < o ? o : v;
+            v = (lower == ascending) ? lo : hi;
+        }
+    }
+    return v;
+}
+
+// the need-th smallest (1-based) of U.key[0, n); need <= n
+template <int UCAP>
+__device__ unsigned long long select_kth(WarpStore<UCAP>& U, int n, int need, int lane) {
+    unsigned long long prefix = 0ull, mask = 0ull;
+    unsigned long long* scratch = reinterpret_cast<unsigned long long*>(U.hist);
+    for (int shift = 56; shift >= 0; shift -= 8) {
+#pragma unroll
+        for (int b = 0; b < 8; b++) U.hist[8 * lane + b] = 0u;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            unsigned long long kk = U.key[i];
+            if ((kk & mask) == prefix) atomicAdd(&U.hist[(unsigned)(kk >> shift) & 255u], 1u);
+        }
+        __syncwarp();
+        uint32_t c[8], s = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) { c[b] = U.hist[8 * lane + b]; s += c[b]; }
+        uint32_t incl = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t excl = incl - s;
+        const unsigned own = __ballot_sync(0xffffffffu, excl < (uint32_t)need && (uint32_t)need <= incl);
+        const int owner = own ? __ffs(own) - 1 : 0;
+        int bin = 0;
+        uint32_t before = 0, cnt = 0;
+        if (lane == owner) {
+            uint32_t run = excl;
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                if (cnt == 0 && (uint32_t)need <= run + c[b]) { bin = 8 * lane + b; before = run; cnt = c[b]; }
+                run += c[b];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, owner);
+        before = __shfl_sync(0xffffffffu, before, owner);
+        cnt = __shfl_sync(0xffffffffu, cnt, owner);
+        need -= (int)before;
+        prefix |= (unsigned long long)bin << shift;
+        mask |= 0xffull << shift;
+        __syncwarp();
+        if (cnt <= 32u) {
+            // the few keys under this prefix: gather one per lane, sort, pick
+            int got = 0;
+            for (int base = 0; base < n; base += 32) {
+                int i = base + lane;
+                unsigned long long kk = i < n ? U.key[i] : ~0ull;
+                bool m = i < n && (kk & mask) == prefix;
+                unsigned bm = __ballot_sync(0xffffffffu, m);
+                if (m) scratch[got + __popc(bm & lanemask_lt())] = kk;
+                got += __popc(bm);
+            }
+            __syncwarp();
+            unsigned long long v = lane < got ? scratch[lane] : ~0ull;
+            __syncwarp();
+            v = warp_sort32(v, lane);
+            return shfl_u64(v, need - 1);
+        }
+    }
+    return prefix;
+}
+
+template <int UCAP>
+__device__ __forceinline__ unsigned long long warp_max_key(const WarpStore<UCAP>& U, int n, int lane) {
+    unsigned long long m = 0ull;
+    for (int i = lane; i < n; i += 32) m = U.key[i] > m ? U.key[i] : m;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long y = shfl_xor_u64(m, o);
+        m = y > m ? y : m;
+    }
+    return m;
+}
 
 // Cell / sub-cell of a point: the quotient (p - min) / cell selects the cell
 // (clamped, CudaPhotonMapping/PhotonGrid.cu:10-23); its fractional part the sub-cell.
@@ -89,51 +156,90 @@ __device__ __forceinline__ float axis_gap(float q, float lo, float hi, bool open
     return fmaxf(fmaxf(a, b), 0.f);
 }
 
-template <int KCAP>
-struct Walk {
+template <int UCAP>
+struct WarpWalk {
     const GatherGrid& G;
+    WarpStore<UCAP>& U;
     V3 q;
     float r;
-    int k;
-    TopK<KCAP> H;
-    float lim2;        // squared pre-filter: a candidate with s > lim2 cannot enter
-    float lim;         // distance bound used for pruning cells / sub-cells
-    __device__ Walk(const GatherGrid& g, V3 qq, float rr, int kk) : G(g), q(qq), r(rr), k(kk) {
-        H.size = 0;
-        lim = r;
-        lim2 = r * r * 1.000001f;
-    }
-    __device__ __forceinline__ void tighten() {
-        if (H.size == k) {
-            float dk = __uint_as_float((uint32_t)(H.key[0] >> 32));
-            lim = fminf(r, dk);
+    int k, lane;
+    int n;                    // keys in the store
+    unsigned long long T;     // a candidate enters when its key < T
+    float lim, lim2;          // distance bound for pruning; squared pre-filter bound
+
+    __device__ WarpWalk(const GatherGrid& g, WarpStore<UCAP>& u, V3 qq, float rr, int kk, int ln)
+        : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f) {}
+
+    // keep the k best keys of the store, tighten the threshold
+    __device__ void merge() {
+        __syncwarp();
+        if (n > k) {
+            T = select_kth(U, n, k, lane);
+            int w = 0;
+            for (int base = 0; base < n; base += 32) {
+                int i = base + lane;
+                unsigned long long kk = i < n ? U.key[i] : 0ull;
+                uint32_t sl = i < n ? U.slot[i] : 0u;
+                bool keep = i < n && kk <= T;
+                unsigned m = __ballot_sync(0xffffffffu, keep);
+                __syncwarp();
+                if (keep) {
+                    int pos = w + __popc(m & lanemask_lt());
+                    U.key[pos] = kk;
+                    U.slot[pos] = sl;
+                }
+                w += __popc(m);
+                __syncwarp();
+            }
+            n = w;
+        } else if (n == k) {
+            T = warp_max_key(U, n, lane);
+        }
+        if (n == k) {
+            lim = fminf(r, __uint_as_float((uint32_t)(T >> 32)));
             lim2 = lim * lim * 1.000001f;
         }
+        __syncwarp();
     }
-    // scan the photons of one sub-cell key
-    __device__ __forceinline__ void scan(uint32_t key) {
-        const uint32_t a = __ldg(G.key_starts + key), b = __ldg(G.key_starts + key + 1);
-        for (uint32_t j = a; j < b; j++) {
-            float4 p = __ldg(G.gpos + j);
-            float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-            float s = dx * dx + dy * dy + dz * dz;
-            if (s <= lim2) {
-                float d = sqrtf(s);
-                if (d <= r) {
-                    unsigned long long kk = ((unsigned long long)__float_as_uint(d) << 32) | __float_as_uint(p.w);
-                    if (H.size < k || kk < H.key[0]) {
-                        H.push(kk, j, k);
-                        tighten();
+
+    // photons [a, b) of one sub-cell
+    __device__ void scan(uint32_t a, uint32_t b) {
+        for (uint32_t base = a; base < b; base += 32) {
+            const uint32_t j = base + lane;
+            bool ok = false;
+            unsigned long long kk = 0ull;
+            if (j < b) {
+                float4 p = __ldg(G.gpos + j);
+                float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+                float s = dx * dx + dy * dy + dz * dz;
+                if (s <= lim2) {
+                    float d = sqrtf(s);
+                    if (d <= r) {
+                        kk = ((unsigned long long)__float_as_uint(d) << 32) | __float_as_uint(p.w);
+                        ok = kk < T;
                     }
                 }
             }
+            unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (m) {
+                if (ok) {
+                    int pos = n + __popc(m & lanemask_lt());
+                    U.key[pos] = kk;
+                    U.slot[pos] = j;
+                }
+                n += __popc(m);
+                if (n + 32 > UCAP) merge();
+            }
         }
     }
-    // visit the sub-cells of cell (x, y, z) that lie within lim of q
-    __device__ __forceinline__ void cell(int x, int y, int z, uint32_t skip_key) {
+
+    __device__ void scan_key(uint32_t key) { scan(__ldg(G.key_starts + key), __ldg(G.key_starts + key + 1)); }
+
+    // the sub-cells of cell (x, y, z) within lim of q
+    __device__ void cell(int x, int y, int z, uint32_t skip_key) {
         const float c = G.cell, pad = c * 1e-4f;
         const float m = 1.f + 1e-5f;
-        float lo_x = G.mn[0] + (float)x * c, lo_y = G.mn[1] + (float)y * c, lo_z = G.mn[2] + (float)z * c;
+        const float lo_x = G.mn[0] + (float)x * c, lo_y = G.mn[1] + (float)y * c, lo_z = G.mn[2] + (float)z * c;
         const bool ox0 = x == 0, ox1 = x == G.gx - 1, oy0 = y == 0, oy1 = y == G.gy - 1, oz0 = z == 0, oz1 = z == G.gz - 1;
         float L = lim * m;
         float gx = axis_gap(q.x, lo_x - pad, lo_x + c + pad, ox0, ox1);
@@ -143,13 +249,12 @@ struct Walk {
         const int S = G.S;
         const float sc = c / (float)S;
         const uint32_t base = (uint32_t)(x + y * G.gx + z * G.gx * G.gy) * (uint32_t)(S * S * S);
-        // sub-cell index ranges along each axis that the sphere of radius lim can reach
-        int sx0 = ox0 ? 0 : max(0, (int)floorf((q.x - L - pad - lo_x) / sc));
-        int sx1 = ox1 ? S - 1 : min(S - 1, (int)floorf((q.x + L + pad - lo_x) / sc));
-        int sy0 = oy0 ? 0 : max(0, (int)floorf((q.y - L - pad - lo_y) / sc));
-        int sy1 = oy1 ? S - 1 : min(S - 1, (int)floorf((q.y + L + pad - lo_y) / sc));
-        int sz0 = oz0 ? 0 : max(0, (int)floorf((q.z - L - pad - lo_z) / sc));
-        int sz1 = oz1 ? S - 1 : min(S - 1, (int)floorf((q.z + L + pad - lo_z) / sc));
+        const int sx0 = ox0 ? 0 : max(0, (int)floorf((q.x - L - pad - lo_x) / sc));
+        const int sx1 = ox1 ? S - 1 : min(S - 1, (int)floorf((q.x + L + pad - lo_x) / sc));
+        const int sy0 = oy0 ? 0 : max(0, (int)floorf((q.y - L - pad - lo_y) / sc));
+        const int sy1 = oy1 ? S - 1 : min(S - 1, (int)floorf((q.y + L + pad - lo_y) / sc));
+        const int sz0 = oz0 ? 0 : max(0, (int)floorf((q.z - L - pad - lo_z) / sc));
+        const int sz1 = oz1 ? S - 1 : min(S - 1, (int)floorf((q.z + L + pad - lo_z) / sc));
         for (int sz = sz0; sz <= sz1; sz++)
             for (int sy = sy0; sy <= sy1; sy++)
                 for (int sx = sx0; sx <= sx1; sx++) {
@@ -160,38 +265,40 @@ struct Walk {
                     float ay = axis_gap(q.y, lo_y + sy * sc - pad, lo_y + (sy + 1) * sc + pad, oy0 && sy == 0, oy1 && sy == S - 1);
                     float az = axis_gap(q.z, lo_z + sz * sc - pad, lo_z + (sz + 1) * sc + pad, oz0 && sz == 0, oz1 && sz == S - 1);
                     if (ax * ax + ay * ay + az * az > L * L) continue;
-                    scan(key);
+                    scan_key(key);
                 }
     }
 };
 
-template <int KCAP>
-__global__ void __launch_bounds__(GATHER_THREADS)
+template <int UCAP>
+__global__ void __launch_bounds__(WARPS * 32, 3)
 k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, GatherOut O) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = (int64_t)blockIdx.x * WARPS + warp;
     if (i >= Q.n) return;
+    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
     V3 q, nrm;
+    bool active = true;
     if (Q.pos3) {
         q = ld3(Q.pos3 + 3 * i);
         nrm = ld3(Q.nrm3 + 3 * i);
     } else {
         float4 a = Q.pos4[i], b = Q.nrm4[i];
-        if ((__float_as_uint(b.w) & Q.flag_mask) == 0u) {
-            st3(O.rad + 3 * i, v3(0.f, 0.f, 0.f));
-            if (O.cnt) O.cnt[i] = 0;
-            if (O.rk) O.rk[i] = 0.f;
-            return;
-        }
+        active = (__float_as_uint(b.w) & Q.flag_mask) != 0u;
         q = xyz(a);
         nrm = xyz(b);
     }
-    if (k <= 0) {
-        st3(O.rad + 3 * i, v3(0.f, 0.f, 0.f));
-        if (O.cnt) O.cnt[i] = 0;
-        if (O.rk) O.rk[i] = 0.f;
+    if (!active || k <= 0) {
+        if (lane == 0) {
+            st3(O.rad + 3 * i, v3(0.f, 0.f, 0.f));
+            if (O.cnt) O.cnt[i] = 0;
+            if (O.rk) O.rk[i] = 0.f;
+        }
+        if (O.ids) for (int e = lane; e < k; e += 32) O.ids[i * k + e] = 0xffffffffu;
         return;
     }
-    Walk<KCAP> W(G, q, r, k);
+    WarpWalk<UCAP> W(G, U, q, r, k, lane);
     int hx, hy, hz, sx, sy, sz;
     locate(q.x, G.mn[0], G.cell, G.gx, G.S, hx, sx);
     locate(q.y, G.mn[1], G.cell, G.gy, G.S, hy, sy);
@@ -201,7 +308,8 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
                               (uint32_t)(sx + S * (sy + S * sz));
     // the query's own sub-cell first, then the rest of its cell, then the cube
     // of cells of half width ceil(r / cell) (CudaPhotonMapping/PhotonGrid.cu:257-284)
-    W.scan(home_key);
+    W.scan_key(home_key);
+    if (W.n >= k) W.merge();
     W.cell(hx, hy, hz, home_key);
     const int rc = (int)ceilf(r / G.cell);
     const int x0 = max(0, hx - rc), y0 = max(0, hy - rc), z0 = max(0, hz - rc);
@@ -212,41 +320,70 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
                 if (x == hx && y == hy && z == hz) continue;
                 W.cell(x, y, z, 0xffffffffu);
             }
-    TopK<KCAP>& H = W.H;
-    H.sort_ascending();
-    const int cnt = H.size;
-    float rk = cnt ? __uint_as_float((uint32_t)(H.key[cnt - 1] >> 32)) : 0.f;
-    if (O.ids) {
-        for (int e = 0; e < k; e++)
-            O.ids[i * k + e] = e < cnt ? (uint32_t)(H.key[e] & 0xffffffffull) : 0xffffffffu;
-    }
-    if (O.cnt) O.cnt[i] = cnt;
-    if (O.rk) O.rk[i] = rk;
+    W.merge();
+    const int cnt = W.n;
+    const float rk = cnt ? __uint_as_float((uint32_t)(warp_max_key(U, cnt, lane) >> 32)) : 0.f;
+
+    // estimate (Raytracer.cuh:110-138): lanes take entries, then a fixed-order reduction
     V3 res = v3(0.f, 0.f, 0.f);
     if (cnt > 0 && !(require_full && cnt != k)) {
         const float alpha = 1.818f, beta = 1.953f;
-        float fr = rk * rk;
-        for (int e = 0; e < cnt; e++) {
-            uint32_t s = H.slot[e];
+        const float fr = rk * rk;
+        for (int e = lane; e < cnt; e += 32) {
+            uint32_t s = U.slot[e];
             V3 pd = ld3(G.gdir + 3 * (size_t)s);
             float cs = vdot(nrm, vneg(pd));
             if (cs > 0) {
-                float d = __uint_as_float((uint32_t)(H.key[e] >> 32));
+                float d = __uint_as_float((uint32_t)(U.key[e] >> 32));
                 float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / (1.f - expf(-beta)));
                 res = vadd(res, vscale(ld3(G.gpow + 3 * (size_t)s), filter));
             }
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            res.x += __shfl_xor_sync(0xffffffffu, res.x, o);
+            res.y += __shfl_xor_sync(0xffffffffu, res.y, o);
+            res.z += __shfl_xor_sync(0xffffffffu, res.z, o);
+        }
         float common = 1.f / (3.14159265358979f * (rk * rk) * 1);
         res = vscale(res, common);
     }
-    st3(O.rad + 3 * i, res);
+    if (lane == 0) {
+        st3(O.rad + 3 * i, res);
+        if (O.cnt) O.cnt[i] = cnt;
+        if (O.rk) O.rk[i] = rk;
+    }
+    if (O.ids) {
+        // ascending (distance, id): bitonic sort of the store's keys (padded to a power of two)
+        int P = 32;
+        while (P < cnt) P <<= 1;
+        for (int e = cnt + lane; e < P; e += 32) U.key[e] = ~0ull;
+        __syncwarp();
+        for (int size = 2; size <= P; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int e = lane; e < P; e += 32) {
+                    int o = e ^ stride;
+                    if (o > e) {
+                        unsigned long long a = U.key[e], b = U.key[o];
+                        bool ascending = (e & size) == 0;
+                        if ((a > b) == ascending) { U.key[e] = b; U.key[o] = a; }
+                    }
+                }
+                __syncwarp();
+            }
+        for (int e = lane; e < k; e += 32)
+            O.ids[i * k + e] = e < cnt ? (uint32_t)(U.key[e] & 0xffffffffull) : 0xffffffffu;
+    }
 }
 
-template <int KCAP>
+template <int UCAP>
 cudaError_t launch(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full, const GatherOut& O,
                    cudaStream_t st) {
-    unsigned blocks = (unsigned)((Q.n + GATHER_THREADS - 1) / GATHER_THREADS);
-    k_gather<KCAP><<<blocks, GATHER_THREADS, 0, st>>>(G, Q, r, k, require_full, O);
+    const size_t smem = sizeof(WarpStore<UCAP>) * WARPS;
+    cudaError_t e = cudaFuncSetAttribute(k_gather<UCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    unsigned blocks = (unsigned)((Q.n + WARPS - 1) / WARPS);
+    k_gather<UCAP><<<blocks, WARPS * 32, smem, st>>>(G, Q, r, k, require_full, O);
     return cudaGetLastError();
 }
 
@@ -256,11 +393,8 @@ cudaError_t gather(const GatherGrid& G, const GatherQueries& Q, float r, int k, 
                    const GatherOut& O, unsigned* status, cudaStream_t st) {
     (void)status;
     if (Q.n <= 0) return cudaSuccess;
-    if (k <= 16) return launch<16>(G, Q, r, k, require_full, O, st);
-    if (k <= 32) return launch<32>(G, Q, r, k, require_full, O, st);
-    if (k <= 64) return launch<64>(G, Q, r, k, require_full, O, st);
-    if (k <= 128) return launch<128>(G, Q, r, k, require_full, O, st);
-    if (k <= 256) return launch<256>(G, Q, r, k, require_full, O, st);
+    if (k <= 96) return launch<256>(G, Q, r, k, require_full, O, st);
+    if (k <= 256) return launch<512>(G, Q, r, k, require_full, O, st);
     return cudaErrorInvalidValue;
 }
 
