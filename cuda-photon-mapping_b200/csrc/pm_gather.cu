@@ -12,9 +12,10 @@
 // reference's length(p - q) in IEEE float, so the sets are bit-exact.
 //
 // One warp per query.  Photons are stored by (cell, sub-cell); the warp walks
-// the query's sub-cell first, then the other sub-cells of the reference's cube
-// of cells, skipping every (sub-)cell whose box lies farther than the current
-// k-th distance (with a margin far above float rounding).  Lanes read 32
+// the query's sub-cell first, then rings of sub-cells outwards (nearest first),
+// within the reference's cube of cells, skipping every sub-cell whose box lies
+// farther than the current k-th distance (with a margin far above float
+// rounding) and stopping at the first ring that lies entirely farther.  Lanes read 32
 // consecutive photons at a time (one 16-byte load each), test the squared
 // distance against a bound slightly above the threshold's square, take the
 // correctly rounded sqrt only for survivors, and append the survivors' 64-bit
@@ -235,38 +236,59 @@ struct WarpWalk {
 
     __device__ void scan_key(uint32_t key) { scan(__ldg(G.key_starts + key), __ldg(G.key_starts + key + 1)); }
 
-    // the sub-cells of cell (x, y, z) within lim of q
-    __device__ void cell(int x, int y, int z, uint32_t skip_key) {
-        const float c = G.cell, pad = c * 1e-4f;
-        const float m = 1.f + 1e-5f;
-        const float lo_x = G.mn[0] + (float)x * c, lo_y = G.mn[1] + (float)y * c, lo_z = G.mn[2] + (float)z * c;
-        const bool ox0 = x == 0, ox1 = x == G.gx - 1, oy0 = y == 0, oy1 = y == G.gy - 1, oz0 = z == 0, oz1 = z == G.gz - 1;
-        float L = lim * m;
-        float gx = axis_gap(q.x, lo_x - pad, lo_x + c + pad, ox0, ox1);
-        float gy = axis_gap(q.y, lo_y - pad, lo_y + c + pad, oy0, oy1);
-        float gz = axis_gap(q.z, lo_z - pad, lo_z + c + pad, oz0, oz1);
-        if (gx * gx + gy * gy + gz * gz > L * L) return;
+    // Nearest-first walk: rings of sub-cells at Chebyshev distance R = 1, 2, ...
+    // from the query's sub-cell (global sub-cell coordinates), restricted to the
+    // sub-cells of the reference's cube of cells [lo, hi].  Lanes test 32 ring
+    // members at a time (box distance, non-empty range); the survivors are
+    // scanned one after another.  A ring whose nearest possible point is
+    // farther than the current bound ends the walk.
+    __device__ void rings(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz) {
         const int S = G.S;
-        const float sc = c / (float)S;
-        const uint32_t base = (uint32_t)(x + y * G.gx + z * G.gx * G.gy) * (uint32_t)(S * S * S);
-        const int sx0 = ox0 ? 0 : max(0, (int)floorf((q.x - L - pad - lo_x) / sc));
-        const int sx1 = ox1 ? S - 1 : min(S - 1, (int)floorf((q.x + L + pad - lo_x) / sc));
-        const int sy0 = oy0 ? 0 : max(0, (int)floorf((q.y - L - pad - lo_y) / sc));
-        const int sy1 = oy1 ? S - 1 : min(S - 1, (int)floorf((q.y + L + pad - lo_y) / sc));
-        const int sz0 = oz0 ? 0 : max(0, (int)floorf((q.z - L - pad - lo_z) / sc));
-        const int sz1 = oz1 ? S - 1 : min(S - 1, (int)floorf((q.z + L + pad - lo_z) / sc));
-        for (int sz = sz0; sz <= sz1; sz++)
-            for (int sy = sy0; sy <= sy1; sy++)
-                for (int sx = sx0; sx <= sx1; sx++) {
-                    const uint32_t key = base + (uint32_t)(sx + S * (sy + S * sz));
-                    if (key == skip_key) continue;
-                    L = lim * m;
-                    float ax = axis_gap(q.x, lo_x + sx * sc - pad, lo_x + (sx + 1) * sc + pad, ox0 && sx == 0, ox1 && sx == S - 1);
-                    float ay = axis_gap(q.y, lo_y + sy * sc - pad, lo_y + (sy + 1) * sc + pad, oy0 && sy == 0, oy1 && sy == S - 1);
-                    float az = axis_gap(q.z, lo_z + sz * sc - pad, lo_z + (sz + 1) * sc + pad, oz0 && sz == 0, oz1 && sz == S - 1);
-                    if (ax * ax + ay * ay + az * az > L * L) continue;
-                    scan_key(key);
+        const float sc = G.cell / (float)S, pad = G.cell * 1e-4f;
+        const float m = 1.f + 1e-5f;
+        const int GX = G.gx * S - 1, GY = G.gy * S - 1, GZ = G.gz * S - 1;
+        const int Rmax = max(max(max(X0 - lx, hx - X0), max(Y0 - ly, hy - Y0)), max(Z0 - lz, hz - Z0));
+        for (int R = 1; R <= Rmax; R++) {
+            if ((float)(R - 1) * sc - pad > lim * m) break;
+            const int side = 2 * R + 1;
+            const int total = side * side * side;
+            for (int base = 0; base < total; base += 32) {
+                const int t = base + lane;
+                bool ok = false;
+                uint32_t a = 0, b = 0;
+                float dist2 = 0.f;
+                if (t < total) {
+                    const int dx = t % side - R, dy = (t / side) % side - R, dz = t / (side * side) - R;
+                    const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
+                    if (max(max(abs(dx), abs(dy)), abs(dz)) == R && X >= lx && X <= hx && Y >= ly && Y <= hy &&
+                        Z >= lz && Z <= hz) {
+                        float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
+                        float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
+                        float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
+                        dist2 = ax * ax + ay * ay + az * az;
+                        const float L = lim * m;
+                        if (dist2 <= L * L) {
+                            const uint32_t cellid = (uint32_t)(X / S + (Y / S) * G.gx + (Z / S) * G.gx * G.gy);
+                            const uint32_t key = cellid * (uint32_t)(S * S * S) +
+                                                 (uint32_t)(X % S + S * (Y % S + S * (Z % S)));
+                            a = __ldg(G.key_starts + key);
+                            b = __ldg(G.key_starts + key + 1);
+                            ok = b > a;
+                        }
+                    }
                 }
+                unsigned todo = __ballot_sync(0xffffffffu, ok);
+                while (todo) {
+                    const int src = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const uint32_t sa = __shfl_sync(0xffffffffu, a, src);
+                    const uint32_t sb = __shfl_sync(0xffffffffu, b, src);
+                    const float d2 = __shfl_sync(0xffffffffu, dist2, src);
+                    const float L = lim * m;
+                    if (d2 <= L * L) scan(sa, sb);
+                }
+            }
+        }
     }
 };
 
@@ -306,20 +328,15 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
     const int S = G.S;
     const uint32_t home_key = (uint32_t)(hx + hy * G.gx + hz * G.gx * G.gy) * (uint32_t)(S * S * S) +
                               (uint32_t)(sx + S * (sy + S * sz));
-    // the query's own sub-cell first, then the rest of its cell, then the cube
-    // of cells of half width ceil(r / cell) (CudaPhotonMapping/PhotonGrid.cu:257-284)
+    // the query's own sub-cell first, then rings of sub-cells outwards, within the
+    // cube of cells of half width ceil(r / cell) (CudaPhotonMapping/PhotonGrid.cu:257-284)
     W.scan_key(home_key);
     if (W.n >= k) W.merge();
-    W.cell(hx, hy, hz, home_key);
     const int rc = (int)ceilf(r / G.cell);
     const int x0 = max(0, hx - rc), y0 = max(0, hy - rc), z0 = max(0, hz - rc);
     const int x1 = min(G.gx - 1, hx + rc), y1 = min(G.gy - 1, hy + rc), z1 = min(G.gz - 1, hz + rc);
-    for (int z = z0; z <= z1; z++)
-        for (int y = y0; y <= y1; y++)
-            for (int x = x0; x <= x1; x++) {
-                if (x == hx && y == hy && z == hz) continue;
-                W.cell(x, y, z, 0xffffffffu);
-            }
+    W.rings(hx * S + sx, hy * S + sy, hz * S + sz, x0 * S, y0 * S, z0 * S, x1 * S + S - 1, y1 * S + S - 1,
+            z1 * S + S - 1);
     W.merge();
     const int cnt = W.n;
     const float rk = cnt ? __uint_as_float((uint32_t)(warp_max_key(U, cnt, lane) >> 32)) : 0.f;
