@@ -107,21 +107,23 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- CPU leg
-def cpu_reference_estimate(sc, w, rows=8, trace_photons=3000, threads=None):
+def cpu_reference_estimate(sc, w, rows=8, trace_photons=5000, threads=None):
     """The reference's CPU path on the host cores, on a bounded sample, scaled
     to one full frame of the workload.
 
     * photon pass: the reference has no CPU tracer (emit is __device__); its
-      algorithm is timed as the oracle's restatement (brute-force closest hit,
-      OpenMP over the host cores) on ``trace_photons`` photons and scaled to
-      the workload's photon count;
-    * grid: the oracle's grid build on those photons, scaled linearly;
+      algorithm (brute-force closest hit) is timed as the oracle's restatement,
+      OpenMP over the host cores, on ``trace_photons`` photons, scaled to the
+      workload's photon count;
+    * grid: the oracle's grid build over a map of the workload's size (the
+      traced sample replicated with a 1e-4 jitter);
     * frame: the reference's own Raytracer::render_trace (oracle/_ref, its CPU
-      mode) on ``rows`` full image rows, one process per host core, over a map
-      with the workload's photon density (the traced sample replicated with a
-      1e-4 jitter up to the workload's photon count), scaled to all rows.
+      mode, single-threaded by design) on ``rows`` image rows spread over the
+      frame, one process per host core, over that map; the mean row time is
+      scaled to all rows and divided over the cores.
     """
     import multiprocessing as mp
+    import tempfile
     from oracle import Oracle
     orc = Oracle()
     s = orc.scene(sc)
@@ -129,40 +131,45 @@ def cpu_reference_estimate(sc, w, rows=8, trace_photons=3000, threads=None):
     t0 = time.perf_counter()
     tr = s.trace_photons(w["seed"], w["max_bounces"], trace_photons)
     t_trace = (time.perf_counter() - t0) * (w["photons"] / trace_photons)
-    t0 = time.perf_counter()
-    orc.grid_build(tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
-    t_grid = (time.perf_counter() - t0) * (w["photons"] / trace_photons)
     n = w["photons"]
     rep = int(np.ceil(n / trace_photons))
     rng = np.random.default_rng(1)
-    pos = (np.tile(tr["g_pos"], (rep, 1))[:n] + rng.normal(scale=1e-4, size=(n, 3))).astype(np.float32)
+    pos = (np.tile(tr["g_pos"], (rep, 1))[:n] + rng.normal(scale=1e-4, size=(n, 3)).astype(np.float32)).astype(np.float32)
     dirs = np.tile(tr["g_dir"], (rep, 1))[:n]
     pw = np.tile(tr["g_pow"], (rep, 1))[:n]
+    t0 = time.perf_counter()
     g = orc.grid_build(pos, pw, dirs, s.aabb())
+    t_grid = time.perf_counter() - t0
     H = w["height"]
     ys = np.linspace(0, H - 1, rows).astype(int)
-    ctx = mp.get_context("spawn")
-    args = [(sc, w, g, int(y)) for y in ys]
-    t0 = time.perf_counter()
-    with ctx.Pool(min(threads, rows)) as pool:
-        per_row = pool.map(_ref_row, args)
-    wall = time.perf_counter() - t0
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in ("spos", "sdir", "spow", "starts", "sizes", "dims", "aabb"):
+            np.save(os.path.join(tmp, name + ".npy"), getattr(g, name))
+        np.save(os.path.join(tmp, "cell.npy"), np.float32(g.cell))
+        ctx = mp.get_context("spawn")
+        args = [(w, tmp, int(y), sc) for y in ys]
+        t0 = time.perf_counter()
+        with ctx.Pool(min(threads, rows)) as pool:
+            per_row = pool.map(_ref_row, args)
+        wall = time.perf_counter() - t0
     t_row = float(np.mean(per_row))
     t_frame = t_row * H / threads
     total = t_trace + t_grid + t_frame
     return dict(step_s=total, trace_s=t_trace, grid_s=t_grid, frame_s=t_frame, row_s=t_row, cores=threads,
-                sample=f"{trace_photons} photons traced (scaled to {n}); {rows} of {H} rows rendered by the "
-                       f"reference's render_trace over a {n}-photon map (sample replicated), {threads} processes",
-                wall_s=wall)
+                sample=f"{trace_photons} photons traced by the oracle (scaled to {n}); grid of {n} photons "
+                       f"(sample replicated); {rows} of {H} rows rendered by the reference's render_trace, "
+                       f"{threads} processes", wall_s=wall)
 
 
 def _ref_row(arg):
-    sc, w, g, y = arg
+    w, tmp, y, sc = arg
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import RefHost
+    from oracle import GridResult, RefHost
     from photonmap import scenes
-    ref = RefHost()
-    rs = ref.scene(sc)
+    ld = lambda nm: np.load(os.path.join(tmp, nm + ".npy"), mmap_mode="r")  # noqa: E731
+    g = GridResult(np.array(ld("aabb")), np.array(ld("dims")), float(ld("cell")), np.array(ld("starts")),
+                   np.array(ld("sizes")), None, np.array(ld("spos")), np.array(ld("sdir")), np.array(ld("spow")), None)
+    rs = RefHost().scene(sc)
     cam = scenes.default_camera(w["width"], w["height"])
     t0 = time.perf_counter()
     rs.render(cam, g, w["k"], w["radius"], w["max_depth"], y0=y, y1=y + 1)
@@ -302,7 +309,7 @@ def run_reference(args):
     sc, cs, w = scenes.workload(args.workload)
     times = []
     for i in range(args.warmup + args.steps):
-        est = cpu_reference_estimate(sc, w, rows=8, trace_photons=1500)
+        est = cpu_reference_estimate(sc, w, rows=8, trace_photons=2000)
         if i >= args.warmup:
             times.append(est["step_s"])
     step_s = float(np.mean(times))
