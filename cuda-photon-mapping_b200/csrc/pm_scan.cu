@@ -1,4 +1,6 @@
 // pm_scan.cu -- decoupled look-back scan (see pm_scan.cuh).
+#include <mutex>
+#include "../../include/pm_api.h"
 #include "pm_scan.cuh"
 #include "pm_device.cuh"
 
@@ -139,3 +141,65 @@ cudaError_t scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive
 }
 
 }  // namespace pm
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the scan (pm_scan_u32_noalloc in pm_api.h).
+//
+// Some callers may not allocate device memory at all: an engine that reserves
+// the whole device for its own pool before loading this library, or a render
+// loop that must not call cudaMalloc / cudaFree while frames are in flight
+// (those calls can synchronise the device and stall other streams).  For
+// them this entry point takes only the caller's input and output buffers; the
+// look-back workspace (tile states, tile counter, status word) lives in a
+// fixed array in the library's own device memory, which every GPU that loads
+// the library holds until the process exits.
+//
+// Limit: n <= PM_NOALLOC_SCAN_MAX (4096 tiles of 4096 = 16,777,216 values),
+// i.e. 4096 tile-state words + 2 control words = 32,784 bytes per device.
+// The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress, once per device, that device current); make that
+// first call before capturing a stream.  All calls share the array, which
+// keeps the last call's contents, so calls whose work overlaps on the GPU (two
+// streams, two host threads) race; serialise them.  Each call clears the part
+// it uses (tile states, counter, status word) before launching.
+namespace {
+
+constexpr int NOALLOC_TILES = 4096;
+static __device__ __align__(256) unsigned long long g_noalloc_scan_ws[NOALLOC_TILES + 2];
+
+std::once_flag g_noalloc_once[64];
+void* g_noalloc_ptr[64] = {};
+cudaError_t g_noalloc_err[64] = {};
+
+}  // namespace
+
+extern "C" int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclusive, void* stream) {
+    using namespace pm;
+    static_assert((int64_t)NOALLOC_TILES * SCAN_TILE == PM_NOALLOC_SCAN_MAX, "limit mismatch");
+    if (n < 0 || (n > 0 && (!in || !out))) return PM_ERR_INVALID;
+    if (n > PM_NOALLOC_SCAN_MAX) return PM_ERR_INVALID;                     // beyond the fixed workspace
+    if (n == 0) return PM_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PM_ERR_CUDA;
+    // once per device, with that device current: the device address of the array
+    std::call_once(g_noalloc_once[dev], [dev]() {
+        void* p = nullptr;
+        g_noalloc_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scan_ws);
+        g_noalloc_ptr[dev] = p;
+    });
+    if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev]) return PM_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    unsigned long long* state = (unsigned long long*)g_noalloc_ptr[dev];
+    unsigned* counter = (unsigned*)(state + NOALLOC_TILES);
+    unsigned* status = counter + 2;
+    // tile states, the tile counter and the status word must start at zero
+    if (cudaMemsetAsync(state, 0, (size_t)tiles * 8, st) != cudaSuccess) return PM_ERR_CUDA;
+    if (cudaMemsetAsync(counter, 0, 16, st) != cudaSuccess) return PM_ERR_CUDA;
+    k_scan_u32<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, inclusive, state, counter, nullptr, status);
+    if (cudaGetLastError() != cudaSuccess) return PM_ERR_CUDA;
+    unsigned bits = 0;
+    if (cudaMemcpyAsync(&bits, status, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PM_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return PM_ERR_CUDA;
+    return (bits & ST_TIMEOUT) ? PM_ERR_TIMEOUT : PM_OK;
+}

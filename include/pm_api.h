@@ -185,6 +185,23 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, uin
  * exclusive (inclusive = 0) or inclusive scan of n u32 device values. */
 int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive);
 
+/* Allocation-free scan (no counterpart in the reference).  For callers that
+ * may not allocate device memory: hosts that reserve the whole device for their
+ * own pool, or frame loops that must not call cudaMalloc / cudaFree (which can
+ * synchronise the device) while work is in flight.  Same scan as pm_scan_u32
+ * on the caller's device buffers (in, out: n u32 each), issued on `stream`
+ * (a cudaStream_t; NULL = the default stream) of the current device, which
+ * is synchronised before returning.  Needs no pm_ctx: the look-back workspace
+ * is a fixed 32,784-byte array in the library's device memory, held on every
+ * GPU that loads the library until the process exits.  n above
+ * PM_NOALLOC_SCAN_MAX returns PM_ERR_INVALID.  The first call on a device
+ * looks up the array's address (once per device); make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race, so
+ * serialise them.  Errors are returned as codes only (there is no context
+ * for pm_last_error). */
+#define PM_NOALLOC_SCAN_MAX 16777216
+int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclusive, void* stream);
+
 /* Per-stage device times of the last pm_trace_photons / pm_build_grid /
  * pm_render calls in milliseconds (CUDA events on the context stream):
  * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather, [4] resolve. */
