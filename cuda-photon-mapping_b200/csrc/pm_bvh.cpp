@@ -4,9 +4,11 @@
 // of every model whose box it meets (CudaPhotonMapping/Model.cuh:366-446); its
 // kd-tree code only reduces a model's triangles to one AABB
 // (KdTree.cu:395-464).  This is a binary BVH built with binned SAH (16 bins on
-// the widest centroid axis, leaves of <= 4 triangles, depth <= 60).  Node boxes
-// are padded so that culling is conservative with respect to the exact
-// triangle test; the traversal (pm_scene.cuh) keeps the reference's answer.
+// the widest centroid axis, leaves of <= 4 triangles, depth <= 60), stored as
+// interior nodes that carry both children's boxes, so one 64-byte fetch tests
+// both children.  Boxes are padded so that culling is conservative with
+// respect to the exact triangle test; the traversal (pm_scene.cuh) keeps the
+// reference's answer.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -44,8 +46,8 @@ struct Task { int node, b, e, depth; };
 
 }  // namespace
 
-// nodes_out: 8 floats per node = lo.xyz, bits(left child | first prim), hi.xyz, bits(count)
-// (count > 0: leaf over prim[first, first + count); count == 0: children left, left + 1)
+// nodes_out: 16 floats per interior node (both children's boxes and refs, see below);
+// node 0 is the root.  prim: leaf triangle indices.
 void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& nodes_out, std::vector<int>& prim) {
     std::vector<Box> pb(ntri);
     std::vector<float> cen(3 * (size_t)ntri);
@@ -67,7 +69,7 @@ void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& no
         nodes[tk.node].box = nb;
         const int n = tk.e - tk.b;
         auto make_leaf = [&]() { nodes[tk.node].first = tk.b; nodes[tk.node].count = n; };
-        if (n <= 4 || tk.depth >= 60) { make_leaf(); continue; }
+        if (n <= 4 || (tk.depth >= 60 && n <= 255)) { make_leaf(); continue; }
         int axis = 0;
         float ext[3];
         for (int a = 0; a < 3; a++) ext[a] = cb.hi[a] - cb.lo[a];
@@ -120,19 +122,45 @@ void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& no
         stack.push_back(Task{left_idx + 1, mid, tk.e, tk.depth + 1});
         stack.push_back(Task{left_idx, tk.b, mid, tk.depth + 1});
     }
-    nodes_out.resize(8 * nodes.size());
-    for (size_t i = 0; i < nodes.size(); i++) {
-        float* o = &nodes_out[8 * i];
-        const Node& nd = nodes[i];
+    // Output: interior nodes only, each holding both children's padded boxes
+    // (16 floats = 4 x float4): (lo0, ref0), (hi0, 0), (lo1, ref1), (hi1, 0).
+    // ref >= 0: interior node index; ref < 0: leaf, ~ref = first << 8 | count.
+    std::vector<int> remap(nodes.size(), -1);
+    int ninterior = 0;
+    for (size_t i = 0; i < nodes.size(); i++)
+        if (nodes[i].count == 0) remap[i] = ninterior++;
+    auto ref_of = [&](size_t c) -> int {
+        if (nodes[c].count == 0) return remap[c];
+        return ~((nodes[c].first << 8) | nodes[c].count);
+    };
+    auto put_box = [&](float* o, const Box& b, int ref) {
         for (int a = 0; a < 3; a++) {
-            float span = std::max(std::fabs(nd.box.lo[a]), std::fabs(nd.box.hi[a]));
+            float span = std::max(std::fabs(b.lo[a]), std::fabs(b.hi[a]));
             float p = pad + span * 1e-5f;
-            o[a] = nd.box.lo[a] - p;
-            o[4 + a] = nd.box.hi[a] + p;
+            o[a] = b.lo[a] - p;
+            o[4 + a] = b.hi[a] + p;
         }
-        int f = nd.first, c = nd.count;
-        std::memcpy(&o[3], &f, 4);
-        std::memcpy(&o[7], &c, 4);
+        std::memcpy(&o[3], &ref, 4);
+        o[7] = 0.f;
+    };
+    if (ninterior == 0) {
+        // a single leaf: one interior node holding it and an empty box
+        nodes_out.assign(16, 0.f);
+        put_box(&nodes_out[0], nodes[0].box, ref_of(0));
+        Box empty;
+        for (int a = 0; a < 3; a++) { nodes_out[8 + a] = 3.0e38f; nodes_out[12 + a] = -3.0e38f; }
+        int r = ~0;
+        std::memcpy(&nodes_out[11], &r, 4);
+        (void)empty;
+        return;
+    }
+    nodes_out.assign(16 * (size_t)ninterior, 0.f);
+    for (size_t i = 0; i < nodes.size(); i++) {
+        if (nodes[i].count != 0) continue;
+        float* o = &nodes_out[16 * (size_t)remap[i]];
+        size_t c0 = nodes[i].first, c1 = c0 + 1;
+        put_box(o, nodes[c0].box, ref_of(c0));
+        put_box(o + 8, nodes[c1].box, ref_of(c1));
     }
 }
 

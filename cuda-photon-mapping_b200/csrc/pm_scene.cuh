@@ -15,7 +15,8 @@
 //     AABB passes for the ray (evaluated lazily, once per model per ray);
 //   * BVH node boxes are padded, and a node is skipped only when its entry
 //     distance is strictly larger than the best t, so no candidate that could
-//     win (including exact ties) is culled.
+//     win (including exact ties) is culled.  (The slab arithmetic uses
+//     box * (1/d) - o * (1/d); the padding dwarfs its rounding.)
 #pragma once
 #include "pm_device.cuh"
 
@@ -29,7 +30,7 @@ struct DevScene {
     const float* tri_pos;     // 9 per triangle (vertex positions, as given)
     const float* tri_nrm;     // 9 per triangle (vertex normals)
     const float* tri_diffuse; // 3 per triangle or null
-    const float4* nodes;      // 2 per node: (lo, left|first), (hi, count)
+    const float4* nodes;      // 4 per interior node: both children's (lo, ref), (hi, -)
     const int* prim;          // leaf triangle indices
     const float* maabb;       // 6 per model (min xyz, max xyz)
     const float* mats;        // 12 per model
@@ -125,8 +126,14 @@ __device__ __forceinline__ float safe_inv(float x) { return 1.0f / (x == 0.0f ? 
 // triangles of models >= min_model whose model gate passes; also reports the
 // largest model index with a gated hit at exactly t == 0 (zmodel, -1 if none),
 // its lowest such triangle and that triangle's barycentrics.
+//
+// While-while traversal with postponed leaves (Aila & Laine, "Understanding the
+// efficiency of ray traversal on GPUs", HPG 2009): lanes descend interior
+// nodes until every lane of the warp holds a leaf, then test triangles
+// together.  Each interior node carries both children's boxes.
 static __device__ __noinline__ bool traverse(const DevScene& S, V3 o, V3 d, int min_model, Hit& h, int& zmodel,
                                              int& ztri, V3& zuvw) {
+    constexpr int SENTINEL = 0x76543210;
     float best_t = __int_as_float(0x7f800000);
     int best_tri = 0x7fffffff;
     V3 best_uvw = v3(0.f, 0.f, 0.f);
@@ -134,64 +141,74 @@ static __device__ __noinline__ bool traverse(const DevScene& S, V3 o, V3 d, int 
     ztri = 0x7fffffff;
     unsigned long long gate_known = 0ull, gate_pass = 0ull;
     const float ix = safe_inv(d.x), iy = safe_inv(d.y), iz = safe_inv(d.z);
+    const float ox = o.x * ix, oy = o.y * iy, oz = o.z * iz;
     int stack[64];
     int sp = 0;
+    stack[0] = SENTINEL;
     int node = 0;
-    while (true) {
-        float4 a = __ldg(S.nodes + 2 * node);
-        float4 b = __ldg(S.nodes + 2 * node + 1);
-        float tx0 = (a.x - o.x) * ix, tx1 = (b.x - o.x) * ix;
-        float ty0 = (a.y - o.y) * iy, ty1 = (b.y - o.y) * iy;
-        float tz0 = (a.z - o.z) * iz, tz1 = (b.z - o.z) * iz;
-        float tmin = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-        float tmax = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
-        bool visit = tmin <= tmax && tmin <= best_t;
-        if (visit) {
-            int count = __float_as_int(b.w);
-            int first = __float_as_int(a.w);
-            if (count > 0) {
-                for (int i = 0; i < count; i++) {
-                    int tri = __ldg(S.prim + first + i);
-                    const float4* T = S.tri + 5 * (size_t)tri;
-                    int m = __float_as_int(__ldg(&T[2].w));
-                    if (m < min_model) continue;
-                    float t; V3 uvw;
-                    if (!tri_test(T, o, d, best_t, tri, best_tri, t, uvw)) continue;
-                    const bool zero = t == 0.0f;
-                    if (zero && (m < zmodel || (m == zmodel && tri > ztri))) continue;
-                    bool pass;
-                    if (m < 64) {
-                        unsigned long long bit = 1ull << m;
-                        if (!(gate_known & bit)) {
-                            gate_known |= bit;
-                            if (model_gate(S.maabb + 6 * m, o, d)) gate_pass |= bit;
-                        }
-                        pass = (gate_pass & bit) != 0ull;
-                    } else {
-                        pass = model_gate(S.maabb + 6 * m, o, d);
-                    }
-                    if (!pass) continue;
-                    if (zero) { zmodel = m; ztri = tri; zuvw = uvw; }
-                    else { best_t = t; best_tri = tri; best_uvw = uvw; }
-                }
+    int leaf = 0;
+    while (node != SENTINEL) {
+        while ((unsigned)node < (unsigned)SENTINEL) {
+            const float4* N = S.nodes + 4 * (size_t)node;
+            const float4 a0 = __ldg(N), b0 = __ldg(N + 1), a1 = __ldg(N + 2), b1 = __ldg(N + 3);
+            float t0x = a0.x * ix - ox, t1x = b0.x * ix - ox;
+            float t0y = a0.y * iy - oy, t1y = b0.y * iy - oy;
+            float t0z = a0.z * iz - oz, t1z = b0.z * iz - oz;
+            const float c0min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+            const float c0max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
+            t0x = a1.x * ix - ox; t1x = b1.x * ix - ox;
+            t0y = a1.y * iy - oy; t1y = b1.y * iy - oy;
+            t0z = a1.z * iz - oz; t1z = b1.z * iz - oz;
+            const float c1min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+            const float c1max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
+            const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
+            if (!h0 && !h1) {
+                node = stack[sp--];
             } else {
-                // interior: children first and first + 1; nearer child first
-                int c0 = first, c1 = first + 1;
-                float4 a0 = __ldg(S.nodes + 2 * c0), b0 = __ldg(S.nodes + 2 * c0 + 1);
-                float4 a1 = __ldg(S.nodes + 2 * c1), b1 = __ldg(S.nodes + 2 * c1 + 1);
-                float e0 = fmaxf(fmaxf(fminf((a0.x - o.x) * ix, (b0.x - o.x) * ix), fminf((a0.y - o.y) * iy, (b0.y - o.y) * iy)),
-                                 fminf((a0.z - o.z) * iz, (b0.z - o.z) * iz));
-                float e1 = fmaxf(fmaxf(fminf((a1.x - o.x) * ix, (b1.x - o.x) * ix), fminf((a1.y - o.y) * iy, (b1.y - o.y) * iy)),
-                                 fminf((a1.z - o.z) * iz, (b1.z - o.z) * iz));
-                int nearc = e0 <= e1 ? c0 : c1;
-                int farc = e0 <= e1 ? c1 : c0;
-                if (sp < 64) stack[sp++] = farc;
-                node = nearc;
-                continue;
+                const int r0 = __float_as_int(a0.w), r1 = __float_as_int(a1.w);
+                node = h0 ? r0 : r1;
+                if (h0 && h1) {
+                    int other = r1;
+                    if (c1min < c0min) { node = r1; other = r0; }
+                    if (sp < 63) stack[++sp] = other;
+                }
             }
+            if (node < 0 && leaf >= 0) {   // first leaf: postpone it, keep descending
+                leaf = node;
+                node = stack[sp--];
+            }
+            if (!__any_sync(__activemask(), leaf >= 0)) break;   // every lane holds a leaf
         }
-        if (sp == 0) break;
-        node = stack[--sp];
+        while (leaf < 0) {
+            const int packed = ~leaf;
+            const int first = packed >> 8, count = packed & 255;
+            for (int i = 0; i < count; i++) {
+                const int tri = __ldg(S.prim + first + i);
+                const float4* T = S.tri + 5 * (size_t)tri;
+                const int m = __float_as_int(__ldg(&T[2].w));
+                if (m < min_model) continue;
+                float t; V3 uvw;
+                if (!tri_test(T, o, d, best_t, tri, best_tri, t, uvw)) continue;
+                const bool zero = t == 0.0f;
+                if (zero && (m < zmodel || (m == zmodel && tri > ztri))) continue;
+                bool pass;
+                if (m < 64) {
+                    const unsigned long long bit = 1ull << m;
+                    if (!(gate_known & bit)) {
+                        gate_known |= bit;
+                        if (model_gate(S.maabb + 6 * m, o, d)) gate_pass |= bit;
+                    }
+                    pass = (gate_pass & bit) != 0ull;
+                } else {
+                    pass = model_gate(S.maabb + 6 * m, o, d);
+                }
+                if (!pass) continue;
+                if (zero) { zmodel = m; ztri = tri; zuvw = uvw; }
+                else { best_t = t; best_tri = tri; best_uvw = uvw; }
+            }
+            leaf = node;                    // another postponed leaf: process it as well
+            if (node < 0) node = stack[sp--];
+        }
     }
     if (best_tri == 0x7fffffff) { h.tri = -1; return false; }
     h.t = best_t; h.tri = best_tri; h.uvw = best_uvw;
