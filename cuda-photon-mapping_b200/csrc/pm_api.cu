@@ -67,6 +67,10 @@ struct pm_ctx {
     cudaEvent_t ev[12] = {};
     float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t launches = 0;      // kernels this context has launched
+    // photons per traced path seen by the last pm_trace_photons on this scene
+    // (sizes the next call's first batch; the output never depends on it)
+    double yield_g = 0.0, yield_c = 0.0;
+    int yield_bounces = 0;
 };
 
 namespace {
@@ -349,6 +353,8 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
     ctx->default_ior = sd->default_ior;
     std::memcpy(ctx->aabb, aabb, sizeof aabb);
     ctx->has_scene = true;
+    ctx->yield_g = ctx->yield_c = 0.0;
+    ctx->yield_bounces = 0;
     for (auto& m : ctx->maps) { m.built = false; m.n = 0; }
     return PM_OK;
 }
@@ -405,8 +411,23 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     G.n = C.n = 0;
     float power[3];
     for (int a = 0; a < 3; a++) power[a] = ctx->light_intensity[a] / (float)cg;
-    const int64_t MAX_BATCH = (int64_t)1 << 23;
-    int64_t nb = std::min<int64_t>(std::max<int64_t>(cg + cc, 4096), MAX_BATCH);
+    // Batch sizing: paths are traced in batches until both lists are full; the
+    // canonical order makes the result independent of the batch boundaries.
+    // The first batch is a pilot unless an earlier call on this scene measured
+    // the yield (photons per path); later batches aim at the remaining count.
+    const int64_t MAX_BATCH = std::max<int64_t>(4096, std::min<int64_t>((int64_t)1 << 25,
+                                                 ((int64_t)12 << 30) / (32 * (int64_t)std::max(o->max_bounces, 1))));
+    auto batch_for = [&](double yg, double yc, int64_t need_g, int64_t need_c) -> int64_t {
+        double need = 0.0;
+        if (need_g > 0) need = std::max(need, yg > 0 ? (double)need_g / yg : (double)MAX_BATCH);
+        if (need_c > 0) need = std::max(need, yc > 0 ? (double)need_c / yc : (double)MAX_BATCH);
+        return std::min<int64_t>(MAX_BATCH, std::max<int64_t>(4096, (int64_t)(need * 1.01) + 1024));
+    };
+    int64_t nb;
+    if (ctx->yield_bounces == o->max_bounces && (ctx->yield_g > 0 || cg == 0) && (ctx->yield_c > 0 || cc == 0))
+        nb = batch_for(ctx->yield_g, ctx->yield_c, cg, cc);
+    else
+        nb = std::min<int64_t>(std::max<int64_t>(cg + cc, 4096), 262144);
     int64_t fg = 0, fc = 0, p0 = 0;
     double yg = 0.0, yc = 0.0;   // photons per path so far
     int64_t got_g = 0, got_c = 0;
@@ -433,10 +454,12 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         p0 += nb;
         yg = (double)got_g / (double)p0;
         yc = (double)got_c / (double)p0;
-        double need = 0.0;
-        if (fg < cg) need = std::max(need, yg > 0 ? (double)(cg - fg) / yg : (double)MAX_BATCH);
-        if (fc < cc) need = std::max(need, yc > 0 ? (double)(cc - fc) / yc : (double)MAX_BATCH);
-        nb = std::min<int64_t>(MAX_BATCH, std::max<int64_t>(4096, (int64_t)(need * 1.02) + 1024));
+        nb = batch_for(yg, yc, cg - fg, cc - fc);
+    }
+    if (p0 > 0) {
+        ctx->yield_g = yg;
+        ctx->yield_c = yc;
+        ctx->yield_bounces = o->max_bounces;
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(cudaEventSynchronize(ctx->ev[1]));
