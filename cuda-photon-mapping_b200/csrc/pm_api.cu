@@ -89,9 +89,13 @@ int cuda_fail(pm_ctx* c, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #expr);        \
     } while (0)
 
+// Grow-only device buffer; a grown buffer gets 1/8 headroom so sizes that
+// wobble from call to call (batch sizes follow measured yields) do not
+// re-allocate every time.
 cudaError_t ensure(DevBuf& b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return cudaSuccess;
+    if (b.p) bytes += bytes / 8;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
