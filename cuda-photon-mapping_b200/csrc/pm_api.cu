@@ -50,6 +50,7 @@ struct pm_ctx {
     bool own_stream = false;
     std::string err;
     int sm_count = 148;
+    int trace_refill = 0;      // k_trace refill threshold; 0: the kernel's default
     // scene
     bool has_scene = false;
     int ntri = 0, nmodel = 0, light_model = 0, light_first = 0, light_count = 0, nca = 0;
@@ -189,6 +190,9 @@ int pm_create(pm_ctx** out, const pm_device_opts* opts) {
         ctx->own_stream = true;
     }
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    // tuning knob for the photon tracer's lane refill (1..32 lanes); the photons
+    // traced do not depend on it
+    if (const char* r = std::getenv("PM_TRACE_REFILL")) ctx->trace_refill = std::atoi(r);
     for (auto& ev : ctx->ev) {
         if (cudaEventCreate(&ev) != cudaSuccess) { pm_destroy(ctx); return PM_ERR_CUDA; }
     }
@@ -398,6 +402,7 @@ static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, Tr
     B.scan_ws = ctx->trace_ws.p;
     B.status = P<unsigned>(ctx->status);
     B.sm_count = ctx->sm_count;
+    B.refill = ctx->trace_refill;
     return PM_OK;
 }
 

@@ -122,117 +122,161 @@ __device__ __forceinline__ bool tri_test(const float4* T, V3 o, V3 d, float best
 
 __device__ __forceinline__ float safe_inv(float x) { return 1.0f / (x == 0.0f ? 1e-30f : x); }
 
-// One BVH traversal.  Returns the smallest (t, triangle) with t > 0 among the
-// triangles of models >= min_model whose model gate passes; also reports the
-// largest model index with a gated hit at exactly t == 0 (zmodel, -1 if none),
-// its lowest such triangle and that triangle's barycentrics.
+// BVH traversal state of one ray.  A query is one or two passes (see
+// intersect below); each pass returns the smallest (t, triangle) with t > 0
+// among the triangles of models >= min_model whose model gate passes.  The
+// first pass (min_model == 0) also records the largest model index with a
+// gated hit at exactly t == 0 (zmodel, -1 if none), its lowest such triangle
+// and that triangle's barycentrics; the second pass keeps that record and
+// ignores hits at t == 0 (every one of them belongs to a model <= zmodel).
 //
-// While-while traversal with postponed leaves (Aila & Laine, "Understanding the
-// efficiency of ray traversal on GPUs", HPG 2009): lanes descend interior
+// Traversal is while-while with postponed leaves (Aila & Laine, "Understanding
+// the efficiency of ray traversal on GPUs", HPG 2009): lanes descend interior
 // nodes until every lane of the warp holds a leaf, then test triangles
-// together.  Each interior node carries both children's boxes.
-static __device__ __noinline__ bool traverse(const DevScene& S, V3 o, V3 d, int min_model, Hit& h, int& zmodel,
-                                             int& ztri, V3& zuvw) {
-    constexpr int SENTINEL = 0x76543210;
-    float best_t = __int_as_float(0x7f800000);
-    int best_tri = 0x7fffffff;
-    V3 best_uvw = v3(0.f, 0.f, 0.f);
-    zmodel = -1;
-    ztri = 0x7fffffff;
-    unsigned long long gate_known = 0ull, gate_pass = 0ull;
-    const float ix = safe_inv(d.x), iy = safe_inv(d.y), iz = safe_inv(d.z);
-    const float ox = o.x * ix, oy = o.y * iy, oz = o.z * iz;
-    int stack[64];
-    int sp = 0;
-    stack[0] = SENTINEL;
-    int node = 0;
-    int leaf = 0;
-    while (node != SENTINEL) {
-        while ((unsigned)node < (unsigned)SENTINEL) {
-            const float4* N = S.nodes + 4 * (size_t)node;
-            const float4 a0 = __ldg(N), b0 = __ldg(N + 1), a1 = __ldg(N + 2), b1 = __ldg(N + 3);
-            float t0x = a0.x * ix - ox, t1x = b0.x * ix - ox;
-            float t0y = a0.y * iy - oy, t1y = b0.y * iy - oy;
-            float t0z = a0.z * iz - oz, t1z = b0.z * iz - oz;
-            const float c0min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
-            const float c0max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
-            t0x = a1.x * ix - ox; t1x = b1.x * ix - ox;
-            t0y = a1.y * iy - oy; t1y = b1.y * iy - oy;
-            t0z = a1.z * iz - oz; t1z = b1.z * iz - oz;
-            const float c1min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
-            const float c1max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
-            const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
-            if (!h0 && !h1) {
-                node = stack[sp--];
-            } else {
-                const int r0 = __float_as_int(a0.w), r1 = __float_as_int(a1.w);
-                node = h0 ? r0 : r1;
-                if (h0 && h1) {
-                    int other = r1;
-                    if (c1min < c0min) { node = r1; other = r0; }
-                    if (sp < 63) stack[++sp] = other;
-                }
-            }
-            if (node < 0 && leaf >= 0) {   // first leaf: postpone it, keep descending
-                leaf = node;
-                node = stack[sp--];
-            }
-            if (!__any_sync(__activemask(), leaf >= 0)) break;   // every lane holds a leaf
-        }
-        while (leaf < 0) {
-            const int packed = ~leaf;
-            const int first = packed >> 8, count = packed & 255;
-            for (int i = 0; i < count; i++) {
-                const int tri = __ldg(S.prim + first + i);
-                const float4* T = S.tri + 5 * (size_t)tri;
-                const int m = __float_as_int(__ldg(&T[2].w));
-                if (m < min_model) continue;
-                float t; V3 uvw;
-                if (!tri_test(T, o, d, best_t, tri, best_tri, t, uvw)) continue;
-                const bool zero = t == 0.0f;
-                if (zero && (m < zmodel || (m == zmodel && tri > ztri))) continue;
-                bool pass;
-                if (m < 64) {
-                    const unsigned long long bit = 1ull << m;
-                    if (!(gate_known & bit)) {
-                        gate_known |= bit;
-                        if (model_gate(S.maabb + 6 * m, o, d)) gate_pass |= bit;
-                    }
-                    pass = (gate_pass & bit) != 0ull;
-                } else {
-                    pass = model_gate(S.maabb + 6 * m, o, d);
-                }
-                if (!pass) continue;
-                if (zero) { zmodel = m; ztri = tri; zuvw = uvw; }
-                else { best_t = t; best_tri = tri; best_uvw = uvw; }
-            }
-            leaf = node;                    // another postponed leaf: process it as well
-            if (node < 0) node = stack[sp--];
-        }
-    }
-    if (best_tri == 0x7fffffff) { h.tri = -1; return false; }
-    h.t = best_t; h.tri = best_tri; h.uvw = best_uvw;
-    return true;
-}
+// together.  Each interior node carries both children's boxes.  The state is
+// resumable: trav_step runs one descend + leaf round, so a caller can stop a
+// warp's traversal between rounds and give finished lanes new rays.
+constexpr int TRAV_SENTINEL = 0x76543210;
+constexpr int TRAV_STACK = 64;
+constexpr int TRAV_NONE = 0x7fffffff;
 
-// Closest hit with the reference's model-loop semantics (PhotonTracing.cu:187-198,
-// Raytracer.cuh:73-84): a running "intersection" that starts at 0 means "no hit
-// yet", so a model whose nearest hit is at exactly t = 0 is taken only when no
-// later model is hit at all.  Hence: with z the last model hit at t = 0, the
-// answer is the nearest (t, triangle) hit among models after z, else z's hit.
-static __device__ __forceinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit& h) {
+struct Trav {
+    float ix, iy, iz, ox, oy, oz;      // slab terms: 1/d and o/d
+    float best_t;
+    int best_tri;
+    V3 best_uvw;
     int zmodel, ztri;
     V3 zuvw;
-    bool hit = traverse(S, o, d, 0, h, zmodel, ztri, zuvw);
-    if (zmodel < 0) return hit;
-    if (hit && hit_model_raw(S, h.tri) > zmodel) return true;
-    int z2, t2;
-    V3 u2;
-    if (traverse(S, o, d, zmodel + 1, h, z2, t2, u2)) return true;
-    h.t = 0.0f;
-    h.tri = ztri;
-    h.uvw = zuvw;
-    return true;
+    unsigned long long gate_known, gate_pass;
+    int node, leaf, sp, min_model;
+};
+
+__device__ __forceinline__ void trav_pass(Trav& T, int min_model, int* stack) {
+    T.best_t = __int_as_float(0x7f800000);
+    T.best_tri = TRAV_NONE;
+    T.best_uvw = v3(0.f, 0.f, 0.f);
+    T.min_model = min_model;
+    T.node = 0;
+    T.leaf = 0;
+    T.sp = 0;
+    stack[0] = TRAV_SENTINEL;
+}
+
+__device__ __forceinline__ void trav_init(Trav& T, V3 o, V3 d, int* stack) {
+    T.ix = safe_inv(d.x); T.iy = safe_inv(d.y); T.iz = safe_inv(d.z);
+    T.ox = o.x * T.ix; T.oy = o.y * T.iy; T.oz = o.z * T.iz;
+    T.zmodel = -1;
+    T.ztri = TRAV_NONE;
+    T.zuvw = v3(0.f, 0.f, 0.f);
+    T.gate_known = 0ull;
+    T.gate_pass = 0ull;
+    trav_pass(T, 0, stack);
+}
+
+// One round: descend until this lane holds a leaf (or every active lane does),
+// then test the held leaves.  Returns true when the pass is complete.
+__device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, int* stack) {
+    int node = T.node, leaf = T.leaf, sp = T.sp;
+    const float ix = T.ix, iy = T.iy, iz = T.iz, ox = T.ox, oy = T.oy, oz = T.oz;
+    while ((unsigned)node < (unsigned)TRAV_SENTINEL) {
+        const float4* N = S.nodes + 4 * (size_t)node;
+        const float4 a0 = __ldg(N), b0 = __ldg(N + 1), a1 = __ldg(N + 2), b1 = __ldg(N + 3);
+        const float best_t = T.best_t;
+        float t0x = a0.x * ix - ox, t1x = b0.x * ix - ox;
+        float t0y = a0.y * iy - oy, t1y = b0.y * iy - oy;
+        float t0z = a0.z * iz - oz, t1z = b0.z * iz - oz;
+        const float c0min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+        const float c0max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
+        t0x = a1.x * ix - ox; t1x = b1.x * ix - ox;
+        t0y = a1.y * iy - oy; t1y = b1.y * iy - oy;
+        t0z = a1.z * iz - oz; t1z = b1.z * iz - oz;
+        const float c1min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+        const float c1max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
+        const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
+        if (!h0 && !h1) {
+            node = stack[sp--];
+        } else {
+            const int r0 = __float_as_int(a0.w), r1 = __float_as_int(a1.w);
+            node = h0 ? r0 : r1;
+            if (h0 && h1) {
+                int other = r1;
+                if (c1min < c0min) { node = r1; other = r0; }
+                if (sp < TRAV_STACK - 1) stack[++sp] = other;
+            }
+        }
+        if (node < 0 && leaf >= 0) {   // first leaf: postpone it, keep descending
+            leaf = node;
+            node = stack[sp--];
+        }
+        if (!__any_sync(__activemask(), leaf >= 0)) break;   // every lane holds a leaf
+    }
+    while (leaf < 0) {
+        const int packed = ~leaf;
+        const int first = packed >> 8, count = packed & 255;
+        for (int i = 0; i < count; i++) {
+            const int tri = __ldg(S.prim + first + i);
+            const float4* Q = S.tri + 5 * (size_t)tri;
+            const int m = __float_as_int(__ldg(&Q[2].w));
+            if (m < T.min_model) continue;
+            float t; V3 uvw;
+            if (!tri_test(Q, o, d, T.best_t, tri, T.best_tri, t, uvw)) continue;
+            const bool zero = t == 0.0f;
+            if (zero && (T.min_model != 0 || m < T.zmodel || (m == T.zmodel && tri > T.ztri))) continue;
+            bool pass;
+            if (m < 64) {
+                const unsigned long long bit = 1ull << m;
+                if (!(T.gate_known & bit)) {
+                    T.gate_known |= bit;
+                    if (model_gate(S.maabb + 6 * m, o, d)) T.gate_pass |= bit;
+                }
+                pass = (T.gate_pass & bit) != 0ull;
+            } else {
+                pass = model_gate(S.maabb + 6 * m, o, d);
+            }
+            if (!pass) continue;
+            if (zero) { T.zmodel = m; T.ztri = tri; T.zuvw = uvw; }
+            else { T.best_t = t; T.best_tri = tri; T.best_uvw = uvw; }
+        }
+        leaf = node;                    // another postponed leaf: process it as well
+        if (node < 0) node = stack[sp--];
+    }
+    T.node = node; T.leaf = leaf; T.sp = sp;
+    return node == TRAV_SENTINEL;
+}
+
+// After a completed pass, apply the reference's model-loop semantics
+// (PhotonTracing.cu:187-198, Raytracer.cuh:73-84): a running "intersection"
+// that starts at 0 means "no hit yet", so a model whose nearest hit is at
+// exactly t = 0 is taken only when no later model is hit at all.  With z the
+// last model hit at t = 0, the answer is the nearest (t, triangle) hit among
+// models after z, else z's hit.  Returns TRAV_AGAIN after starting the second
+// pass (models > z), TRAV_HIT with h filled, or TRAV_MISS.
+enum { TRAV_HIT = 0, TRAV_MISS = 1, TRAV_AGAIN = 2 };
+__device__ __forceinline__ int trav_resolve(const DevScene& S, Trav& T, Hit& h, int* stack) {
+    if (T.best_tri != TRAV_NONE &&
+        (T.min_model != 0 || T.zmodel < 0 || hit_model_raw(S, T.best_tri) > T.zmodel)) {
+        h.t = T.best_t; h.tri = T.best_tri; h.uvw = T.best_uvw;
+        return TRAV_HIT;
+    }
+    if (T.zmodel < 0) return TRAV_MISS;
+    if (T.min_model == 0) {
+        trav_pass(T, T.zmodel + 1, stack);
+        return TRAV_AGAIN;
+    }
+    h.t = 0.0f; h.tri = T.ztri; h.uvw = T.zuvw;
+    return TRAV_HIT;
+}
+
+// Closest hit of one ray, both passes run to completion.
+static __device__ __noinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit& h) {
+    int stack[TRAV_STACK];
+    Trav T;
+    trav_init(T, o, d, stack);
+    while (true) {
+        while (!trav_step(S, T, o, d, stack)) {}
+        const int r = trav_resolve(S, T, h, stack);
+        if (r != TRAV_AGAIN) return r == TRAV_HIT;
+    }
 }
 
 // interpolated vertex normal, reciprocal-normalised (Model.cuh:436-443)

@@ -28,7 +28,8 @@ namespace {
 
 constexpr int TRACE_THREADS = 128;
 constexpr int MAX_STACK = 32;
-constexpr int REJECT_LIMIT = 1 << 16;   // emission rejection loop bound (acceptance ~1/2 on valid lights)
+constexpr int REJECT_LIMIT = 1 << 16;
+constexpr int TRACE_REFILL = 8;          // default for KParams::refill   // emission rejection loop bound (acceptance ~1/2 on valid lights)
 
 enum { DIF = 0, SPEC = 1, ABSORB = 2, REFR = 3, NONE = 4 };
 
@@ -55,6 +56,7 @@ struct KParams {
     uint32_t* cnt_g;
     uint32_t* cnt_c;
     unsigned* status;
+    int refill;             // lanes with a finished query that end a warp's traversal loop
 };
 
 // light point + cosine-weighted direction by rejection (PhotonTracing.cu:345-369)
@@ -126,11 +128,10 @@ __device__ __forceinline__ float schlick(float cosNL, float n1, float n2) {
     return f0 + (1.f - f0) * c5;
 }
 
-// one bounce of lane L (PhotonTracing.cu:278-326); returns false when the path ends
-__device__ __forceinline__ bool bounce(const KParams& P, Lane& L, float* sior, int* sid, int64_t j) {
+// the surface interaction of one bounce of lane L at hit h (PhotonTracing.cu:278-326);
+// returns false when the path ends
+__device__ __forceinline__ bool shade(const KParams& P, Lane& L, const Hit& h, float* sior, int* sid, int64_t j) {
     const DevScene& S = P.S;
-    Hit h;
-    if (!intersect(S, L.ray.o, L.ray.d, h)) return false;
     const int model = hit_model(S, h.tri);
     const Material m = load_mat(S, model);
     V3 n = shading_normal(S, h);
@@ -205,40 +206,76 @@ __device__ __forceinline__ bool bounce(const KParams& P, Lane& L, float* sior, i
     return true;
 }
 
+// Lane states of k_trace.
+enum { L_IDLE = 0, L_RAY = 1, L_TRACE = 2, L_HIT = 3, L_DONE = 4 };
+
+// Persistent photon tracer.  Each lane runs a small state machine:
+//   IDLE  -> takes the next path of the batch (RAY) or finds none (DONE);
+//   RAY   -> starts the traversal of its current ray (TRACE);
+//   TRACE -> traversal rounds; a completed query moves it to HIT;
+//   HIT   -> the second pass of the t == 0 rule (TRACE), or the surface
+//            interaction: the next ray (RAY) or the end of the path (IDLE).
+// A warp leaves its traversal loop as soon as P.refill of its lanes have
+// finished their query, serves those lanes, and resumes: lanes whose ray is
+// long (rays grazing the heightfield cross hundreds of leaves) keep their
+// traversal state while the others get new rays, instead of holding the whole
+// warp until the longest ray of a bounce is done.
 __global__ void __launch_bounds__(TRACE_THREADS)
 k_trace(KParams P) {
     const int lane = threadIdx.x & 31;
     Lane L;
+    Trav T;
+    int stack[TRAV_STACK];
     float sior[MAX_STACK];
     int sid[MAX_STACK];
-    int64_t j = -1;          // batch-local path index of this lane, -1: idle
-    bool done = false;
+    int64_t j = -1;          // batch-local path index of this lane
+    int state = L_IDLE;
     while (true) {
-        bool need = !done && j < 0;
-        unsigned m = __ballot_sync(0xffffffffu, need);
+        const bool need = state == L_IDLE;
+        const unsigned m = __ballot_sync(0xffffffffu, need);
         if (m) {
-            int leader = __ffs(m) - 1;
+            const int leader = __ffs(m) - 1;
             unsigned long long base = 0;
             if (lane == leader) base = atomicAdd(P.counter, (unsigned long long)__popc(m));
             base = __shfl_sync(0xffffffffu, base, leader);
             if (need) {
-                unsigned long long mine = base + (unsigned long long)__popc(m & lanemask_lt());
+                const unsigned long long mine = base + (unsigned long long)__popc(m & lanemask_lt());
                 if ((int64_t)mine < P.npaths) {
                     j = (int64_t)mine;
                     start_path(P, L, P.p0 + j);
+                    state = L_RAY;
                 } else {
-                    done = true;
+                    state = L_DONE;
                 }
             }
         }
-        if (__all_sync(0xffffffffu, done)) break;
-        if (j >= 0) {
-            bool alive = bounce(P, L, sior, sid, j);
-            L.bounce++;
-            if (!alive || L.bounce > P.max_bounces - 1) {
-                P.cnt_g[j] = (uint32_t)L.ng;
-                P.cnt_c[j] = (uint32_t)L.nc;
-                j = -1;
+        if (__all_sync(0xffffffffu, state == L_DONE)) break;
+        if (state == L_RAY) {
+            trav_init(T, L.ray.o, L.ray.d, stack);
+            state = L_TRACE;
+        }
+        while (true) {
+            const bool tr = state == L_TRACE;
+            if (!__any_sync(0xffffffffu, tr)) break;
+            if (__popc(__ballot_sync(0xffffffffu, state == L_HIT)) >= P.refill) break;
+            if (tr && trav_step(P.S, T, L.ray.o, L.ray.d, stack)) state = L_HIT;
+        }
+        if (state == L_HIT) {
+            Hit h;
+            const int r = trav_resolve(P.S, T, h, stack);
+            if (r == TRAV_AGAIN) {
+                state = L_TRACE;
+            } else {
+                const bool alive = r == TRAV_HIT && shade(P, L, h, sior, sid, j);
+                L.bounce++;
+                if (!alive || L.bounce > P.max_bounces - 1) {
+                    P.cnt_g[j] = (uint32_t)L.ng;
+                    P.cnt_c[j] = (uint32_t)L.nc;
+                    j = -1;
+                    state = L_IDLE;
+                } else {
+                    state = L_RAY;
+                }
             }
         }
     }
@@ -288,6 +325,7 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
     P.stage_pos = B.stage_pos; P.stage_dir = B.stage_dir;
     P.cnt_g = B.cnt_g; P.cnt_c = B.cnt_c;
     P.status = B.status;
+    P.refill = B.refill > 0 ? std::min(B.refill, 32) : TRACE_REFILL;
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace, TRACE_THREADS, 0)) != cudaSuccess) return e;
     int64_t want = (B.npaths + TRACE_THREADS - 1) / TRACE_THREADS;

@@ -25,6 +25,7 @@ struct TraceBatch {
     void* scan_ws;
     unsigned* status;
     int sm_count;
+    int refill;               // k_trace refill threshold in lanes (1..32); 0: the default
 };
 
 struct PhotonList {
