@@ -265,7 +265,7 @@ def run_ours(args):
     hbm, src = peaks()
     line = None
     if rank == 0:
-        nreq = W * H   # lower bound: one gather per primary hit pixel
+        nreq = ctx.render_requests()   # kNN queries of the frame's gather
         gather_bytes = nreq * (w["k"] * 40 + 44)
         gather_ms = stages[3]
         achieved = gather_bytes / (gather_ms * 1e-3) / 1e9 if gather_ms > 0 else 0.0
@@ -288,7 +288,7 @@ def run_ours(args):
                           "resolve": stages[4]},
             "roofline": {"kernel": "k_gather (kNN + estimate)", "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": None,
-                         "algorithmic_bytes_per_launch": gather_bytes},
+                         "algorithmic_bytes_per_launch": gather_bytes, "queries_per_launch": nreq},
             "e2e": {"value": world * w["photons"] / (e2e_ms * 1e-3) / 1e6, "unit": "Mphotons/s",
                     "ms_per_step": e2e_ms, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3},
             "gpu_launches": launches,

@@ -68,6 +68,7 @@ struct pm_ctx {
     cudaEvent_t ev[12] = {};
     float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t launches = 0;      // kernels this context has launched
+    int64_t last_requests = 0; // gather requests of the last pm_render
     // photons per traced path seen by the last pm_trace_photons on this scene
     // (sizes the next call's first batch; the output never depends on it)
     double yield_g = 0.0, yield_c = 0.0;
@@ -244,6 +245,12 @@ int pm_status(pm_ctx* ctx, uint32_t* out_bits) {
 int pm_launch_count(pm_ctx* ctx, int64_t* out) {
     if (!ctx || !out) return PM_ERR_INVALID;
     *out = ctx->launches;
+    return PM_OK;
+}
+
+int pm_render_requests(pm_ctx* ctx, int64_t* out) {
+    if (!ctx || !out) return PM_ERR_INVALID;
+    *out = ctx->last_requests;
     return PM_OK;
 }
 
@@ -790,6 +797,7 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_
     CK(cudaMemcpyAsync(&nreq, R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     nreq = std::min<unsigned long long>(nreq, (unsigned long long)cap);
+    ctx->last_requests = (int64_t)nreq;
     GatherQueries Q{};
     Q.n = (int64_t)nreq; Q.pos4 = R.a; Q.nrm4 = R.b; Q.flag_mask = 1u;
     GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};

@@ -34,11 +34,15 @@ namespace {
 
 constexpr int WARPS = 8;   // queries per block
 
+constexpr int QCAP = 64;   // queued sub-cells per warp
+
 template <int UCAP>
 struct WarpStore {
     unsigned long long key[UCAP];
     uint32_t slot[UCAP];
     uint32_t hist[256];   // radix-select histogram; doubles as 32 x u64 scratch
+    uint32_t qa[QCAP];    // queued sub-cells: first photon, photon count
+    uint32_t qc[QCAP];
 };
 
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
@@ -64,30 +68,51 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, 
     return v;
 }
 
-// the need-th smallest (1-based) of U.key[0, n); need <= n
+// the need-th smallest (1-based) of U.key[0, n); need <= n; keys are unique.
+// MSB-first radix select: the bits above the highest bit in which two keys
+// differ are skipped, each round histograms the next (up to) 8 bits of the keys
+// still in play (lanes with equal digits add once, __match_any_sync), and the
+// round that leaves <= 32 keys finishes with a 32-lane bitonic sort.
 template <int UCAP>
 __device__ unsigned long long select_kth(WarpStore<UCAP>& U, int n, int need, int lane) {
-    unsigned long long prefix = 0ull, mask = 0ull;
     unsigned long long* scratch = reinterpret_cast<unsigned long long*>(U.hist);
-    for (int shift = 56; shift >= 0; shift -= 8) {
+    const unsigned long long k0 = U.key[0];
+    unsigned long long diff = 0ull;
+    for (int i = lane; i < n; i += 32) diff |= U.key[i] ^ k0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) diff |= shfl_xor_u64(diff, o);
+    if (diff == 0ull) return k0;
+    int hi = 64 - __clzll((long long)diff);          // bits [hi, 64) are common to all keys
+    unsigned long long mask = hi == 64 ? 0ull : ~0ull << hi;
+    unsigned long long prefix = k0 & mask;
+    while (true) {
+        const int shift = hi > 8 ? hi - 8 : 0;
+        const unsigned dmask = (1u << (hi - shift)) - 1u;
 #pragma unroll
         for (int b = 0; b < 8; b++) U.hist[8 * lane + b] = 0u;
         __syncwarp();
-        for (int i = lane; i < n; i += 32) {
-            unsigned long long kk = U.key[i];
-            if ((kk & mask) == prefix) atomicAdd(&U.hist[(unsigned)(kk >> shift) & 255u], 1u);
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            const unsigned long long kk = i < n ? U.key[i] : 0ull;
+            const bool m = i < n && (kk & mask) == prefix;
+            const unsigned d = (unsigned)(kk >> shift) & dmask;
+            const unsigned act = __ballot_sync(0xffffffffu, m);
+            if (m) {
+                const unsigned peers = __match_any_sync(act, d);
+                if ((peers & lanemask_lt()) == 0u) atomicAdd(&U.hist[d], (uint32_t)__popc(peers));
+            }
         }
         __syncwarp();
-        uint32_t c[8], s = 0;
+        uint32_t c[8], sum = 0;
 #pragma unroll
-        for (int b = 0; b < 8; b++) { c[b] = U.hist[8 * lane + b]; s += c[b]; }
-        uint32_t incl = s;
+        for (int b = 0; b < 8; b++) { c[b] = U.hist[8 * lane + b]; sum += c[b]; }
+        uint32_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        const uint32_t excl = incl - s;
+        const uint32_t excl = incl - sum;
         const unsigned own = __ballot_sync(0xffffffffu, excl < (uint32_t)need && (uint32_t)need <= incl);
         const int owner = own ? __ffs(own) - 1 : 0;
         int bin = 0;
@@ -105,9 +130,10 @@ __device__ unsigned long long select_kth(WarpStore<UCAP>& U, int n, int need, in
         cnt = __shfl_sync(0xffffffffu, cnt, owner);
         need -= (int)before;
         prefix |= (unsigned long long)bin << shift;
-        mask |= 0xffull << shift;
+        mask |= (unsigned long long)dmask << shift;
+        hi = shift;
         __syncwarp();
-        if (cnt <= 32u) {
+        if (cnt <= 32u || hi == 0) {
             // the few keys under this prefix: gather one per lane, sort, pick
             int got = 0;
             for (int base = 0; base < n; base += 32) {
@@ -125,7 +151,6 @@ __device__ unsigned long long select_kth(WarpStore<UCAP>& U, int n, int need, in
             return shfl_u64(v, need - 1);
         }
     }
-    return prefix;
 }
 
 template <int UCAP>
@@ -157,6 +182,43 @@ __device__ __forceinline__ float axis_gap(float q, float lo, float hi, bool open
     return fmaxf(fmaxf(a, b), 0.f);
 }
 
+// u / d for 0 <= u < 2^22, d > 0: float estimate, one correction step
+__device__ __forceinline__ int small_div(int u, int d, float inv) {
+    int q = (int)(((float)u + 0.5f) * inv);
+    const int r = u - q * d;
+    if (r < 0) q--;
+    else if (r >= d) q++;
+    return q;
+}
+
+// Offsets of the t-th sub-cell of the shell at Chebyshev distance R around a
+// sub-cell (side = 2R + 1; 2 side^2 + 4 (side - 1)(side - 2) members): the two
+// full z faces, then the perimeter of each inner z layer.
+__device__ __forceinline__ void shell_member(int t, int R, int side, float inv_side, float inv_per, int& dx,
+                                             int& dy, int& dz) {
+    const int sq = side * side;
+    int x, y;
+    if (t < 2 * sq) {
+        const bool lo = t < sq;
+        dz = lo ? -R : R;
+        const int u = lo ? t : t - sq;
+        y = small_div(u, side, inv_side);
+        x = u - y * side;
+    } else {
+        const int e = side - 1, per = 4 * e;
+        const int u = t - 2 * sq;
+        const int layer = small_div(u, per, inv_per);
+        const int p = u - layer * per;
+        dz = -R + 1 + layer;
+        if (p < e) { x = p; y = 0; }
+        else if (p < 2 * e) { x = e; y = p - e; }
+        else if (p < 3 * e) { x = 3 * e - p; y = e; }
+        else { x = 0; y = 4 * e - p; }
+    }
+    dx = x - R;
+    dy = y - R;
+}
+
 template <int UCAP>
 struct WarpWalk {
     const GatherGrid& G;
@@ -165,11 +227,12 @@ struct WarpWalk {
     float r;
     int k, lane;
     int n;                    // keys in the store
+    int qn;                   // queued sub-cells
     unsigned long long T;     // a candidate enters when its key < T
     float lim, lim2;          // distance bound for pruning; squared pre-filter bound
 
     __device__ WarpWalk(const GatherGrid& g, WarpStore<UCAP>& u, V3 qq, float rr, int kk, int ln)
-        : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f) {}
+        : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), qn(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f) {}
 
     // keep the k best keys of the store, tighten the threshold
     __device__ void merge() {
@@ -203,92 +266,152 @@ struct WarpWalk {
         __syncwarp();
     }
 
-    // photons [a, b) of one sub-cell
-    __device__ void scan(uint32_t a, uint32_t b) {
-        for (uint32_t base = a; base < b; base += 32) {
-            const uint32_t j = base + lane;
-            bool ok = false;
-            unsigned long long kk = 0ull;
-            if (j < b) {
-                float4 p = __ldg(G.gpos + j);
-                float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
-                float s = dx * dx + dy * dy + dz * dz;
-                if (s <= lim2) {
-                    float d = sqrtf(s);
-                    if (d <= r) {
-                        kk = ((unsigned long long)__float_as_uint(d) << 32) | __float_as_uint(p.w);
-                        ok = kk < T;
-                    }
+    // test photon slot j (when valid); survivors enter the store
+    __device__ __forceinline__ void consider(float4 p, uint32_t j, bool valid) {
+        bool ok = false;
+        unsigned long long kk = 0ull;
+        if (valid) {
+            float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+            float s = dx * dx + dy * dy + dz * dz;
+            if (s <= lim2) {
+                float d = sqrtf(s);
+                if (d <= r) {
+                    kk = ((unsigned long long)__float_as_uint(d) << 32) | __float_as_uint(p.w);
+                    ok = kk < T;
                 }
             }
-            unsigned m = __ballot_sync(0xffffffffu, ok);
-            if (m) {
-                if (ok) {
-                    int pos = n + __popc(m & lanemask_lt());
-                    U.key[pos] = kk;
-                    U.slot[pos] = j;
-                }
-                n += __popc(m);
-                if (n + 32 > UCAP) merge();
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (m) {
+            if (ok) {
+                const int pos = n + __popc(m & lanemask_lt());
+                U.key[pos] = kk;
+                U.slot[pos] = j;
             }
+            n += __popc(m);
+            if (n + 32 > UCAP) merge();
         }
     }
 
-    __device__ void scan_key(uint32_t key) { scan(__ldg(G.key_starts + key), __ldg(G.key_starts + key + 1)); }
+    // Scan the photons of queued sub-cells [0, cnt) (cnt <= 32) as one list:
+    // lane l takes list entries base + l, so one round of loads covers 32
+    // photons whichever sub-cells they belong to.
+    __device__ void drain(int cnt) {
+        __syncwarp();
+        uint32_t a = 0u, c = 0u;
+        if (lane < cnt) { a = U.qa[lane]; c = U.qc[lane]; }
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t excl = incl - c;
+        for (uint32_t base = 0; base < total; base += 64) {
+            const uint32_t o0 = base + lane, o1 = o0 + 32;
+            int m0 = 0, m1 = 0;   // the last queued sub-cell whose first list entry is <= o
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1) {
+                const uint32_t e0 = __shfl_sync(0xffffffffu, excl, m0 + st);
+                const uint32_t e1 = __shfl_sync(0xffffffffu, excl, m1 + st);
+                if (e0 <= o0) m0 += st;
+                if (e1 <= o1) m1 += st;
+            }
+            const uint32_t j0 = __shfl_sync(0xffffffffu, a, m0) + (o0 - __shfl_sync(0xffffffffu, excl, m0));
+            const uint32_t j1 = __shfl_sync(0xffffffffu, a, m1) + (o1 - __shfl_sync(0xffffffffu, excl, m1));
+            const bool v0 = o0 < total, v1 = o1 < total;
+            const float4 p0 = v0 ? __ldg(G.gpos + j0) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 p1 = v1 ? __ldg(G.gpos + j1) : make_float4(0.f, 0.f, 0.f, 0.f);
+            consider(p0, j0, v0);
+            consider(p1, j1, v1);
+        }
+        __syncwarp();
+    }
 
-    // Nearest-first walk: rings of sub-cells at Chebyshev distance R = 1, 2, ...
-    // from the query's sub-cell (global sub-cell coordinates), restricted to the
-    // sub-cells of the reference's cube of cells [lo, hi].  Lanes test 32 ring
-    // members at a time (box distance, non-empty range); the survivors are
-    // scanned one after another.  A ring whose nearest possible point is
-    // farther than the current bound ends the walk.
-    __device__ void rings(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz) {
-        const int S = G.S;
+    // append this lane's sub-cell (when ok) to the queue; drain 32 when it holds 32
+    __device__ __forceinline__ void enqueue(bool ok, uint32_t a, uint32_t c) {
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const int pos = qn + __popc(m & lanemask_lt());
+            U.qa[pos] = a;
+            U.qc[pos] = c;
+        }
+        qn += __popc(m);
+        if (qn >= 32) {
+            drain(32);
+            const int rest = qn - 32;
+            uint32_t ra = 0u, rc = 0u;
+            if (lane < rest) { ra = U.qa[32 + lane]; rc = U.qc[32 + lane]; }
+            __syncwarp();
+            if (lane < rest) { U.qa[lane] = ra; U.qc[lane] = rc; }
+            __syncwarp();
+            qn = rest;
+        }
+    }
+
+    __device__ __forceinline__ void flush() {
+        if (qn > 0) drain(qn);
+        qn = 0;
+    }
+
+    // Nearest-first walk over the sub-cells of the reference's cube of cells
+    // [lo, hi] (global sub-cell coordinates): the query's sub-cell, then shells
+    // at Chebyshev distance R = 1, 2, ...  Lanes test 32 shell members at a
+    // time (box distance against the current bound, non-empty photon range);
+    // the survivors are queued and scanned together.  After each shell the
+    // store is cut to the k best, tightening the bound; a shell whose nearest
+    // possible point is farther than the bound ends the walk.
+    __device__ void walk(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz) {
+        const int S = G.S, sh = __ffs(S) - 1;
         const float sc = G.cell / (float)S, pad = G.cell * 1e-4f;
         const float m = 1.f + 1e-5f;
         const int GX = G.gx * S - 1, GY = G.gy * S - 1, GZ = G.gz * S - 1;
+        const uint32_t S3 = (uint32_t)(S * S * S);
+        auto key_of = [&](int X, int Y, int Z) -> uint32_t {
+            const uint32_t cellid = (uint32_t)((X >> sh) + (Y >> sh) * G.gx + (Z >> sh) * G.gx * G.gy);
+            return cellid * S3 + (uint32_t)((X & (S - 1)) + S * ((Y & (S - 1)) + S * (Z & (S - 1))));
+        };
+        {   // the query's own sub-cell
+            const uint32_t key = key_of(X0, Y0, Z0);
+            uint32_t a = 0u, b = 0u;
+            if (lane == 0) { a = __ldg(G.key_starts + key); b = __ldg(G.key_starts + key + 1); }
+            enqueue(lane == 0 && b > a, a, b - a);
+        }
         const int Rmax = max(max(max(X0 - lx, hx - X0), max(Y0 - ly, hy - Y0)), max(Z0 - lz, hz - Z0));
         for (int R = 1; R <= Rmax; R++) {
             if ((float)(R - 1) * sc - pad > lim * m) break;
             const int side = 2 * R + 1;
-            const int total = side * side * side;
+            const int total = 2 * side * side + 4 * (side - 1) * (side - 2);
+            const float inv_side = 1.0f / (float)side, inv_per = 1.0f / (float)(4 * (side - 1));
             for (int base = 0; base < total; base += 32) {
                 const int t = base + lane;
                 bool ok = false;
                 uint32_t a = 0, b = 0;
-                float dist2 = 0.f;
                 if (t < total) {
-                    const int dx = t % side - R, dy = (t / side) % side - R, dz = t / (side * side) - R;
+                    int dx, dy, dz;
+                    shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
                     const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
-                    if (max(max(abs(dx), abs(dy)), abs(dz)) == R && X >= lx && X <= hx && Y >= ly && Y <= hy &&
-                        Z >= lz && Z <= hz) {
+                    if (X >= lx && X <= hx && Y >= ly && Y <= hy && Z >= lz && Z <= hz) {
                         float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
                         float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
                         float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
-                        dist2 = ax * ax + ay * ay + az * az;
+                        const float dist2 = ax * ax + ay * ay + az * az;
                         const float L = lim * m;
                         if (dist2 <= L * L) {
-                            const uint32_t cellid = (uint32_t)(X / S + (Y / S) * G.gx + (Z / S) * G.gx * G.gy);
-                            const uint32_t key = cellid * (uint32_t)(S * S * S) +
-                                                 (uint32_t)(X % S + S * (Y % S + S * (Z % S)));
+                            const uint32_t key = key_of(X, Y, Z);
                             a = __ldg(G.key_starts + key);
                             b = __ldg(G.key_starts + key + 1);
                             ok = b > a;
                         }
                     }
                 }
-                unsigned todo = __ballot_sync(0xffffffffu, ok);
-                while (todo) {
-                    const int src = __ffs(todo) - 1;
-                    todo &= todo - 1;
-                    const uint32_t sa = __shfl_sync(0xffffffffu, a, src);
-                    const uint32_t sb = __shfl_sync(0xffffffffu, b, src);
-                    const float d2 = __shfl_sync(0xffffffffu, dist2, src);
-                    const float L = lim * m;
-                    if (d2 <= L * L) scan(sa, sb);
-                }
+                enqueue(ok, a, b - a);
             }
+            flush();
+            if (n > k) merge();
         }
+        flush();
     }
 };
 
@@ -326,17 +449,13 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
     locate(q.y, G.mn[1], G.cell, G.gy, G.S, hy, sy);
     locate(q.z, G.mn[2], G.cell, G.gz, G.S, hz, sz);
     const int S = G.S;
-    const uint32_t home_key = (uint32_t)(hx + hy * G.gx + hz * G.gx * G.gy) * (uint32_t)(S * S * S) +
-                              (uint32_t)(sx + S * (sy + S * sz));
-    // the query's own sub-cell first, then rings of sub-cells outwards, within the
+    // the query's own sub-cell first, then shells of sub-cells outwards, within the
     // cube of cells of half width ceil(r / cell) (CudaPhotonMapping/PhotonGrid.cu:257-284)
-    W.scan_key(home_key);
-    if (W.n >= k) W.merge();
     const int rc = (int)ceilf(r / G.cell);
     const int x0 = max(0, hx - rc), y0 = max(0, hy - rc), z0 = max(0, hz - rc);
     const int x1 = min(G.gx - 1, hx + rc), y1 = min(G.gy - 1, hy + rc), z1 = min(G.gz - 1, hz + rc);
-    W.rings(hx * S + sx, hy * S + sy, hz * S + sz, x0 * S, y0 * S, z0 * S, x1 * S + S - 1, y1 * S + S - 1,
-            z1 * S + S - 1);
+    W.walk(hx * S + sx, hy * S + sy, hz * S + sz, x0 * S, y0 * S, z0 * S, x1 * S + S - 1, y1 * S + S - 1,
+           z1 * S + S - 1);
     W.merge();
     const int cnt = W.n;
     const float rk = cnt ? __uint_as_float((uint32_t)(warp_max_key(U, cnt, lane) >> 32)) : 0.f;
@@ -346,13 +465,14 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
     if (cnt > 0 && !(require_full && cnt != k)) {
         const float alpha = 1.818f, beta = 1.953f;
         const float fr = rk * rk;
+        const float norm = 1.f - expf(-beta);
         for (int e = lane; e < cnt; e += 32) {
             uint32_t s = U.slot[e];
             V3 pd = ld3(G.gdir + 3 * (size_t)s);
             float cs = vdot(nrm, vneg(pd));
             if (cs > 0) {
                 float d = __uint_as_float((uint32_t)(U.key[e] >> 32));
-                float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / (1.f - expf(-beta)));
+                float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / norm);
                 res = vadd(res, vscale(ld3(G.gpow + 3 * (size_t)s), filter));
             }
         }

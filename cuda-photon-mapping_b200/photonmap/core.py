@@ -107,6 +107,7 @@ def library():
         "pm_stage_times": ([vp, vp], C.c_int),
         "pm_status": ([vp, vp], C.c_int),
         "pm_launch_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
+        "pm_render_requests": ([vp, C.POINTER(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -292,6 +293,12 @@ class Context:
         self._check(self.L.pm_stage_times(self.h, out.ctypes.data), "pm_stage_times")
         return dict(trace_ms=float(out[0]), grid_ms=float(out[1]), eye_ms=float(out[2]), gather_ms=float(out[3]),
                     resolve_ms=float(out[4]))
+
+    def render_requests(self):
+        """kNN queries answered by the last render's global-map gather."""
+        out = C.c_int64()
+        self._check(self.L.pm_render_requests(self.h, C.byref(out)), "pm_render_requests")
+        return out.value
 
     def launch_count(self):
         out = C.c_int64()

@@ -207,6 +207,10 @@ int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclus
  * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather, [4] resolve. */
 int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
 
+/* Gather requests (eye-path hits that query the global map) of the last
+ * pm_render call: the number of kNN queries its gather stage answered. */
+int pm_render_requests(pm_ctx* ctx, int64_t* out);
+
 /* Number of kernels this context has launched so far. */
 int pm_launch_count(pm_ctx* ctx, int64_t* out);
 
