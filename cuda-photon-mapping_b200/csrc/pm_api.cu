@@ -39,7 +39,7 @@ struct MapState {
     float aabb[6] = {0, 0, 0, 0, 0, 0};
     int S = 1;
     DevBuf starts, sizes, gpos, gdir, gpow, key_counts, key_starts;
-    DevBuf cid, keys0, keys1, vals0, vals1, hist, scan_ws, small;
+    DevBuf cid, keys0, keys1, vals0, vals1, hist, scan_ws, small, counts2;
 };
 
 }  // namespace
@@ -218,7 +218,7 @@ void pm_destroy(pm_ctx* ctx) {
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
                         &m.keys0, &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small,
-                        &m.key_counts, &m.key_starts};
+                        &m.key_counts, &m.key_starts, &m.counts2};
         for (DevBuf* b : mb) release(*b);
     }
     for (auto& ev : ctx->ev) if (ev) cudaEventDestroy(ev);
@@ -570,6 +570,7 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     ENSURE(m.vals0, (size_t)n * 4);
     ENSURE(m.vals1, (size_t)n * 4);
     ENSURE(m.small, 64);
+    ENSURE(m.counts2, (size_t)((int64_t)d2[0] * d2[1] * d2[2]) * 4);
     GridBuffers B;
     B.pos = P<float>(m.pos); B.dir = P<float>(m.dir); B.pow = P<float>(m.pow); B.n = n;
     B.cell_starts = P<uint32_t>(m.starts); B.cell_sizes = P<uint32_t>(m.sizes);
@@ -578,6 +579,7 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     B.keys[0] = P<uint32_t>(m.keys0); B.keys[1] = P<uint32_t>(m.keys1);
     B.vals[0] = P<uint32_t>(m.vals0); B.vals[1] = P<uint32_t>(m.vals1);
     B.small = P<uint32_t>(m.small);
+    B.counts2 = P<uint32_t>(m.counts2);
     B.status = P<unsigned>(ctx->status);
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     GridPlan plan;
@@ -596,12 +598,7 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     B.key_counts = P<uint32_t>(m.key_counts);
     B.key_starts = P<uint32_t>(m.key_starts);
     CK(grid_sort(B, box, plan, S, ctx->st));
-    {
-        int bits = 1;
-        while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)keys) bits++;
-        const int64_t regrid = (plan.cells == (int64_t)d1[0] * d1[1] * d1[2]) ? 0 : 1;
-        ctx->launches += 2 * (1 + regrid) + (S > 1 ? 3 : 1) + 3 * ((bits + 7) / 8) + 1;
-    }
+    ctx->launches += plan.launches;
     CK(cudaEventRecord(ctx->ev[3], ctx->st));
     CK(cudaEventSynchronize(ctx->ev[3]));
     if (map == PM_MAP_GLOBAL) ctx->stage_ms[1] = elapsed(ctx->ev[2], ctx->ev[3]);

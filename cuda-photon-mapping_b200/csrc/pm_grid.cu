@@ -8,12 +8,14 @@
 // trace order, which makes the sorted arrays a pure function of the photon
 // list; cell_starts / cell_sizes are the reference's exactly.  Pipeline (one stream, no host round trip except the
 // re-grid decision the reference also takes on the host):
-//   k_cell_count   cell id per photon (stored) + per-cell counts (atomics)
-//   k_max          the largest cell count -> host decides on the re-grid
-//   k_key_count    (sub-cell split S > 1) key = cell * S^3 + sub-cell + counts
+//   k_count_cells  per-cell counts of both candidate grids (the desired
+//                  resolution and the re-grid one) and their largest counts
+//                  (shared-memory counters + k_count_max when both grids fit)
+//                  -> host decides on the re-grid and on S
+//   k_key_count    key = cell * S^3 + sub-cell per photon + key counts
 //   scan_u32       exclusive scan of key counts (decoupled look-back) ->
 //                  key_starts; cell_starts / cell_sizes follow exactly
-//   LSD radix sort of the keys, 8 bits per pass, carrying the photon index:
+//   LSD radix sort of the keys, <= 9 bits per pass, carrying the photon index:
 //     k_radix_upsweep    per-tile digit histogram, digit-major
 //     scan_u32           offsets of every (digit, tile)
 //     k_radix_downsweep  stable in-tile ranks (warp match) + scatter
@@ -32,6 +34,8 @@ constexpr int RADIX_THREADS = 256;
 constexpr int RADIX_ITEMS = 16;
 constexpr int RADIX_TILE = RADIX_THREADS * RADIX_ITEMS;
 constexpr int RADIX_WARPS = RADIX_THREADS / 32;
+constexpr int RADIX_MAX_BITS = 9;
+constexpr int RADIX_MAX_BINS = 1 << RADIX_MAX_BITS;
 
 struct GridGeom {
     float mnx, mny, mnz;
@@ -49,14 +53,85 @@ __device__ __forceinline__ uint32_t cell_of(const GridGeom& g, float px, float p
     return (uint32_t)(x + y * g.gx + z * g.gx * g.gy);
 }
 
-__global__ void k_cell_count(const float* __restrict__ pos, int64_t n, GridGeom g, uint32_t* __restrict__ cid,
-                             uint32_t* __restrict__ counts) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float* p = pos + 3 * i;
-    uint32_t c = cell_of(g, p[0], p[1], p[2]);
-    cid[i] = c;
-    atomicAdd(counts + c, 1u);
+// Shared-memory variant of k_count_cells for grids whose cells fit in shared
+// memory as 16-bit counters (two per 32-bit word; a block counts at most
+// COUNT_CHUNK <= 65535 photons, so a half-word never carries into its
+// neighbour).  Photons land on a few thousand hot surface cells, so global
+// atomics on the cell counters contend; here each block adds into its own
+// copy and flushes its non-zero counters once.
+constexpr int COUNT_THREADS = 1024;
+constexpr int COUNT_CHUNK = 65535;
+constexpr int COUNT_SMEM_WORDS = 56 * 1024;   // 224 KB: 114,688 16-bit counters
+
+__global__ void __launch_bounds__(COUNT_THREADS)
+k_count_cells_smem(const float* __restrict__ pos, int64_t n, GridGeom ga, GridGeom gb, int two, int cells_a,
+                   int cells_b, uint32_t* __restrict__ ca, uint32_t* __restrict__ cb) {
+    extern __shared__ uint32_t h16[];
+    const int words_a = (cells_a + 1) >> 1, words = words_a + (two ? (cells_b + 1) >> 1 : 0);
+    for (int i = threadIdx.x; i < words; i += COUNT_THREADS) h16[i] = 0u;
+    __syncthreads();
+    const int64_t first = (int64_t)blockIdx.x * COUNT_CHUNK;
+    const int64_t last = min(first + (int64_t)COUNT_CHUNK, n);
+    for (int64_t i = first + threadIdx.x; i < last; i += COUNT_THREADS) {
+        const float* p = pos + 3 * i;
+        const float x = p[0], y = p[1], z = p[2];
+        const uint32_t c = cell_of(ga, x, y, z);
+        atomicAdd(&h16[c >> 1], 1u << (16 * (c & 1u)));
+        if (two) {
+            const uint32_t c2 = cell_of(gb, x, y, z);
+            atomicAdd(&h16[words_a + (c2 >> 1)], 1u << (16 * (c2 & 1u)));
+        }
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < words; w += COUNT_THREADS) {
+        const uint32_t v = h16[w];
+        if (!v) continue;
+        const bool in_a = w < words_a;
+        uint32_t* dst = in_a ? ca : cb;
+        const int cell = 2 * (in_a ? w : w - words_a);
+        if (v & 0xffffu) atomicAdd(dst + cell, v & 0xffffu);
+        if (v >> 16) atomicAdd(dst + cell + 1, v >> 16);
+    }
+}
+
+// largest counts of the two count arrays: mx[0] (a), mx[1] (b)
+__global__ void k_count_max(const uint32_t* __restrict__ ca, int64_t na, const uint32_t* __restrict__ cb, int64_t nb,
+                            uint32_t* mx) {
+    uint32_t ma = 0u, mb = 0u;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += stride) ma = max(ma, ca[i]);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += stride) mb = max(mb, cb[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ma = max(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+        mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (ma) atomicMax(mx, ma);
+        if (mb) atomicMax(mx + 1, mb);
+    }
+}
+
+// photon counts of grid a and (when two) grid b; mx[0], mx[1] = largest counts
+__global__ void k_count_cells(const float* __restrict__ pos, int64_t n, GridGeom ga, GridGeom gb, int two,
+                              uint32_t* __restrict__ ca, uint32_t* __restrict__ cb, uint32_t* mx) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t ma = 0u, mb = 0u;
+    if (i < n) {
+        const float* p = pos + 3 * i;
+        const float x = p[0], y = p[1], z = p[2];
+        ma = atomicAdd(ca + cell_of(ga, x, y, z), 1u) + 1u;
+        if (two) mb = atomicAdd(cb + cell_of(gb, x, y, z), 1u) + 1u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ma = max(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+        mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (ma) atomicMax(mx, ma);
+        if (mb) atomicMax(mx + 1, mb);
+    }
 }
 
 // sub-cell key: cell * S^3 + sub-cell, the sub-cell taken from the fractional
@@ -92,46 +167,54 @@ __global__ void k_cells_from_keys(const uint32_t* __restrict__ key_starts, int64
     sizes[c] = b - a;
 }
 
-__global__ void k_max(const uint32_t* __restrict__ a, int64_t n, uint32_t* out) {
-    uint32_t m = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        m = max(m, a[i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
-}
-
 __global__ void __launch_bounds__(RADIX_THREADS)
-k_radix_upsweep(const uint32_t* __restrict__ keys, int64_t n, int shift, uint32_t* __restrict__ hist, int tiles) {
-    __shared__ uint32_t h[256];
-    const int tid = threadIdx.x;
-    h[tid] = 0;
+k_radix_upsweep(const uint32_t* __restrict__ keys, int64_t n, int shift, int bits, uint32_t* __restrict__ hist,
+                int tiles) {
+    __shared__ uint32_t h[RADIX_MAX_BINS];
+    const int tid = threadIdx.x, bins = 1 << bits;
+    const uint32_t dm = (uint32_t)bins - 1u;
+    for (int b = tid; b < bins; b += RADIX_THREADS) h[b] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * RADIX_TILE;
 #pragma unroll 4
     for (int i = 0; i < RADIX_ITEMS; i++) {
         int64_t gi = base + i * RADIX_THREADS + tid;
-        if (gi < n) atomicAdd(&h[(keys[gi] >> shift) & 255u], 1u);
+        if (gi < n) atomicAdd(&h[(keys[gi] >> shift) & dm], 1u);
     }
     __syncthreads();
-    hist[(int64_t)tid * tiles + blockIdx.x] = h[tid];
+    for (int b = tid; b < bins; b += RADIX_THREADS) hist[(int64_t)b * tiles + blockIdx.x] = h[b];
 }
 
 // Stable scatter of one radix pass.  A warp owns 512 consecutive keys and walks
 // them 32 at a time in order; equal digits inside a step are ranked by lane with
 // __match_any_sync, across steps by a per-warp running count, across warps by a
-// prefix over the warps' counts.  vals_in == null means vals = index.
+// prefix over the warps' counts.  The tile is then staged in shared memory in
+// digit order, so that consecutive threads write consecutive slots of each
+// digit's output run (coalesced) instead of one scattered word per key.
+// vals_in == null means vals = index.
+struct RadixSmem {
+    uint32_t wh[RADIX_WARPS][RADIX_MAX_BINS];   // per-warp digit counts, then warp offsets
+    uint32_t dbase[RADIX_MAX_BINS];             // global start of the tile's run of each digit
+    uint32_t lbase[RADIX_MAX_BINS];             // start of each digit inside the staged tile
+    uint32_t wsum[RADIX_WARPS];
+    uint32_t key[RADIX_TILE];
+    uint32_t val[RADIX_TILE];
+};
+
 __global__ void __launch_bounds__(RADIX_THREADS)
 k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, int64_t n, int shift,
-                  const uint32_t* __restrict__ offsets, int tiles, uint32_t* __restrict__ keys_out,
+                  int bits, const uint32_t* __restrict__ offsets, int tiles, uint32_t* __restrict__ keys_out,
                   uint32_t* __restrict__ vals_out) {
-    __shared__ uint32_t wh[RADIX_WARPS][256];
-    __shared__ uint32_t dbase[256];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < RADIX_WARPS * 256; i += RADIX_THREADS) (&wh[0][0])[i] = 0u;
-    dbase[tid] = offsets[(int64_t)tid * tiles + blockIdx.x];
+    extern __shared__ __align__(16) unsigned char radix_smem[];
+    RadixSmem& R = *reinterpret_cast<RadixSmem*>(radix_smem);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, bins = 1 << bits;
+    const uint32_t dm = (uint32_t)bins - 1u;
+    for (int i = tid; i < RADIX_WARPS * RADIX_MAX_BINS; i += RADIX_THREADS) (&R.wh[0][0])[i] = 0u;
+    for (int b = tid; b < bins; b += RADIX_THREADS) R.dbase[b] = offsets[(int64_t)b * tiles + blockIdx.x];
     __syncthreads();
-    const int64_t wbase = (int64_t)blockIdx.x * RADIX_TILE + (int64_t)warp * (32 * RADIX_ITEMS);
+    const int64_t tbase = (int64_t)blockIdx.x * RADIX_TILE;
+    const int64_t wbase = tbase + (int64_t)warp * (32 * RADIX_ITEMS);
+    const int tcount = (int)min((int64_t)RADIX_TILE, n - tbase);
     uint32_t k[RADIX_ITEMS], v[RADIX_ITEMS], r[RADIX_ITEMS];
 #pragma unroll
     for (int j = 0; j < RADIX_ITEMS; j++) {
@@ -142,13 +225,13 @@ k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restri
         v[j] = valid ? (vals_in ? vals_in[gi] : (uint32_t)gi) : 0u;
         r[j] = 0u;
         if (valid) {
-            uint32_t d = (k[j] >> shift) & 255u;
+            uint32_t d = (k[j] >> shift) & dm;
             unsigned peers = __match_any_sync(vm, d);
             int leader = __ffs(peers) - 1;
             uint32_t old = 0u;
             if (lane == leader) {
-                old = wh[warp][d];
-                wh[warp][d] = old + (uint32_t)__popc(peers);
+                old = R.wh[warp][d];
+                R.wh[warp][d] = old + (uint32_t)__popc(peers);
             }
             old = __shfl_sync(peers, old, leader);
             r[j] = old + (uint32_t)__popc(peers & lanemask_lt());
@@ -156,25 +239,61 @@ k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restri
         __syncwarp();
     }
     __syncthreads();
-    {   // exclusive prefix over warps for digit tid
-        uint32_t run = 0;
+    // per digit: exclusive prefix over warps; the tile's count of the digit
+    constexpr int BPT = RADIX_MAX_BINS / RADIX_THREADS;   // bins per thread
+    uint32_t tot[BPT], part = 0;
 #pragma unroll
-        for (int w = 0; w < RADIX_WARPS; w++) {
-            uint32_t c = wh[w][tid];
-            wh[w][tid] = run;
-            run += c;
+    for (int q = 0; q < BPT; q++) {
+        const int b = tid * BPT + q;
+        uint32_t run = 0;
+        if (b < bins) {
+#pragma unroll
+            for (int w = 0; w < RADIX_WARPS; w++) {
+                uint32_t c = R.wh[w][b];
+                R.wh[w][b] = run;
+                run += c;
+            }
         }
+        tot[q] = run;
+        part += run;
+    }
+    // block-wide exclusive scan of the per-thread digit totals -> lbase
+    uint32_t incl = part;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) R.wsum[warp] = incl;
+    __syncthreads();
+    uint32_t off = incl - part;
+    for (int w = 0; w < warp; w++) off += R.wsum[w];
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int b = tid * BPT + q;
+        if (b < bins) R.lbase[b] = off;
+        off += tot[q];
     }
     __syncthreads();
+    // stage the tile in digit order
 #pragma unroll
     for (int j = 0; j < RADIX_ITEMS; j++) {
         int64_t gi = wbase + j * 32 + lane;
         if (gi < n) {
-            uint32_t d = (k[j] >> shift) & 255u;
-            uint32_t p = dbase[d] + wh[warp][d] + r[j];
-            if (keys_out) keys_out[p] = k[j];
-            vals_out[p] = v[j];
+            const uint32_t d = (k[j] >> shift) & dm;
+            const uint32_t lp = R.lbase[d] + R.wh[warp][d] + r[j];
+            R.key[lp] = k[j];
+            R.val[lp] = v[j];
         }
+    }
+    __syncthreads();
+    // write out: slot i of the staged tile goes to dbase[d] + (i - lbase[d])
+    for (int i = tid; i < tcount; i += RADIX_THREADS) {
+        const uint32_t kk = R.key[i];
+        const uint32_t d = (kk >> shift) & dm;
+        const uint32_t p = R.dbase[d] + ((uint32_t)i - R.lbase[d]);
+        if (keys_out) keys_out[p] = kk;
+        vals_out[p] = R.val[i];
     }
 }
 
@@ -212,8 +331,8 @@ void grid_dims(const float aabb[6], int64_t n, int desired, int dims[3], float* 
 
 void grid_scratch_sizes(int64_t n, int64_t max_keys, size_t* hist_elems, size_t* scan_ws_bytes) {
     int64_t tiles = std::max<int64_t>(1, (n + RADIX_TILE - 1) / RADIX_TILE);
-    *hist_elems = (size_t)256 * tiles;
-    *scan_ws_bytes = std::max(scan_workspace_bytes((int64_t)256 * tiles), scan_workspace_bytes(max_keys + 1));
+    *hist_elems = (size_t)RADIX_MAX_BINS * tiles;
+    *scan_ws_bytes = std::max(scan_workspace_bytes((int64_t)RADIX_MAX_BINS * tiles), scan_workspace_bytes(max_keys + 1));
 }
 
 int grid_auto_subdiv(uint32_t max_count, int k_hint) {
@@ -227,30 +346,53 @@ cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int reg
                        GridPlan* plan, cudaStream_t st) {
     cudaError_t e;
     const int64_t n = B.n;
-    GridGeom g;
-    g.mnx = aabb[0]; g.mny = aabb[1]; g.mnz = aabb[2];
-    for (int pass = 0; pass < 2; pass++) {
-        int want = pass == 0 ? desired : std::max(desired / regrid_div, 1);
-        grid_dims(aabb, n, want, plan->dims, &plan->cell);
-        g.gx = plan->dims[0]; g.gy = plan->dims[1]; g.gz = plan->dims[2]; g.cell = plan->cell;
-        plan->cells = (int64_t)g.gx * g.gy * g.gz;
-        if ((e = cudaMemsetAsync(B.cell_sizes, 0, (size_t)plan->cells * 4, st)) != cudaSuccess) return e;
-        if (n > 0) {
-            k_cell_count<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, g, B.cid, B.cell_sizes);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        }
-        if ((e = cudaMemsetAsync(B.small, 0, 4, st)) != cudaSuccess) return e;
-        k_max<<<std::min<int64_t>(blocks_for(plan->cells, 256), 1184), 256, 0, st>>>(B.cell_sizes, plan->cells, B.small);
-        uint32_t mx = 0;
-        if ((e = cudaMemcpyAsync(&mx, B.small, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-        plan->max_count = mx;
-        if (pass == 0 && !(mx > (uint32_t)(regrid_mult * desired))) break;
+    GridPlan pa{}, pb{};
+    grid_dims(aabb, n, desired, pa.dims, &pa.cell);
+    pa.cells = (int64_t)pa.dims[0] * pa.dims[1] * pa.dims[2];
+    const int want_b = std::max(desired / regrid_div, 1);
+    const bool two = want_b != desired;
+    grid_dims(aabb, n, want_b, pb.dims, &pb.cell);
+    pb.cells = (int64_t)pb.dims[0] * pb.dims[1] * pb.dims[2];
+    auto geom = [&](const GridPlan& p) {
+        GridGeom g;
+        g.mnx = aabb[0]; g.mny = aabb[1]; g.mnz = aabb[2];
+        g.gx = p.dims[0]; g.gy = p.dims[1]; g.gz = p.dims[2]; g.cell = p.cell;
+        return g;
+    };
+    if ((e = cudaMemsetAsync(B.cell_sizes, 0, (size_t)pa.cells * 4, st)) != cudaSuccess) return e;
+    if (two && (e = cudaMemsetAsync(B.counts2, 0, (size_t)pb.cells * 4, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(B.small, 0, 8, st)) != cudaSuccess) return e;
+    int launches = 0;
+    const int64_t smem_words = (pa.cells + 1) / 2 + (two ? (pb.cells + 1) / 2 : 0);
+    if (n > 0 && smem_words <= COUNT_SMEM_WORDS) {
+        const int smem = (int)smem_words * 4;
+        if ((e = cudaFuncSetAttribute(k_count_cells_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+            return e;
+        k_count_cells_smem<<<blocks_for(n, COUNT_CHUNK), COUNT_THREADS, smem, st>>>(
+            B.pos, n, geom(pa), geom(pb), two ? 1 : 0, (int)pa.cells, (int)pb.cells, B.cell_sizes, B.counts2);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        k_count_max<<<std::min<int64_t>(blocks_for(std::max(pa.cells, pb.cells), 256), 296), 256, 0, st>>>(
+            B.cell_sizes, pa.cells, B.counts2, two ? pb.cells : 0, B.small);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        launches = 2;
+    } else if (n > 0) {
+        k_count_cells<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, geom(pa), geom(pb), two ? 1 : 0, B.cell_sizes,
+                                                            B.counts2, B.small);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        launches = 1;
     }
+    uint32_t mx[2] = {0u, 0u};
+    if ((e = cudaMemcpyAsync(mx, B.small, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    pa.max_count = mx[0];
+    pb.max_count = two ? mx[1] : mx[0];
+    // the reference rebuilds at the finer resolution when a cell is overfull
+    *plan = (mx[0] > (uint32_t)(regrid_mult * desired)) ? pb : pa;
+    plan->launches = launches;
     return cudaSuccess;
 }
 
-cudaError_t grid_sort(GridBuffers& B, const float aabb[6], const GridPlan& plan, int S, cudaStream_t st) {
+cudaError_t grid_sort(GridBuffers& B, const float aabb[6], GridPlan& plan, int S, cudaStream_t st) {
     cudaError_t e;
     const int64_t n = B.n;
     const int64_t cells = plan.cells;
@@ -259,43 +401,47 @@ cudaError_t grid_sort(GridBuffers& B, const float aabb[6], const GridPlan& plan,
     GridGeom g;
     g.mnx = aabb[0]; g.mny = aabb[1]; g.mnz = aabb[2];
     g.gx = plan.dims[0]; g.gy = plan.dims[1]; g.gz = plan.dims[2]; g.cell = plan.cell;
-    if (S == 1) {
-        // keys are the cell ids already in B.cid; counts are cell_sizes
-        if ((e = scan_u32(B.cell_sizes, B.key_starts, cells, 0, B.key_starts + cells, B.scan_ws, B.status, st)) != cudaSuccess) return e;
-        if ((e = cudaMemcpyAsync(B.cell_starts, B.key_starts, (size_t)cells * 4, cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
-    } else {
-        if ((e = cudaMemsetAsync(B.key_counts, 0, (size_t)keys * 4, st)) != cudaSuccess) return e;
-        if (n > 0) {
-            k_key_count<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, g, S, B.cid, B.key_counts);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        }
-        if ((e = scan_u32(B.key_counts, B.key_starts, keys, 0, B.key_starts + keys, B.scan_ws, B.status, st)) != cudaSuccess) return e;
-        k_cells_from_keys<<<blocks_for(cells, 256), 256, 0, st>>>(B.key_starts, cells, S3, B.cell_starts, B.cell_sizes);
+    if ((e = cudaMemsetAsync(B.key_counts, 0, (size_t)keys * 4, st)) != cudaSuccess) return e;
+    if (n > 0) {
+        k_key_count<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, g, S, B.cid, B.key_counts);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        plan.launches++;
     }
+    if ((e = scan_u32(B.key_counts, B.key_starts, keys, 0, B.key_starts + keys, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+    k_cells_from_keys<<<blocks_for(cells, 256), 256, 0, st>>>(B.key_starts, cells, S3, B.cell_starts, B.cell_sizes);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    plan.launches += 2;
     if (n == 0) return cudaSuccess;
 
-    // LSD radix sort of the keys (stable), carrying the photon index
+    // LSD radix sort of the keys (stable), carrying the photon index; digits of
+    // equal width <= 9 bits
     int bits = 1;
     while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)keys) bits++;
-    const int passes = (bits + 7) / 8;
+    const int passes = (bits + RADIX_MAX_BITS - 1) / RADIX_MAX_BITS;
+    const int width = (bits + passes - 1) / passes;
     const int tiles = (int)((n + RADIX_TILE - 1) / RADIX_TILE);
+    const int64_t hist_n = ((int64_t)1 << width) * tiles;
     const uint32_t* kin = B.cid;
     const uint32_t* vin = nullptr;
+    if ((e = cudaFuncSetAttribute(k_radix_downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RadixSmem))) !=
+        cudaSuccess)
+        return e;
     for (int p = 0; p < passes; p++) {
-        const int shift = 8 * p;
+        const int shift = width * p;
         const bool last = p == passes - 1;
         uint32_t* kout = last ? nullptr : B.keys[p & 1];
         uint32_t* vout = B.vals[p & 1];
-        k_radix_upsweep<<<tiles, RADIX_THREADS, 0, st>>>(kin, n, shift, B.hist, tiles);
+        k_radix_upsweep<<<tiles, RADIX_THREADS, 0, st>>>(kin, n, shift, width, B.hist, tiles);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = scan_u32(B.hist, B.hist, (int64_t)256 * tiles, 0, nullptr, B.scan_ws, B.status, st)) != cudaSuccess) return e;
-        k_radix_downsweep<<<tiles, RADIX_THREADS, 0, st>>>(kin, vin, n, shift, B.hist, tiles, kout, vout);
+        if ((e = scan_u32(B.hist, B.hist, hist_n, 0, nullptr, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+        k_radix_downsweep<<<tiles, RADIX_THREADS, sizeof(RadixSmem), st>>>(kin, vin, n, shift, width, B.hist, tiles,
+                                                                           kout, vout);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         kin = kout;
         vin = vout;
     }
     k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(vin, n, B.pos, B.dir, B.pow, B.gpos, B.gdir, B.gpow, B.status);
+    plan.launches += 3 * passes + 1;
     return cudaGetLastError();
 }
 

@@ -27,7 +27,8 @@ struct GridBuffers {
     uint32_t* cid;        // n
     uint32_t* keys[2];    // n each
     uint32_t* vals[2];    // n each
-    uint32_t* hist;       // 256 * tiles
+    uint32_t* counts2;    // cells of the re-grid resolution (count scratch)
+    uint32_t* hist;       // 512 * tiles
     void* scan_ws;
     uint32_t* small;      // 16 u32 of device scratch (max count, totals)
     unsigned* status;
@@ -38,13 +39,15 @@ struct GridPlan {
     float cell;
     int64_t cells;
     uint32_t max_count;   // photons in the fullest cell of the chosen grid
+    int launches;         // kernels launched by grid_count + grid_sort
 };
 
-// Phase 1: per-cell counts of the reference's grid, including its re-grid rule
-// (desired photons per cell, 1000 in the reference; rebuilt at desired /
-// regrid_div when a cell holds more than regrid_mult * desired, 5 and 5).
-// Writes cell ids (B.cid), cell_sizes and the plan.  Synchronises the stream
-// once (the re-grid decision is taken on the host, as in the reference).
+// Phase 1: the reference's grid, including its re-grid rule (desired photons
+// per cell, 1000 in the reference; rebuilt at desired / regrid_div when a cell
+// holds more than regrid_mult * desired, 5 and 5).  One pass counts the photons
+// of both candidate grids (scratch: cell_sizes, counts2) and their fullest
+// cells; the plan is the chosen grid.  Synchronises the stream once (the
+// re-grid decision is taken on the host, as in the reference).
 cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int regrid_mult, int regrid_div,
                        GridPlan* plan, cudaStream_t st);
 
@@ -52,7 +55,7 @@ cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int reg
 // is split into S^3 sub-cells (S = 1, 2, 4 or 8), and write cell_starts /
 // cell_sizes (exactly the reference's), key_starts (sub-cell ranges) and the
 // sorted arrays.  Buffers: key arrays sized for cells * S^3 (+1).
-cudaError_t grid_sort(GridBuffers& B, const float aabb[6], const GridPlan& plan, int S, cudaStream_t st);
+cudaError_t grid_sort(GridBuffers& B, const float aabb[6], GridPlan& plan, int S, cudaStream_t st);
 
 // sub-cell division for a grid whose fullest cell holds max_count photons:
 // about 2k photons per sub-cell slab of a surface crossing the cell
