@@ -12,19 +12,24 @@
 // reference's length(p - q) in IEEE float, so the sets are bit-exact.
 //
 // One warp per query.  Photons are stored by (cell, sub-cell); the warp walks
-// the query's sub-cell first, then rings of sub-cells outwards (nearest first),
-// within the reference's cube of cells, skipping every sub-cell whose box lies
-// farther than the current k-th distance (with a margin far above float
-// rounding) and stopping at the first ring that lies entirely farther.  Lanes read 32
-// consecutive photons at a time (one 16-byte load each), test the squared
-// distance against a bound slightly above the threshold's square, take the
-// correctly rounded sqrt only for survivors, and append the survivors' 64-bit
-// keys (distance bits << 32 | source id; non-negative float bits order like the
-// floats, so integer order is the lexicographic order) to a per-warp
-// shared-memory store by ballot.  When the store fills, an MSB-first radix
-// select (8-bit digits, finished by a 32-lane bitonic sort) finds the exact
-// k-th key, the store is compacted to the k best and the threshold tightens.
-// The answer is the exhaustive walk's.
+// the query's sub-cell and the shell of sub-cells around it, then shells
+// further out (nearest first), within the reference's cube of cells, skipping
+// every sub-cell whose box lies farther than the current bound on the k-th
+// distance (with a margin far above float rounding) and stopping at the first
+// shell that lies entirely farther.  Non-empty sub-cells are queued and their
+// photons scanned as one list, one photon per lane (one 16-byte load each):
+// lanes test the squared distance against a bound slightly above the
+// threshold's square, take the correctly rounded sqrt only for survivors, and
+// append the survivors' 64-bit keys (distance bits << 32 | source id;
+// non-negative float bits order like the floats, so integer order is the
+// lexicographic order) to a per-warp shared-memory store by ballot, counting
+// each in a 256-bin histogram of distance over [0, r].  After each shell the
+// histogram bounds the k-th distance (the upper edge of the bin where the
+// running count reaches k).  When the store fills, and at the end, the exact
+// k-th key is found from the histogram: the keys of its bin (a handful) are
+// sorted by the warp (an MSB-first radix select over the store when the bin
+// holds more than 32), and the store is cut to the k best.  The answer is the
+// exhaustive walk's.
 #include "pm_gather.cuh"
 #include "pm_device.cuh"
 
@@ -36,11 +41,15 @@ constexpr int WARPS = 8;   // queries per block
 
 constexpr int QCAP = 64;   // queued sub-cells per warp
 
+constexpr int DBINS = 256;   // distance histogram bins over [0, r]
+
 template <int UCAP>
 struct WarpStore {
     unsigned long long key[UCAP];
     uint32_t slot[UCAP];
     uint32_t hist[256];   // radix-select histogram; doubles as 32 x u64 scratch
+    uint32_t dh[DBINS];   // distance histogram of the keys in the store
+    unsigned long long sel[32];
     uint32_t qa[QCAP];    // queued sub-cells: first photon, photon count
     uint32_t qc[QCAP];
 };
@@ -230,15 +239,105 @@ struct WarpWalk {
     int qn;                   // queued sub-cells
     unsigned long long T;     // a candidate enters when its key < T
     float lim, lim2;          // distance bound for pruning; squared pre-filter bound
+    float bscale;             // DBINS / r: distance histogram bin of d = min(DBINS - 1, (int)(d * bscale))
 
     __device__ WarpWalk(const GatherGrid& g, WarpStore<UCAP>& u, V3 qq, float rr, int kk, int ln)
-        : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), qn(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f) {}
+        : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), qn(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f),
+          bscale((float)DBINS / rr) {
+#pragma unroll
+        for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+        __syncwarp();
+    }
+
+    __device__ __forceinline__ uint32_t bin_of(float d) const {
+        return (uint32_t)min((int)(d * bscale), DBINS - 1);   // non-decreasing in d
+    }
+
+    // The k-th smallest key of the store (n > k).  The distance histogram
+    // locates the bin holding it; the keys of that bin (normally a handful)
+    // are sorted by one warp, else the radix select runs over the store.
+    __device__ unsigned long long kth_key() {
+        uint32_t c[DBINS / 32], sum = 0;
+#pragma unroll
+        for (int b = 0; b < DBINS / 32; b++) { c[b] = U.dh[(DBINS / 32) * lane + b]; sum += c[b]; }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t excl = incl - sum;
+        const unsigned own = __ballot_sync(0xffffffffu, excl < (uint32_t)k && (uint32_t)k <= incl);
+        const int owner = own ? __ffs(own) - 1 : 0;
+        uint32_t bin = 0, before = 0, cnt = 0;
+        if (lane == owner) {
+            uint32_t run = excl;
+#pragma unroll
+            for (int b = 0; b < DBINS / 32; b++) {
+                if (cnt == 0 && (uint32_t)k <= run + c[b]) { bin = (DBINS / 32) * lane + b; before = run; cnt = c[b]; }
+                run += c[b];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, owner);
+        before = __shfl_sync(0xffffffffu, before, owner);
+        cnt = __shfl_sync(0xffffffffu, cnt, owner);
+        if (!own || cnt > 32u) return select_kth(U, n, k, lane);
+        int got = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            const unsigned long long kk = i < n ? U.key[i] : ~0ull;
+            const bool m = i < n && bin_of(__uint_as_float((uint32_t)(kk >> 32))) == bin;
+            const unsigned bm = __ballot_sync(0xffffffffu, m);
+            if (m) U.sel[got + __popc(bm & lanemask_lt())] = kk;
+            got += __popc(bm);
+        }
+        __syncwarp();
+        unsigned long long v = lane < got ? U.sel[lane] : ~0ull;
+        __syncwarp();
+        v = warp_sort32(v, lane);
+        return shfl_u64(v, k - (int)before - 1);
+    }
+
+    // Tighten the distance bound from the histogram alone (n > k): the k-th
+    // smallest distance lies in the bin where the running count reaches k, so
+    // the bin's upper edge (with a margin over the rounding of d * bscale) bounds it.
+    __device__ void bound() {
+        uint32_t c[DBINS / 32], sum = 0;
+#pragma unroll
+        for (int b = 0; b < DBINS / 32; b++) { c[b] = U.dh[(DBINS / 32) * lane + b]; sum += c[b]; }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t excl = incl - sum;
+        const unsigned own = __ballot_sync(0xffffffffu, excl < (uint32_t)k && (uint32_t)k <= incl);
+        if (!own) return;
+        const int owner = __ffs(own) - 1;
+        int bin = 0;
+        if (lane == owner) {
+            uint32_t run = excl;
+            bool found = false;
+#pragma unroll
+            for (int b = 0; b < DBINS / 32; b++) {
+                if (!found && (uint32_t)k <= run + c[b]) { bin = (DBINS / 32) * lane + b; found = true; }
+                run += c[b];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, owner);
+        const float edge = (float)(bin + 1) * (r / (float)DBINS) * (1.f + 1e-5f);
+        if (edge < lim) {
+            lim = edge;
+            lim2 = lim * lim * 1.000001f;
+        }
+    }
 
     // keep the k best keys of the store, tighten the threshold
     __device__ void merge() {
         __syncwarp();
         if (n > k) {
-            T = select_kth(U, n, k, lane);
+            T = kth_key();
             int w = 0;
             for (int base = 0; base < n; base += 32) {
                 int i = base + lane;
@@ -256,6 +355,11 @@ struct WarpWalk {
                 __syncwarp();
             }
             n = w;
+            // the histogram counts the store's keys again
+#pragma unroll
+            for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+            __syncwarp();
+            for (int i = lane; i < n; i += 32) atomicAdd(&U.dh[bin_of(__uint_as_float((uint32_t)(U.key[i] >> 32)))], 1u);
         } else if (n == k) {
             T = warp_max_key(U, n, lane);
         }
@@ -270,11 +374,12 @@ struct WarpWalk {
     __device__ __forceinline__ void consider(float4 p, uint32_t j, bool valid) {
         bool ok = false;
         unsigned long long kk = 0ull;
+        float d = 0.f;
         if (valid) {
             float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
             float s = dx * dx + dy * dy + dz * dz;
             if (s <= lim2) {
-                float d = sqrtf(s);
+                d = sqrtf(s);
                 if (d <= r) {
                     kk = ((unsigned long long)__float_as_uint(d) << 32) | __float_as_uint(p.w);
                     ok = kk < T;
@@ -287,6 +392,7 @@ struct WarpWalk {
                 const int pos = n + __popc(m & lanemask_lt());
                 U.key[pos] = kk;
                 U.slot[pos] = j;
+                atomicAdd(&U.dh[bin_of(d)], 1u);
             }
             n += __popc(m);
             if (n + 32 > UCAP) merge();
@@ -294,9 +400,10 @@ struct WarpWalk {
     }
 
     // Scan the photons of queued sub-cells [0, cnt) (cnt <= 32) as one list:
-    // lane l takes list entries base + l, so one round of loads covers 32
-    // photons whichever sub-cells they belong to.
+    // lane l takes list entries base + l + 32 i (i < 4), so one round of loads
+    // covers 128 photons whichever sub-cells they belong to.
     __device__ void drain(int cnt) {
+        constexpr int NL = 1;
         __syncwarp();
         uint32_t a = 0u, c = 0u;
         if (lane < cnt) { a = U.qa[lane]; c = U.qc[lane]; }
@@ -308,23 +415,27 @@ struct WarpWalk {
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         const uint32_t excl = incl - c;
-        for (uint32_t base = 0; base < total; base += 64) {
-            const uint32_t o0 = base + lane, o1 = o0 + 32;
-            int m0 = 0, m1 = 0;   // the last queued sub-cell whose first list entry is <= o
+        for (uint32_t base = 0; base < total; base += 32 * NL) {
+            uint32_t j[NL];
+            bool v[NL];
+            float4 p[NL];
 #pragma unroll
-            for (int st = 16; st > 0; st >>= 1) {
-                const uint32_t e0 = __shfl_sync(0xffffffffu, excl, m0 + st);
-                const uint32_t e1 = __shfl_sync(0xffffffffu, excl, m1 + st);
-                if (e0 <= o0) m0 += st;
-                if (e1 <= o1) m1 += st;
+            for (int u = 0; u < NL; u++) {
+                const uint32_t o = base + 32 * u + lane;
+                int mm = 0;   // the last queued sub-cell whose first list entry is <= o
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const uint32_t e = __shfl_sync(0xffffffffu, excl, mm + st);
+                    if (e <= o) mm += st;
+                }
+                j[u] = __shfl_sync(0xffffffffu, a, mm) + (o - __shfl_sync(0xffffffffu, excl, mm));
+                v[u] = o < total;
             }
-            const uint32_t j0 = __shfl_sync(0xffffffffu, a, m0) + (o0 - __shfl_sync(0xffffffffu, excl, m0));
-            const uint32_t j1 = __shfl_sync(0xffffffffu, a, m1) + (o1 - __shfl_sync(0xffffffffu, excl, m1));
-            const bool v0 = o0 < total, v1 = o1 < total;
-            const float4 p0 = v0 ? __ldg(G.gpos + j0) : make_float4(0.f, 0.f, 0.f, 0.f);
-            const float4 p1 = v1 ? __ldg(G.gpos + j1) : make_float4(0.f, 0.f, 0.f, 0.f);
-            consider(p0, j0, v0);
-            consider(p1, j1, v1);
+#pragma unroll
+            for (int u = 0; u < NL; u++) p[u] = v[u] ? __ldg(G.gpos + j[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < NL; u++)
+                if (base + 32 * u < total) consider(p[u], j[u], v[u]);
         }
         __syncwarp();
     }
@@ -356,13 +467,14 @@ struct WarpWalk {
     }
 
     // Nearest-first walk over the sub-cells of the reference's cube of cells
-    // [lo, hi] (global sub-cell coordinates): the query's sub-cell, then shells
-    // at Chebyshev distance R = 1, 2, ...  Lanes test 32 shell members at a
-    // time (box distance against the current bound, non-empty photon range);
-    // the survivors are queued and scanned together.  After each shell the
-    // store is cut to the k best, tightening the bound; a shell whose nearest
-    // possible point is farther than the bound ends the walk.
+    // [lo, hi] (global sub-cell coordinates): the query's sub-cell with the
+    // shell at Chebyshev distance 1, then shells R = 2, 3, ...  Lanes test 32
+    // shell members at a time (box distance against the current bound,
+    // non-empty photon range); the survivors are queued and scanned together.
+    // After each shell the distance histogram tightens the bound; a shell whose
+    // nearest possible point is farther than the bound ends the walk.
     __device__ void walk(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz) {
+        constexpr int NM = 1;
         const int S = G.S, sh = __ffs(S) - 1;
         const float sc = G.cell / (float)S, pad = G.cell * 1e-4f;
         const float m = 1.f + 1e-5f;
@@ -372,51 +484,57 @@ struct WarpWalk {
             const uint32_t cellid = (uint32_t)((X >> sh) + (Y >> sh) * G.gx + (Z >> sh) * G.gx * G.gy);
             return cellid * S3 + (uint32_t)((X & (S - 1)) + S * ((Y & (S - 1)) + S * (Z & (S - 1))));
         };
-        {   // the query's own sub-cell
+        const int Rmax = max(max(max(X0 - lx, hx - X0), max(Y0 - ly, hy - Y0)), max(Z0 - lz, hz - Z0));
+        if (Rmax == 0) {   // the query's sub-cell is the whole cube
             const uint32_t key = key_of(X0, Y0, Z0);
             uint32_t a = 0u, b = 0u;
             if (lane == 0) { a = __ldg(G.key_starts + key); b = __ldg(G.key_starts + key + 1); }
             enqueue(lane == 0 && b > a, a, b - a);
+            flush();
+            return;
         }
-        const int Rmax = max(max(max(X0 - lx, hx - X0), max(Y0 - ly, hy - Y0)), max(Z0 - lz, hz - Z0));
         for (int R = 1; R <= Rmax; R++) {
             if ((float)(R - 1) * sc - pad > lim * m) break;
             const int side = 2 * R + 1;
-            const int total = 2 * side * side + 4 * (side - 1) * (side - 2);
+            const int shell = 2 * side * side + 4 * (side - 1) * (side - 2);
+            const int total = shell + (R == 1 ? 1 : 0);   // ring 1 also carries the query's own sub-cell
             const float inv_side = 1.0f / (float)side, inv_per = 1.0f / (float)(4 * (side - 1));
-            for (int base = 0; base < total; base += 32) {
-                const int t = base + lane;
-                bool ok = false;
-                uint32_t a = 0, b = 0;
-                if (t < total) {
-                    int dx, dy, dz;
-                    shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
-                    const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
-                    if (X >= lx && X <= hx && Y >= ly && Y <= hy && Z >= lz && Z <= hz) {
-                        float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
-                        float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
-                        float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
-                        const float dist2 = ax * ax + ay * ay + az * az;
-                        const float L = lim * m;
-                        if (dist2 <= L * L) {
-                            const uint32_t key = key_of(X, Y, Z);
-                            a = __ldg(G.key_starts + key);
-                            b = __ldg(G.key_starts + key + 1);
-                            ok = b > a;
+            const float L = lim * m;
+            for (int base = 0; base < total; base += 32 * NM) {
+                uint32_t a[NM], b[NM];
+#pragma unroll
+                for (int u = 0; u < NM; u++) {
+                    const int t = base + 32 * u + lane;
+                    a[u] = 0u; b[u] = 0u;
+                    if (t < total) {
+                        int dx = 0, dy = 0, dz = 0;
+                        if (t < shell) shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
+                        const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
+                        if (X >= lx && X <= hx && Y >= ly && Y <= hy && Z >= lz && Z <= hz) {
+                            float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
+                            float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
+                            float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
+                            if (ax * ax + ay * ay + az * az <= L * L) {
+                                const uint32_t key = key_of(X, Y, Z);
+                                a[u] = __ldg(G.key_starts + key);
+                                b[u] = __ldg(G.key_starts + key + 1);
+                            }
                         }
                     }
                 }
-                enqueue(ok, a, b - a);
+#pragma unroll
+                for (int u = 0; u < NM; u++)
+                    if (base + 32 * u < total) enqueue(b[u] > a[u], a[u], b[u] - a[u]);
             }
             flush();
-            if (n > k) merge();
+            if (n > k) bound();
         }
         flush();
     }
 };
 
 template <int UCAP>
-__global__ void __launch_bounds__(WARPS * 32, 3)
+__global__ void __launch_bounds__(WARPS * 32, 4)
 k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, GatherOut O) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -466,14 +584,22 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
         const float alpha = 1.818f, beta = 1.953f;
         const float fr = rk * rk;
         const float norm = 1.f - expf(-beta);
-        for (int e = lane; e < cnt; e += 32) {
-            uint32_t s = U.slot[e];
-            V3 pd = ld3(G.gdir + 3 * (size_t)s);
-            float cs = vdot(nrm, vneg(pd));
-            if (cs > 0) {
-                float d = __uint_as_float((uint32_t)(U.key[e] >> 32));
+        for (int e0 = 0; e0 < cnt; e0 += 64) {
+            const int ea = e0 + lane, eb = ea + 32;
+            const bool va = ea < cnt, vb = eb < cnt;
+            const uint32_t sa = va ? U.slot[ea] : 0u, sb = vb ? U.slot[eb] : 0u;
+            V3 pda = v3(0.f, 0.f, 0.f), pdb = pda, pwa = pda, pwb = pda;
+            if (va) { pda = ld3(G.gdir + 3 * (size_t)sa); pwa = ld3(G.gpow + 3 * (size_t)sa); }
+            if (vb) { pdb = ld3(G.gdir + 3 * (size_t)sb); pwb = ld3(G.gpow + 3 * (size_t)sb); }
+            if (va && vdot(nrm, vneg(pda)) > 0) {
+                float d = __uint_as_float((uint32_t)(U.key[ea] >> 32));
                 float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / norm);
-                res = vadd(res, vscale(ld3(G.gpow + 3 * (size_t)s), filter));
+                res = vadd(res, vscale(pwa, filter));
+            }
+            if (vb && vdot(nrm, vneg(pdb)) > 0) {
+                float d = __uint_as_float((uint32_t)(U.key[eb] >> 32));
+                float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / norm);
+                res = vadd(res, vscale(pwb, filter));
             }
         }
 #pragma unroll
