@@ -11,6 +11,7 @@
 #include "pm_device.cuh"
 #include "pm_gather.cuh"
 #include "pm_grid.cuh"
+#include "pm_mlp.cuh"
 #include "pm_render.cuh"
 #include "pm_scan.cuh"
 #include "pm_scene.cuh"
@@ -65,6 +66,12 @@ struct pm_ctx {
     // render scratch
     DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, est_c;
     DevBuf status, gws;
+    // learned radiance cache
+    bool has_cache = false;
+    DevBuf cache_w32, cache_w16, cache_m, cache_v, cache_grad, cache_loss;
+    pm_cache_opts cache_opts = {};
+    float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};
+    int cache_step = 0;
     cudaEvent_t ev[12] = {};
     float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t launches = 0;      // kernels this context has launched
@@ -213,7 +220,8 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage_pos, &ctx->stage_dir,
                       &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
                       &ctx->scratch_pow, &ctx->req_a, &ctx->req_b, &ctx->req_c, &ctx->req_counter, &ctx->px_base,
-                      &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws};
+                      &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws, &ctx->cache_w32,
+                      &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -245,6 +253,159 @@ int pm_status(pm_ctx* ctx, uint32_t* out_bits) {
 int pm_launch_count(pm_ctx* ctx, int64_t* out) {
     if (!ctx || !out) return PM_ERR_INVALID;
     *out = ctx->launches;
+    return PM_OK;
+}
+
+namespace {
+
+MlpNet cache_net(pm_ctx* ctx) {
+    MlpNet net;
+    net.w = P<__nv_bfloat16>(ctx->cache_w16);
+    for (int a = 0; a < 3; a++) { net.lo[a] = ctx->cache_lo[a]; net.inv[a] = ctx->cache_inv[a]; }
+    net.out_scale = ctx->cache_opts.out_scale;
+    return net;
+}
+
+MlpInputs cache_inputs(const float* pos, const float* nrm, int64_t n) {
+    MlpInputs in{};
+    in.n = n;
+    in.pos3 = pos;
+    in.nrm3 = nrm;
+    return in;
+}
+
+// loss and gradient of n samples into ctx->cache_grad (zeroed first); loss_out: mean squared error
+int cache_backprop(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                   int64_t n, float* loss_out) {
+    CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
+    CK(cudaMemsetAsync(ctx->cache_loss.p, 0, 4, ctx->st));
+    const float grad_scale = 2.f / (3.f * (float)n);
+    CK(mlp_train(cache_net(ctx), cache_inputs(pos, nrm, n), target, weight, grad_scale, P<float>(ctx->cache_grad),
+                 P<float>(ctx->cache_loss), P<unsigned>(ctx->status), ctx->sm_count, ctx->st));
+    ctx->launches += 1;
+    if (loss_out) {
+        float l = 0.f;
+        CK(cudaMemcpyAsync(&l, ctx->cache_loss.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        *loss_out = l / (3.f * (float)n);
+    }
+    return PM_OK;
+}
+
+uint64_t splitmix64(uint64_t& x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+int pm_cache_init(pm_ctx* ctx, const pm_cache_opts* o) {
+    if (!ctx || !o) return PM_ERR_INVALID;
+    if (!(o->lr >= 0.f) || !(o->beta1 >= 0.f && o->beta1 < 1.f) || !(o->beta2 >= 0.f && o->beta2 < 1.f) ||
+        !(o->eps > 0.f) || !(o->out_scale > 0.f))
+        return fail(ctx, PM_ERR_INVALID, "cache options: lr >= 0, 0 <= beta < 1, eps > 0, out_scale > 0");
+    CK(cudaSetDevice(ctx->device));
+    const float* box = o->aabb;
+    bool zero = true;
+    for (int a = 0; a < 6; a++) zero = zero && box[a] == 0.f;
+    if (zero) {
+        if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "cache: no encoding box and no scene");
+        box = ctx->aabb;
+    }
+    for (int a = 0; a < 3; a++) {
+        const float ext = box[3 + a] - box[a];
+        ctx->cache_lo[a] = box[a];
+        ctx->cache_inv[a] = ext > 0.f ? 1.f / ext : 1.f;
+    }
+    ENSURE(ctx->cache_w32, (size_t)PM_CACHE_PARAMS * 4);
+    ENSURE(ctx->cache_w16, (size_t)PM_CACHE_PARAMS * 2);
+    ENSURE(ctx->cache_m, (size_t)PM_CACHE_PARAMS * 4);
+    ENSURE(ctx->cache_v, (size_t)PM_CACHE_PARAMS * 4);
+    ENSURE(ctx->cache_grad, (size_t)PM_CACHE_PARAMS * 4);
+    ENSURE(ctx->cache_loss, 16);
+    // He-uniform weights for the ReLU layers, a small output layer; padding zero
+    std::vector<float> w(PM_CACHE_PARAMS, 0.f);
+    uint64_t state = o->seed;
+    for (int l = 0; l < MLP_LAYERS; l++) {
+        const int fan_in = l == 0 ? MLP_FEATURES : MLP_DIM;
+        const int outs = l == MLP_LAYERS - 1 ? 3 : MLP_DIM;
+        const float b = (l == MLP_LAYERS - 1 ? 0.5f : 1.f) * std::sqrt(6.f / (float)fan_in);
+        for (int r = 0; r < outs; r++)
+            for (int c = 0; c < fan_in; c++) {
+                const double u = (double)(splitmix64(state) >> 11) * (1.0 / 9007199254740992.0);
+                w[(size_t)l * MLP_LAYER_STRIDE + r * MLP_DIM + c] = (float)((2.0 * u - 1.0) * b);
+            }
+    }
+    CK(cudaMemcpyAsync(ctx->cache_w32.p, w.data(), (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemsetAsync(ctx->cache_m.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
+    CK(cudaMemsetAsync(ctx->cache_v.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
+    CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
+    CK(mlp_to_bf16(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->launches += 1;
+    ctx->cache_opts = *o;
+    ctx->cache_step = 0;
+    ctx->has_cache = true;
+    return PM_OK;
+}
+
+int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                        int64_t n, float* out_loss) {
+    if (!ctx) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    if (n <= 0 || !pos || !nrm || !target) return fail(ctx, PM_ERR_INVALID, "cache train: n > 0 and sample arrays required");
+    CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_backprop(ctx, pos, nrm, target, weight, n, out_loss)) return rc;
+    ctx->cache_step++;
+    const pm_cache_opts& o = ctx->cache_opts;
+    CK(mlp_adam(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), P<float>(ctx->cache_grad),
+                P<float>(ctx->cache_m), P<float>(ctx->cache_v), ctx->cache_step, o.lr, o.beta1, o.beta2, o.eps, ctx->st));
+    ctx->launches += 1;
+    return check_status(ctx, "cache train");
+}
+
+int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                      int64_t n, float* out_grad_host, float* out_loss) {
+    if (!ctx || !out_grad_host) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    if (n <= 0 || !pos || !nrm || !target) return fail(ctx, PM_ERR_INVALID, "cache gradient: n > 0 and sample arrays required");
+    CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_backprop(ctx, pos, nrm, target, weight, n, out_loss)) return rc;
+    CK(cudaMemcpyAsync(out_grad_host, ctx->cache_grad.p, (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return check_status(ctx, "cache gradient");
+}
+
+int pm_cache_infer(pm_ctx* ctx, const float* pos, const float* nrm, int64_t n, float* out_rgb) {
+    if (!ctx) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    if (n < 0 || (n > 0 && (!pos || !nrm || !out_rgb))) return fail(ctx, PM_ERR_INVALID, "cache infer: bad arguments");
+    CK(cudaSetDevice(ctx->device));
+    CK(mlp_infer(cache_net(ctx), cache_inputs(pos, nrm, n), out_rgb, P<unsigned>(ctx->status), ctx->sm_count, ctx->st));
+    if (n > 0) ctx->launches += 1;
+    return check_status(ctx, "cache infer");
+}
+
+int pm_cache_get_params(pm_ctx* ctx, float* out) {
+    if (!ctx || !out) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(out, ctx->cache_w32.p, (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return PM_OK;
+}
+
+int pm_cache_set_params(pm_ctx* ctx, const float* in) {
+    if (!ctx || !in) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->cache_w32.p, in, (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(mlp_to_bf16(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->launches += 1;
     return PM_OK;
 }
 

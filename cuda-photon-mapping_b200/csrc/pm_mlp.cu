@@ -1,0 +1,515 @@
+// pm_mlp.cu -- learned radiance cache kernels (see pm_mlp.cuh).
+//
+// Tensor-core path (sm_100a): tcgen05.mma.cta_group::1.kind::f16 with BF16
+// operands read from shared memory through matrix descriptors and FP32
+// accumulators in tensor memory (TMEM), issued by one thread, completion
+// signalled through tcgen05.commit on an mbarrier, accumulators read back with
+// tcgen05.ld (32 lanes x 32 bits per warp).
+//
+// Every operand lives in shared memory in the no-swizzle canonical layout of
+// 8 x 8 core matrices (8 rows of 16 bytes), column blocks outermost:
+//   (r, c) of an R-row matrix -> ((c / 8) * (R / 8) + r / 8) * 128 + (r % 8) * 16 + (c % 8) * 2.
+// The same bytes serve as a K-major operand (rows = M or N, columns = K:
+// leading byte offset 16 R between K blocks, stride byte offset 128 between
+// row blocks) and as an MN-major operand (rows = K, columns = M or N: leading
+// byte offset 128, stride byte offset 16 R).  So activations [sample][feature]
+// feed the forward product (K-major A) and the weight gradient (MN-major A),
+// output gradients [sample][out] feed the input gradient (K-major A) and the
+// weight gradient (MN-major B), and weights [out][in] feed the forward product
+// (K-major B) and the input gradient (MN-major B) without any copy.
+//
+// Per 128-sample tile (one thread per sample row, 4 warps):
+//   forward   D[128 x out] = X_l[128 x 64] W_l^T               M=128, 4 MMAs (K=16)
+//   backward  dW_l += X_l^T[64 x 128] dY_l[128 x out]         M=64,  8 MMAs, accumulated in TMEM over tiles
+//             dX   = dY_l[128 x out] W_l[out x 64]             M=128, out/16 MMAs
+// TMEM columns: [0, 64) forward / input-gradient tile, [64 + 64 l, ...) the
+// weight-gradient accumulator of layer l (M=64: rows 16 w + i in lanes 32 w + i).
+#include <cmath>
+#include <algorithm>
+#include "pm_mlp.cuh"
+#include "pm_device.cuh"
+
+namespace pm {
+
+namespace {
+
+constexpr int TILE = 128;
+constexpr int THREADS = 128;
+constexpr int WAIT_LIMIT = 1 << 24;        // polls of an mbarrier before giving up
+constexpr uint32_t TMEM_COLS_TRAIN = 512;
+constexpr uint32_t TMEM_COLS_INFER = 64;
+
+// shared-memory carve-up (bytes)
+constexpr uint32_t W_BYTES = 4 * 8192 + 2048;       // layers 0-3: 64x64, layer 4: 16x64
+constexpr uint32_t X_BYTES = TILE * MLP_DIM * 2;    // one [128][64] activation / gradient tile
+constexpr uint32_t TRAIN_OFF_X = W_BYTES;                       // X_0 .. X_4
+constexpr uint32_t TRAIN_OFF_G = TRAIN_OFF_X + 5 * X_BYTES;     // two gradient tiles
+constexpr uint32_t TRAIN_OFF_BAR = TRAIN_OFF_G + 2 * X_BYTES;
+constexpr uint32_t TRAIN_SMEM = TRAIN_OFF_BAR + 64;
+constexpr uint32_t INFER_OFF_X = W_BYTES;                       // two activation tiles
+constexpr uint32_t INFER_OFF_BAR = INFER_OFF_X + 2 * X_BYTES;
+constexpr uint32_t INFER_SMEM = INFER_OFF_BAR + 64;
+
+__host__ __device__ constexpr uint32_t w_off(int l) { return (uint32_t)l * 8192u; }
+
+__device__ __forceinline__ uint32_t cm_off(int r, int c, int R) {
+    return (uint32_t)(((c >> 3) * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (c & 7) * 2);
+}
+
+// shared-memory matrix descriptor: start address, leading / stride byte
+// offsets (16-byte units), descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3fffu) | ((uint64_t)((lbo >> 4) & 0x3fffu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fffu) << 32) | ((uint64_t)1 << 46);
+}
+
+// instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :: "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(a) : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// bounded wait for the completion of phase `phase`; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+    for (int it = 0; it < WAIT_LIMIT; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(a), "r"(phase) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {   // whole warp
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(dst), "r"(cols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {   // whole warp
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(cols) : "memory");
+}
+// 16 consecutive 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ void unpack_bf16(uint32_t u, float& a, float& b) {
+    const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&u);
+    a = __low2float(h);
+    b = __high2float(h);
+}
+
+// weights (global [layer][out][in] bf16) -> core-matrix layout
+__device__ void load_weights(const __nv_bfloat16* __restrict__ w, unsigned char* sW) {
+    constexpr int CHUNKS = (4 * 64 + 16) * 8;   // 16-byte chunks
+    for (int q = threadIdx.x; q < CHUNKS; q += THREADS) {
+        const int row = q >> 3, j = q & 7;                  // global row over all layers, 8-column block
+        const int l = row < 256 ? row >> 6 : 4;
+        const int o = row < 256 ? row & 63 : row - 256;
+        const uint4 v = *reinterpret_cast<const uint4*>(w + (size_t)l * MLP_LAYER_STRIDE + o * MLP_DIM + 8 * j);
+        *reinterpret_cast<uint4*>(sW + w_off(l) + cm_off(o, 8 * j, mlp_out_dim(l))) = v;
+    }
+}
+
+// one input sample: position, normal, whether it is used
+__device__ __forceinline__ bool load_sample(const MlpInputs& in, int64_t i, V3& p, V3& n) {
+    p = v3(0.f, 0.f, 0.f);
+    n = v3(0.f, 0.f, 1.f);
+    if (i >= in.n) return false;
+    if (in.pos3) {
+        p = ld3(in.pos3 + 3 * i);
+        n = ld3(in.nrm3 + 3 * i);
+        return true;
+    }
+    const float4 a = in.rec_pos[i], b = in.rec_nrm[i];
+    p = xyz(a);
+    n = xyz(b);
+    return (__float_as_uint(b.w) & in.flag_mask) != 0u;
+}
+
+// Encoding: u = (p - lo) * inv per axis, and the octahedral map of the normal
+// to [0, 1]^2; each of the 5 values s gives sin(pi 2^f s), cos(pi 2^f s) for
+// f = 0..5 (60 features, then 4 zeros).  Written as row `row` of an [128][64] tile.
+__device__ __forceinline__ void write_features(unsigned char* sX, int row, const MlpNet& net, V3 p, V3 n) {
+    float s[5];
+    s[0] = (p.x - net.lo[0]) * net.inv[0];
+    s[1] = (p.y - net.lo[1]) * net.inv[1];
+    s[2] = (p.z - net.lo[2]) * net.inv[2];
+    float a = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
+    if (!(a > 0.f)) a = 1.f;
+    float ox = n.x / a, oy = n.y / a;
+    if (n.z < 0.f) {
+        const float tx = (1.f - fabsf(oy)) * (ox >= 0.f ? 1.f : -1.f);
+        const float ty = (1.f - fabsf(ox)) * (oy >= 0.f ? 1.f : -1.f);
+        ox = tx;
+        oy = ty;
+    }
+    s[3] = 0.5f * ox + 0.5f;
+    s[4] = 0.5f * oy + 0.5f;
+    uint32_t pk[32];
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            float sn, cs;
+            sincospif(s[j] * (float)(1 << f), &sn, &cs);
+            pk[6 * j + f] = pack_bf16(sn, cs);
+        }
+    }
+    pk[30] = 0u;
+    pk[31] = 0u;
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+        *reinterpret_cast<uint4*>(sX + cm_off(row, 8 * c, TILE)) =
+            make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+}
+
+// forward product of layer l into TMEM columns [0, out)
+__device__ __forceinline__ void issue_forward(int l, uint32_t tm, uint32_t xa, uint32_t wa) {
+    const int out = mlp_out_dim(l);
+    const uint32_t lbo_w = 16u * (uint32_t)out;
+    const uint32_t id = idesc_bf16(TILE, out, 0, 0);
+#pragma unroll
+    for (int s = 0; s < 4; s++) umma(tm, sdesc(xa + 4096u * s, 2048u, 128u), sdesc(wa + 2u * lbo_w * s, lbo_w, 128u), id, s > 0);
+}
+
+// ReLU of a [128 x 64] TMEM tile row (this thread's) -> bf16 row of the next activation tile
+__device__ __forceinline__ void relu_row_to_smem(uint32_t taddr, unsigned char* dst, int row) {
+#pragma unroll
+    for (int c0 = 0; c0 < 64; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr + c0, v);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            uint4 q;
+            q.x = pack_bf16(fmaxf(v[8 * h + 0], 0.f), fmaxf(v[8 * h + 1], 0.f));
+            q.y = pack_bf16(fmaxf(v[8 * h + 2], 0.f), fmaxf(v[8 * h + 3], 0.f));
+            q.z = pack_bf16(fmaxf(v[8 * h + 4], 0.f), fmaxf(v[8 * h + 5], 0.f));
+            q.w = pack_bf16(fmaxf(v[8 * h + 6], 0.f), fmaxf(v[8 * h + 7], 0.f));
+            *reinterpret_cast<uint4*>(dst + cm_off(row, c0 + 8 * h, TILE)) = q;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const float* __restrict__ weight,
+            float grad_scale, float* __restrict__ grad, float* __restrict__ loss_sum, unsigned* status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char* sW = smem;
+    unsigned char* sX = smem + TRAIN_OFF_X;
+    unsigned char* sG = smem + TRAIN_OFF_G;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + TRAIN_OFF_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TRAIN_OFF_BAR + 8);
+    load_weights(net.w, sW);
+    if (tid == 0) mbar_init(bar);
+    if (warp == 0) tmem_alloc(tslot, TMEM_COLS_TRAIN);
+    fence_async_smem();
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tm = *tslot;
+    const uint32_t my_lanes = (uint32_t)(32 * warp) << 16;
+    const uint32_t sW_a = (uint32_t)__cvta_generic_to_shared(sW);
+    const uint32_t sX_a = (uint32_t)__cvta_generic_to_shared(sX);
+    const uint32_t sG_a = (uint32_t)__cvta_generic_to_shared(sG);
+    const float inv_scale = 1.f / net.out_scale;
+    uint32_t phase = 0;
+    bool ok = true, any = false;
+    float loss = 0.f;
+    const int64_t tiles = (in.n + TILE - 1) / TILE;
+    int iter = 0;
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, iter++) {
+        const int64_t i = tile * TILE + tid;
+        V3 p, n;
+        const bool use = load_sample(in, i, p, n);
+        const float wgt = use ? (weight ? weight[i] : 1.f) : 0.f;
+        const V3 t = use ? ld3(target + 3 * i) : v3(0.f, 0.f, 0.f);
+        write_features(sX, tid, net, p, n);
+        fence_async_smem();
+        tc_before();
+        __syncthreads();
+        tc_after();
+        float y[3] = {0.f, 0.f, 0.f};
+        for (int l = 0; l < MLP_LAYERS && ok; l++) {
+            if (tid == 0) {
+                issue_forward(l, tm, sX_a + l * X_BYTES, sW_a + w_off(l));
+                umma_commit(bar);
+            }
+            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            phase ^= 1u;
+            tc_after();
+            if (!ok) break;
+            if (l < MLP_LAYERS - 1) {
+                relu_row_to_smem(tm + my_lanes, sX + (l + 1) * X_BYTES, tid);
+            } else {
+                float v[16];
+                tmem_ld16(tm + my_lanes, v);
+                y[0] = v[0]; y[1] = v[1]; y[2] = v[2];
+            }
+            tc_before();
+            fence_async_smem();
+            __syncthreads();
+            tc_after();
+        }
+        if (!ok) break;
+        // d(loss)/dy for the MSE against target / out_scale
+        const float d0 = y[0] - t.x * inv_scale, d1 = y[1] - t.y * inv_scale, d2 = y[2] - t.z * inv_scale;
+        loss += wgt * (d0 * d0 + d1 * d1 + d2 * d2);
+        const float g = grad_scale * wgt;
+        *reinterpret_cast<uint4*>(sG + cm_off(tid, 0, TILE)) =
+            make_uint4(pack_bf16(g * d0, g * d1), pack_bf16(g * d2, 0.f), 0u, 0u);
+        *reinterpret_cast<uint4*>(sG + cm_off(tid, 8, TILE)) = make_uint4(0u, 0u, 0u, 0u);
+        fence_async_smem();
+        tc_before();
+        __syncthreads();
+        tc_after();
+        int cur = 0;
+        for (int l = MLP_LAYERS - 1; l >= 0; l--) {
+            const int out = mlp_out_dim(l);
+            const uint32_t xa = sX_a + l * X_BYTES, ga = sG_a + cur * X_BYTES, wa = sW_a + w_off(l);
+            if (tid == 0) {
+                const uint32_t idw = idesc_bf16(64, out, 1, 1);
+#pragma unroll
+                for (int s = 0; s < TILE / 16; s++)
+                    umma(tm + 64u + 64u * l, sdesc(xa + 256u * s, 128u, 2048u), sdesc(ga + 256u * s, 128u, 2048u),
+                         idw, (iter > 0 || s > 0) ? 1u : 0u);
+                if (l > 0) {
+                    const uint32_t idx = idesc_bf16(TILE, 64, 0, 1);
+                    for (int s = 0; s < out / 16; s++)
+                        umma(tm, sdesc(ga + 4096u * s, 2048u, 128u), sdesc(wa + 256u * s, 128u, 16u * (uint32_t)out),
+                             idx, s > 0);
+                }
+                umma_commit(bar);
+            }
+            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            phase ^= 1u;
+            tc_after();
+            if (!ok) break;
+            if (l > 0) {
+                // dY_{l-1} = dX * [X_l > 0], bf16, into the other gradient tile
+                unsigned char* xrow = sX + l * X_BYTES;
+                unsigned char* dst = sG + (cur ^ 1) * X_BYTES;
+#pragma unroll
+                for (int c0 = 0; c0 < 64; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(tm + my_lanes + c0, v);
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const uint4 xq = *reinterpret_cast<const uint4*>(xrow + cm_off(tid, c0 + 8 * h, TILE));
+                        const uint32_t xs[4] = {xq.x, xq.y, xq.z, xq.w};
+                        uint32_t o[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            float xa0, xa1;
+                            unpack_bf16(xs[e], xa0, xa1);
+                            o[e] = pack_bf16(xa0 > 0.f ? v[8 * h + 2 * e] : 0.f, xa1 > 0.f ? v[8 * h + 2 * e + 1] : 0.f);
+                        }
+                        *reinterpret_cast<uint4*>(dst + cm_off(tid, c0 + 8 * h, TILE)) = make_uint4(o[0], o[1], o[2], o[3]);
+                    }
+                }
+            }
+            tc_before();
+            fence_async_smem();
+            __syncthreads();
+            tc_after();
+            cur ^= 1;
+        }
+        any = true;
+    }
+    if (!ok) {
+        if (tid == 0) raise_status(status, ST_TIMEOUT);
+        (void)mbar_wait(bar, phase);   // let a late product land before the columns are freed
+    } else if (any) {
+        // weight gradients: lanes 0-15 of each warp hold rows 16 w + lane (input index)
+        for (int l = 0; l < MLP_LAYERS; l++) {
+            const int out = mlp_out_dim(l);
+            for (int c0 = 0; c0 < out; c0 += 16) {
+                float v[16];
+                tmem_ld16(tm + my_lanes + 64u + 64u * l + c0, v);
+                if (lane < 16) {
+                    const int m = 16 * warp + lane;
+#pragma unroll
+                    for (int e = 0; e < 16; e++) atomicAdd(grad + (size_t)l * MLP_LAYER_STRIDE + (c0 + e) * MLP_DIM + m, v[e]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+    if (lane == 0 && loss != 0.f) atomicAdd(loss_sum, loss);
+    tc_before();
+    __syncthreads();
+    tc_after();
+    if (warp == 0) tmem_dealloc(tm, TMEM_COLS_TRAIN);
+}
+
+__global__ void __launch_bounds__(THREADS)
+k_mlp_infer(MlpNet net, MlpInputs in, float* __restrict__ out, unsigned* status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    unsigned char* sW = smem;
+    unsigned char* sX = smem + INFER_OFF_X;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + INFER_OFF_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + INFER_OFF_BAR + 8);
+    load_weights(net.w, sW);
+    if (tid == 0) mbar_init(bar);
+    if (warp == 0) tmem_alloc(tslot, TMEM_COLS_INFER);
+    fence_async_smem();
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tm = *tslot;
+    const uint32_t my_lanes = (uint32_t)(32 * warp) << 16;
+    const uint32_t sW_a = (uint32_t)__cvta_generic_to_shared(sW);
+    const uint32_t sX_a = (uint32_t)__cvta_generic_to_shared(sX);
+    uint32_t phase = 0;
+    bool ok = true;
+    const int64_t tiles = (in.n + TILE - 1) / TILE;
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const int64_t i = tile * TILE + tid;
+        V3 p, n;
+        const bool use = load_sample(in, i, p, n);
+        write_features(sX, tid, net, p, n);
+        fence_async_smem();
+        tc_before();
+        __syncthreads();
+        tc_after();
+        float y[3] = {0.f, 0.f, 0.f};
+        for (int l = 0; l < MLP_LAYERS && ok; l++) {
+            const int src = l & 1;
+            if (tid == 0) {
+                issue_forward(l, tm, sX_a + src * X_BYTES, sW_a + w_off(l));
+                umma_commit(bar);
+            }
+            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            phase ^= 1u;
+            tc_after();
+            if (!ok) break;
+            if (l < MLP_LAYERS - 1) {
+                relu_row_to_smem(tm + my_lanes, sX + (src ^ 1) * X_BYTES, tid);
+            } else {
+                float v[16];
+                tmem_ld16(tm + my_lanes, v);
+                y[0] = v[0]; y[1] = v[1]; y[2] = v[2];
+            }
+            tc_before();
+            fence_async_smem();
+            __syncthreads();
+            tc_after();
+        }
+        if (!ok) break;
+        if (i < in.n) {
+            const float sc = use ? net.out_scale : 0.f;
+            out[3 * i] = y[0] * sc;
+            out[3 * i + 1] = y[1] * sc;
+            out[3 * i + 2] = y[2] * sc;
+        }
+    }
+    if (!ok) {
+        if (tid == 0) raise_status(status, ST_TIMEOUT);
+        (void)mbar_wait(bar, phase);
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    if (warp == 0) tmem_dealloc(tm, TMEM_COLS_INFER);
+}
+
+__global__ void k_adam(float* __restrict__ w32, __nv_bfloat16* __restrict__ w16, float* __restrict__ grad,
+                       float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MLP_PARAMS) return;
+    const float g = grad[i];
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    const float w = w32[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    w32[i] = w;
+    w16[i] = __float2bfloat16_rn(w);
+    grad[i] = 0.f;
+}
+
+__global__ void k_to_bf16(const float* __restrict__ w32, __nv_bfloat16* __restrict__ w16) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < MLP_PARAMS) w16[i] = __float2bfloat16_rn(w32[i]);
+}
+
+}  // namespace
+
+cudaError_t mlp_train(const MlpNet& net, const MlpInputs& in, const float* target, const float* weight,
+                      float grad_scale, float* grad, float* loss_sum, unsigned* status, int sm_count,
+                      cudaStream_t st) {
+    if (in.n <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM);
+    if (e != cudaSuccess) return e;
+    const int64_t tiles = (in.n + TILE - 1) / TILE;
+    const int grid = (int)std::min<int64_t>(tiles, std::max(sm_count, 1));   // one CTA per SM: 512 TMEM columns each
+    k_mlp_train<<<grid, THREADS, TRAIN_SMEM, st>>>(net, in, target, weight, grad_scale, grad, loss_sum, status);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_infer(const MlpNet& net, const MlpInputs& in, float* out, unsigned* status, int sm_count,
+                      cudaStream_t st) {
+    if (in.n <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INFER_SMEM);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer, THREADS, INFER_SMEM)) != cudaSuccess)
+        return e;
+    per_sm = std::min(std::max(per_sm, 1), 512 / (int)TMEM_COLS_INFER);
+    const int64_t tiles = (in.n + TILE - 1) / TILE;
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)per_sm * std::max(sm_count, 1));
+    k_mlp_infer<<<grid, THREADS, INFER_SMEM, st>>>(net, in, out, status);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_adam(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int step, float lr,
+                     float beta1, float beta2, float eps, cudaStream_t st) {
+    const float c1 = (float)(1.0 / (1.0 - std::pow((double)beta1, step)));
+    const float c2 = (float)(1.0 / (1.0 - std::pow((double)beta2, step)));
+    k_adam<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(w32, w16, grad, m, v, lr, beta1, beta2, eps, c1, c2);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_to_bf16(const float* w32, __nv_bfloat16* w16, cudaStream_t st) {
+    k_to_bf16<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(w32, w16);
+    return cudaGetLastError();
+}
+
+}  // namespace pm

@@ -60,6 +60,14 @@ class Camera(C.Structure):
                         [self.viewport_w, self.viewport_h, self.focal], np.float32)
 
 
+class _CacheOpts(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("eps", C.c_float), ("out_scale", C.c_float), ("aabb", C.c_float * 6)]
+
+
+CACHE_PARAMS = 5 * 64 * 64
+
+
 class _RenderOpts(C.Structure):
     _fields_ = [("max_depth", C.c_int32), ("k_global", C.c_int32), ("r_global", C.c_float),
                 ("k_caustic", C.c_int32), ("r_caustic", C.c_float), ("faithful_caustic", C.c_int32)]
@@ -108,6 +116,12 @@ def library():
         "pm_status": ([vp, vp], C.c_int),
         "pm_launch_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
         "pm_render_requests": ([vp, C.POINTER(C.c_int64)], C.c_int),
+        "pm_cache_init": ([vp, C.POINTER(_CacheOpts)], C.c_int),
+        "pm_cache_train_step": ([vp, vp, vp, vp, vp, i64, vp], C.c_int),
+        "pm_cache_gradient": ([vp, vp, vp, vp, vp, i64, vp, vp], C.c_int),
+        "pm_cache_infer": ([vp, vp, vp, i64, vp], C.c_int),
+        "pm_cache_get_params": ([vp, vp], C.c_int),
+        "pm_cache_set_params": ([vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -267,6 +281,48 @@ class Context:
         self._check(self.L.pm_gather(self.h, map_id, n, _ptr(qpos), _ptr(qnrm), int(k), float(radius), _ptr(rad),
                                      _ptr(ids), _ptr(cnt)), "pm_gather")
         return rad, ids, cnt
+
+    # ------------------------------------------------------------ learned radiance cache
+    def cache_init(self, seed=0, lr=1e-3, beta1=0.9, beta2=0.99, eps=1e-8, out_scale=1.0, aabb=None):
+        box = (C.c_float * 6)(*([0.0] * 6 if aabb is None else [float(x) for x in aabb]))
+        o = _CacheOpts(int(seed), float(lr), float(beta1), float(beta2), float(eps), float(out_scale), box)
+        self._check(self.L.pm_cache_init(self.h, C.byref(o)), "pm_cache_init")
+
+    def _samples(self, *arrays):
+        torch = self.torch
+        return [None if a is None else torch.as_tensor(a).to(self.device, torch.float32).contiguous() for a in arrays]
+
+    def cache_train_step(self, pos, nrm, target, weight=None):
+        """One Adam step; returns the step's mean squared error (network units, before the update)."""
+        pos, nrm, target, weight = self._samples(pos, nrm, target, weight)
+        loss = C.c_float()
+        self._check(self.L.pm_cache_train_step(self.h, _ptr(pos), _ptr(nrm), _ptr(target), _ptr(weight),
+                                               pos.shape[0], C.byref(loss)), "pm_cache_train_step")
+        return loss.value
+
+    def cache_gradient(self, pos, nrm, target, weight=None):
+        pos, nrm, target, weight = self._samples(pos, nrm, target, weight)
+        g = np.zeros(CACHE_PARAMS, np.float32)
+        loss = C.c_float()
+        self._check(self.L.pm_cache_gradient(self.h, _ptr(pos), _ptr(nrm), _ptr(target), _ptr(weight),
+                                             pos.shape[0], g.ctypes.data, C.byref(loss)), "pm_cache_gradient")
+        return g, loss.value
+
+    def cache_infer(self, pos, nrm):
+        pos, nrm = self._samples(pos, nrm)
+        out = self.torch.empty((pos.shape[0], 3), dtype=self.torch.float32, device=self.device)
+        self._check(self.L.pm_cache_infer(self.h, _ptr(pos), _ptr(nrm), pos.shape[0], _ptr(out)), "pm_cache_infer")
+        return out
+
+    def cache_params(self):
+        w = np.zeros(CACHE_PARAMS, np.float32)
+        self._check(self.L.pm_cache_get_params(self.h, w.ctypes.data), "pm_cache_get_params")
+        return w
+
+    def cache_set_params(self, w):
+        w = np.ascontiguousarray(w, np.float32).reshape(-1)
+        assert w.size == CACHE_PARAMS
+        self._check(self.L.pm_cache_set_params(self.h, w.ctypes.data), "pm_cache_set_params")
 
     # ------------------------------------------------------------ render
     def render(self, cam: Camera, k_global, r_global, max_depth=4, k_caustic=0, r_caustic=0.2,

@@ -207,6 +207,47 @@ int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclus
  * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather, [4] resolve. */
 int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
 
+/* ---------------------------------------------------------------------------
+ * Learned radiance cache (no counterpart in the reference).  A small MLP maps
+ * (hit point, shading normal) to the global-map radiance estimate that
+ * Raytracer::get_color_from_photon_grid (CudaPhotonMapping/Raytracer.cuh:110-138)
+ * computes by a kNN gather.  Inputs: the point normalised to a box and the
+ * octahedral normal, encoded with sin / cos at 6 octaves (60 features); 4
+ * hidden layers of width 64 with ReLU; RGB output.  BF16 weights and
+ * activations on the tensor cores with FP32 accumulation; FP32 Adam.
+ * Parameters are PM_CACHE_PARAMS floats: 5 layers x [64 out][64 in], layer 0
+ * reads inputs 0..59, layer 4 writes outputs 0..2 (the rest stays zero).
+ * All sample arrays are device pointers, 3 floats per sample. */
+#define PM_CACHE_PARAMS (5 * 64 * 64)
+
+typedef struct pm_cache_opts {
+    uint64_t seed;          /* weight initialisation */
+    float lr, beta1, beta2, eps;   /* Adam */
+    float out_scale;        /* radiance = out_scale * network output (targets are divided by it) */
+    float aabb[6];          /* encoding box (min xyz, max xyz); all zero: the scene's box */
+} pm_cache_opts;
+
+/* (Re)initialise the cache: weights from the seed, Adam moments zero. */
+int pm_cache_init(pm_ctx* ctx, const pm_cache_opts* opts);
+
+/* One Adam step on the mean squared error over n samples (target: radiance,
+ * weight: per-sample weight or null).  *out_loss (optional) = the step's mean
+ * squared error in network units (before the update). */
+int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                        int64_t n, float* out_loss);
+
+/* Gradient of that loss with respect to the parameters, without an update
+ * (host output of PM_CACHE_PARAMS floats), and the loss. */
+int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                      int64_t n, float* out_grad_host, float* out_loss);
+
+/* Radiance predicted for n samples (out_rgb: device, 3 floats per sample). */
+int pm_cache_infer(pm_ctx* ctx, const float* pos, const float* nrm, int64_t n, float* out_rgb);
+
+/* Host copies of the FP32 master parameters (get / set, PM_CACHE_PARAMS floats). */
+int pm_cache_get_params(pm_ctx* ctx, float* out_params_host);
+int pm_cache_set_params(pm_ctx* ctx, const float* params_host);
+
 /* Gather requests (eye-path hits that query the global map) of the last
  * pm_render call: the number of kNN queries its gather stage answered. */
 int pm_render_requests(pm_ctx* ctx, int64_t* out);
