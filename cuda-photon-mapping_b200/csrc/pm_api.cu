@@ -11,6 +11,7 @@
 #include "pm_device.cuh"
 #include "pm_gather.cuh"
 #include "pm_grid.cuh"
+#include "pm_learned.cuh"
 #include "pm_mlp.cuh"
 #include "pm_render.cuh"
 #include "pm_scan.cuh"
@@ -69,6 +70,7 @@ struct pm_ctx {
     // learned radiance cache
     bool has_cache = false;
     DevBuf cache_w32, cache_w16, cache_m, cache_v, cache_grad, cache_loss;
+    DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts;
     pm_cache_opts cache_opts = {};
     float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};
     int cache_step = 0;
@@ -221,7 +223,9 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
                       &ctx->scratch_pow, &ctx->req_a, &ctx->req_b, &ctx->req_c, &ctx->req_counter, &ctx->px_base,
                       &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws, &ctx->cache_w32,
-                      &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss};
+                      &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
+                      &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
+                      &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -909,8 +913,18 @@ int pm_camera_setup(const float position[3], const float direction[3], const flo
     return PM_OK;
 }
 
-int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance) {
-    if (!ctx || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
+namespace {
+
+// state of one render between the eye pass and the resolve
+struct FrameSetup {
+    CameraDev cd;
+    Requests R;
+    DevScene S;
+    int64_t npx = 0, cap = 0, nreq = 0;
+    bool caustic = false;
+};
+
+int render_checks(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o) {
     if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
     if (o->max_depth < 0 || o->max_depth > RENDER_MAX_DEPTH) return fail(ctx, PM_ERR_INVALID, "max_depth must be 0..5");
     if (o->k_global < 0 || o->k_global > 256 || o->k_caustic < 0 || o->k_caustic > 256)
@@ -919,65 +933,168 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     MapState& C = ctx->maps[PM_MAP_CAUSTIC];
     if (!G.built) return fail(ctx, PM_ERR_INVALID, "global map grid not built");
-    CK(cudaSetDevice(ctx->device));
-    const int64_t npx = (int64_t)cam->width * cam->height;
-    const int64_t per_px = ((int64_t)1 << std::max(o->max_depth, 1)) - 1;
-    const int64_t cap = npx * per_px;
-    ENSURE(ctx->req_a, (size_t)cap * 16);
-    ENSURE(ctx->req_b, (size_t)cap * 16);
-    ENSURE(ctx->req_c, (size_t)cap * 16);
-    ENSURE(ctx->req_counter, 8);
-    ENSURE(ctx->px_base, (size_t)npx * 4);
-    ENSURE(ctx->px_count, (size_t)npx * 4);
-    ENSURE(ctx->est_g, (size_t)cap * 12);
-    const bool caustic = C.built;
-    if (caustic && o->faithful_caustic && C.n > G.n)
+    if (C.built && o->faithful_caustic && C.n > G.n)
         return fail(ctx, PM_ERR_INVALID, "faithful caustic estimate reads the global map with caustic indices: "
                                          "the caustic map must not be larger than the global map");
-    if (caustic) ENSURE(ctx->est_c, (size_t)cap * 12);
-    DevScene S = dev_scene(ctx);
+    return PM_OK;
+}
+
+// buffers, eye pass (timed into ev[4] .. ev[5]) and the request count
+int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F) {
+    MapState& C = ctx->maps[PM_MAP_CAUSTIC];
+    F.npx = (int64_t)cam->width * cam->height;
+    const int64_t per_px = ((int64_t)1 << std::max(o->max_depth, 1)) - 1;
+    F.cap = F.npx * per_px;
+    ENSURE(ctx->req_a, (size_t)F.cap * 16);
+    ENSURE(ctx->req_b, (size_t)F.cap * 16);
+    ENSURE(ctx->req_c, (size_t)F.cap * 16);
+    ENSURE(ctx->req_counter, 8);
+    ENSURE(ctx->px_base, (size_t)F.npx * 4);
+    ENSURE(ctx->px_count, (size_t)F.npx * 4);
+    ENSURE(ctx->est_g, (size_t)F.cap * 12);
+    F.caustic = C.built;
+    if (F.caustic) ENSURE(ctx->est_c, (size_t)F.cap * 12);
+    F.S = dev_scene(ctx);
+    for (int a = 0; a < 3; a++) {
+        F.cd.pos[a] = cam->position[a]; F.cd.fwd[a] = cam->forward[a]; F.cd.right[a] = cam->right[a]; F.cd.up[a] = cam->up[a];
+    }
+    F.cd.vw = cam->viewport_w; F.cd.vh = cam->viewport_h; F.cd.focal = cam->focal;
+    F.cd.W = cam->width; F.cd.H = cam->height;
+    Requests& R = F.R;
+    R.a = P<float4>(ctx->req_a); R.b = P<float4>(ctx->req_b); R.c = P<float4>(ctx->req_c);
+    R.cap = F.cap;
+    R.counter = P<unsigned long long>(ctx->req_counter);
+    R.px_base = P<uint32_t>(ctx->px_base);
+    R.px_count = P<uint32_t>(ctx->px_count);
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), ctx->st));
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    unsigned long long nreq = 0;
+    CK(cudaMemcpyAsync(&nreq, R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    F.nreq = (int64_t)std::min<unsigned long long>(nreq, (unsigned long long)F.cap);
+    ctx->last_requests = F.nreq;
+    ctx->launches += 1;
+    return PM_OK;
+}
+
+// caustic gather, resolve (ev[7] .. ev[8]) and the stage times
+int render_finish(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* out_rgb8, float* out_radiance) {
+    MapState& G = ctx->maps[PM_MAP_GLOBAL];
+    MapState& C = ctx->maps[PM_MAP_CAUSTIC];
+    if (F.caustic) {
+        GatherQueries Q{};
+        Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = 2u;
+        GatherOut OC{P<float>(ctx->est_c), nullptr, nullptr, nullptr};
+        CK(gather(grid_of(C, o->faithful_caustic ? G : C), Q, o->r_caustic, o->k_caustic, 1, OC,
+                  P<unsigned>(ctx->status), ctx->st));
+        ctx->launches += 1;
+    }
+    CK(cudaEventRecord(ctx->ev[7], ctx->st));
+    const float tone_t = (float)std::pow((double)0.6f, -1);
+    CK(resolve(F.S, F.cd, F.R, P<float>(ctx->est_g), F.caustic ? P<float>(ctx->est_c) : nullptr, tone_t, out_rgb8,
+               out_radiance, ctx->st));
+    CK(cudaEventRecord(ctx->ev[8], ctx->st));
+    ctx->launches += 1;
+    CK(cudaEventSynchronize(ctx->ev[8]));
+    ctx->stage_ms[2] = elapsed(ctx->ev[4], ctx->ev[5]);
+    ctx->stage_ms[3] = elapsed(ctx->ev[6], ctx->ev[7]);
+    ctx->stage_ms[4] = elapsed(ctx->ev[7], ctx->ev[8]);
+    return PM_OK;
+}
+
+}  // namespace
+
+int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance) {
+    if (!ctx || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
+    if (int rc = render_checks(ctx, cam, o)) return rc;
+    CK(cudaSetDevice(ctx->device));
+    FrameSetup F;
+    if (int rc = render_eye(ctx, cam, o, F)) return rc;
+    MapState& G = ctx->maps[PM_MAP_GLOBAL];
+    GatherQueries Q{};
+    Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = 1u;
+    GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OG, P<unsigned>(ctx->status), ctx->st));
+    ctx->launches += 1;
+    if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
+    return check_status(ctx, "render");
+}
+
+int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, const pm_learned_opts* lo,
+                      uint8_t* out_rgb8, float* out_radiance, pm_learned_stats* out_stats) {
+    if (!ctx || !cam || !o || !lo || !out_rgb8) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    if (lo->tile < 1 || lo->tile > 256 || lo->probes < 1 || lo->probes > 64 || lo->max_rel_err != lo->max_rel_err)
+        return fail(ctx, PM_ERR_INVALID, "learned options: tile 1..256, probes 1..64, max_rel_err not NaN");
+    if (int rc = render_checks(ctx, cam, o)) return rc;
+    CK(cudaSetDevice(ctx->device));
+    FrameSetup F;
+    if (int rc = render_eye(ctx, cam, o, F)) return rc;
+    MapState& G = ctx->maps[PM_MAP_GLOBAL];
+    const int T = lo->tile, Pn = lo->probes;
+    const int64_t ntiles = (int64_t)((cam->width + T - 1) / T) * ((cam->height + T - 1) / T);
+    const int64_t nprobe = ntiles * Pn;
+    ENSURE(ctx->est_mlp, (size_t)F.cap * 12);
+    ENSURE(ctx->est_fb, (size_t)F.cap * 12);
+    ENSURE(ctx->probe_pos, (size_t)nprobe * 16);
+    ENSURE(ctx->probe_nrm, (size_t)nprobe * 16);
+    ENSURE(ctx->probe_req, (size_t)nprobe * 4);
+    ENSURE(ctx->probe_est, (size_t)nprobe * 12);
+    ENSURE(ctx->tile_flag, (size_t)ntiles);
+    ENSURE(ctx->learned_counts, 16);
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    // the cache answers every global request
+    MlpInputs in{};
+    in.n = F.nreq; in.rec_pos = F.R.a; in.rec_nrm = F.R.b; in.flag_mask = 1u;
+    CK(mlp_infer(cache_net(ctx), in, P<float>(ctx->est_mlp), P<unsigned>(ctx->status), ctx->sm_count, ctx->st));
+    // exact gathers at the probes; tiles whose cache error is too large fall back
+    CK(learned_probes(F.cd, F.R, T, Pn, P<float4>(ctx->probe_pos), P<float4>(ctx->probe_nrm), P<uint32_t>(ctx->probe_req),
+                      ctx->st));
+    GatherQueries PQ{};
+    PQ.n = nprobe; PQ.pos4 = P<float4>(ctx->probe_pos); PQ.nrm4 = P<float4>(ctx->probe_nrm); PQ.flag_mask = 1u;
+    GatherOut PO{P<float>(ctx->probe_est), nullptr, nullptr, nullptr};
+    CK(gather(grid_of(G, G), PQ, o->r_global, o->k_global, 0, PO, P<unsigned>(ctx->status), ctx->st));
+    CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 16, ctx->st));
+    CK(learned_select(F.cd, F.R, F.nreq, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
+                      P<float>(ctx->est_mlp), lo->max_rel_err, P<uint8_t>(ctx->tile_flag),
+                      P<unsigned long long>(ctx->learned_counts), ctx->st));
+    GatherQueries Q{};
+    Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = LEARNED_FALLBACK;
+    GatherOut OF{P<float>(ctx->est_fb), nullptr, nullptr, nullptr};
+    CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OF, P<unsigned>(ctx->status), ctx->st));
+    CK(learned_merge(F.R, F.nreq, P<float>(ctx->est_mlp), P<float>(ctx->est_fb), P<float>(ctx->est_g), ctx->st));
+    ctx->launches += (F.nreq > 0 ? 1 : 0) + 1 + 1 + 1 + (F.nreq > 0 ? 1 : 0) + 1 + (F.nreq > 0 ? 1 : 0);
+    if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
+    if (out_stats) {
+        unsigned long long cnt[2] = {0, 0};
+        CK(cudaMemcpyAsync(cnt, ctx->learned_counts.p, 16, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        out_stats->tiles = ntiles;
+        out_stats->fallback_tiles = (int64_t)cnt[0];
+        out_stats->requests = F.nreq;
+        out_stats->fallback_requests = (int64_t)cnt[1];
+    }
+    return check_status(ctx, "learned render");
+}
+
+int pm_cache_sample_points(pm_ctx* ctx, const pm_camera* cam, int64_t n, uint64_t seed, float* out_pos, float* out_nrm,
+                           float* out_weight) {
+    if (!ctx || !cam) return PM_ERR_INVALID;
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
+    if (n < 0 || (n > 0 && (!out_pos || !out_nrm || !out_weight))) return fail(ctx, PM_ERR_INVALID, "sample points: bad arguments");
+    if (cam->width <= 0 || cam->height <= 0) return fail(ctx, PM_ERR_INVALID, "bad camera size");
+    CK(cudaSetDevice(ctx->device));
     CameraDev cd;
     for (int a = 0; a < 3; a++) {
         cd.pos[a] = cam->position[a]; cd.fwd[a] = cam->forward[a]; cd.right[a] = cam->right[a]; cd.up[a] = cam->up[a];
     }
     cd.vw = cam->viewport_w; cd.vh = cam->viewport_h; cd.focal = cam->focal;
     cd.W = cam->width; cd.H = cam->height;
-    Requests R;
-    R.a = P<float4>(ctx->req_a); R.b = P<float4>(ctx->req_b); R.c = P<float4>(ctx->req_c);
-    R.cap = cap;
-    R.counter = P<unsigned long long>(ctx->req_counter);
-    R.px_base = P<uint32_t>(ctx->px_base);
-    R.px_count = P<uint32_t>(ctx->px_count);
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
-    CK(eye_pass(S, cd, o->max_depth, R, P<unsigned>(ctx->status), ctx->st));
-    CK(cudaEventRecord(ctx->ev[5], ctx->st));
-    unsigned long long nreq = 0;
-    CK(cudaMemcpyAsync(&nreq, R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    nreq = std::min<unsigned long long>(nreq, (unsigned long long)cap);
-    ctx->last_requests = (int64_t)nreq;
-    GatherQueries Q{};
-    Q.n = (int64_t)nreq; Q.pos4 = R.a; Q.nrm4 = R.b; Q.flag_mask = 1u;
-    GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};
-    CK(cudaEventRecord(ctx->ev[6], ctx->st));
-    CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OG, P<unsigned>(ctx->status), ctx->st));
-    if (caustic) {
-        Q.flag_mask = 2u;
-        GatherOut OC{P<float>(ctx->est_c), nullptr, nullptr, nullptr};
-        CK(gather(grid_of(C, o->faithful_caustic ? G : C), Q, o->r_caustic, o->k_caustic, 1, OC,
-                  P<unsigned>(ctx->status), ctx->st));
-    }
-    CK(cudaEventRecord(ctx->ev[7], ctx->st));
-    const float tone_t = (float)std::pow((double)0.6f, -1);
-    CK(resolve(S, cd, R, P<float>(ctx->est_g), caustic ? P<float>(ctx->est_c) : nullptr, tone_t, out_rgb8,
-               out_radiance, ctx->st));
-    CK(cudaEventRecord(ctx->ev[8], ctx->st));
-    ctx->launches += 3 + (caustic ? 1 : 0);
-    CK(cudaEventSynchronize(ctx->ev[8]));
-    ctx->stage_ms[2] = elapsed(ctx->ev[4], ctx->ev[5]);
-    ctx->stage_ms[3] = elapsed(ctx->ev[6], ctx->ev[7]);
-    ctx->stage_ms[4] = elapsed(ctx->ev[7], ctx->ev[8]);
-    return check_status(ctx, "render");
+    CK(sample_primary_hits(dev_scene(ctx), cd, n, seed, out_pos, out_nrm, out_weight, ctx->st));
+    if (n > 0) ctx->launches += 1;
+    return check_status(ctx, "sample points");
 }
 
 int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive) {

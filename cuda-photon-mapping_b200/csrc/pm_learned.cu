@@ -1,0 +1,143 @@
+// pm_learned.cu -- the learned render's tile check and fallback selection.
+//
+// The learned render answers every global-map request of the eye pass with the
+// radiance cache, then checks the cache per screen tile: P probe requests per
+// tile (the first request of the pixels at fixed positions inside the tile)
+// are also answered by the exact kNN gather, and a tile whose mean relative
+// L1 error over its probes exceeds a threshold takes the exact gather for all
+// of its requests.  Probe slots are fixed per (tile, probe), so the result
+// does not depend on scheduling.
+#include "pm_learned.cuh"
+#include "pm_device.cuh"
+
+namespace pm {
+
+namespace {
+
+// probe position k of P inside a tile of edge T: a ceil(sqrt(P)) grid of cell centres
+__device__ __forceinline__ void probe_xy(int k, int P, int T, int& dx, int& dy) {
+    int g = 1;
+    while (g * g < P) g++;
+    dx = ((k % g) * 2 + 1) * T / (2 * g);
+    dy = ((k / g) * 2 + 1) * T / (2 * g);
+}
+
+__global__ void k_probe_select(CameraDev cam, Requests R, int tile, int P, int tiles_x, int64_t ntiles,
+                               float4* __restrict__ ppos, float4* __restrict__ pnrm, uint32_t* __restrict__ preq) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ntiles * P) return;
+    const int64_t t = s / P;
+    const int k = (int)(s % P);
+    int dx, dy;
+    probe_xy(k, P, tile, dx, dy);
+    const int x = (int)(t % tiles_x) * tile + dx, y = (int)(t / tiles_x) * tile + dy;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = make_float4(0.f, 0.f, 1.f, 0.f);
+    uint32_t q = 0xffffffffu;
+    if (x < cam.W && y < cam.H) {
+        const int64_t px = (int64_t)y * cam.W + x;
+        if (R.px_count[px] > 0) {
+            const uint32_t r = R.px_base[px];
+            const float4 rb = R.b[r];
+            if (__float_as_uint(rb.w) & 1u) {
+                a = R.a[r];
+                b = make_float4(rb.x, rb.y, rb.z, __uint_as_float(1u));
+                q = r;
+            }
+        }
+    }
+    ppos[s] = a;
+    pnrm[s] = b;
+    preq[s] = q;
+}
+
+// per tile: mean relative L1 error of the cache over its probes; flag > threshold
+// (a negative threshold flags every tile: the exact render)
+__global__ void k_tile_flags(int64_t ntiles, int P, const uint32_t* __restrict__ preq, const float* __restrict__ exact,
+                             const float* __restrict__ cached, float max_rel_err, uint8_t* __restrict__ flag,
+                             unsigned long long* __restrict__ nflag) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    float sum = 0.f;
+    int cnt = 0;
+    for (int k = 0; k < P; k++) {
+        const int64_t s = t * P + k;
+        const uint32_t q = preq[s];
+        if (q == 0xffffffffu) continue;
+        const V3 e = ld3(exact + 3 * s), c = ld3(cached + 3 * (size_t)q);
+        const float num = fabsf(c.x - e.x) + fabsf(c.y - e.y) + fabsf(c.z - e.z);
+        const float den = fabsf(e.x) + fabsf(e.y) + fabsf(e.z);
+        sum += num / fmaxf(den, 1e-12f);
+        cnt++;
+    }
+    const bool f = max_rel_err < 0.f || (cnt > 0 && sum > max_rel_err * (float)cnt);
+    flag[t] = f ? 1 : 0;
+    if (f) atomicAdd(nflag, 1ull);
+}
+
+// requests of flagged tiles that need the global estimate get flag bit 2
+__global__ void k_mark_fallback(int64_t nreq, Requests R, int W, int tile, int tiles_x, const uint8_t* __restrict__ flag,
+                                unsigned long long* __restrict__ nfb) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool fb = false;
+    if (q < nreq) {
+        float4 b = R.b[q];
+        uint32_t flags = __float_as_uint(b.w);
+        const uint32_t px = __float_as_uint(R.c[q].w);
+        const int x = (int)(px % (uint32_t)W), y = (int)(px / (uint32_t)W);
+        flags &= ~LEARNED_FALLBACK;
+        if ((flags & 1u) && flag[(int64_t)(y / tile) * tiles_x + x / tile]) {
+            flags |= LEARNED_FALLBACK;
+            fb = true;
+        }
+        b.w = __uint_as_float(flags);
+        R.b[q] = b;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, fb);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(nfb, (unsigned long long)__popc(m));
+}
+
+// est = exact for fallback requests, else the cache
+__global__ void k_merge(int64_t nreq, Requests R, const float* __restrict__ cached, const float* __restrict__ exact,
+                        float* __restrict__ est) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nreq) return;
+    const bool fb = (__float_as_uint(R.b[q].w) & LEARNED_FALLBACK) != 0u;
+    const float* src = fb ? exact : cached;
+    est[3 * q] = src[3 * q];
+    est[3 * q + 1] = src[3 * q + 1];
+    est[3 * q + 2] = src[3 * q + 2];
+}
+
+inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, int P, float4* ppos, float4* pnrm,
+                           uint32_t* preq, cudaStream_t st) {
+    const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
+    const int64_t ntiles = (int64_t)tx * ty;
+    k_probe_select<<<blocks(ntiles * P, 256), 256, 0, st>>>(cam, R, tile, P, tx, ntiles, ppos, pnrm, preq);
+    return cudaGetLastError();
+}
+
+cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
+                           const float* probe_exact, const float* cached, float max_rel_err, uint8_t* tile_flag,
+                           unsigned long long* counts, cudaStream_t st) {
+    const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
+    const int64_t ntiles = (int64_t)tx * ty;
+    k_tile_flags<<<blocks(ntiles, 256), 256, 0, st>>>(ntiles, P, preq, probe_exact, cached, max_rel_err, tile_flag,
+                                                      counts);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || nreq <= 0) return e;
+    k_mark_fallback<<<blocks(nreq, 256), 256, 0, st>>>(nreq, R, cam.W, tile, tx, tile_flag, counts + 1);
+    return cudaGetLastError();
+}
+
+cudaError_t learned_merge(const Requests& R, int64_t nreq, const float* cached, const float* exact, float* est,
+                          cudaStream_t st) {
+    if (nreq <= 0) return cudaSuccess;
+    k_merge<<<blocks(nreq, 256), 256, 0, st>>>(nreq, R, cached, exact, est);
+    return cudaGetLastError();
+}
+
+}  // namespace pm

@@ -1,0 +1,28 @@
+// pm_learned.cuh -- the learned render's per-tile cache check (see pm_learned.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "pm_render.cuh"
+
+namespace pm {
+
+constexpr uint32_t LEARNED_FALLBACK = 4u;   // request flag: answered by the exact gather
+
+// P probe records per tile of edge `tile` (float4 position / normal records with
+// flag 1 when the probe pixel's first request needs the global estimate, else 0)
+// and the request each probe stands for (UINT32_MAX: none).
+cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, int P, float4* ppos, float4* pnrm,
+                           uint32_t* preq, cudaStream_t st);
+
+// Tile flags from the probes' exact and cached estimates, then flag bit
+// LEARNED_FALLBACK on every global request of a flagged tile.
+// counts[0] += flagged tiles, counts[1] += fallback requests.
+cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
+                           const float* probe_exact, const float* cached, float max_rel_err, uint8_t* tile_flag,
+                           unsigned long long* counts, cudaStream_t st);
+
+// est = exact estimate for fallback requests, the cache's otherwise
+cudaError_t learned_merge(const Requests& R, int64_t nreq, const float* cached, const float* exact, float* est,
+                          cudaStream_t st);
+
+}  // namespace pm

@@ -128,6 +128,40 @@ __device__ __forceinline__ V3 camera_dir(const CameraDev& c, int x, int y) {
     return vsub(vadd(vadd(llc, vscale(hor, u)), vscale(ver, v)), pos);
 }
 
+__device__ __forceinline__ V3 camera_dir_at(const CameraDev& c, float u, float v) {
+    V3 pos = ld3(c.pos);
+    V3 hor = vscale(ld3(c.right), c.vw);
+    V3 ver = vscale(ld3(c.up), c.vh);
+    V3 llc = vsub(vsub(vscale(vadd(pos, ld3(c.fwd)), c.focal), vscale(hor, 0.5f)), vscale(ver, 0.5f));
+    return vsub(vadd(vadd(llc, vscale(hor, u)), vscale(ver, v)), pos);
+}
+
+constexpr uint32_t SAMPLE_TAG = 0x53414d50u;   // stream tag of the training-point sampler
+
+__global__ void k_sample_hits(DevScene S, CameraDev cam, int64_t n, uint64_t seed, float* __restrict__ pos,
+                              float* __restrict__ nrm, float* __restrict__ weight) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Stream rs;
+    rs.init(seed, (uint64_t)i, SAMPLE_TAG);
+    const float u = rs.next(), v = rs.next();   // (0, 1]
+    Ray ray;
+    ray.o = ld3(cam.pos);
+    ray.d = vnorm_div(camera_dir_at(cam, u, v));
+    Hit h;
+    V3 p = v3(0.f, 0.f, 0.f), nn = v3(0.f, 1.f, 0.f);
+    float w = 0.f;
+    if (intersect(S, ray.o, ray.d, h)) {
+        const Material m = load_mat(S, hit_model(S, h.tri));
+        nn = shading_normal(S, h);
+        p = vadd(vscale(ray.d, h.t), ray.o);
+        w = vnull(tri_albedo(S, h.tri, m)) ? 0.f : 1.f;
+    }
+    st3(pos + 3 * i, p);
+    st3(nrm + 3 * i, nn);
+    weight[i] = w;
+}
+
 __global__ void __launch_bounds__(EYE_THREADS)
 k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
     const int64_t npx = (int64_t)cam.W * cam.H;
@@ -251,6 +285,13 @@ cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Req
     cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
     if (e != cudaSuccess) return e;
     k_eye<<<(unsigned)((npx + EYE_THREADS - 1) / EYE_THREADS), EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status);
+    return cudaGetLastError();
+}
+
+cudaError_t sample_primary_hits(const DevScene& S, const CameraDev& cam, int64_t n, uint64_t seed, float* pos,
+                                float* nrm, float* weight, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_sample_hits<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, cam, n, seed, pos, nrm, weight);
     return cudaGetLastError();
 }
 

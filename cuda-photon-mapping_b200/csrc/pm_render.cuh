@@ -31,6 +31,13 @@ struct Requests {
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
                      cudaStream_t st);
 
+// Primary hits of n camera rays through uniformly jittered image positions
+// (sample i draws its position from the Philox stream (seed, i, tag)): hit
+// point, shading normal as the eye pass stores it, weight 1 where the eye pass
+// would request the global-map estimate (hit, albedo non-zero), else 0.
+cudaError_t sample_primary_hits(const DevScene& S, const CameraDev& cam, int64_t n, uint64_t seed, float* pos,
+                                float* nrm, float* weight, cudaStream_t st);
+
 // Combines the estimates of each pixel's requests in hit order, tone-maps and
 // quantises (CudaPhotonMapping/Raytracer.cuh:187-211, 238-240, 277).
 // est_c may be null (no caustic map).  rgb8: 3 bytes per pixel; radiance: 3

@@ -68,6 +68,15 @@ class _CacheOpts(C.Structure):
 CACHE_PARAMS = 5 * 64 * 64
 
 
+class _LearnedOpts(C.Structure):
+    _fields_ = [("tile", C.c_int32), ("probes", C.c_int32), ("max_rel_err", C.c_float)]
+
+
+class _LearnedStats(C.Structure):
+    _fields_ = [("tiles", C.c_int64), ("fallback_tiles", C.c_int64), ("requests", C.c_int64),
+                ("fallback_requests", C.c_int64)]
+
+
 class _RenderOpts(C.Structure):
     _fields_ = [("max_depth", C.c_int32), ("k_global", C.c_int32), ("r_global", C.c_float),
                 ("k_caustic", C.c_int32), ("r_caustic", C.c_float), ("faithful_caustic", C.c_int32)]
@@ -122,6 +131,8 @@ def library():
         "pm_cache_infer": ([vp, vp, vp, i64, vp], C.c_int),
         "pm_cache_get_params": ([vp, vp], C.c_int),
         "pm_cache_set_params": ([vp, vp], C.c_int),
+        "pm_cache_sample_points": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
+        "pm_render_learned": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -323,6 +334,33 @@ class Context:
         w = np.ascontiguousarray(w, np.float32).reshape(-1)
         assert w.size == CACHE_PARAMS
         self._check(self.L.pm_cache_set_params(self.h, w.ctypes.data), "pm_cache_set_params")
+
+    def cache_sample_points(self, cam, n, seed=0):
+        """Training points: primary hits of n jittered camera rays -> (pos, nrm, weight) device tensors."""
+        torch = self.torch
+        pos = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        nrm = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        w = torch.empty(n, dtype=torch.float32, device=self.device)
+        self._check(self.L.pm_cache_sample_points(self.h, C.byref(cam), int(n), int(seed), _ptr(pos), _ptr(nrm),
+                                                  _ptr(w)), "pm_cache_sample_points")
+        return pos, nrm, w
+
+    def render_learned(self, cam: Camera, k_global, r_global, max_depth=4, tile=16, probes=4, max_rel_err=0.05,
+                       k_caustic=0, r_caustic=0.2, faithful_caustic=True, radiance=True, out_rgb8=None,
+                       out_radiance=None):
+        torch = self.torch
+        W, H = cam.width, cam.height
+        rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
+        rad = out_radiance
+        if rad is None and radiance:
+            rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
+        o = _RenderOpts(max_depth, k_global, r_global, k_caustic, r_caustic, int(faithful_caustic))
+        lo = _LearnedOpts(int(tile), int(probes), float(max_rel_err))
+        st = _LearnedStats()
+        self._check(self.L.pm_render_learned(self.h, C.byref(cam), C.byref(o), C.byref(lo), _ptr(rgb), _ptr(rad),
+                                             C.byref(st)), "pm_render_learned")
+        return rgb, rad, dict(tiles=st.tiles, fallback_tiles=st.fallback_tiles, requests=st.requests,
+                              fallback_requests=st.fallback_requests)
 
     # ------------------------------------------------------------ render
     def render(self, cam: Camera, k_global, r_global, max_depth=4, k_caustic=0, r_caustic=0.2,

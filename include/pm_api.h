@@ -244,6 +244,30 @@ int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const flo
 /* Radiance predicted for n samples (out_rgb: device, 3 floats per sample). */
 int pm_cache_infer(pm_ctx* ctx, const float* pos, const float* nrm, int64_t n, float* out_rgb);
 
+/* Training points: the primary hits of n camera rays through uniformly
+ * jittered image positions (seeded), 3 floats of position and shading normal
+ * and a weight (1 where the render gathers the global map there, else 0) per
+ * sample; device outputs.  Label them with pm_gather. */
+int pm_cache_sample_points(pm_ctx* ctx, const pm_camera* cam, int64_t n, uint64_t seed, float* out_pos,
+                           float* out_nrm, float* out_weight);
+
+typedef struct pm_learned_opts {
+    int32_t tile;           /* screen tile edge in pixels */
+    int32_t probes;         /* exact-gather probes per tile (first request of fixed pixels) */
+    float max_rel_err;      /* a tile whose mean relative L1 probe error exceeds this uses the exact gather;
+                               negative: every tile does (the plain render's estimates) */
+} pm_learned_opts;
+
+typedef struct pm_learned_stats {
+    int64_t tiles, fallback_tiles, requests, fallback_requests;
+} pm_learned_stats;
+
+/* pm_render with the global-map estimate taken from the cache, checked per
+ * tile against exact gathers at the probes; tiles above max_rel_err (and all
+ * caustic estimates) use the kNN gather.  out_stats optional. */
+int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, const pm_learned_opts* lopts,
+                      uint8_t* out_rgb8, float* out_radiance, pm_learned_stats* out_stats);
+
 /* Host copies of the FP32 master parameters (get / set, PM_CACHE_PARAMS floats). */
 int pm_cache_get_params(pm_ctx* ctx, float* out_params_host);
 int pm_cache_set_params(pm_ctx* ctx, const float* params_host);
