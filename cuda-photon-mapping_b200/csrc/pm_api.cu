@@ -78,6 +78,7 @@ struct pm_ctx {
     float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t launches = 0;      // kernels this context has launched
     int64_t last_requests = 0; // gather requests of the last pm_render
+    int64_t last_pixels = 0;
     // photons per traced path seen by the last pm_trace_photons on this scene
     // (sizes the next call's first batch; the output never depends on it)
     double yield_g = 0.0, yield_c = 0.0;
@@ -267,6 +268,7 @@ MlpNet cache_net(pm_ctx* ctx) {
     net.w = P<__nv_bfloat16>(ctx->cache_w16);
     for (int a = 0; a < 3; a++) { net.lo[a] = ctx->cache_lo[a]; net.inv[a] = ctx->cache_inv[a]; }
     net.out_scale = ctx->cache_opts.out_scale;
+    net.freq0 = (float)(1 << ctx->cache_opts.octave0);
     return net;
 }
 
@@ -308,8 +310,8 @@ uint64_t splitmix64(uint64_t& x) {
 int pm_cache_init(pm_ctx* ctx, const pm_cache_opts* o) {
     if (!ctx || !o) return PM_ERR_INVALID;
     if (!(o->lr >= 0.f) || !(o->beta1 >= 0.f && o->beta1 < 1.f) || !(o->beta2 >= 0.f && o->beta2 < 1.f) ||
-        !(o->eps > 0.f) || !(o->out_scale > 0.f))
-        return fail(ctx, PM_ERR_INVALID, "cache options: lr >= 0, 0 <= beta < 1, eps > 0, out_scale > 0");
+        !(o->eps > 0.f) || !(o->out_scale > 0.f) || o->octave0 < 0 || o->octave0 > 8)
+        return fail(ctx, PM_ERR_INVALID, "cache options: lr >= 0, 0 <= beta < 1, eps > 0, out_scale > 0, octave0 0..8");
     CK(cudaSetDevice(ctx->device));
     const float* box = o->aabb;
     bool zero = true;
@@ -410,6 +412,20 @@ int pm_cache_set_params(pm_ctx* ctx, const float* in) {
     CK(mlp_to_bf16(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     ctx->launches += 1;
+    return PM_OK;
+}
+
+int pm_get_requests(pm_ctx* ctx, pm_request_view* out) {
+    if (!ctx || !out) return PM_ERR_INVALID;
+    std::memset(out, 0, sizeof *out);
+    out->count = ctx->last_requests;
+    out->pixels = ctx->last_pixels;
+    out->a = P<float>(ctx->req_a);
+    out->b = P<float>(ctx->req_b);
+    out->c = P<float>(ctx->req_c);
+    out->px_base = P<uint32_t>(ctx->px_base);
+    out->px_count = P<uint32_t>(ctx->px_count);
+    out->est_global = P<float>(ctx->est_g);
     return PM_OK;
 }
 
@@ -974,6 +990,7 @@ int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, Frame
     CK(cudaStreamSynchronize(ctx->st));
     F.nreq = (int64_t)std::min<unsigned long long>(nreq, (unsigned long long)F.cap);
     ctx->last_requests = F.nreq;
+    ctx->last_pixels = F.npx;
     ctx->launches += 1;
     return PM_OK;
 }

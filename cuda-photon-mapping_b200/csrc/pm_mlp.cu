@@ -161,8 +161,8 @@ __device__ __forceinline__ bool load_sample(const MlpInputs& in, int64_t i, V3& 
 }
 
 // Encoding: u = (p - lo) * inv per axis, and the octahedral map of the normal
-// to [0, 1]^2; each of the 5 values s gives sin(pi 2^f s), cos(pi 2^f s) for
-// f = 0..5 (60 features, then 4 zeros).  Written as row `row` of an [128][64] tile.
+// to [0, 1]^2; each of the 5 values s gives sin(pi F 2^f s), cos(pi F 2^f s)
+// for f = 0..5, F = freq0 (60 features, then 4 zeros).  Written as row `row` of an [128][64] tile.
 __device__ __forceinline__ void write_features(unsigned char* sX, int row, const MlpNet& net, V3 p, V3 n) {
     float s[5];
     s[0] = (p.x - net.lo[0]) * net.inv[0];
@@ -185,7 +185,7 @@ __device__ __forceinline__ void write_features(unsigned char* sX, int row, const
 #pragma unroll
         for (int f = 0; f < 6; f++) {
             float sn, cs;
-            sincospif(s[j] * (float)(1 << f), &sn, &cs);
+            sincospif(s[j] * (net.freq0 * (float)(1 << f)), &sn, &cs);
             pk[6 * j + f] = pack_bf16(sn, cs);
         }
     }

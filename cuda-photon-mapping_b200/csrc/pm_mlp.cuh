@@ -4,7 +4,8 @@
 // Network: the hit point (3, normalised to the scene box) and the octahedral
 // shading normal (2) are encoded with sin / cos at 6 octaves each (60 inputs,
 // padded to 64), then 4 hidden layers of width 64 with ReLU and an RGB output
-// (padded to 16):  64 -> 64 -> 64 -> 64 -> 64 -> 16.  Weights are FP32 master
+// (padded to 16):  64 -> 64 -> 64 -> 64 -> 64 -> 16.  Octaves f = octave0 ..
+// octave0 + 5 (octave0 = 0 by default).  Weights are FP32 master
 // copies updated by Adam; the kernels read BF16 copies.  Activations and
 // gradients between layers are BF16; every product accumulates in FP32.
 #pragma once
@@ -26,6 +27,7 @@ __host__ __device__ constexpr int mlp_out_dim(int l) { return l == MLP_LAYERS - 
 struct MlpNet {
     const __nv_bfloat16* w;     // MLP_PARAMS bf16 weights
     float lo[3], inv[3];        // encoding box: u = (p - lo) * inv
+    float freq0;                // lowest encoding frequency multiplier: 2^octave0
     float out_scale;            // radiance = out_scale * network output
 };
 

@@ -144,7 +144,13 @@ __global__ void k_sample_hits(DevScene S, CameraDev cam, int64_t n, uint64_t see
     if (i >= n) return;
     Stream rs;
     rs.init(seed, (uint64_t)i, SAMPLE_TAG);
-    const float u = rs.next(), v = rs.next();   // (0, 1]
+    // stratified: sample i lies in pixel floor(i * W * H / n) (row-major), so
+    // consecutive samples are image neighbours (coherent for the gather)
+    const int64_t npx = (int64_t)cam.W * cam.H;
+    const int64_t px = (int64_t)(((unsigned __int128)i * (unsigned __int128)npx) / (unsigned __int128)n);
+    const float ju = rs.next(), jv = rs.next();   // (0, 1]
+    const float u = ((float)(px % cam.W) + 1.f - ju) / (float)cam.W;
+    const float v = ((float)(px / cam.W) + 1.f - jv) / (float)cam.H;
     Ray ray;
     ray.o = ld3(cam.pos);
     ray.d = vnorm_div(camera_dir_at(cam, u, v));

@@ -62,10 +62,15 @@ class Camera(C.Structure):
 
 class _CacheOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
-                ("eps", C.c_float), ("out_scale", C.c_float), ("aabb", C.c_float * 6)]
+                ("eps", C.c_float), ("out_scale", C.c_float), ("aabb", C.c_float * 6), ("octave0", C.c_int32)]
 
 
 CACHE_PARAMS = 5 * 64 * 64
+
+
+class _RequestView(C.Structure):
+    _fields_ = [("count", C.c_int64), ("pixels", C.c_int64), ("a", C.c_void_p), ("b", C.c_void_p),
+                ("c", C.c_void_p), ("px_base", C.c_void_p), ("px_count", C.c_void_p), ("est_global", C.c_void_p)]
 
 
 class _LearnedOpts(C.Structure):
@@ -133,6 +138,7 @@ def library():
         "pm_cache_set_params": ([vp, vp], C.c_int),
         "pm_cache_sample_points": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
         "pm_render_learned": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "pm_get_requests": ([vp, C.POINTER(_RequestView)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -294,9 +300,10 @@ class Context:
         return rad, ids, cnt
 
     # ------------------------------------------------------------ learned radiance cache
-    def cache_init(self, seed=0, lr=1e-3, beta1=0.9, beta2=0.99, eps=1e-8, out_scale=1.0, aabb=None):
+    def cache_init(self, seed=0, lr=1e-3, beta1=0.9, beta2=0.99, eps=1e-8, out_scale=1.0, aabb=None, octave0=0):
         box = (C.c_float * 6)(*([0.0] * 6 if aabb is None else [float(x) for x in aabb]))
-        o = _CacheOpts(int(seed), float(lr), float(beta1), float(beta2), float(eps), float(out_scale), box)
+        o = _CacheOpts(int(seed), float(lr), float(beta1), float(beta2), float(eps), float(out_scale), box,
+                       int(octave0))
         self._check(self.L.pm_cache_init(self.h, C.byref(o)), "pm_cache_init")
 
     def _samples(self, *arrays):
@@ -336,7 +343,7 @@ class Context:
         self._check(self.L.pm_cache_set_params(self.h, w.ctypes.data), "pm_cache_set_params")
 
     def cache_sample_points(self, cam, n, seed=0):
-        """Training points: primary hits of n jittered camera rays -> (pos, nrm, weight) device tensors."""
+        """Training points: primary hits of n stratified jittered camera rays -> (pos, nrm, weight) device tensors."""
         torch = self.torch
         pos = torch.empty((n, 3), dtype=torch.float32, device=self.device)
         nrm = torch.empty((n, 3), dtype=torch.float32, device=self.device)
@@ -345,7 +352,7 @@ class Context:
                                                   _ptr(w)), "pm_cache_sample_points")
         return pos, nrm, w
 
-    def render_learned(self, cam: Camera, k_global, r_global, max_depth=4, tile=16, probes=4, max_rel_err=0.05,
+    def render_learned(self, cam: Camera, k_global, r_global, max_depth=4, tile=16, probes=16, max_rel_err=0.05,
                        k_caustic=0, r_caustic=0.2, faithful_caustic=True, radiance=True, out_rgb8=None,
                        out_radiance=None):
         torch = self.torch
@@ -387,6 +394,23 @@ class Context:
         self._check(self.L.pm_stage_times(self.h, out.ctypes.data), "pm_stage_times")
         return dict(trace_ms=float(out[0]), grid_ms=float(out[1]), eye_ms=float(out[2]), gather_ms=float(out[3]),
                     resolve_ms=float(out[4]))
+
+    def requests(self):
+        """Copies of the last render's gather requests (see pm_request_view) as torch tensors."""
+        torch = self.torch
+        v = _RequestView()
+        self._check(self.L.pm_get_requests(self.h, C.byref(v)), "pm_get_requests")
+        n, npx = v.count, v.pixels
+
+        def dev(ptr, count, dtype, shape):
+            if not count:
+                return torch.empty(shape, dtype=dtype, device=self.device)
+            return torch.as_tensor(_DeviceArray(ptr, shape, dtype), device=self.device).clone()
+
+        return dict(a=dev(v.a, n, torch.float32, (n, 4)), b=dev(v.b, n, torch.float32, (n, 4)),
+                    c=dev(v.c, n, torch.float32, (n, 4)), px_base=dev(v.px_base, npx, torch.int32, (npx,)),
+                    px_count=dev(v.px_count, npx, torch.int32, (npx,)),
+                    est_global=dev(v.est_global, n, torch.float32, (n, 3)))
 
     def render_requests(self):
         """kNN queries answered by the last render's global-map gather."""

@@ -225,6 +225,7 @@ typedef struct pm_cache_opts {
     float lr, beta1, beta2, eps;   /* Adam */
     float out_scale;        /* radiance = out_scale * network output (targets are divided by it) */
     float aabb[6];          /* encoding box (min xyz, max xyz); all zero: the scene's box */
+    int32_t octave0;        /* lowest encoding octave (frequencies pi 2^(octave0 + f), f = 0..5), 0..8 */
 } pm_cache_opts;
 
 /* (Re)initialise the cache: weights from the seed, Adam moments zero. */
@@ -244,8 +245,9 @@ int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const flo
 /* Radiance predicted for n samples (out_rgb: device, 3 floats per sample). */
 int pm_cache_infer(pm_ctx* ctx, const float* pos, const float* nrm, int64_t n, float* out_rgb);
 
-/* Training points: the primary hits of n camera rays through uniformly
- * jittered image positions (seeded), 3 floats of position and shading normal
+/* Training points: the primary hits of n camera rays through stratified
+ * jittered image positions (sample i lies in pixel floor(i * W * H / n) in
+ * row-major order, at a seeded uniform offset), 3 floats of position and shading normal
  * and a weight (1 where the render gathers the global map there, else 0) per
  * sample; device outputs.  Label them with pm_gather. */
 int pm_cache_sample_points(pm_ctx* ctx, const pm_camera* cam, int64_t n, uint64_t seed, float* out_pos,
@@ -254,7 +256,8 @@ int pm_cache_sample_points(pm_ctx* ctx, const pm_camera* cam, int64_t n, uint64_
 typedef struct pm_learned_opts {
     int32_t tile;           /* screen tile edge in pixels */
     int32_t probes;         /* exact-gather probes per tile (first request of fixed pixels) */
-    float max_rel_err;      /* a tile whose mean relative L1 probe error exceeds this uses the exact gather;
+    float max_rel_err;      /* a tile whose cache bias over its probes, sum_c |sum_k (cache - exact)| /
+                               sum_c sum_k exact, exceeds this uses the exact gather;
                                negative: every tile does (the plain render's estimates) */
 } pm_learned_opts;
 
@@ -271,6 +274,23 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
 /* Host copies of the FP32 master parameters (get / set, PM_CACHE_PARAMS floats). */
 int pm_cache_get_params(pm_ctx* ctx, float* out_params_host);
 int pm_cache_set_params(pm_ctx* ctx, const float* params_host);
+
+/* Read-only device view of the last render's gather requests (valid until
+ * the next render).  Request q: a[q] = (hit point, triangle index bits),
+ * b[q] = (shading normal, flag bits: 1 global estimate, 2 caustic estimate,
+ * 4 exact fallback of the learned render), c[q] = (path weight, pixel index
+ * bits); the requests of pixel p are px_base[p] .. px_base[p] + px_count[p] - 1
+ * in hit order. */
+typedef struct pm_request_view {
+    int64_t count, pixels;
+    const float* a;
+    const float* b;
+    const float* c;
+    const uint32_t* px_base;
+    const uint32_t* px_count;
+    const float* est_global;   /* the global estimates the resolve used, 3 floats per request */
+} pm_request_view;
+int pm_get_requests(pm_ctx* ctx, pm_request_view* out);
 
 /* Gather requests (eye-path hits that query the global map) of the last
  * pm_render call: the number of kNN queries its gather stage answered. */

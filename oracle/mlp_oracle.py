@@ -9,7 +9,7 @@ kernels' arithmetic contract:
 
   * encoding: u = (p - lo) * inv per axis; octahedral normal
     (x, y) / (|x| + |y| + |z|), folded for z < 0, mapped by 0.5 v + 0.5; each
-    of the 5 values s gives sin(pi 2^f s), cos(pi 2^f s), f = 0..5, in that
+    of the 5 values s gives sin(pi F 2^f s), cos(pi F 2^f s), f = 0..5, F = 2^octave0, in that
     order (feature 12 j + 2 f, 12 j + 2 f + 1); 4 zero features follow;
   * BF16 (round to nearest even) at the same points as the kernels: the
     encoded features, the weights, every ReLU output, the output gradient and
@@ -57,8 +57,8 @@ def octahedral(n: np.ndarray) -> np.ndarray:
     return np.stack([np.float32(0.5) * ox + np.float32(0.5), np.float32(0.5) * oy + np.float32(0.5)], 1).astype(np.float32)
 
 
-def encode(pos: np.ndarray, nrm: np.ndarray, lo, inv) -> np.ndarray:
-    """(n, 64) float32 features before BF16 rounding."""
+def encode(pos: np.ndarray, nrm: np.ndarray, lo, inv, octave0: int = 0) -> np.ndarray:
+    """(n, 64) float32 features before BF16 rounding (frequencies pi 2^(octave0 + f))."""
     pos = np.asarray(pos, np.float32)
     lo = np.asarray(lo, np.float32)
     inv = np.asarray(inv, np.float32)
@@ -67,7 +67,7 @@ def encode(pos: np.ndarray, nrm: np.ndarray, lo, inv) -> np.ndarray:
     feats = np.zeros((pos.shape[0], DIM), np.float32)
     for j in range(5):
         for f in range(6):
-            x = (s[:, j] * np.float32(1 << f)).astype(np.float32).astype(np.float64)
+            x = (s[:, j] * (np.float32(1 << octave0) * np.float32(1 << f))).astype(np.float32).astype(np.float64)
             feats[:, 12 * j + 2 * f] = np.sin(np.pi * x).astype(np.float32)
             feats[:, 12 * j + 2 * f + 1] = np.cos(np.pi * x).astype(np.float32)
     return feats

@@ -21,14 +21,10 @@ def setup():
 
 
 def _train(ctx, cam, w, steps, seed=1):
-    pos, nrm, wt = ctx.cache_sample_points(cam, 1 << 18, seed=seed)
-    lab, _, _ = ctx.gather(pos, nrm, w["k"], w["radius"])
-    scale = float(lab[wt > 0].mean())
-    ctx.cache_init(seed=0, lr=3e-3, out_scale=scale)
-    b = 16384
-    for it in range(steps):
-        s = (it * b) % pos.shape[0]
-        ctx.cache_train_step(pos[s:s + b], nrm[s:s + b], lab[s:s + b], wt[s:s + b])
+    from photonmap import learned
+    pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=1 << 18, seed=seed)
+    ctx.cache_init(seed=0, lr=3e-3, out_scale=pool.scale)
+    learned.cache_fit(ctx, pool, steps, batch=16384)
 
 
 @pytest.mark.gpu
@@ -69,3 +65,56 @@ def test_trained_cache_replaces_most_gathers(setup):
     a, b = rad_l.cpu().numpy(), rad_p.cpu().numpy()
     rel = np.abs(a - b).mean() / np.abs(b).mean()
     assert rel < 0.1, (rel, st1)
+
+
+def _rms(x):
+    return float(np.sqrt(np.mean(np.square(x))))
+
+
+@pytest.mark.gpu
+def test_rmse_against_fp64_oracle():
+    """Plain render = the FP64 oracle's estimator (fidelity); learned vs plain
+    against an FP64 reference averaged over independent photon maps."""
+    import photonmap
+    from photonmap import scenes
+    import render64
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ctx = photonmap.Context(0)
+    sc, cs, w = scenes.workload("cornell_hf_1080p")
+    W, H, photons, k, r, depth = 480, 270, 2_000_000, w["k"], w["radius"], w["max_depth"]
+    cam = photonmap.camera_setup(cs.position, cs.direction, cs.up, cs.fov_deg, W, H)
+    ctx.set_scene(sc)
+    tables = render64.scene_tables(sc)
+
+    def trace(seed):
+        ctx.trace_photons(seed, w["max_bounces"], photons)
+        ctx.build_grid(photonmap.PM_MAP_GLOBAL)
+        ph = ctx.photons(photonmap.PM_MAP_GLOBAL, sorted_=False)
+        return render64.PhotonMap64(ph["list_pos"].cpu().numpy(), ph["list_dir"].cpu().numpy(),
+                                    ph["list_power"].cpu().numpy())
+
+    m0 = trace(0)
+    _, rad_p = ctx.render(cam, k, r, depth)
+    req = {key: v.cpu().numpy() for key, v in ctx.requests().items()}
+    pixels = np.arange(0, W * H, 5)
+
+    def fp64(m):
+        return render64.resolve64(req, pixels, tables,
+                                  lambda q: m.estimate(req["a"][q, :3], req["b"][q, :3], k, r))
+
+    plain = rad_p.cpu().numpy()[pixels]
+    same = fp64(m0)
+    fidelity = _rms(plain - same) / _rms(same)
+    assert fidelity < 1e-3, fidelity
+    ref = np.mean([fp64(trace(s)) for s in range(1, 5)], axis=0)
+    # the learned render, its cache trained on map 0's estimates
+    trace(0)
+    _train(ctx, cam, w, 3000)
+    _, rad_l, st = ctx.render_learned(cam, k, r, depth, max_rel_err=0.05)
+    learned = rad_l.cpu().numpy()[pixels]
+    rmse_plain = _rms(plain - ref) / _rms(ref)
+    rmse_learned = _rms(learned - ref) / _rms(ref)
+    print(f"\nrelative RMSE vs FP64 4-map reference: plain {rmse_plain:.4f} learned {rmse_learned:.4f}; "
+          f"fidelity of plain to the FP64 same-map oracle {fidelity:.2e}; fallback {st}")
+    assert rmse_learned <= 1.1 * rmse_plain, (rmse_plain, rmse_learned, st)
