@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache frame comparison")
     # size overrides (profiling captures run reduced cases of the same workload)
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--width", type=int, default=0)
@@ -55,17 +56,43 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """SM clocks and clock-event reasons sampled every 10 ms while running
+    (read-only NVML queries of the device torch uses; nvidia-smi at 200 ms
+    when NVML is unavailable)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.samples = []
+        self.stop_evt = threading.Event()
+        self.nv = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            self.nv, self.h = self._nvml_handle()
+            self.max_mhz = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -75,11 +102,30 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nv, self.h
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_evt.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(get_reasons(h))))
+            except Exception:
+                pass
+            self.stop_evt.wait(0.01)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nv is not None:
+            self.stop_evt.set()
+            self.t.join(timeout=2)
+            if not self.samples:
+                return None
+            reasons = sorted(nm for nm, bit in self.BITS.items() if any(r & bit for _, r in self.samples))
+            return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(self.samples), "source": "nvml 10 ms"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -103,7 +149,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi 200 ms"}
 
 
 # ----------------------------------------------------------------- CPU leg
@@ -190,6 +237,80 @@ def override(w, cs, args):
 
 
 # ----------------------------------------------------------------- GPU arm
+def learned_frames(ctx, cam, w, rgb, args, world):
+    """Frame time of the plain render against the learned render on the same
+    photon map (the map stays resident, as in the reference's render loop).
+    Learned frame = online training on TRAIN_PER_FRAME pooled samples + the
+    cache-answered render with its per-tile exact-gather fallback.  The pool
+    (stratified primary hits labelled by the kNN gather) is built once per map."""
+    import torch
+    import torch.distributed as dist
+    from photonmap import learned
+    TRAIN_PER_FRAME, BATCH, WARM_STEPS, THR = 1 << 18, 1 << 16, 3000, 0.05
+    pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=1 << 20, seed=1)
+    ctx.cache_init(seed=0, lr=3e-3, out_scale=pool.scale)
+    learned.cache_fit(ctx, pool, WARM_STEPS, batch=BATCH)
+    K = max(args.steps, 3)
+
+    def plain():
+        ctx.render(cam, w["k"], w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb)
+
+    off = [0]
+    stats = {}
+
+    def learned_frame():
+        _, off[0] = learned.cache_fit(ctx, pool, TRAIN_PER_FRAME // BATCH, batch=BATCH, offset=off[0])
+        _, _, st = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], max_rel_err=THR, radiance=False,
+                                      out_rgb8=rgb)
+        stats.update(st)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(K):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / K
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t[0])
+        return ms
+
+    ms_plain = timed(plain)
+    ms_learned = timed(learned_frame)
+    # tensor-core throughput of the cache kernels (forward 32,640 flop per sample, backward ~2x)
+    fwd = 2 * (60 * 64 + 3 * 64 * 64 + 64 * 3)
+    n = min(pool.n, 1 << 20)
+
+    def infer():
+        ctx.cache_infer(pool.pos[:n], pool.nrm[:n])
+
+    def train():
+        learned.cache_fit(ctx, pool, 1, batch=min(BATCH * 4, pool.n))
+
+    ms_inf = timed(infer)
+    ms_tr = timed(train)
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"] \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
+    inf_tf = fwd * n / (ms_inf * 1e-3) / 1e12
+    tr_tf = 3 * fwd * min(BATCH * 4, pool.n) / (ms_tr * 1e-3) / 1e12
+    return {"ms_per_frame_plain": ms_plain, "ms_per_frame_learned": ms_learned, "speedup": ms_plain / ms_learned,
+            "frame": "eye pass + global estimate + resolve, photon map resident",
+            "train_samples_per_frame": TRAIN_PER_FRAME, "pool": pool.n, "warmup_steps": WARM_STEPS,
+            "max_rel_err": THR, "fallback_tiles_frac": stats["fallback_tiles"] / max(stats["tiles"], 1),
+            "fallback_requests_frac": stats["fallback_requests"] / max(stats["requests"], 1),
+            "mlp": {"infer_tflops": inf_tf, "train_tflops": tr_tf, "peak_bf16_tflops": peak,
+                    "infer_frac": inf_tf / peak, "train_frac": tr_tf / peak, "unit": "TFLOP/s",
+                    "flop_per_sample_forward": fwd}}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -261,6 +382,9 @@ def run_ours(args):
 
     # gather kernel roofline: compulsory bytes per query = k neighbours x (16 B position
     # + 12 B direction + 12 B power) + 32 B request (point, normal) + 12 B estimate
+    learned_block = None
+    if not args.no_learned:
+        learned_block = learned_frames(ctx, cam, w, rgb, args, world)
     ph = ctx.photons(0, sorted_=False)  # noqa: F841  (map still resident)
     hbm, src = peaks()
     line = None
@@ -294,6 +418,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "learned": learned_block,
         }
     ctx.close()
     if world > 1:
