@@ -24,68 +24,9 @@ void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& no
 
 using namespace pm;
 
-namespace {
+#include "pm_context.cuh"
 
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
-struct MapState {
-    int64_t n = 0;                       // photons in the list
-    DevBuf pos, dir, pow;                // traced-order list (3 floats per photon)
-    bool built = false;
-    int dims[3] = {0, 0, 0};
-    float cell = 0.f;
-    int64_t cells = 0;
-    float aabb[6] = {0, 0, 0, 0, 0, 0};
-    int S = 1;
-    DevBuf starts, sizes, gpos, gdir, gpow, key_counts, key_starts;
-    DevBuf cid, keys0, keys1, vals0, vals1, hist, scan_ws, small, counts2;
-};
-
-}  // namespace
-
-struct pm_ctx {
-    int device = 0;
-    cudaStream_t st = nullptr;
-    bool own_stream = false;
-    std::string err;
-    int sm_count = 148;
-    int trace_refill = 0;      // k_trace refill threshold; 0: the kernel's default
-    // scene
-    bool has_scene = false;
-    int ntri = 0, nmodel = 0, light_model = 0, light_first = 0, light_count = 0, nca = 0;
-    float light_intensity[3] = {1, 1, 1};
-    float default_ior = 1.f;
-    float aabb[6] = {0, 0, 0, 0, 0, 0};
-    bool has_tri_diffuse = false;
-    DevBuf tri, tri_pos, tri_nrm, tri_diffuse, nodes, prim, maabb, mats, ca;
-    MapState maps[2];
-    // photon-pass scratch
-    DevBuf counter, stage_pos, stage_dir, cnt_g, cnt_c, scan_g, scan_c, totals, trace_ws, scratch_pow;
-    // render scratch
-    DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, est_c;
-    DevBuf status, gws;
-    // learned radiance cache
-    bool has_cache = false;
-    DevBuf cache_w32, cache_w16, cache_m, cache_v, cache_grad, cache_loss;
-    DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts;
-    pm_cache_opts cache_opts = {};
-    float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};
-    int cache_step = 0;
-    cudaEvent_t ev[12] = {};
-    float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t launches = 0;      // kernels this context has launched
-    int64_t last_requests = 0; // gather requests of the last pm_render
-    int64_t last_pixels = 0;
-    // photons per traced path seen by the last pm_trace_photons on this scene
-    // (sizes the next call's first batch; the output never depends on it)
-    double yield_g = 0.0, yield_c = 0.0;
-    int yield_bounces = 0;
-};
-
-namespace {
+namespace pm {
 
 int fail(pm_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -95,15 +36,6 @@ int cuda_fail(pm_ctx* c, cudaError_t e, const char* what) {
     return fail(c, e == cudaErrorMemoryAllocation ? PM_ERR_OOM : PM_ERR_CUDA,
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
-#define CK(expr)                                                        \
-    do {                                                                \
-        cudaError_t e_ = (expr);                                        \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #expr);        \
-    } while (0)
-
-// Grow-only device buffer; a grown buffer gets 1/8 headroom so sizes that
-// wobble from call to call (batch sizes follow measured yields) do not
-// re-allocate every time.
 cudaError_t ensure(DevBuf& b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return cudaSuccess;
@@ -120,9 +52,7 @@ void release(DevBuf& b) {
     b.p = nullptr;
     b.bytes = 0;
 }
-template <class T> T* P(DevBuf& b) { return (T*)b.p; }
 
-#define ENSURE(buf, bytes) CK(ensure(buf, bytes))
 
 DevScene dev_scene(pm_ctx* c) {
     DevScene S;
@@ -182,7 +112,20 @@ int valid_map(pm_ctx* ctx, int map) {
     return PM_OK;
 }
 
-}  // namespace
+GatherGrid grid_of(MapState& m, MapState& est_src) {
+    GatherGrid G;
+    G.gpos = P<float4>(m.gpos);
+    G.gdir = P<float>(est_src.gdir);
+    G.gpow = P<float>(est_src.gpow);
+    G.key_starts = P<uint32_t>(m.key_starts);
+    G.mn[0] = m.aabb[0]; G.mn[1] = m.aabb[1]; G.mn[2] = m.aabb[2];
+    G.gx = m.dims[0]; G.gy = m.dims[1]; G.gz = m.dims[2];
+    G.cell = m.cell;
+    G.S = m.S;
+    return G;
+}
+
+}  // namespace pm
 
 extern "C" {
 
@@ -869,18 +812,6 @@ int pm_load_photons(pm_ctx* ctx, int map, const char* path) {
     return pm_set_photons(ctx, map, (int64_t)cnt, pos.data(), pw.data(), dir.data());
 }
 
-static GatherGrid grid_of(MapState& m, MapState& est_src) {
-    GatherGrid G;
-    G.gpos = P<float4>(m.gpos);
-    G.gdir = P<float>(est_src.gdir);
-    G.gpow = P<float>(est_src.gpow);
-    G.key_starts = P<uint32_t>(m.key_starts);
-    G.mn[0] = m.aabb[0]; G.mn[1] = m.aabb[1]; G.mn[2] = m.aabb[2];
-    G.gx = m.dims[0]; G.gy = m.dims[1]; G.gz = m.dims[2];
-    G.cell = m.cell;
-    G.S = m.S;
-    return G;
-}
 
 int pm_gather(pm_ctx* ctx, int map, int64_t n, const float* qpos, const float* qnrm, int k, float radius,
               float* out_rad, uint32_t* out_ids, int32_t* out_cnt) {

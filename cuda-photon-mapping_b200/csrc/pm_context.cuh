@@ -1,0 +1,99 @@
+// pm_context.cuh -- the library context (opaque pm_ctx of the C ABI) and the
+// host helpers the entry points share.  Internal: not part of the ABI.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/pm_api.h"
+#include "pm_gather.cuh"
+#include "pm_scene.cuh"
+
+namespace pm {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct MapState {
+    int64_t n = 0;                       // photons in the list
+    DevBuf pos, dir, pow;                // traced-order list (3 floats per photon)
+    bool built = false;
+    int dims[3] = {0, 0, 0};
+    float cell = 0.f;
+    int64_t cells = 0;
+    float aabb[6] = {0, 0, 0, 0, 0, 0};
+    int S = 1;
+    DevBuf starts, sizes, gpos, gdir, gpow, key_counts, key_starts;
+    DevBuf cid, keys0, keys1, vals0, vals1, hist, scan_ws, small, counts2;
+};
+
+}  // namespace pm
+
+struct pm_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int sm_count = 148;
+    int trace_refill = 0;      // k_trace refill threshold; 0: the kernel's default
+    // scene
+    bool has_scene = false;
+    int ntri = 0, nmodel = 0, light_model = 0, light_first = 0, light_count = 0, nca = 0;
+    float light_intensity[3] = {1, 1, 1};
+    float default_ior = 1.f;
+    float aabb[6] = {0, 0, 0, 0, 0, 0};
+    bool has_tri_diffuse = false;
+    pm::DevBuf tri, tri_pos, tri_nrm, tri_diffuse, nodes, prim, maabb, mats, ca;
+    pm::MapState maps[2];
+    // photon-pass scratch
+    pm::DevBuf counter, stage_pos, stage_dir, cnt_g, cnt_c, scan_g, scan_c, totals, trace_ws, scratch_pow;
+    // render scratch
+    pm::DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, est_c;
+    pm::DevBuf status, gws;
+    // learned radiance cache
+    bool has_cache = false;
+    pm::DevBuf cache_w32, cache_w16, cache_m, cache_v, cache_grad, cache_loss;
+    pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts;
+    pm_cache_opts cache_opts = {};
+    float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};
+    int cache_step = 0;
+    cudaEvent_t ev[12] = {};
+    float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;      // kernels this context has launched
+    int64_t last_requests = 0; // gather requests of the last pm_render
+    int64_t last_pixels = 0;
+    // photons per traced path seen by the last pm_trace_photons on this scene
+    // (sizes the next call's first batch; the output never depends on it)
+    double yield_g = 0.0, yield_c = 0.0;
+    int yield_bounces = 0;
+};
+
+namespace pm {
+
+int fail(pm_ctx* c, int code, const std::string& msg);
+int cuda_fail(pm_ctx* c, cudaError_t e, const char* what);
+// grow-only device buffer (1/8 headroom on growth)
+cudaError_t ensure(DevBuf& b, size_t bytes);
+void release(DevBuf& b);
+template <class T> T* P(DevBuf& b) { return (T*)b.p; }
+DevScene dev_scene(pm_ctx* c);
+// reads and clears the device status word; PM_ERR_TIMEOUT / PM_ERR_OVERFLOW
+int check_status(pm_ctx* ctx, const char* what);
+float elapsed(cudaEvent_t a, cudaEvent_t b);
+// gather view of map m, estimates read from est_src's direction / power arrays
+GatherGrid grid_of(MapState& m, MapState& est_src);
+
+}  // namespace pm
+
+#define CK(expr)                                                        \
+    do {                                                                \
+        cudaError_t e_ = (expr);                                        \
+        if (e_ != cudaSuccess) return pm::cuda_fail(ctx, e_, #expr);        \
+    } while (0)
+
+// Grow-only device buffer; a grown buffer gets 1/8 headroom so sizes that
+// wobble from call to call (batch sizes follow measured yields) do not
+// re-allocate every time.
+
+#define ENSURE(buf, bytes) CK(ensure(buf, bytes))

@@ -30,6 +30,7 @@
 // sorted by the warp (an MSB-first radix select over the store when the bin
 // holds more than 32), and the store is cut to the k best.  The answer is the
 // exhaustive walk's.
+#include <algorithm>
 #include "pm_gather.cuh"
 #include "pm_device.cuh"
 
@@ -533,34 +534,10 @@ struct WarpWalk {
     }
 };
 
+// one query (one warp): the k nearest photons within r of q and the estimate
 template <int UCAP>
-__global__ void __launch_bounds__(WARPS * 32, 4)
-k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, GatherOut O) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t i = (int64_t)blockIdx.x * WARPS + warp;
-    if (i >= Q.n) return;
-    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
-    V3 q, nrm;
-    bool active = true;
-    if (Q.pos3) {
-        q = ld3(Q.pos3 + 3 * i);
-        nrm = ld3(Q.nrm3 + 3 * i);
-    } else {
-        float4 a = Q.pos4[i], b = Q.nrm4[i];
-        active = (__float_as_uint(b.w) & Q.flag_mask) != 0u;
-        q = xyz(a);
-        nrm = xyz(b);
-    }
-    if (!active || k <= 0) {
-        if (lane == 0) {
-            st3(O.rad + 3 * i, v3(0.f, 0.f, 0.f));
-            if (O.cnt) O.cnt[i] = 0;
-            if (O.rk) O.rk[i] = 0.f;
-        }
-        if (O.ids) for (int e = lane; e < k; e += 32) O.ids[i * k + e] = 0xffffffffu;
-        return;
-    }
+__device__ __forceinline__ void gather_query(const GatherGrid& G, WarpStore<UCAP>& U, int64_t i, V3 q, V3 nrm,
+                                             float r, int k, int require_full, const GatherOut& O, int lane) {
     WarpWalk<UCAP> W(G, U, q, r, k, lane);
     int hx, hy, hz, sx, sy, sz;
     locate(q.x, G.mn[0], G.cell, G.gx, G.S, hx, sx);
@@ -639,6 +616,86 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
     }
 }
 
+__device__ __forceinline__ void gather_zero(int64_t i, int k, const GatherOut& O, int lane) {
+    if (lane == 0) {
+        st3(O.rad + 3 * i, v3(0.f, 0.f, 0.f));
+        if (O.cnt) O.cnt[i] = 0;
+        if (O.rk) O.rk[i] = 0.f;
+    }
+    if (O.ids) for (int e = lane; e < k; e += 32) O.ids[i * k + e] = 0xffffffffu;
+}
+
+template <int UCAP>
+__global__ void __launch_bounds__(WARPS * 32, 4)
+k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, GatherOut O) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = (int64_t)blockIdx.x * WARPS + warp;
+    if (i >= Q.n) return;
+    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
+    V3 q, nrm;
+    bool active = true;
+    if (Q.pos3) {
+        q = ld3(Q.pos3 + 3 * i);
+        nrm = ld3(Q.nrm3 + 3 * i);
+    } else {
+        float4 a = Q.pos4[i], b = Q.nrm4[i];
+        active = (__float_as_uint(b.w) & Q.flag_mask) != 0u;
+        q = xyz(a);
+        nrm = xyz(b);
+    }
+    if (!active || k <= 0) {
+        gather_zero(i, k, O, lane);
+        return;
+    }
+    gather_query<UCAP>(G, U, i, q, nrm, r, k, require_full, O, lane);
+}
+
+__device__ __forceinline__ int find_instance_px(const int64_t* __restrict__ off, int ninst, int64_t g) {
+    int lo = 0, hi = ninst - 1;   // last i with off[i] <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Requests of several instances, one persistent work queue: warps take
+// request indices from *queue until *n_req (the eye pass's device counter) is
+// reached.  Request q belongs to the instance of its pixel (c.w bits, a
+// global pixel index in [px_off[i], px_off[i+1])) and is answered with that
+// instance's grid, r and k.  Only instances whose store class matches this
+// launch (cls) are answered here; the other requests are left for the other
+// launch.
+template <int UCAP, int NW>
+__global__ void __launch_bounds__(NW * 32, 32 / NW)
+k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict__ px_off, int ninst,
+               GatherQueries Q, const float4* __restrict__ rec_c, const unsigned long long* __restrict__ n_req,
+               unsigned long long* __restrict__ queue, int cls, GatherOut O) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
+    const int64_t n = (int64_t)min(*n_req, (unsigned long long)Q.n);
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(queue, 1ull);
+        const int64_t i = (int64_t)__shfl_sync(0xffffffffu, t, 0);
+        if (i >= n) break;
+        const int inst = find_instance_px(px_off, ninst, (int64_t)__float_as_uint(rec_c[i].w));
+        const GatherInstDev& T = tab[inst];
+        if (T.cls != cls) continue;
+        const float4 a = Q.pos4[i], b = Q.nrm4[i];
+        if (!((__float_as_uint(b.w) & Q.flag_mask) != 0u) || T.k <= 0) {
+            gather_zero(i, T.k, O, lane);
+            continue;
+        }
+        const GatherGrid G = T.G;
+        gather_query<UCAP>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
+        __syncwarp();
+    }
+}
+
 template <int UCAP>
 cudaError_t launch(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full, const GatherOut& O,
                    cudaStream_t st) {
@@ -651,6 +708,37 @@ cudaError_t launch(const GatherGrid& G, const GatherQueries& Q, float r, int k, 
 }
 
 }  // namespace
+
+template <int UCAP, int NW>
+cudaError_t launch_multi(const GatherInstDev* tab, const int64_t* px_off, int ninst, const GatherQueries& Q,
+                         const float4* rec_c, const unsigned long long* n_req, unsigned long long* queue, int cls,
+                         const GatherOut& O, int sm_count, cudaStream_t st) {
+    const size_t smem = sizeof(WarpStore<UCAP>) * NW;
+    cudaError_t e = cudaFuncSetAttribute(k_gather_multi<UCAP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_multi<UCAP, NW>, NW * 32, smem)) != cudaSuccess)
+        return e;
+    k_gather_multi<UCAP, NW><<<(unsigned)(std::max(per_sm, 1) * sm_count), NW * 32, smem, st>>>(
+        tab, px_off, ninst, Q, rec_c, n_req, queue, cls, O);
+    return cudaGetLastError();
+}
+
+cudaError_t gather_multi(const GatherInstDev* tab, const int64_t* px_off, int ninst, const GatherQueries& Q,
+                         const float4* rec_c, const unsigned long long* n_req, unsigned long long* queues,
+                         const GatherOut& O, int warps, int sm_count, cudaStream_t st) {
+    if (Q.n <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(queues, 0, 16, st);
+    if (e != cudaSuccess) return e;
+    if (warps == 4) {
+        if ((e = launch_multi<256, 4>(tab, px_off, ninst, Q, rec_c, n_req, queues, 0, O, sm_count, st)) != cudaSuccess) return e;
+        return launch_multi<512, 4>(tab, px_off, ninst, Q, rec_c, n_req, queues + 1, 1, O, sm_count, st);
+    }
+    if ((e = launch_multi<256, 8>(tab, px_off, ninst, Q, rec_c, n_req, queues, 0, O, sm_count, st)) != cudaSuccess) return e;
+    return launch_multi<512, 8>(tab, px_off, ninst, Q, rec_c, n_req, queues + 1, 1, O, sm_count, st);
+}
+
+int gather_class(int k) { return k <= 96 ? 0 : 1; }
 
 cudaError_t gather(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full,
                    const GatherOut& O, unsigned* status, cudaStream_t st) {

@@ -40,4 +40,21 @@ struct GatherOut {
 cudaError_t gather(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full,
                    const GatherOut& O, unsigned* status, cudaStream_t st);
 
+// ---- requests of several instances in one work queue ----
+struct GatherInstDev {
+    GatherGrid G;
+    float r;
+    int k;
+    int cls;                  // gather_class(k): which store size answers it
+};
+int gather_class(int k);
+// Q: the request records (pos4 / nrm4 with flag_mask), Q.n = their capacity;
+// rec_c: their third records (global pixel bits in w); n_req: device count of
+// requests; queues: 2 device counters (scratch); px_off: ninst + 1 pixel
+// offsets; warps: block shape, 4 or 8 warps per block.  Two persistent
+// launches (store classes of k <= 96 and k <= 256).
+cudaError_t gather_multi(const GatherInstDev* tab, const int64_t* px_off, int ninst, const GatherQueries& Q,
+                         const float4* rec_c, const unsigned long long* n_req, unsigned long long* queues,
+                         const GatherOut& O, int warps, int sm_count, cudaStream_t st);
+
 }  // namespace pm

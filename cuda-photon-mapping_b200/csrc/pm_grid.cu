@@ -142,20 +142,71 @@ __device__ __forceinline__ int sub_of(float u, int c, int S) {
     return min(max(s, 0), S - 1);
 }
 
-__global__ void k_key_count(const float* __restrict__ pos, int64_t n, GridGeom g, int S, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ counts) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float* p = pos + 3 * i;
+__device__ __forceinline__ uint32_t sub_cell_key(const GridGeom& g, int S, const float* p) {
     float ux = (p[0] - g.mnx) / g.cell, uy = (p[1] - g.mny) / g.cell, uz = (p[2] - g.mnz) / g.cell;
     int x = min(max((int)ux, 0), g.gx - 1);
     int y = min(max((int)uy, 0), g.gy - 1);
     int z = min(max((int)uz, 0), g.gz - 1);
     uint32_t c = (uint32_t)(x + y * g.gx + z * g.gx * g.gy);
     uint32_t sk = (uint32_t)(sub_of(ux, x, S) + S * (sub_of(uy, y, S) + S * sub_of(uz, z, S)));
-    uint32_t k = c * (uint32_t)(S * S * S) + sk;
+    return c * (uint32_t)(S * S * S) + sk;
+}
+
+__global__ void k_key_count(const float* __restrict__ pos, int64_t n, GridGeom g, int S, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ counts) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = sub_cell_key(g, S, pos + 3 * i);
     key[i] = k;
     atomicAdd(counts + k, 1u);
+}
+
+__device__ __forceinline__ int find_range(const int64_t* __restrict__ off, int n, int64_t v) {
+    int lo = 0, hi = n - 1;   // last i with off[i] <= v
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Several instances in one key space: photon p of instance i's region (the
+// first min(cap, filled) of its slots are photons) gets key key0 + its
+// sub-cell key in the instance's grid; other slots get `sentinel`.
+__global__ void k_key_count_multi(const float* __restrict__ pos, int64_t n, const GridInstDev* __restrict__ tab,
+                                  const int64_t* __restrict__ ph_off, int ninst, const int64_t* __restrict__ filled,
+                                  uint32_t sentinel, uint32_t* __restrict__ key, uint32_t* __restrict__ counts) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int i = find_range(ph_off, ninst, p);
+    const GridInstDev t = tab[i];
+    const int64_t local = p - t.ph0;
+    uint32_t k = sentinel;
+    if (local < min(t.cap, filled[i])) {
+        GridGeom g;
+        g.mnx = t.mn[0]; g.mny = t.mn[1]; g.mnz = t.mn[2];
+        g.gx = t.gx; g.gy = t.gy; g.gz = t.gz; g.cell = t.cell;
+        k = (uint32_t)t.key0 + sub_cell_key(g, t.S, pos + 3 * p);
+    }
+    key[p] = k;
+    atomicAdd(counts + k, 1u);
+}
+
+// per global cell: the instance-relative start and size of its photons
+__global__ void k_cells_multi(int64_t cells, const GridInstDev* __restrict__ tab, const int64_t* __restrict__ cell_off,
+                              int ninst, const uint32_t* __restrict__ key_starts, uint32_t* __restrict__ starts,
+                              uint32_t* __restrict__ sizes) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    const int i = find_range(cell_off, ninst, c);
+    const GridInstDev t = tab[i];
+    const int64_t S3 = (int64_t)t.S * t.S * t.S;
+    const int64_t lc = c - t.cell0;
+    const uint32_t base = key_starts[t.key0];
+    const uint32_t a = key_starts[t.key0 + lc * S3], b = key_starts[t.key0 + (lc + 1) * S3];
+    starts[c] = a - base;
+    sizes[c] = b - a;
 }
 
 __global__ void k_cells_from_keys(const uint32_t* __restrict__ key_starts, int64_t cells, int S3,
@@ -413,10 +464,18 @@ cudaError_t grid_sort(GridBuffers& B, const float aabb[6], GridPlan& plan, int S
     plan.launches += 2;
     if (n == 0) return cudaSuccess;
 
-    // LSD radix sort of the keys (stable), carrying the photon index; digits of
-    // equal width <= 9 bits
+    int launches = 0;
+    e = radix_and_gather(B, n, keys, &launches, st);
+    plan.launches += launches;
+    return e;
+}
+
+// LSD radix sort of B.cid (keys < key_space, stable), carrying the photon
+// index; digits of equal width <= 9 bits; then the sorted records.
+cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* launches, cudaStream_t st) {
+    cudaError_t e;
     int bits = 1;
-    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)keys) bits++;
+    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)key_space) bits++;
     const int passes = (bits + RADIX_MAX_BITS - 1) / RADIX_MAX_BITS;
     const int width = (bits + passes - 1) / passes;
     const int tiles = (int)((n + RADIX_TILE - 1) / RADIX_TILE);
@@ -441,8 +500,30 @@ cudaError_t grid_sort(GridBuffers& B, const float aabb[6], GridPlan& plan, int S
         vin = vout;
     }
     k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(vin, n, B.pos, B.dir, B.pow, B.gpos, B.gdir, B.gpow, B.status);
-    plan.launches += 3 * passes + 1;
+    *launches += 3 * passes + 1;
     return cudaGetLastError();
+}
+
+cudaError_t grid_multi(GridBuffers& B, const GridMulti& M, int* launches, cudaStream_t st) {
+    cudaError_t e;
+    const int64_t n = B.n;
+    const int64_t key_space = M.total_keys + 1;           // + the sentinel of empty slots
+    if ((e = cudaMemsetAsync(B.key_counts, 0, (size_t)key_space * 4, st)) != cudaSuccess) return e;
+    if (n > 0) {
+        k_key_count_multi<<<blocks_for(n, 256), 256, 0, st>>>(B.pos, n, M.tab, M.ph_off, M.ninst, M.filled,
+                                                             (uint32_t)M.total_keys, B.cid, B.key_counts);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        *launches += 1;
+    }
+    if ((e = scan_u32(B.key_counts, B.key_starts, key_space, 0, B.key_starts + key_space, B.scan_ws, B.status, st)) !=
+        cudaSuccess)
+        return e;
+    k_cells_multi<<<blocks_for(M.total_cells, 256), 256, 0, st>>>(M.total_cells, M.tab, M.cell_off, M.ninst,
+                                                                  B.key_starts, B.cell_starts, B.cell_sizes);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    *launches += 2;
+    if (n == 0) return cudaSuccess;
+    return radix_and_gather(B, n, key_space, launches, st);
 }
 
 }  // namespace pm

@@ -57,6 +57,29 @@ cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int reg
 // sorted arrays.  Buffers: key arrays sized for cells * S^3 (+1).
 cudaError_t grid_sort(GridBuffers& B, const float aabb[6], GridPlan& plan, int S, cudaStream_t st);
 
+// ---- several instances in one key space ----
+struct GridInstDev {
+    float mn[3];
+    int gx, gy, gz;
+    float cell;
+    int S;
+    int64_t key0;             // first key of the instance
+    int64_t cell0;            // first global cell of the instance
+    int64_t ph0, cap;         // the instance's photon slots [ph0, ph0 + cap)
+};
+struct GridMulti {
+    int ninst;
+    const GridInstDev* tab;   // device, ninst
+    const int64_t* ph_off;    // device, ninst + 1: slot offsets (ph0 of each instance, then the total)
+    const int64_t* cell_off;  // device, ninst + 1
+    const int64_t* filled;    // device, ninst: photons each instance produced (slots past min(cap, filled) are empty)
+    int64_t total_keys, total_cells;
+};
+// B.n = all slots; B.key_counts >= total_keys + 1, B.key_starts >= total_keys + 2,
+// cell arrays >= total_cells; cell_starts are instance-relative.
+cudaError_t grid_multi(GridBuffers& B, const GridMulti& M, int* launches, cudaStream_t st);
+cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* launches, cudaStream_t st);
+
 // sub-cell division for a grid whose fullest cell holds max_count photons:
 // about 2k photons per sub-cell slab of a surface crossing the cell
 int grid_auto_subdiv(uint32_t max_count, int k_hint);

@@ -168,14 +168,13 @@ __global__ void k_sample_hits(DevScene S, CameraDev cam, int64_t n, uint64_t see
     weight[i] = w;
 }
 
-__global__ void __launch_bounds__(EYE_THREADS)
-k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
-    const int64_t npx = (int64_t)cam.W * cam.H;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < npx;
-    float4 ha[RENDER_MAX_HITS], hb[RENDER_MAX_HITS], hc[RENDER_MAX_HITS];
+// the eye path of local pixel `li` (image of `cam`): its gather requests in hit
+// order (c.w = pixel bits `px`); returns the number of hits
+__device__ __forceinline__ int eye_hits(const DevScene& S, const CameraDev& cam, int D, int64_t li, uint32_t px,
+                                        float4* ha, float4* hb, float4* hc, unsigned* status) {
     int nh = 0;
-    if (valid) {
+    const int64_t i = li;
+    {
         const int x = (int)(i % cam.W), y = (int)(i / cam.W);
         Ray ray;
         ray.o = ld3(cam.pos);
@@ -199,7 +198,7 @@ k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
             if (nh < RENDER_MAX_HITS) {
                 ha[nh] = make_float4(ip.x, ip.y, ip.z, __int_as_float(h.tri));
                 hb[nh] = make_float4(n.x, n.y, n.z, __uint_as_float(flags));
-                hc[nh] = make_float4(coef.x, coef.y, coef.z, __uint_as_float((uint32_t)i));
+                hc[nh] = make_float4(coef.x, coef.y, coef.z, __uint_as_float(px));
                 nh++;
             } else {
                 raise_status(status, ST_OVERFLOW);
@@ -220,7 +219,13 @@ k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
         }
         if (M.overflow) raise_status(status, ST_STACK);
     }
-    // reserve nh consecutive request slots: one atomic per warp
+    return nh;
+}
+
+// reserve nh consecutive request slots (one atomic per warp) and write them;
+// every lane of the warp calls this, `valid` lanes own pixel gi
+__device__ __forceinline__ void eye_emit(Requests& R, bool valid, int64_t gi, int nh, const float4* ha,
+                                         const float4* hb, const float4* hc, unsigned* status) {
     const int lane = threadIdx.x & 31;
     unsigned incl = (unsigned)nh;
 #pragma unroll
@@ -235,8 +240,8 @@ k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
     if (!valid) return;
     if ((int64_t)(base + nh) > R.cap) {
         raise_status(status, ST_OVERFLOW);
-        R.px_base[i] = 0;
-        R.px_count[i] = 0;
+        R.px_base[gi] = 0;
+        R.px_count[gi] = 0;
         return;
     }
     for (int k = 0; k < nh; k++) {
@@ -244,16 +249,51 @@ k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
         R.b[base + k] = hb[k];
         R.c[base + k] = hc[k];
     }
-    R.px_base[i] = (uint32_t)base;
-    R.px_count[i] = (uint32_t)nh;
+    R.px_base[gi] = (uint32_t)base;
+    R.px_count[gi] = (uint32_t)nh;
 }
 
-__global__ void k_resolve(DevScene S, int64_t npx, Requests R, const float* __restrict__ est_g,
-                          const float* __restrict__ est_c, float tone_t, uint8_t* __restrict__ rgb8,
-                          float* __restrict__ radiance) {
+__global__ void __launch_bounds__(EYE_THREADS)
+k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
+    const int64_t npx = (int64_t)cam.W * cam.H;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npx) return;
-    const uint32_t base = R.px_base[i], cnt = R.px_count[i];
+    const bool valid = i < npx;
+    float4 ha[RENDER_MAX_HITS], hb[RENDER_MAX_HITS], hc[RENDER_MAX_HITS];
+    const int nh = valid ? eye_hits(S, cam, D, i, (uint32_t)i, ha, hb, hc, status) : 0;
+    eye_emit(R, valid, i, nh, ha, hb, hc, status);
+}
+
+__device__ __forceinline__ int find_pixel_instance(const int64_t* __restrict__ off, int ninst, int64_t g) {
+    int lo = 0, hi = ninst - 1;   // last i with off[i] <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// all instances' pixels in one launch: global pixel g of instance i (off[i] <= g < off[i+1])
+__global__ void __launch_bounds__(EYE_THREADS)
+k_eye_multi(const RenderInstDev* __restrict__ tab, const int64_t* __restrict__ px_off, int ninst, int64_t npx,
+            Requests R, unsigned* status) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = g < npx;
+    float4 ha[RENDER_MAX_HITS], hb[RENDER_MAX_HITS], hc[RENDER_MAX_HITS];
+    int nh = 0;
+    if (valid) {
+        const int i = find_pixel_instance(px_off, ninst, g);
+        const RenderInstDev& T = tab[i];
+        nh = eye_hits(T.S, T.cam, T.max_depth, g - __ldg(px_off + i), (uint32_t)g, ha, hb, hc, status);
+    }
+    eye_emit(R, valid, g, nh, ha, hb, hc, status);
+}
+
+// combine pixel gi's requests with the scene's materials, tone-map, quantise
+__device__ __forceinline__ void resolve_pixel(const DevScene& S, int64_t gi, const Requests& R,
+                                              const float* __restrict__ est_g, const float* __restrict__ est_c,
+                                              float tone_t, uint8_t* __restrict__ rgb8, float* __restrict__ radiance) {
+    const uint32_t base = R.px_base[gi], cnt = R.px_count[gi];
     V3 acc = v3(0.f, 0.f, 0.f);
     for (uint32_t r = 0; r < cnt; r++) {
         const size_t q = (size_t)base + r;
@@ -272,14 +312,31 @@ __global__ void k_resolve(DevScene S, int64_t npx, Requests R, const float* __re
         color = vmin1(color, 1.f);
         acc = vadd(acc, vmul(color, xyz(c)));
     }
-    if (radiance) st3(radiance + 3 * i, acc);
+    if (radiance) st3(radiance + 3 * gi, acc);
     V3 e = v3(expf(-tone_t * acc.x), expf(-tone_t * acc.y), expf(-tone_t * acc.z));
     V3 mp = vsub(v3(1.f, 1.f, 1.f), e);
     const float rg = 1.0f / 2.2f;
     V3 l = vmin1(v3(powf(mp.x, rg), powf(mp.y, rg), powf(mp.z, rg)), 1.f);
-    rgb8[3 * i] = (uint8_t)(l.x * 255);
-    rgb8[3 * i + 1] = (uint8_t)(l.y * 255);
-    rgb8[3 * i + 2] = (uint8_t)(l.z * 255);
+    rgb8[3 * gi] = (uint8_t)(l.x * 255);
+    rgb8[3 * gi + 1] = (uint8_t)(l.y * 255);
+    rgb8[3 * gi + 2] = (uint8_t)(l.z * 255);
+}
+
+__global__ void k_resolve(DevScene S, int64_t npx, Requests R, const float* __restrict__ est_g,
+                          const float* __restrict__ est_c, float tone_t, uint8_t* __restrict__ rgb8,
+                          float* __restrict__ radiance) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npx) return;
+    resolve_pixel(S, i, R, est_g, est_c, tone_t, rgb8, radiance);
+}
+
+__global__ void k_resolve_multi(const RenderInstDev* __restrict__ tab, const int64_t* __restrict__ px_off, int ninst,
+                                int64_t npx, Requests R, const float* __restrict__ est_g, float tone_t,
+                                uint8_t* __restrict__ rgb8, float* __restrict__ radiance) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= npx) return;
+    const int i = find_pixel_instance(px_off, ninst, g);
+    resolve_pixel(tab[i].S, g, R, est_g, nullptr, tone_t, rgb8, radiance);
 }
 
 }  // namespace
@@ -291,6 +348,23 @@ cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Req
     cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
     if (e != cudaSuccess) return e;
     k_eye<<<(unsigned)((npx + EYE_THREADS - 1) / EYE_THREADS), EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status);
+    return cudaGetLastError();
+}
+
+cudaError_t eye_pass_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
+                           unsigned* status, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
+    if (e != cudaSuccess || npx <= 0) return e;
+    k_eye_multi<<<(unsigned)((npx + EYE_THREADS - 1) / EYE_THREADS), EYE_THREADS, 0, st>>>(tab, px_off, ninst, npx, R,
+                                                                                          status);
+    return cudaGetLastError();
+}
+
+cudaError_t resolve_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
+                          const float* est_g, float tone_t, uint8_t* rgb8, float* radiance, cudaStream_t st) {
+    if (npx <= 0) return cudaSuccess;
+    k_resolve_multi<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(tab, px_off, ninst, npx, R, est_g, tone_t, rgb8,
+                                                                   radiance);
     return cudaGetLastError();
 }
 

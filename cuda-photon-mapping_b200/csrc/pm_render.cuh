@@ -31,6 +31,18 @@ struct Requests {
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
                      cudaStream_t st);
 
+// ---- several instances in one launch: global pixel g of instance i lies in
+// [px_off[i], px_off[i+1]); requests and outputs are indexed by global pixel ----
+struct RenderInstDev {
+    DevScene S;
+    CameraDev cam;
+    int max_depth;
+};
+cudaError_t eye_pass_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
+                           unsigned* status, cudaStream_t st);
+cudaError_t resolve_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
+                          const float* est_g, float tone_t, uint8_t* rgb8, float* radiance, cudaStream_t st);
+
 // Primary hits of n camera rays through uniformly jittered image positions
 // (sample i draws its position from the Philox stream (seed, i, tag)): hit
 // point, shading normal as the eye pass stores it, weight 1 where the eye pass

@@ -19,6 +19,7 @@
 // A path that misses all geometry ends there and stores nothing (the reference
 // returns an undefined value from trace() in that case); a refraction that
 // yields no ray also ends the path.
+#include <vector>
 #include "pm_trace.cuh"
 #include "pm_scan.cuh"
 
@@ -281,6 +282,122 @@ k_trace(KParams P) {
     }
 }
 
+// Several scene instances in one launch: one queue over the concatenated path
+// ranges; a lane that takes global path g traces path g - off[i] (+ the
+// instance's p0) of instance i, off[i] <= g < off[i+1], with that instance's
+// parameters (tab[i]: scene, stream seed, power; stage and count arrays are
+// shared, indexed by g with stride tab[i].npaths = the total).  The photons of
+// each instance are those of a single-instance trace of it.
+__device__ __forceinline__ int find_instance(const int64_t* __restrict__ off, int ninst, int64_t g) {
+    int lo = 0, hi = ninst - 1;   // last i with off[i] <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(TRACE_THREADS)
+k_trace_multi(const KParams* __restrict__ tab, const int64_t* __restrict__ off, int ninst, int64_t total,
+              unsigned long long* counter, int refill) {
+    const int lane = threadIdx.x & 31;
+    Lane L;
+    Trav T;
+    int stack[TRAV_STACK];
+    float sior[MAX_STACK];
+    int sid[MAX_STACK];
+    int64_t j = -1;          // global path index of this lane
+    int inst = 0;
+    int state = L_IDLE;
+    while (true) {
+        const bool need = state == L_IDLE;
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const unsigned long long mine = base + (unsigned long long)__popc(m & lanemask_lt());
+                if ((int64_t)mine < total) {
+                    j = (int64_t)mine;
+                    inst = find_instance(off, ninst, j);
+                    const KParams& P = tab[inst];
+                    start_path(P, L, P.p0 + (j - __ldg(off + inst)));
+                    state = L_RAY;
+                } else {
+                    state = L_DONE;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, state == L_DONE)) break;
+        const KParams& P = tab[inst];
+        if (state == L_RAY) {
+            trav_init(T, L.ray.o, L.ray.d, stack);
+            state = L_TRACE;
+        }
+        while (true) {
+            const bool tr = state == L_TRACE;
+            if (!__any_sync(0xffffffffu, tr)) break;
+            if (__popc(__ballot_sync(0xffffffffu, state == L_HIT)) >= refill) break;
+            if (tr && trav_step(P.S, T, L.ray.o, L.ray.d, stack)) state = L_HIT;
+        }
+        if (state == L_HIT) {
+            Hit h;
+            const int r = trav_resolve(P.S, T, h, stack);
+            if (r == TRAV_AGAIN) {
+                state = L_TRACE;
+            } else {
+                const bool alive = r == TRAV_HIT && shade(P, L, h, sior, sid, j);
+                L.bounce++;
+                if (!alive || L.bounce > P.max_bounces - 1) {
+                    P.cnt_g[j] = (uint32_t)L.ng;
+                    P.cnt_c[j] = (uint32_t)L.nc;
+                    j = -1;
+                    state = L_IDLE;
+                } else {
+                    state = L_RAY;
+                }
+            }
+        }
+    }
+}
+
+// Canonical-order append of a multi-instance trace: instance i's global-map
+// photons go to pos/dir/pow[ph0[i] + local offset], cut at cap[i];
+// inst_total[i] = global photons the instance produced before the cut.  A
+// batch builds no caustic map: caustic photons are dropped.
+__global__ void k_compact_multi(int64_t total, const int64_t* __restrict__ off, int ninst,
+                                const TraceInstOut* __restrict__ io, const float4* __restrict__ stage_pos,
+                                const float4* __restrict__ stage_dir, const uint32_t* __restrict__ cnt_g,
+                                const uint32_t* __restrict__ cnt_c, const uint32_t* __restrict__ scan_g,
+                                const uint32_t* __restrict__ grand_total, float* gpos, float* gdir, float* gpow,
+                                int64_t* __restrict__ inst_total) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ninst) {
+        const int64_t a = __ldg(off + g), b = __ldg(off + g + 1);
+        const uint32_t sa = a < total ? scan_g[a] : *grand_total;
+        const uint32_t sb = b < total ? scan_g[b] : *grand_total;
+        inst_total[g] = (int64_t)(sb - sa);
+    }
+    if (g >= total) return;
+    const int i = find_instance(off, ninst, g);
+    const TraceInstOut o = io[i];
+    int64_t og = (int64_t)(scan_g[g] - scan_g[__ldg(off + i)]);
+    const int slots = (int)(cnt_g[g] + cnt_c[g]);
+    for (int k = 0; k < slots && og < o.cap; k++) {
+        const size_t sidx = (size_t)k * (size_t)total + (size_t)g;
+        const float4 p = stage_pos[sidx];
+        if (__float_as_int(p.w) == 2) continue;
+        const float4 d = stage_dir[sidx];
+        const int64_t idx = o.ph0 + og++;
+        gpos[3 * idx] = p.x; gpos[3 * idx + 1] = p.y; gpos[3 * idx + 2] = p.z;
+        gdir[3 * idx] = d.x; gdir[3 * idx + 1] = d.y; gdir[3 * idx + 2] = d.z;
+        gpow[3 * idx] = o.power[0]; gpow[3 * idx + 1] = o.power[1]; gpow[3 * idx + 2] = o.power[2];
+    }
+}
+
 // canonical-order append of one batch into the two photon lists
 __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage_pos, const float4* __restrict__ stage_dir,
                           const uint32_t* __restrict__ cnt_g, const uint32_t* __restrict__ cnt_c,
@@ -312,6 +429,48 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage_pos, 
 }
 
 }  // namespace
+
+size_t trace_multi_table_bytes(int ninst) { return (size_t)ninst * sizeof(KParams); }
+
+cudaError_t trace_multi_tables(const TraceMulti& M, const TraceInst* insts, cudaStream_t st) {
+    std::vector<KParams> tab((size_t)M.ninst);
+    for (int i = 0; i < M.ninst; i++) {
+        KParams& P = tab[(size_t)i];
+        const TraceInst& I = insts[i];
+        P.S = I.S; P.seed = I.seed; P.tag = I.tag; P.max_bounces = I.max_bounces;
+        P.p0 = I.p0; P.npaths = M.total;
+        P.power = v3(I.power[0], I.power[1], I.power[2]);
+        P.counter = M.path_counter;
+        P.stage_pos = M.stage_pos; P.stage_dir = M.stage_dir;
+        P.cnt_g = M.cnt_g; P.cnt_c = M.cnt_c;
+        P.status = M.status;
+        P.refill = M.refill > 0 ? std::min(M.refill, 32) : TRACE_REFILL;
+    }
+    cudaError_t e = cudaMemcpyAsync(M.table, tab.data(), tab.size() * sizeof(KParams), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t trace_multi(const TraceMulti& M, cudaStream_t st) {
+    cudaError_t e;
+    if (M.total <= 0) return cudaSuccess;
+    if ((e = cudaMemsetAsync(M.path_counter, 0, 8, st)) != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_multi, TRACE_THREADS, 0)) != cudaSuccess)
+        return e;
+    const int64_t want = (M.total + TRACE_THREADS - 1) / TRACE_THREADS;
+    const int64_t grid = std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * M.sm_count);
+    const int refill = M.refill > 0 ? std::min(M.refill, 32) : TRACE_REFILL;
+    k_trace_multi<<<(unsigned)grid, TRACE_THREADS, 0, st>>>((const KParams*)M.table, M.path_off, M.ninst, M.total,
+                                                            M.path_counter, refill);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = scan_u32(M.cnt_g, M.scan_g, M.total, 0, M.totals, M.scan_ws, M.status, st)) != cudaSuccess) return e;
+    const int64_t n = std::max<int64_t>(M.total, M.ninst);
+    k_compact_multi<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        M.total, M.path_off, M.ninst, M.outs, M.stage_pos, M.stage_dir, M.cnt_g, M.cnt_c, M.scan_g, M.totals, M.pos,
+        M.dir, M.pow, M.inst_total);
+    return cudaGetLastError();
+}
 
 cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_t st) {
     cudaError_t e;

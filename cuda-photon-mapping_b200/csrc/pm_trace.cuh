@@ -36,6 +36,47 @@ struct PhotonList {
     int64_t filled;           // photons already in the list before this batch
 };
 
+// ---- several scene instances in one launch (global map only) ----
+struct TraceInst {
+    DevScene S;
+    uint64_t seed;
+    uint32_t tag;
+    int max_bounces;
+    int64_t p0;               // first path index of the instance's stream
+    float power[3];
+};
+struct TraceInstOut {         // where the instance's photons go
+    int64_t ph0, cap;
+    float power[3];
+};
+struct TraceMulti {
+    int ninst;
+    int64_t total;            // paths over all instances
+    const int64_t* path_off;  // device, ninst + 1: instance i traces global paths [off[i], off[i+1])
+    void* table;              // device, trace_multi_table_bytes(ninst): per-instance parameters
+    const TraceInstOut* outs; // device, ninst
+    unsigned long long* path_counter;
+    float4* stage_pos;        // max_bounces * total each
+    float4* stage_dir;
+    uint32_t* cnt_g;          // total each
+    uint32_t* cnt_c;
+    uint32_t* scan_g;
+    uint32_t* totals;         // [0] global photons of all instances
+    void* scan_ws;
+    float* pos;               // global photon list: 3 floats per photon, instance regions at ph0
+    float* dir;
+    float* pow;
+    int64_t* inst_total;      // device, ninst: photons produced before the cut
+    unsigned* status;
+    int sm_count;
+    int refill;
+};
+size_t trace_multi_table_bytes(int ninst);
+// upload the per-instance parameter table (synchronises the stream)
+cudaError_t trace_multi_tables(const TraceMulti& M, const TraceInst* insts, cudaStream_t st);
+// one launch over all instances' paths, scan, canonical-order compaction (no host round trip)
+cudaError_t trace_multi(const TraceMulti& M, cudaStream_t st);
+
 // trace one batch and append its photons (canonical order) to the two lists;
 // totals[0..1] receive the batch's photon counts before the capacity cut
 cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_t st);
