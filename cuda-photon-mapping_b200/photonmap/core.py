@@ -73,6 +73,23 @@ class _RequestView(C.Structure):
                 ("c", C.c_void_p), ("px_base", C.c_void_p), ("px_count", C.c_void_p), ("est_global", C.c_void_p)]
 
 
+class _BatchInstance(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("seed", C.c_uint64), ("photons", C.c_int64),
+                ("max_bounces", C.c_int32), ("k", C.c_int32), ("radius", C.c_float), ("max_depth", C.c_int32)]
+
+
+class _BatchOpts(C.Structure):
+    _fields_ = [("device", C.c_int32), ("autotune", C.c_int32), ("use_graph", C.c_int32)]
+
+
+class _BatchInfo(C.Structure):
+    _fields_ = [("instances", C.c_int32), ("paths", C.c_int64), ("photon_slots", C.c_int64), ("keys", C.c_int64),
+                ("pixels", C.c_int64), ("request_capacity", C.c_int64), ("desired_per_cell", C.c_int32),
+                ("gather_warps", C.c_int32), ("trace_refill", C.c_int32), ("graph", C.c_int32),
+                ("launches_per_frame", C.c_int32), ("ms_last_frame", C.c_float), ("photons_last_frame", C.c_int64),
+                ("requests_last_frame", C.c_int64), ("underfilled", C.c_int32)]
+
+
 class _LearnedOpts(C.Structure):
     _fields_ = [("tile", C.c_int32), ("probes", C.c_int32), ("max_rel_err", C.c_float)]
 
@@ -139,6 +156,12 @@ def library():
         "pm_cache_sample_points": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
         "pm_render_learned": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "pm_get_requests": ([vp, C.POINTER(_RequestView)], C.c_int),
+        "pm_batch_create": ([C.POINTER(C.c_void_p), vp, C.c_int32, C.POINTER(_BatchOpts)], C.c_int),
+        "pm_batch_destroy": ([vp], None),
+        "pm_batch_last_error": ([vp], C.c_char_p),
+        "pm_batch_frame": ([vp, C.c_uint64], C.c_int),
+        "pm_batch_image": ([vp, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "pm_batch_get_info": ([vp, C.POINTER(_BatchInfo)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -158,6 +181,19 @@ def camera_setup(position, direction, up, fov_deg, width, height) -> Camera:
     if rc:
         raise PMError(rc, "pm_camera_setup")
     return cam
+
+
+def _scene_desc(sc):
+    """pm_scene_desc of a photonmap.scenes.Scene and the arrays it points into (keep them alive)."""
+    pos = np.ascontiguousarray(sc.tri_pos, np.float32)
+    nrm = np.ascontiguousarray(sc.tri_nrm, np.float32)
+    tm = np.ascontiguousarray(sc.tri_model, np.int32)
+    mats = np.ascontiguousarray(sc.materials, np.float32)
+    td = None if sc.tri_diffuse is None else np.ascontiguousarray(sc.tri_diffuse, np.float32)
+    d = _SceneDesc(sc.ntri, pos.ctypes.data, nrm.ctypes.data, tm.ctypes.data,
+                   None if td is None else td.ctypes.data, sc.nmodel, mats.ctypes.data, int(sc.light_model),
+                   (C.c_float * 3)(*[float(x) for x in sc.light_intensity]), float(sc.default_ior))
+    return d, (pos, nrm, tm, mats, td)
 
 
 def _ptr(t):
@@ -199,14 +235,7 @@ class Context:
 
     # ------------------------------------------------------------ scene
     def set_scene(self, sc):
-        pos = np.ascontiguousarray(sc.tri_pos, np.float32)
-        nrm = np.ascontiguousarray(sc.tri_nrm, np.float32)
-        tm = np.ascontiguousarray(sc.tri_model, np.int32)
-        mats = np.ascontiguousarray(sc.materials, np.float32)
-        td = None if sc.tri_diffuse is None else np.ascontiguousarray(sc.tri_diffuse, np.float32)
-        d = _SceneDesc(sc.ntri, pos.ctypes.data, nrm.ctypes.data, tm.ctypes.data,
-                       None if td is None else td.ctypes.data, sc.nmodel, mats.ctypes.data, int(sc.light_model),
-                       (C.c_float * 3)(*[float(x) for x in sc.light_intensity]), float(sc.default_ior))
+        d, _keep = _scene_desc(sc)
         self._check(self.L.pm_set_scene(self.h, C.byref(d)), "pm_set_scene")
         self._scene = sc
 
@@ -439,3 +468,58 @@ class _DeviceArray:
     def __init__(self, ptr, shape, dtype):
         self.__cuda_array_interface__ = {"shape": tuple(int(x) for x in shape), "typestr": self._TYPESTR[str(dtype)],
                                          "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+class Batch:
+    """Many scene instances rendered per frame by one work queue per stage
+    (pm_batch_* in the C ABI).  instances: dicts with scene (scenes.Scene),
+    camera (Camera), seed, photons, max_bounces, k, radius, max_depth."""
+
+    def __init__(self, instances, device=0, autotune=False, use_graph=True):
+        import torch
+        self.torch = torch
+        self.L = library()
+        self.device = torch.device("cuda", device)
+        descs = [_scene_desc(i["scene"]) for i in instances]
+        arr = (_BatchInstance * len(instances))()
+        for j, (i, (d, _)) in enumerate(zip(instances, descs)):
+            arr[j] = _BatchInstance(C.cast(C.pointer(d), C.c_void_p), i["camera"], int(i["seed"]), int(i["photons"]),
+                                    int(i["max_bounces"]), int(i["k"]), float(i["radius"]), int(i["max_depth"]))
+        self.h = C.c_void_p()
+        o = _BatchOpts(device, int(bool(autotune)), int(bool(use_graph)))
+        rc = self.L.pm_batch_create(C.byref(self.h), arr, len(instances), C.byref(o))
+        if rc != 0:
+            msg = self.L.pm_batch_last_error(self.h).decode() if self.h.value else "no batch"
+            self.close()
+            raise RuntimeError(f"pm_batch_create failed ({rc}): {msg}")
+        self.n = len(instances)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc}): {self.L.pm_batch_last_error(self.h).decode()}")
+
+    def frame(self, frame=0):
+        self._check(self.L.pm_batch_frame(self.h, int(frame)), "pm_batch_frame")
+
+    def image(self, i):
+        """Copy of instance i's last image as a (height, width, 3) uint8 tensor."""
+        p, w, h = C.c_void_p(), C.c_int32(), C.c_int32()
+        self._check(self.L.pm_batch_image(self.h, int(i), C.byref(p), C.byref(w), C.byref(h)), "pm_batch_image")
+        return self.torch.as_tensor(_DeviceArray(p.value, (h.value, w.value, 3), self.torch.uint8),
+                                    device=self.device).clone()
+
+    def info(self):
+        o = _BatchInfo()
+        self._check(self.L.pm_batch_get_info(self.h, C.byref(o)), "pm_batch_get_info")
+        return {k: getattr(o, k) for k, _ in _BatchInfo._fields_}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.pm_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -218,3 +218,24 @@ def workload(name):
     sc = cornell(**w["scene"], seed=w["seed"])
     cam = default_camera(w["width"], w["height"])
     return sc, cam, w
+
+
+def batch_instances(n=64, seed=0, photons_range=(10_000, 2_000_000), res_range=(128, 1024), ks=(32, 64, 128),
+                    radius=0.1, max_bounces=8, max_depth=4):
+    """Seeded instances of the batched workload: the small room with the light
+    jittered uniformly by +-0.2 (x, z), sphere radii uniform in [0.15, 0.4],
+    photon counts log-uniform in photons_range, square images with edge
+    log-uniform in res_range, k drawn from ks.  Returns dicts of scene, camera
+    spec and parameters."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        lx, lz = rng.uniform(-0.2, 0.2, 2)
+        rg, rm = rng.uniform(0.15, 0.4, 2)
+        sc = cornell(sphere_level=3, seed=seed + i, light_offset=(float(lx), 0.0, float(lz)),
+                     glass_radius=float(rg), mirror_radius=float(rm))
+        photons = int(round(math.exp(rng.uniform(math.log(photons_range[0]), math.log(photons_range[1])))))
+        edge = int(round(math.exp(rng.uniform(math.log(res_range[0]), math.log(res_range[1])))))
+        out.append(dict(scene=sc, camera_spec=default_camera(edge, edge), seed=seed * 1000 + i, photons=photons,
+                        max_bounces=max_bounces, k=int(rng.choice(ks)), radius=radius, max_depth=max_depth))
+    return out

@@ -292,6 +292,64 @@ typedef struct pm_request_view {
 } pm_request_view;
 int pm_get_requests(pm_ctx* ctx, pm_request_view* out);
 
+/* ---------------------------------------------------------------------------
+ * Batched form (no counterpart in the reference).  Many scene instances,
+ * each with its own scene, camera, photon budget, k and radius, rendered per
+ * frame by kernels that take all instances' work from one queue per stage:
+ * one photon-tracing launch over every instance's paths, one grid build (one
+ * sort over all instances' keys), one eye pass over all pixels, one
+ * persistent gather over all requests, one resolve.  The frame is captured
+ * once into a CUDA graph and replayed.  Each instance's image equals a
+ * single-instance pm_trace_photons + pm_build_grid + pm_render of it with the
+ * same grid sizing (bit for bit when the batch uses the reference's sizing;
+ * autotuned cell sizes change only the float summation order of estimates).
+ * A batch builds global maps only (no caustic map). */
+typedef struct pm_batch pm_batch;
+
+typedef struct pm_batch_instance {
+    const pm_scene_desc* scene;   /* host arrays, copied at creation */
+    pm_camera camera;
+    uint64_t seed;                /* photon streams (frame f uses seed + f) */
+    int64_t photons;              /* global-map capacity */
+    int32_t max_bounces;          /* 1..32 */
+    int32_t k;                    /* 1..256 */
+    float radius;
+    int32_t max_depth;            /* eye path depth 0..5 */
+} pm_batch_instance;
+
+typedef struct pm_batch_opts {
+    int32_t device;
+    int32_t autotune;             /* 1: cell size, gather block shape and trace refill chosen by timing
+                                     candidate frames at creation; 0: the reference's grid sizing */
+    int32_t use_graph;            /* 1: capture the frame into a CUDA graph and replay it */
+} pm_batch_opts;
+
+typedef struct pm_batch_info {
+    int32_t instances;
+    int64_t paths, photon_slots, keys, pixels, request_capacity;
+    int32_t desired_per_cell;     /* chosen grid sizing (photons per cell) */
+    int32_t gather_warps;         /* chosen gather block shape (warps per block) */
+    int32_t trace_refill;         /* chosen trace refill threshold */
+    int32_t graph;                /* 1 when frames replay a captured graph */
+    int32_t launches_per_frame;   /* kernels one frame launches */
+    float ms_last_frame;          /* device time of the last frame (CUDA events) */
+    int64_t photons_last_frame;   /* photons stored by the last frame (after the capacity cuts) */
+    int64_t requests_last_frame;
+    int32_t underfilled;          /* instances whose last frame produced fewer photons than their capacity */
+} pm_batch_info;
+
+/* Creation traces each instance once (calibration), builds the grids, runs
+ * the autotuner when asked, and captures the frame graph.  On failure *out
+ * may still hold the batch: read pm_batch_last_error, then pm_batch_destroy. */
+int pm_batch_create(pm_batch** out, const pm_batch_instance* instances, int32_t n, const pm_batch_opts* opts);
+void pm_batch_destroy(pm_batch* b);
+const char* pm_batch_last_error(const pm_batch* b);
+/* One frame of every instance (photon streams seeded with seed + frame). */
+int pm_batch_frame(pm_batch* b, uint64_t frame);
+/* Device pointer to instance i's last image (uchar3, width x height, rows as pm_render). */
+int pm_batch_image(pm_batch* b, int32_t i, const uint8_t** out_rgb8, int32_t* width, int32_t* height);
+int pm_batch_get_info(pm_batch* b, pm_batch_info* out);
+
 /* Gather requests (eye-path hits that query the global map) of the last
  * pm_render call: the number of kNN queries its gather stage answered. */
 int pm_render_requests(pm_ctx* ctx, int64_t* out);
