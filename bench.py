@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache frame comparison")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched workload")
+    ap.add_argument("--batch-instances", type=int, default=64)
     # size overrides (profiling captures run reduced cases of the same workload)
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--width", type=int, default=0)
@@ -237,6 +239,74 @@ def override(w, cs, args):
 
 
 # ----------------------------------------------------------------- GPU arm
+def batched_frames(args, rank):
+    """The batched workload: seeded instances of the small room (light jitter,
+    sphere radii, photon counts log-uniform in [10k, 2M], square images with
+    edge log-uniform in [128, 1024], k in {32, 64, 128}), one frame of all of
+    them per step through the batch (one work queue per stage, autotuned,
+    replayed from a CUDA graph), against the same instances rendered one after
+    another through the single-instance API (trace + grid + render each)."""
+    import torch
+    import photonmap
+    from photonmap import scenes
+    insts = []
+    for d in scenes.batch_instances(n=args.batch_instances, seed=rank):
+        cs = d.pop("camera_spec")
+        d["camera"] = photonmap.camera_setup(cs.position, cs.direction, cs.up, cs.fov_deg, cs.width, cs.height)
+        insts.append(d)
+    t0 = time.perf_counter()
+    b = photonmap.Batch(insts, autotune=True, use_graph=True)
+    t_create = time.perf_counter() - t0
+    K = max(args.steps, 3)
+    for f in range(2):
+        b.frame(f)
+    ms_dev = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for f in range(K):
+        b.frame(2 + f)
+        ms_dev.append(b.info()["ms_last_frame"])
+    torch.cuda.synchronize()
+    ms_wall = (time.perf_counter() - t0) * 1000 / K
+    info = b.info()
+    b.close()
+    # the same instances one after another through the single-instance API
+    ctxs = []
+    for d in insts:
+        c = photonmap.Context(torch.cuda.current_device())
+        c.set_scene(d["scene"])
+        ctxs.append(c)
+
+    def sequential(f):
+        for c, d in zip(ctxs, insts):
+            c.trace_photons(d["seed"] + f, d["max_bounces"], d["photons"])
+            c.build_grid(photonmap.PM_MAP_GLOBAL)
+            c.render(d["camera"], d["k"], d["radius"], d["max_depth"], radiance=False)
+        for c in ctxs:
+            c.sync()
+
+    sequential(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for f in range(K):
+        sequential(2 + f)
+    ms_seq = (time.perf_counter() - t0) * 1000 / K
+    for c in ctxs:
+        c.close()
+    photons = sum(d["photons"] for d in insts)
+    pixels = sum(d["camera"].width * d["camera"].height for d in insts)
+    ms = float(np.median(ms_dev))
+    return {"instances": len(insts), "photons_per_frame": photons, "pixels_per_frame": pixels,
+            "ms_per_frame": ms, "mphotons_per_s": photons / (ms * 1e-3) / 1e6,
+            "ms_per_frame_wall": ms_wall, "ms_per_frame_sequential_api": ms_seq,
+            "speedup_vs_sequential": ms_seq / ms_wall, "launches_per_frame": info["launches_per_frame"],
+            "graph": bool(info["graph"]), "autotuned": {"desired_per_cell": info["desired_per_cell"],
+                                                        "gather_warps": info["gather_warps"],
+                                                        "trace_refill": info["trace_refill"]},
+            "underfilled_instances": info["underfilled"], "create_s": t_create,
+            "stage_ms_eager": info["stage_ms"]}
+
+
 def learned_frames(ctx, cam, w, rgb, args, world):
     """Frame time of the plain render against the learned render on the same
     photon map (the map stays resident, as in the reference's render loop).
@@ -385,6 +455,9 @@ def run_ours(args):
     learned_block = None
     if not args.no_learned:
         learned_block = learned_frames(ctx, cam, w, rgb, args, world)
+    batched_block = None
+    if not args.no_batched:
+        batched_block = batched_frames(args, rank)
     ph = ctx.photons(0, sorted_=False)  # noqa: F841  (map still resident)
     hbm, src = peaks()
     line = None
@@ -419,6 +492,7 @@ def run_ours(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "learned": learned_block,
+            "batched": batched_block,
         }
     ctx.close()
     if world > 1:

@@ -71,6 +71,7 @@ struct pm_batch {
     float ms_last = 0.f;
     int64_t photons_last = 0, requests_last = 0;
     int underfilled = 0;
+    float stage_ms[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -455,6 +456,10 @@ int create(pm_batch* b, const pm_batch_instance* in, int32_t n, const pm_batch_o
     if (int rc = plan_grids(b, 1000)) return rc;
     if (opts && opts->autotune)
         if (int rc = autotune(b)) return rc;
+    // per-stage device times of the chosen configuration (frame 0, eager)
+    if (int rc = launch_stages(b, -1, nullptr)) return rc;
+    for (int stage = 0; stage < 5; stage++)
+        if (int rc = time_stage(b, stage, 1, &b->stage_ms[stage])) return rc;
     if (b->use_graph)
         if (int rc = capture(b)) return rc;
     return PM_OK;
@@ -553,6 +558,7 @@ int pm_batch_get_info(pm_batch* b, pm_batch_info* o) {
     o->photons_last_frame = b->photons_last;
     o->requests_last_frame = b->requests_last;
     o->underfilled = b->underfilled;
+    for (int i = 0; i < 5; i++) o->stage_ms[i] = b->stage_ms[i];
     return PM_OK;
 }
 

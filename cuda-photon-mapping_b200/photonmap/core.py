@@ -87,7 +87,7 @@ class _BatchInfo(C.Structure):
                 ("pixels", C.c_int64), ("request_capacity", C.c_int64), ("desired_per_cell", C.c_int32),
                 ("gather_warps", C.c_int32), ("trace_refill", C.c_int32), ("graph", C.c_int32),
                 ("launches_per_frame", C.c_int32), ("ms_last_frame", C.c_float), ("photons_last_frame", C.c_int64),
-                ("requests_last_frame", C.c_int64), ("underfilled", C.c_int32)]
+                ("requests_last_frame", C.c_int64), ("underfilled", C.c_int32), ("stage_ms", C.c_float * 5)]
 
 
 class _LearnedOpts(C.Structure):
@@ -511,7 +511,9 @@ class Batch:
     def info(self):
         o = _BatchInfo()
         self._check(self.L.pm_batch_get_info(self.h, C.byref(o)), "pm_batch_get_info")
-        return {k: getattr(o, k) for k, _ in _BatchInfo._fields_}
+        d = {k: getattr(o, k) for k, _ in _BatchInfo._fields_}
+        d["stage_ms"] = dict(zip(("trace", "grid", "eye", "gather", "resolve"), [float(x) for x in o.stage_ms]))
+        return d
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

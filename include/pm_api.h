@@ -336,6 +336,7 @@ typedef struct pm_batch_info {
     int64_t photons_last_frame;   /* photons stored by the last frame (after the capacity cuts) */
     int64_t requests_last_frame;
     int32_t underfilled;          /* instances whose last frame produced fewer photons than their capacity */
+    float stage_ms[5];            /* trace, grid, eye, gather, resolve of one eager frame timed at creation */
 } pm_batch_info;
 
 /* Creation traces each instance once (calibration), builds the grids, runs
