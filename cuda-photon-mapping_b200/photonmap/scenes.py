@@ -15,6 +15,9 @@ Workloads (sizes in ``WORKLOADS``):
   cornell_hf_1080p  the same room with a 256 x 256-vertex seeded value-noise
                   heightfield floor (130,050 triangles, amplitude 0.05, per-triangle
                   albedo U[0.3, 0.8]), 10M photons, depth 10, 1920x1080, k 64, r 0.05
+  cornell_stress_4k the small room with 4 more glass spheres (IOR U[1.3, 1.7]) and an
+                  81,920-triangle glass icosphere, 100M photons, depth 16, 3840x2160,
+                  k 200, r 0.02
 """
 from __future__ import annotations
 
@@ -152,11 +155,14 @@ def heightfield(n, amplitude, rng):
 
 
 def cornell(sphere_level=3, heightfield_n=0, seed=0, light_offset=(0.0, 0.0, 0.0),
-            glass_radius=0.3, mirror_radius=0.3):
+            glass_radius=0.3, mirror_radius=0.3, stress=False):
     """The Cornell-style room shared by the workloads.
 
     Models (ids = indices): 0 floor, 1 ceiling, 2 back wall, 3 left wall (red),
     4 right wall (green), 5 light, 6 glass sphere, 7 mirror sphere.
+    stress: also 4 small glass spheres (r 0.15, IOR uniform in [1.3, 1.7],
+    seeded) and a large glass icosphere of 81,920 triangles (subdivision level
+    6, the first icosphere above 64k triangles; r 0.3, IOR 1.5), models 8-12.
     """
     white = (0.75, 0.75, 0.75)
     parts = []   # (pos, nrm, material, per-tri diffuse or None, name)
@@ -185,6 +191,13 @@ def cornell(sphere_level=3, heightfield_n=0, seed=0, light_offset=(0.0, 0.0, 0.0
     parts.append((p, n, material(specular=(1, 1, 1), ior=1.5, opaque=0.0), None, "glass"))
     p, n = icosphere((0.45, -0.7, -0.3), mirror_radius, sphere_level)
     parts.append((p, n, material(specular=(1, 1, 1), opaque=1.0), None, "mirror"))
+    if stress:
+        for c in ((-0.65, -0.85, -0.6), (0.0, -0.85, -0.7), (0.65, -0.85, 0.55), (-0.15, -0.85, 0.7)):
+            ior = float(rng.uniform(1.3, 1.7))
+            p, n = icosphere(c, 0.15, sphere_level)
+            parts.append((p, n, material(specular=(1, 1, 1), ior=ior, opaque=0.0), None, "glass_small"))
+        p, n = icosphere((0.1, 0.05, 0.1), 0.3, 6)
+        parts.append((p, n, material(specular=(1, 1, 1), ior=1.5, opaque=0.0), None, "glass_big"))
 
     pos = np.concatenate([q[0] for q in parts]).astype(np.float32)
     nrm = np.concatenate([q[1] for q in parts]).astype(np.float32)
@@ -210,6 +223,8 @@ WORKLOADS = {
                           width=320, height=240, k=100, radius=0.1, max_depth=4, seed=0),
     "cornell_hf_1080p": dict(scene=dict(sphere_level=3, heightfield_n=256), photons=10_000_000, caustic=0,
                              max_bounces=10, width=1920, height=1080, k=64, radius=0.05, max_depth=4, seed=0),
+    "cornell_stress_4k": dict(scene=dict(sphere_level=3, stress=True), photons=100_000_000, caustic=0,
+                              max_bounces=16, width=3840, height=2160, k=200, radius=0.02, max_depth=4, seed=0),
 }
 
 

@@ -89,6 +89,21 @@ def test_trace_with_caustic_map(ctx, cornell):
     assert np.array_equal(_np(c["list_power"]), tr["c_pow"])
 
 
+def test_trace_stress_scene_nested_glass(ctx, orc):
+    # the stress room: five glass bodies of four IORs, 16 bounces, a caustic map
+    sc, cam, w = scenes.workload("cornell_stress_4k")
+    ctx.set_scene(sc)
+    s = orc.scene(sc)
+    ctx.trace_photons(5, w["max_bounces"], 30_000, 10_000)
+    tr = s.trace_photons(5, w["max_bounces"], 30_000, 10_000)
+    g = ctx.photons(0, sorted_=False)
+    c = ctx.photons(1, sorted_=False)
+    for key, arr in (("g_pos", g["list_pos"]), ("g_dir", g["list_dir"]), ("c_pos", c["list_pos"]),
+                     ("c_dir", c["list_dir"]), ("c_pow", c["list_power"])):
+        assert np.array_equal(_np(arr), tr[key]), key
+    assert ctx.status() == 0
+
+
 def test_trace_paths_heightfield_subset(ctx, orc):
     # the 130k-triangle scene: the BVH must return the reference's closest hits
     sc = scenes.cornell(sphere_level=3, heightfield_n=256, seed=0)
