@@ -469,11 +469,13 @@ struct WarpWalk {
 
     // Nearest-first walk over the sub-cells of the reference's cube of cells
     // [lo, hi] (global sub-cell coordinates): the query's sub-cell with the
-    // shell at Chebyshev distance 1, then shells R = 2, 3, ...  Lanes test 32
-    // shell members at a time (box distance against the current bound,
-    // non-empty photon range); the survivors are queued and scanned together.
-    // After each shell the distance histogram tightens the bound; a shell whose
-    // nearest possible point is farther than the bound ends the walk.
+    // shell at Chebyshev distance 1, then, once k candidates are in the store,
+    // the remaining sub-cells of the bounding box of the bound's sphere in one
+    // pass (box_rest); in sparse regions shells R = 2, 3, ... nearest first.
+    // Lanes test 32 sub-cells at a time (box distance against the current
+    // bound, non-empty photon range); the survivors are queued and scanned
+    // together.  After each shell the distance histogram tightens the bound; a
+    // shell whose nearest possible point is farther than the bound ends the walk.
     __device__ void walk(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz) {
         constexpr int NM = 1;
         const int S = G.S, sh = __ffs(S) - 1;
@@ -496,6 +498,12 @@ struct WarpWalk {
         }
         for (int R = 1; R <= Rmax; R++) {
             if ((float)(R - 1) * sc - pad > lim * m) break;
+            if (R == 2 && n >= k) {
+                // lim now bounds the k-th distance: visit only the sub-cells of
+                // its sphere's bounding box outside the 3x3x3 block done
+                box_rest(X0, Y0, Z0, lx, ly, lz, hx, hy, hz, sc, pad, m, GX, GY, GZ, S3, sh);
+                break;
+            }
             const int side = 2 * R + 1;
             const int shell = 2 * side * side + 4 * (side - 1) * (side - 2);
             const int total = shell + (R == 1 ? 1 : 0);   // ring 1 also carries the query's own sub-cell
@@ -528,9 +536,55 @@ struct WarpWalk {
                     if (base + 32 * u < total) enqueue(b[u] > a[u], a[u], b[u] - a[u]);
             }
             flush();
-            if (n > k) bound();
+            if (n >= k) bound();
         }
         flush();
+    }
+
+    // Sub-cells X in [ceil((q - L - pad - mn) / sc) - 1, floor((q + L + pad - mn) / sc)]
+    // per axis (the padded boxes that can reach the sphere of radius L = lim m
+    // around q), clamped to the cube [lo, hi] (boundary sub-cells with an open
+    // side are then included whenever the sphere reaches past them), minus the
+    // block |X - X0|, |Y - Y0|, |Z - Z0| <= 1; each tested and queued as in walk().
+    __device__ void box_rest(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz, float sc,
+                             float pad, float m, int GX, int GY, int GZ, uint32_t S3, int sh) {
+        const float L = lim * m;
+        auto range = [&](float qc, float mn, int lo, int hi, int& b0, int& b1) {
+            float f0 = ceilf((qc - L - pad - mn) / sc) - 1.f, f1 = floorf((qc + L + pad - mn) / sc);
+            b0 = (int)fminf(fmaxf(f0, (float)lo), (float)hi);
+            b1 = (int)fminf(fmaxf(f1, (float)lo), (float)hi);
+        };
+        int x0, x1, y0, y1, z0, z1;
+        range(q.x, G.mn[0], lx, hx, x0, x1);
+        range(q.y, G.mn[1], ly, hy, y0, y1);
+        range(q.z, G.mn[2], lz, hz, z0, z1);
+        if (x0 >= X0 - 1 && x1 <= X0 + 1 && y0 >= Y0 - 1 && y1 <= Y0 + 1 && z0 >= Z0 - 1 && z1 <= Z0 + 1) return;
+        const int S = G.S;
+        const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1, nxy = nx * ny;
+        const int total = nxy * nz;
+        const float inv_nx = 1.0f / (float)nx, inv_nxy = 1.0f / (float)nxy;
+        for (int base = 0; base < total; base += 32) {
+            const int t = base + lane;
+            uint32_t a = 0u, b = 0u;
+            if (t < total) {
+                const int iz = small_div(t, nxy, inv_nxy), rxy = t - iz * nxy;
+                const int iy = small_div(rxy, nx, inv_nx), ix = rxy - iy * nx;
+                const int X = x0 + ix, Y = y0 + iy, Z = z0 + iz;
+                if (abs(X - X0) > 1 || abs(Y - Y0) > 1 || abs(Z - Z0) > 1) {
+                    float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
+                    float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
+                    float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
+                    if (ax * ax + ay * ay + az * az <= L * L) {
+                        const uint32_t cellid = (uint32_t)((X >> sh) + (Y >> sh) * G.gx + (Z >> sh) * G.gx * G.gy);
+                        const uint32_t key =
+                            cellid * S3 + (uint32_t)((X & (S - 1)) + S * ((Y & (S - 1)) + S * (Z & (S - 1))));
+                        a = __ldg(G.key_starts + key);
+                        b = __ldg(G.key_starts + key + 1);
+                    }
+                }
+            }
+            enqueue(b > a, a, b - a);
+        }
     }
 };
 
