@@ -169,7 +169,7 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws, &ctx->cache_w32,
                       &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
                       &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
-                      &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts};
+                      &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -313,6 +313,32 @@ int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const f
                 P<float>(ctx->cache_m), P<float>(ctx->cache_v), ctx->cache_step, o.lr, o.beta1, o.beta2, o.eps, ctx->st));
     ctx->launches += 1;
     return check_status(ctx, "cache train");
+}
+
+int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                         int64_t n, int64_t batch, int steps, int64_t* inout_offset, float* out_loss) {
+    if (!ctx) return PM_ERR_INVALID;
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    if (n <= 0 || batch <= 0 || steps < 0 || !pos || !nrm || !target)
+        return fail(ctx, PM_ERR_INVALID, "cache train steps: n > 0, batch > 0, steps >= 0 and sample arrays required");
+    CK(cudaSetDevice(ctx->device));
+    const int64_t b = std::min(batch, n);
+    int64_t off = inout_offset ? std::max<int64_t>(*inout_offset, 0) : 0;
+    const pm_cache_opts& o = ctx->cache_opts;
+    for (int s = 0; s < steps; ++s) {
+        if (off + b > n) off = 0;
+        if (int rc = cache_backprop(ctx, pos + off * 3, nrm + off * 3, target + off * 3, weight ? weight + off : nullptr,
+                                    b, s + 1 == steps ? out_loss : nullptr))
+            return rc;
+        ctx->cache_step++;
+        CK(mlp_adam(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), P<float>(ctx->cache_grad),
+                    P<float>(ctx->cache_m), P<float>(ctx->cache_v), ctx->cache_step, o.lr, o.beta1, o.beta2, o.eps,
+                    ctx->st));
+        ctx->launches += 1;
+        off += b;
+    }
+    if (inout_offset) *inout_offset = off;
+    return check_status(ctx, "cache train steps");
 }
 
 int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
@@ -992,6 +1018,7 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     ENSURE(ctx->probe_est, (size_t)nprobe * 12);
     ENSURE(ctx->tile_flag, (size_t)ntiles);
     ENSURE(ctx->learned_counts, 16);
+    ENSURE(ctx->fallback_list, (size_t)std::max<int64_t>(F.nreq, 1) * 4);
     CK(cudaEventRecord(ctx->ev[6], ctx->st));
     // the cache answers every global request
     MlpInputs in{};
@@ -1007,18 +1034,20 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 16, ctx->st));
     CK(learned_select(F.cd, F.R, F.nreq, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
                       P<float>(ctx->est_mlp), lo->max_rel_err, P<uint8_t>(ctx->tile_flag),
-                      P<unsigned long long>(ctx->learned_counts), ctx->st));
+                      P<unsigned long long>(ctx->learned_counts), P<uint32_t>(ctx->fallback_list), ctx->st));
+    // the exact gather for the listed fallback requests only
+    unsigned long long cnt[2] = {0, 0};
+    CK(cudaMemcpyAsync(cnt, ctx->learned_counts.p, 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
     GatherQueries Q{};
-    Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = LEARNED_FALLBACK;
+    Q.n = (int64_t)cnt[1]; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = LEARNED_FALLBACK;
+    Q.idx = P<uint32_t>(ctx->fallback_list);
     GatherOut OF{P<float>(ctx->est_fb), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OF, P<unsigned>(ctx->status), ctx->st));
     CK(learned_merge(F.R, F.nreq, P<float>(ctx->est_mlp), P<float>(ctx->est_fb), P<float>(ctx->est_g), ctx->st));
     ctx->launches += (F.nreq > 0 ? 1 : 0) + 1 + 1 + 1 + (F.nreq > 0 ? 1 : 0) + 1 + (F.nreq > 0 ? 1 : 0);
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
     if (out_stats) {
-        unsigned long long cnt[2] = {0, 0};
-        CK(cudaMemcpyAsync(cnt, ctx->learned_counts.p, 16, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
         out_stats->tiles = ntiles;
         out_stats->fallback_tiles = (int64_t)cnt[0];
         out_stats->requests = F.nreq;

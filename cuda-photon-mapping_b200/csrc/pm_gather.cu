@@ -684,8 +684,9 @@ __global__ void __launch_bounds__(WARPS * 32, 4)
 k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, GatherOut O) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t i = (int64_t)blockIdx.x * WARPS + warp;
-    if (i >= Q.n) return;
+    const int64_t qi = (int64_t)blockIdx.x * WARPS + warp;
+    if (qi >= Q.n) return;
+    const int64_t i = Q.idx ? (int64_t)Q.idx[qi] : qi;
     WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
     V3 q, nrm;
     bool active = true;

@@ -26,6 +26,8 @@ struct GatherQueries {
     const float4* pos4;
     const float4* nrm4;
     uint32_t flag_mask;
+    // optional: query i is record idx[i] (read from and written to that index)
+    const uint32_t* idx;
 };
 
 struct GatherOut {

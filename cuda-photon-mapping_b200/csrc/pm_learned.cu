@@ -79,9 +79,11 @@ __global__ void k_tile_flags(int64_t ntiles, int P, const uint32_t* __restrict__
     if (f) atomicAdd(nflag, 1ull);
 }
 
-// requests of flagged tiles that need the global estimate get flag bit 2
+// requests of flagged tiles that need the global estimate get flag bit 2 and
+// join the list of fallback requests (list order is immaterial: every answer
+// is written at its request's index)
 __global__ void k_mark_fallback(int64_t nreq, Requests R, int W, int tile, int tiles_x, const uint8_t* __restrict__ flag,
-                                unsigned long long* __restrict__ nfb) {
+                                unsigned long long* __restrict__ nfb, uint32_t* __restrict__ list) {
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool fb = false;
     if (q < nreq) {
@@ -98,7 +100,10 @@ __global__ void k_mark_fallback(int64_t nreq, Requests R, int W, int tile, int t
         R.b[q] = b;
     }
     const unsigned m = __ballot_sync(0xffffffffu, fb);
-    if ((threadIdx.x & 31) == 0 && m) atomicAdd(nfb, (unsigned long long)__popc(m));
+    unsigned long long base = 0;
+    if ((threadIdx.x & 31) == 0 && m) base = atomicAdd(nfb, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (fb) list[base + __popc(m & lanemask_lt())] = (uint32_t)q;
 }
 
 // est = exact for fallback requests, else the cache
@@ -127,14 +132,14 @@ cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, in
 
 cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
                            const float* probe_exact, const float* cached, float max_rel_err, uint8_t* tile_flag,
-                           unsigned long long* counts, cudaStream_t st) {
+                           unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st) {
     const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
     const int64_t ntiles = (int64_t)tx * ty;
     k_tile_flags<<<blocks(ntiles, 256), 256, 0, st>>>(ntiles, P, preq, probe_exact, cached, max_rel_err, tile_flag,
                                                       counts);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || nreq <= 0) return e;
-    k_mark_fallback<<<blocks(nreq, 256), 256, 0, st>>>(nreq, R, cam.W, tile, tx, tile_flag, counts + 1);
+    k_mark_fallback<<<blocks(nreq, 256), 256, 0, st>>>(nreq, R, cam.W, tile, tx, tile_flag, counts + 1, fallback_list);
     return cudaGetLastError();
 }
 

@@ -149,6 +149,7 @@ def library():
         "pm_render_requests": ([vp, C.POINTER(C.c_int64)], C.c_int),
         "pm_cache_init": ([vp, C.POINTER(_CacheOpts)], C.c_int),
         "pm_cache_train_step": ([vp, vp, vp, vp, vp, i64, vp], C.c_int),
+        "pm_cache_train_steps": ([vp, vp, vp, vp, vp, i64, i64, C.c_int, vp, vp], C.c_int),
         "pm_cache_gradient": ([vp, vp, vp, vp, vp, i64, vp, vp], C.c_int),
         "pm_cache_infer": ([vp, vp, vp, i64, vp], C.c_int),
         "pm_cache_get_params": ([vp, vp], C.c_int),
@@ -346,6 +347,17 @@ class Context:
         self._check(self.L.pm_cache_train_step(self.h, _ptr(pos), _ptr(nrm), _ptr(target), _ptr(weight),
                                                pos.shape[0], C.byref(loss)), "pm_cache_train_step")
         return loss.value
+
+    def cache_train_steps(self, pos, nrm, target, steps, batch, offset=0, weight=None):
+        """`steps` Adam steps over consecutive `batch`-sample slices of the pool from
+        `offset` (wrapping); returns (last step's loss, next offset)."""
+        pos, nrm, target, weight = self._samples(pos, nrm, target, weight)
+        loss = C.c_float(float("nan"))
+        off = C.c_int64(int(offset))
+        self._check(self.L.pm_cache_train_steps(self.h, _ptr(pos), _ptr(nrm), _ptr(target), _ptr(weight),
+                                                pos.shape[0], int(batch), int(steps), C.byref(off),
+                                                C.byref(loss)), "pm_cache_train_steps")
+        return loss.value, off.value
 
     def cache_gradient(self, pos, nrm, target, weight=None):
         pos, nrm, target, weight = self._samples(pos, nrm, target, weight)

@@ -42,12 +42,6 @@ def training_pool(ctx, cam, k, radius, n=1 << 20, seed=1, map_id=0) -> Pool:
 def cache_fit(ctx, pool: Pool, steps, batch=65536, offset=0):
     """Runs `steps` Adam steps over consecutive batches of the (shuffled) pool,
     starting at `offset`; returns (last loss, next offset)."""
-    b = min(int(batch), pool.n)
-    loss = float("nan")
-    for _ in range(int(steps)):
-        if offset + b > pool.n:
-            offset = 0
-        loss = ctx.cache_train_step(pool.pos[offset:offset + b], pool.nrm[offset:offset + b],
-                                    pool.target[offset:offset + b])
-        offset += b
-    return loss, offset
+    if int(steps) <= 0:
+        return float("nan"), offset
+    return ctx.cache_train_steps(pool.pos, pool.nrm, pool.target, int(steps), int(batch), offset)

@@ -237,6 +237,14 @@ int pm_cache_init(pm_ctx* ctx, const pm_cache_opts* opts);
 int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
                         int64_t n, float* out_loss);
 
+/* `steps` Adam steps over consecutive batches of `batch` samples of the n-sample
+ * pool, starting at *inout_offset (null: 0) and wrapping to 0 where a batch
+ * would run past n; *inout_offset receives the next offset.  One status check
+ * for the whole run (no host synchronisation between steps); *out_loss
+ * (optional) = the last step's loss as pm_cache_train_step reports it. */
+int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
+                         int64_t n, int64_t batch, int steps, int64_t* inout_offset, float* out_loss);
+
 /* Gradient of that loss with respect to the parameters, without an update
  * (host output of PM_CACHE_PARAMS floats), and the loss. */
 int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
