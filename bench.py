@@ -329,7 +329,8 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     stats = {}
 
     def learned_frame():
-        _, off[0] = learned.cache_fit(ctx, pool, TRAIN_PER_FRAME // BATCH, batch=BATCH, offset=off[0])
+        _, off[0] = learned.cache_fit(ctx, pool, TRAIN_PER_FRAME // BATCH, batch=BATCH, offset=off[0],
+                                      want_loss=False)
         _, _, st = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], max_rel_err=THR, radiance=False,
                                       out_rgb8=rgb)
         stats.update(st)

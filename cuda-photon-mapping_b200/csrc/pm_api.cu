@@ -338,7 +338,9 @@ int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const 
         off += b;
     }
     if (inout_offset) *inout_offset = off;
-    return check_status(ctx, "cache train steps");
+    // without a loss to report the steps stay queued: their device status is
+    // reported by the next call on the context that synchronises
+    return out_loss ? check_status(ctx, "cache train steps") : PM_OK;
 }
 
 int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
@@ -1017,7 +1019,7 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     ENSURE(ctx->probe_req, (size_t)nprobe * 4);
     ENSURE(ctx->probe_est, (size_t)nprobe * 12);
     ENSURE(ctx->tile_flag, (size_t)ntiles);
-    ENSURE(ctx->learned_counts, 16);
+    ENSURE(ctx->learned_counts, 32);   // flagged tiles, fallback requests, gather work counter
     ENSURE(ctx->fallback_list, (size_t)std::max<int64_t>(F.nreq, 1) * 4);
     CK(cudaEventRecord(ctx->ev[6], ctx->st));
     // the cache answers every global request
@@ -1031,23 +1033,24 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     PQ.n = nprobe; PQ.pos4 = P<float4>(ctx->probe_pos); PQ.nrm4 = P<float4>(ctx->probe_nrm); PQ.flag_mask = 1u;
     GatherOut PO{P<float>(ctx->probe_est), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), PQ, o->r_global, o->k_global, 0, PO, P<unsigned>(ctx->status), ctx->st));
-    CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 16, ctx->st));
+    CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 32, ctx->st));
     CK(learned_select(F.cd, F.R, F.nreq, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
                       P<float>(ctx->est_mlp), lo->max_rel_err, P<uint8_t>(ctx->tile_flag),
                       P<unsigned long long>(ctx->learned_counts), P<uint32_t>(ctx->fallback_list), ctx->st));
-    // the exact gather for the listed fallback requests only
-    unsigned long long cnt[2] = {0, 0};
-    CK(cudaMemcpyAsync(cnt, ctx->learned_counts.p, 16, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    // the exact gather for the listed fallback requests only (count read on the device)
     GatherQueries Q{};
-    Q.n = (int64_t)cnt[1]; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = LEARNED_FALLBACK;
+    Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = LEARNED_FALLBACK;
     Q.idx = P<uint32_t>(ctx->fallback_list);
     GatherOut OF{P<float>(ctx->est_fb), nullptr, nullptr, nullptr};
-    CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OF, P<unsigned>(ctx->status), ctx->st));
+    unsigned long long* counts = P<unsigned long long>(ctx->learned_counts);
+    CK(gather_listed(grid_of(G, G), Q, counts + 1, counts + 2, o->r_global, o->k_global, OF, ctx->sm_count, ctx->st));
     CK(learned_merge(F.R, F.nreq, P<float>(ctx->est_mlp), P<float>(ctx->est_fb), P<float>(ctx->est_g), ctx->st));
     ctx->launches += (F.nreq > 0 ? 1 : 0) + 1 + 1 + 1 + (F.nreq > 0 ? 1 : 0) + 1 + (F.nreq > 0 ? 1 : 0);
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
     if (out_stats) {
+        unsigned long long cnt[2] = {0, 0};
+        CK(cudaMemcpyAsync(cnt, ctx->learned_counts.p, 16, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
         out_stats->tiles = ntiles;
         out_stats->fallback_tiles = (int64_t)cnt[0];
         out_stats->requests = F.nreq;

@@ -706,6 +706,50 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
     gather_query<UCAP>(G, U, i, q, nrm, r, k, require_full, O, lane);
 }
 
+// Listed queries, persistent: warps take list positions from *queue until
+// min(*n_dev, Q.n) is reached (a device-side count, so no host round trip
+// sits between the list's producer and this launch); position qi answers
+// record Q.idx[qi].
+template <int UCAP>
+__global__ void __launch_bounds__(WARPS * 32, 4)
+k_gather_listed(GatherGrid G, GatherQueries Q, const unsigned long long* __restrict__ n_dev,
+                unsigned long long* __restrict__ queue, float r, int k, GatherOut O) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
+    const int64_t n = (int64_t)min(*n_dev, (unsigned long long)Q.n);
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(queue, 1ull);
+        const int64_t qi = (int64_t)__shfl_sync(0xffffffffu, t, 0);
+        if (qi >= n) break;
+        const int64_t i = (int64_t)Q.idx[qi];
+        const float4 a = Q.pos4[i], b = Q.nrm4[i];
+        if (!((__float_as_uint(b.w) & Q.flag_mask) != 0u) || k <= 0) {
+            gather_zero(i, k, O, lane);
+            continue;
+        }
+        gather_query<UCAP>(G, U, i, xyz(a), xyz(b), r, k, 0, O, lane);
+        __syncwarp();
+    }
+}
+
+template <int UCAP>
+cudaError_t launch_listed(const GatherGrid& G, const GatherQueries& Q, const unsigned long long* n_dev,
+                          unsigned long long* queue, float r, int k, const GatherOut& O, int sm_count,
+                          cudaStream_t st) {
+    const size_t smem = sizeof(WarpStore<UCAP>) * WARPS;
+    cudaError_t e = cudaFuncSetAttribute(k_gather_listed<UCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_listed<UCAP>, WARPS * 32, smem)) != cudaSuccess)
+        return e;
+    const int64_t need = (Q.n + WARPS - 1) / WARPS;
+    const unsigned grid = (unsigned)std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * std::max(sm_count, 1));
+    k_gather_listed<UCAP><<<grid, WARPS * 32, smem, st>>>(G, Q, n_dev, queue, r, k, O);
+    return cudaGetLastError();
+}
+
 __device__ __forceinline__ int find_instance_px(const int64_t* __restrict__ off, int ninst, int64_t g) {
     int lo = 0, hi = ninst - 1;   // last i with off[i] <= g
     while (lo < hi) {
@@ -794,6 +838,18 @@ cudaError_t gather_multi(const GatherInstDev* tab, const int64_t* px_off, int ni
 }
 
 int gather_class(int k) { return k <= 96 ? 0 : 1; }
+
+cudaError_t gather_listed(const GatherGrid& G, const GatherQueries& Q, const unsigned long long* n_dev,
+                          unsigned long long* queue, float r, int k, const GatherOut& O, int sm_count,
+                          cudaStream_t st) {
+    if (Q.n <= 0) return cudaSuccess;
+    if (!Q.idx || !Q.pos4 || !Q.nrm4) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(queue, 0, 8, st);
+    if (e != cudaSuccess) return e;
+    if (k <= 96) return launch_listed<256>(G, Q, n_dev, queue, r, k, O, sm_count, st);
+    if (k <= 256) return launch_listed<512>(G, Q, n_dev, queue, r, k, O, sm_count, st);
+    return cudaErrorInvalidValue;
+}
 
 cudaError_t gather(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full,
                    const GatherOut& O, unsigned* status, cudaStream_t st) {

@@ -39,6 +39,13 @@ struct GatherOut {
 
 // k <= 256.  require_full: the estimate is written only when k neighbours were
 // found (the caustic rule of CudaPhotonMapping/Raytracer.cuh:200), zero otherwise.
+// Queries listed in Q.idx (records in Q.pos4 / Q.nrm4, Q.n = list capacity),
+// as many as the device count *n_dev says; persistent launch over the
+// resident warps, *queue (device scratch) the work counter.
+cudaError_t gather_listed(const GatherGrid& G, const GatherQueries& Q, const unsigned long long* n_dev,
+                          unsigned long long* queue, float r, int k, const GatherOut& O, int sm_count,
+                          cudaStream_t st);
+
 cudaError_t gather(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full,
                    const GatherOut& O, unsigned* status, cudaStream_t st);
 

@@ -37,7 +37,7 @@ constexpr int TILE = 128;
 constexpr int THREADS = 128;
 constexpr int WAIT_LIMIT = 1 << 24;        // polls of an mbarrier before giving up
 constexpr uint32_t TMEM_COLS_TRAIN = 512;
-constexpr uint32_t TMEM_COLS_INFER = 64;
+constexpr uint32_t TMEM_COLS_INFER = 256;   // 64 per warpgroup
 
 // shared-memory carve-up (bytes)
 constexpr uint32_t W_BYTES = 4 * 8192 + 2048;       // layers 0-3: 64x64, layer 4: 16x64
@@ -46,9 +46,14 @@ constexpr uint32_t TRAIN_OFF_X = W_BYTES;                       // X_0 .. X_4
 constexpr uint32_t TRAIN_OFF_G = TRAIN_OFF_X + 5 * X_BYTES;     // two gradient tiles
 constexpr uint32_t TRAIN_OFF_BAR = TRAIN_OFF_G + 2 * X_BYTES;
 constexpr uint32_t TRAIN_SMEM = TRAIN_OFF_BAR + 64;
-constexpr uint32_t INFER_OFF_X = W_BYTES;                       // two activation tiles
-constexpr uint32_t INFER_OFF_BAR = INFER_OFF_X + 2 * X_BYTES;
-constexpr uint32_t INFER_SMEM = INFER_OFF_BAR + 64;
+// inference: INFER_GROUPS independent 128-row pipelines (one warpgroup each)
+// share the weights; each owns one activation tile (the layers run in place),
+// one mbarrier and 64 TMEM columns
+constexpr int INFER_GROUPS = 4;
+constexpr int INFER_THREADS = 128 * INFER_GROUPS;
+constexpr uint32_t INFER_OFF_X = W_BYTES;
+constexpr uint32_t INFER_OFF_BAR = INFER_OFF_X + INFER_GROUPS * X_BYTES;
+constexpr uint32_t INFER_SMEM = INFER_OFF_BAR + 8 * INFER_GROUPS + 16;
 
 __host__ __device__ constexpr uint32_t w_off(int l) { return (uint32_t)l * 8192u; }
 
@@ -100,6 +105,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// barrier `id` over the 128 threads of one warpgroup; true iff v on all of them
+__device__ __forceinline__ bool wg_sync_and(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r) : "r"((uint32_t)v), "r"(id) : "memory");
+    return r != 0;
+}
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {   // whole warp
     const uint32_t dst = (uint32_t)__cvta_generic_to_shared(slot);
@@ -135,7 +149,7 @@ __device__ __forceinline__ void unpack_bf16(uint32_t u, float& a, float& b) {
 // weights (global [layer][out][in] bf16) -> core-matrix layout
 __device__ void load_weights(const __nv_bfloat16* __restrict__ w, unsigned char* sW) {
     constexpr int CHUNKS = (4 * 64 + 16) * 8;   // 16-byte chunks
-    for (int q = threadIdx.x; q < CHUNKS; q += THREADS) {
+    for (int q = threadIdx.x; q < CHUNKS; q += blockDim.x) {
         const int row = q >> 3, j = q & 7;                  // global row over all layers, 8-column block
         const int l = row < 256 ? row >> 6 : 4;
         const int o = row < 256 ? row & 63 : row - 256;
@@ -163,6 +177,10 @@ __device__ __forceinline__ bool load_sample(const MlpInputs& in, int64_t i, V3& 
 // Encoding: u = (p - lo) * inv per axis, and the octahedral map of the normal
 // to [0, 1]^2; each of the 5 values s gives sin(pi F 2^f s), cos(pi F 2^f s)
 // for f = 0..5, F = freq0 (60 features, then 4 zeros).  Written as row `row` of an [128][64] tile.
+// Octave 0 comes from sincospif, each further octave from the double-angle
+// identities sin 2x = 2 sin x cos x, cos 2x = (cos x - sin x)(cos x + sin x):
+// the angle error doubles per octave, 2^5 x a few 1e-8 after five, far below
+// the BF16 rounding (2^-9 relative) the features then get.
 __device__ __forceinline__ void write_features(unsigned char* sX, int row, const MlpNet& net, V3 p, V3 n) {
     float s[5];
     s[0] = (p.x - net.lo[0]) * net.inv[0];
@@ -179,22 +197,28 @@ __device__ __forceinline__ void write_features(unsigned char* sX, int row, const
     }
     s[3] = 0.5f * ox + 0.5f;
     s[4] = 0.5f * oy + 0.5f;
-    uint32_t pk[32];
+    // word w = 6 j + f holds features 2w, 2w + 1; each 8-feature block goes
+    // to shared memory as soon as its four words exist
+    uint32_t pk[4];
 #pragma unroll
     for (int j = 0; j < 5; j++) {
+        float sn, cs;
+        sincospif(s[j] * net.freq0, &sn, &cs);
 #pragma unroll
         for (int f = 0; f < 6; f++) {
-            float sn, cs;
-            sincospif(s[j] * (net.freq0 * (float)(1 << f)), &sn, &cs);
-            pk[6 * j + f] = pack_bf16(sn, cs);
+            if (f > 0) {
+                const float s2 = 2.f * sn * cs;
+                const float c2 = (cs - sn) * (cs + sn);
+                sn = s2;
+                cs = c2;
+            }
+            const int w = 6 * j + f;
+            pk[w & 3] = pack_bf16(sn, cs);
+            if ((w & 3) == 3)
+                *reinterpret_cast<uint4*>(sX + cm_off(row, 2 * (w - 3), TILE)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         }
     }
-    pk[30] = 0u;
-    pk[31] = 0u;
-#pragma unroll
-    for (int c = 0; c < 8; c++)
-        *reinterpret_cast<uint4*>(sX + cm_off(row, 8 * c, TILE)) =
-            make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+    *reinterpret_cast<uint4*>(sX + cm_off(row, 56, TILE)) = make_uint4(pk[0], pk[1], 0u, 0u);
 }
 
 // forward product of layer l into TMEM columns [0, out)
@@ -269,20 +293,21 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
                 issue_forward(l, tm, sX_a + l * X_BYTES, sW_a + w_off(l));
                 umma_commit(bar);
             }
-            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            const bool done = mbar_wait(bar, phase);
             phase ^= 1u;
             tc_after();
-            if (!ok) break;
-            if (l < MLP_LAYERS - 1) {
-                relu_row_to_smem(tm + my_lanes, sX + (l + 1) * X_BYTES, tid);
-            } else {
-                float v[16];
-                tmem_ld16(tm + my_lanes, v);
-                y[0] = v[0]; y[1] = v[1]; y[2] = v[2];
+            if (done) {
+                if (l < MLP_LAYERS - 1) {
+                    relu_row_to_smem(tm + my_lanes, sX + (l + 1) * X_BYTES, tid);
+                } else {
+                    float v[16];
+                    tmem_ld16(tm + my_lanes, v);
+                    y[0] = v[0]; y[1] = v[1]; y[2] = v[2];
+                }
             }
             tc_before();
             fence_async_smem();
-            __syncthreads();
+            ok = __syncthreads_and(done) != 0;
             tc_after();
         }
         if (!ok) break;
@@ -315,11 +340,10 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
                 }
                 umma_commit(bar);
             }
-            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            const bool done = mbar_wait(bar, phase);
             phase ^= 1u;
             tc_after();
-            if (!ok) break;
-            if (l > 0) {
+            if (done && l > 0) {
                 // dY_{l-1} = dX * [X_l > 0], bf16, into the other gradient tile
                 unsigned char* xrow = sX + l * X_BYTES;
                 unsigned char* dst = sG + (cur ^ 1) * X_BYTES;
@@ -344,15 +368,17 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
             }
             tc_before();
             fence_async_smem();
-            __syncthreads();
+            ok = __syncthreads_and(done) != 0;
             tc_after();
+            if (!ok) break;
             cur ^= 1;
         }
+        if (!ok) break;
         any = true;
     }
     if (!ok) {
         if (tid == 0) raise_status(status, ST_TIMEOUT);
-        (void)mbar_wait(bar, phase);   // let a late product land before the columns are freed
+        (void)mbar_wait(bar, phase ^ 1u);   // let the late product land before the columns are freed
     } else if (any) {
         // weight gradients: lanes 0-15 of each warp hold rows 16 w + lane (input index)
         for (int l = 0; l < MLP_LAYERS; l++) {
@@ -377,76 +403,90 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
     if (warp == 0) tmem_dealloc(tm, TMEM_COLS_TRAIN);
 }
 
-__global__ void __launch_bounds__(THREADS)
+// Inference: warpgroup g of the CTA runs its own tiles (g + G * CTA, then
+// strided by G * grid) through the five layers; its 128 threads each own one
+// sample row (row = TMEM lane), thread 0 of the group issues the products.
+// Layer l's product reads the group's activation tile, and once its commit
+// has landed that tile is free, so the ReLU output of layer l overwrites it in
+// place.  The next tile's samples are loaded while the current one runs.
+__global__ void __launch_bounds__(INFER_THREADS, 2)
 k_mlp_infer(MlpNet net, MlpInputs in, float* __restrict__ out, unsigned* status) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = tid >> 7, row = tid & 127;
     unsigned char* sW = smem;
-    unsigned char* sX = smem + INFER_OFF_X;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + INFER_OFF_BAR);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + INFER_OFF_BAR + 8);
+    unsigned char* sX = smem + INFER_OFF_X + g * X_BYTES;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + INFER_OFF_BAR);
+    uint64_t* bar = bars + g;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + INFER_OFF_BAR + 8 * INFER_GROUPS);
     load_weights(net.w, sW);
-    if (tid == 0) mbar_init(bar);
+    if (tid < INFER_GROUPS) mbar_init(bars + tid);
     if (warp == 0) tmem_alloc(tslot, TMEM_COLS_INFER);
     fence_async_smem();
     tc_before();
     __syncthreads();
     tc_after();
-    const uint32_t tm = *tslot;
-    const uint32_t my_lanes = (uint32_t)(32 * warp) << 16;
+    const uint32_t tm = *tslot + 64u * (uint32_t)g;
+    const uint32_t my_lanes = (uint32_t)(32 * (warp & 3)) << 16;
     const uint32_t sW_a = (uint32_t)__cvta_generic_to_shared(sW);
     const uint32_t sX_a = (uint32_t)__cvta_generic_to_shared(sX);
+    const bool leader = row == 0;
+    const int bar_id = 1 + g;
     uint32_t phase = 0;
     bool ok = true;
     const int64_t tiles = (in.n + TILE - 1) / TILE;
-    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const int64_t i = tile * TILE + tid;
-        V3 p, n;
-        const bool use = load_sample(in, i, p, n);
-        write_features(sX, tid, net, p, n);
+    const int64_t stride = (int64_t)gridDim.x * INFER_GROUPS;
+    int64_t tile = (int64_t)blockIdx.x * INFER_GROUPS + g;
+    V3 p, n;
+    bool use = load_sample(in, tile * TILE + row, p, n);
+    for (; tile < tiles && ok; tile += stride) {
+        const int64_t i = tile * TILE + row;
+        write_features(sX, row, net, p, n);
+        const bool use_cur = use;
+        use = load_sample(in, (tile + stride) * TILE + row, p, n);   // next tile's sample, in flight
         fence_async_smem();
         tc_before();
-        __syncthreads();
+        wg_sync_and(bar_id, true);
         tc_after();
         float y[3] = {0.f, 0.f, 0.f};
         for (int l = 0; l < MLP_LAYERS && ok; l++) {
-            const int src = l & 1;
-            if (tid == 0) {
-                issue_forward(l, tm, sX_a + src * X_BYTES, sW_a + w_off(l));
+            if (leader) {
+                issue_forward(l, tm, sX_a, sW_a + w_off(l));
                 umma_commit(bar);
             }
-            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            const bool done = mbar_wait(bar, phase);
             phase ^= 1u;
             tc_after();
-            if (!ok) break;
-            if (l < MLP_LAYERS - 1) {
-                relu_row_to_smem(tm + my_lanes, sX + (src ^ 1) * X_BYTES, tid);
-            } else {
-                float v[16];
-                tmem_ld16(tm + my_lanes, v);
-                y[0] = v[0]; y[1] = v[1]; y[2] = v[2];
+            if (done) {
+                if (l < MLP_LAYERS - 1) {
+                    relu_row_to_smem(tm + my_lanes, sX, row);
+                } else {
+                    float v[16];
+                    tmem_ld16(tm + my_lanes, v);
+                    y[0] = v[0]; y[1] = v[1]; y[2] = v[2];
+                }
             }
             tc_before();
             fence_async_smem();
-            __syncthreads();
+            ok = wg_sync_and(bar_id, done);
             tc_after();
         }
         if (!ok) break;
         if (i < in.n) {
-            const float sc = use ? net.out_scale : 0.f;
+            const float sc = use_cur ? net.out_scale : 0.f;
             out[3 * i] = y[0] * sc;
             out[3 * i + 1] = y[1] * sc;
             out[3 * i + 2] = y[2] * sc;
         }
     }
     if (!ok) {
-        if (tid == 0) raise_status(status, ST_TIMEOUT);
-        (void)mbar_wait(bar, phase);
+        if (leader) raise_status(status, ST_TIMEOUT);
+        (void)mbar_wait(bar, phase ^ 1u);   // let the late product land before the columns are freed
     }
     tc_before();
     __syncthreads();
     tc_after();
-    if (warp == 0) tmem_dealloc(tm, TMEM_COLS_INFER);
+    if (warp == 0) tmem_dealloc(*tslot, TMEM_COLS_INFER);
 }
 
 __global__ void k_adam(float* __restrict__ w32, __nv_bfloat16* __restrict__ w16, float* __restrict__ grad,
@@ -490,12 +530,13 @@ cudaError_t mlp_infer(const MlpNet& net, const MlpInputs& in, float* out, unsign
     cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INFER_SMEM);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer, THREADS, INFER_SMEM)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer, INFER_THREADS, INFER_SMEM)) != cudaSuccess)
         return e;
     per_sm = std::min(std::max(per_sm, 1), 512 / (int)TMEM_COLS_INFER);
     const int64_t tiles = (in.n + TILE - 1) / TILE;
-    const int grid = (int)std::min<int64_t>(tiles, (int64_t)per_sm * std::max(sm_count, 1));
-    k_mlp_infer<<<grid, THREADS, INFER_SMEM, st>>>(net, in, out, status);
+    const int64_t ctas = (tiles + INFER_GROUPS - 1) / INFER_GROUPS;
+    const int grid = (int)std::min<int64_t>(ctas, (int64_t)per_sm * std::max(sm_count, 1));
+    k_mlp_infer<<<grid, INFER_THREADS, INFER_SMEM, st>>>(net, in, out, status);
     return cudaGetLastError();
 }
 

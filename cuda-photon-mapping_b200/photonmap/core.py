@@ -348,15 +348,16 @@ class Context:
                                                pos.shape[0], C.byref(loss)), "pm_cache_train_step")
         return loss.value
 
-    def cache_train_steps(self, pos, nrm, target, steps, batch, offset=0, weight=None):
+    def cache_train_steps(self, pos, nrm, target, steps, batch, offset=0, weight=None, want_loss=True):
         """`steps` Adam steps over consecutive `batch`-sample slices of the pool from
-        `offset` (wrapping); returns (last step's loss, next offset)."""
+        `offset` (wrapping); returns (last step's loss, next offset).  With
+        want_loss=False the steps are only queued (loss nan, no host wait)."""
         pos, nrm, target, weight = self._samples(pos, nrm, target, weight)
         loss = C.c_float(float("nan"))
         off = C.c_int64(int(offset))
         self._check(self.L.pm_cache_train_steps(self.h, _ptr(pos), _ptr(nrm), _ptr(target), _ptr(weight),
                                                 pos.shape[0], int(batch), int(steps), C.byref(off),
-                                                C.byref(loss)), "pm_cache_train_steps")
+                                                C.byref(loss) if want_loss else None), "pm_cache_train_steps")
         return loss.value, off.value
 
     def cache_gradient(self, pos, nrm, target, weight=None):

@@ -39,9 +39,11 @@ def training_pool(ctx, cam, k, radius, n=1 << 20, seed=1, map_id=0) -> Pool:
     return Pool(pos, nrm, target, scale if scale > 0 else 1.0)
 
 
-def cache_fit(ctx, pool: Pool, steps, batch=65536, offset=0):
+def cache_fit(ctx, pool: Pool, steps, batch=65536, offset=0, want_loss=True):
     """Runs `steps` Adam steps over consecutive batches of the (shuffled) pool,
-    starting at `offset`; returns (last loss, next offset)."""
+    starting at `offset`; returns (last loss, next offset).  want_loss=False
+    queues the steps without waiting for them (loss nan)."""
     if int(steps) <= 0:
         return float("nan"), offset
-    return ctx.cache_train_steps(pool.pos, pool.nrm, pool.target, int(steps), int(batch), offset)
+    return ctx.cache_train_steps(pool.pos, pool.nrm, pool.target, int(steps), int(batch), offset,
+                                 want_loss=want_loss)

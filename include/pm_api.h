@@ -239,9 +239,12 @@ int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const f
 
 /* `steps` Adam steps over consecutive batches of `batch` samples of the n-sample
  * pool, starting at *inout_offset (null: 0) and wrapping to 0 where a batch
- * would run past n; *inout_offset receives the next offset.  One status check
- * for the whole run (no host synchronisation between steps); *out_loss
- * (optional) = the last step's loss as pm_cache_train_step reports it. */
+ * would run past n; *inout_offset receives the next offset.  No host
+ * synchronisation between steps.  With out_loss set, the call waits for the
+ * steps, checks their device status and stores the last step's loss (as
+ * pm_cache_train_step reports it); with out_loss null it returns once the
+ * steps are queued on the context's stream, and a device-side failure of
+ * theirs is reported by the next synchronising call on the context. */
 int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
                          int64_t n, int64_t batch, int steps, int64_t* inout_offset, float* out_loss);
 

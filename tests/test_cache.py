@@ -121,3 +121,26 @@ def test_cache_training_reduces_loss(ctx):
     # the trained weights are what the library reports
     w = ctx.cache_params()
     assert np.isfinite(w).all() and np.abs(w).max() > 0
+
+
+@pytest.mark.gpu
+def test_train_steps_match_single_steps(ctx):
+    # the multi-step entry point walks the pool like repeated single steps (wrapping at the end)
+    n, b, steps = 50000, 16384, 5
+    pos, nrm, tgt = _samples(n, 31)
+    ctx.cache_init(seed=2, lr=1e-3, out_scale=1.0, aabb=BOX)
+    off = 0
+    for _ in range(steps):
+        if off + b > n:
+            off = 0
+        ctx.cache_train_step(pos[off:off + b], nrm[off:off + b], tgt[off:off + b])
+        off += b
+    w_single = ctx.cache_params()
+    ctx.cache_init(seed=2, lr=1e-3, out_scale=1.0, aabb=BOX)
+    loss, off2 = ctx.cache_train_steps(pos, nrm, tgt, steps, b, 0, want_loss=False)
+    w_multi = ctx.cache_params()
+    assert off2 == off and np.isnan(loss)
+    # gradient sums are atomics in arbitrary order: equal up to FP32 reassociation
+    np.testing.assert_allclose(w_multi, w_single, rtol=0, atol=2e-5)
+    loss, _ = ctx.cache_train_steps(pos, nrm, tgt, 1, b, off2)
+    assert np.isfinite(loss) and loss > 0
