@@ -316,7 +316,7 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     import torch
     import torch.distributed as dist
     from photonmap import learned
-    TRAIN_PER_FRAME, BATCH, WARM_STEPS, THR = 1 << 18, 1 << 16, 3000, 0.05
+    TRAIN_PER_FRAME, BATCH, WARM_STEPS = 1 << 18, 1 << 16, 3000
     pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=1 << 20, seed=1)
     ctx.cache_init(seed=0, lr=3e-3, out_scale=pool.scale)
     learned.cache_fit(ctx, pool, WARM_STEPS, batch=BATCH)
@@ -331,8 +331,8 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     def learned_frame():
         _, off[0] = learned.cache_fit(ctx, pool, TRAIN_PER_FRAME // BATCH, batch=BATCH, offset=off[0],
                                       want_loss=False)
-        _, _, st = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], max_rel_err=THR, radiance=False,
-                                      out_rgb8=rgb)
+        _, _, st = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb,
+                                      **learned.FRAME_SETTINGS)
         stats.update(st)
 
     def timed(fn):
@@ -375,7 +375,7 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     return {"ms_per_frame_plain": ms_plain, "ms_per_frame_learned": ms_learned, "speedup": ms_plain / ms_learned,
             "frame": "eye pass + global estimate + resolve, photon map resident",
             "train_samples_per_frame": TRAIN_PER_FRAME, "pool": pool.n, "warmup_steps": WARM_STEPS,
-            "max_rel_err": THR, "fallback_tiles_frac": stats["fallback_tiles"] / max(stats["tiles"], 1),
+            "check": dict(learned.FRAME_SETTINGS), "fallback_tiles_frac": stats["fallback_tiles"] / max(stats["tiles"], 1),
             "fallback_requests_frac": stats["fallback_requests"] / max(stats["requests"], 1),
             "mlp": {"infer_tflops": inf_tf, "train_tflops": tr_tf, "peak_bf16_tflops": peak,
                     "infer_frac": inf_tf / peak, "train_frac": tr_tf / peak, "unit": "TFLOP/s",

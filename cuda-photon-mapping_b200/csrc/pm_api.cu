@@ -1002,8 +1002,9 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
                       uint8_t* out_rgb8, float* out_radiance, pm_learned_stats* out_stats) {
     if (!ctx || !cam || !o || !lo || !out_rgb8) return PM_ERR_INVALID;
     if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
-    if (lo->tile < 1 || lo->tile > 256 || lo->probes < 1 || lo->probes > 64 || lo->max_rel_err != lo->max_rel_err)
-        return fail(ctx, PM_ERR_INVALID, "learned options: tile 1..256, probes 1..64, max_rel_err not NaN");
+    if (lo->tile < 1 || lo->tile > 256 || lo->probes < 1 || lo->probes > 64 || lo->max_rel_err != lo->max_rel_err ||
+        !(lo->noise_z >= 0.f && lo->noise_z <= 100.f))
+        return fail(ctx, PM_ERR_INVALID, "learned options: tile 1..256, probes 1..64, max_rel_err not NaN, noise_z 0..100");
     if (int rc = render_checks(ctx, cam, o)) return rc;
     CK(cudaSetDevice(ctx->device));
     FrameSetup F;
@@ -1035,7 +1036,7 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     CK(gather(grid_of(G, G), PQ, o->r_global, o->k_global, 0, PO, P<unsigned>(ctx->status), ctx->st));
     CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 32, ctx->st));
     CK(learned_select(F.cd, F.R, F.nreq, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
-                      P<float>(ctx->est_mlp), lo->max_rel_err, P<uint8_t>(ctx->tile_flag),
+                      P<float>(ctx->est_mlp), lo->max_rel_err, lo->noise_z, P<uint8_t>(ctx->tile_flag),
                       P<unsigned long long>(ctx->learned_counts), P<uint32_t>(ctx->fallback_list), ctx->st));
     // the exact gather for the listed fallback requests only (count read on the device)
     GatherQueries Q{};

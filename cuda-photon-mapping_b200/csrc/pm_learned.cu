@@ -55,26 +55,37 @@ __global__ void k_probe_select(CameraDev cam, Requests R, int tile, int P, int t
 // flagged when above the threshold (a negative threshold flags every tile:
 // the exact render).  The exact probe estimates carry the kNN estimate's own
 // noise (about 1 / sqrt(k) relative); summing signed differences over the
-// probes averages it down, while a systematic cache error stays.
+// probes averages it down, while a systematic cache error stays.  With
+// noise_z > 0 the tile must exceed the threshold by noise_z standard errors of
+// that sum as well (per channel sqrt(n) x the sample standard deviation of the
+// n differences), so that probe noise alone does not flag it.
 __global__ void k_tile_flags(int64_t ntiles, int P, const uint32_t* __restrict__ preq, const float* __restrict__ exact,
-                             const float* __restrict__ cached, float max_rel_err, uint8_t* __restrict__ flag,
-                             unsigned long long* __restrict__ nflag) {
+                             const float* __restrict__ cached, float max_rel_err, float noise_z,
+                             uint8_t* __restrict__ flag, unsigned long long* __restrict__ nflag) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
-    V3 bias = v3(0.f, 0.f, 0.f), ref = v3(0.f, 0.f, 0.f);
+    V3 bias = v3(0.f, 0.f, 0.f), sq = v3(0.f, 0.f, 0.f), ref = v3(0.f, 0.f, 0.f);
     int cnt = 0;
     for (int k = 0; k < P; k++) {
         const int64_t s = t * P + k;
         const uint32_t q = preq[s];
         if (q == 0xffffffffu) continue;
         const V3 e = ld3(exact + 3 * s), c = ld3(cached + 3 * (size_t)q);
-        bias = vadd(bias, vsub(c, e));
+        const V3 d = vsub(c, e);
+        bias = vadd(bias, d);
+        sq = vadd(sq, vmul(d, d));
         ref = vadd(ref, e);
         cnt++;
     }
     const float num = fabsf(bias.x) + fabsf(bias.y) + fabsf(bias.z);
     const float den = fabsf(ref.x) + fabsf(ref.y) + fabsf(ref.z);
-    const bool f = max_rel_err < 0.f || (cnt > 0 && num > max_rel_err * den);
+    float se = 0.f;
+    if (noise_z > 0.f && cnt > 1) {
+        const float n = (float)cnt, m = n / (n - 1.f);
+        se = sqrtf(fmaxf(m * (sq.x - bias.x * bias.x / n), 0.f)) + sqrtf(fmaxf(m * (sq.y - bias.y * bias.y / n), 0.f)) +
+             sqrtf(fmaxf(m * (sq.z - bias.z * bias.z / n), 0.f));
+    }
+    const bool f = max_rel_err < 0.f || (cnt > 0 && num > max_rel_err * den + noise_z * se);
     flag[t] = f ? 1 : 0;
     if (f) atomicAdd(nflag, 1ull);
 }
@@ -131,11 +142,11 @@ cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, in
 }
 
 cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
-                           const float* probe_exact, const float* cached, float max_rel_err, uint8_t* tile_flag,
-                           unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st) {
+                           const float* probe_exact, const float* cached, float max_rel_err, float noise_z,
+                           uint8_t* tile_flag, unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st) {
     const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
     const int64_t ntiles = (int64_t)tx * ty;
-    k_tile_flags<<<blocks(ntiles, 256), 256, 0, st>>>(ntiles, P, preq, probe_exact, cached, max_rel_err, tile_flag,
+    k_tile_flags<<<blocks(ntiles, 256), 256, 0, st>>>(ntiles, P, preq, probe_exact, cached, max_rel_err, noise_z, tile_flag,
                                                       counts);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || nreq <= 0) return e;

@@ -14,13 +14,14 @@ constexpr uint32_t LEARNED_FALLBACK = 4u;   // request flag: answered by the exa
 cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, int P, float4* ppos, float4* pnrm,
                            uint32_t* preq, cudaStream_t st);
 
-// Tile flags from the probes' exact and cached estimates, then flag bit
+// Tile flags from the probes' exact and cached estimates (bias above
+// max_rel_err plus noise_z standard errors), then flag bit
 // LEARNED_FALLBACK on every global request of a flagged tile, whose index also
 // goes to fallback_list (nreq entries of room, any order).
 // counts[0] += flagged tiles, counts[1] += fallback requests (= list length).
 cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
-                           const float* probe_exact, const float* cached, float max_rel_err, uint8_t* tile_flag,
-                           unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st);
+                           const float* probe_exact, const float* cached, float max_rel_err, float noise_z,
+                           uint8_t* tile_flag, unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st);
 
 // est = exact estimate for fallback requests, the cache's otherwise
 cudaError_t learned_merge(const Requests& R, int64_t nreq, const float* cached, const float* exact, float* est,

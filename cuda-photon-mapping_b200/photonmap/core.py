@@ -91,7 +91,7 @@ class _BatchInfo(C.Structure):
 
 
 class _LearnedOpts(C.Structure):
-    _fields_ = [("tile", C.c_int32), ("probes", C.c_int32), ("max_rel_err", C.c_float)]
+    _fields_ = [("tile", C.c_int32), ("probes", C.c_int32), ("max_rel_err", C.c_float), ("noise_z", C.c_float)]
 
 
 class _LearnedStats(C.Structure):
@@ -396,7 +396,7 @@ class Context:
 
     def render_learned(self, cam: Camera, k_global, r_global, max_depth=4, tile=16, probes=16, max_rel_err=0.05,
                        k_caustic=0, r_caustic=0.2, faithful_caustic=True, radiance=True, out_rgb8=None,
-                       out_radiance=None):
+                       out_radiance=None, noise_z=0.0):
         torch = self.torch
         W, H = cam.width, cam.height
         rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
@@ -404,7 +404,7 @@ class Context:
         if rad is None and radiance:
             rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
         o = _RenderOpts(max_depth, k_global, r_global, k_caustic, r_caustic, int(faithful_caustic))
-        lo = _LearnedOpts(int(tile), int(probes), float(max_rel_err))
+        lo = _LearnedOpts(int(tile), int(probes), float(max_rel_err), float(noise_z))
         st = _LearnedStats()
         self._check(self.L.pm_render_learned(self.h, C.byref(cam), C.byref(o), C.byref(lo), _ptr(rgb), _ptr(rad),
                                              C.byref(st)), "pm_render_learned")

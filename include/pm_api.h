@@ -270,6 +270,10 @@ typedef struct pm_learned_opts {
     float max_rel_err;      /* a tile whose cache bias over its probes, sum_c |sum_k (cache - exact)| /
                                sum_c sum_k exact, exceeds this uses the exact gather;
                                negative: every tile does (the plain render's estimates) */
+    float noise_z;          /* 0..100: the bias must also exceed the threshold by noise_z standard
+                               errors of the probe differences' sum (sum_c sqrt(n) s_c, s_c the
+                               sample standard deviation over the n probes), so that the exact
+                               probes' own kNN noise does not flag a tile; 0: threshold only */
 } pm_learned_opts;
 
 typedef struct pm_learned_stats {
