@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache frame comparison")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched workload")
     ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--bvh", default="host_sah", choices=["host_sah", "device_lbvh"],
+                    help="BVH builder of the scene (same photons and image either way)")
     # size overrides (profiling captures run reduced cases of the same workload)
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--width", type=int, default=0)
@@ -403,7 +405,9 @@ def run_ours(args):
     sc, cs, w = scenes.workload(args.workload)
     w, cs = override(w, cs, args)
     ctx = photonmap.Context(local)
+    ctx.set_bvh_builder(args.bvh)
     ctx.set_scene(sc)
+    bvh = ctx.bvh_info()
     cam = photonmap.camera_setup(cs.position, cs.direction, cs.up, cs.fov_deg, cs.width, cs.height)
     W, H = cs.width, cs.height
     rgb = torch.empty(W * H * 3, dtype=torch.uint8, device="cuda")
@@ -480,7 +484,7 @@ def run_ours(args):
             "data": "synthetic (seeded procedural scene, seeded Philox photon streams)",
             "config": {"workload": args.workload, "photons": w["photons"], "max_bounces": w["max_bounces"],
                        "image": f"{W}x{H}", "k": w["k"], "radius": w["radius"], "eye_depth": w["max_depth"],
-                       "triangles": sc.ntri, "l2": "inputs larger than L2 (photon map ~0.5 GB)",
+                       "triangles": sc.ntri, "bvh": bvh, "l2": "inputs larger than L2 (photon map ~0.5 GB)",
                        "parallelism": f"replicas{world}"},
             "stages_ms": {"trace": stages[0], "grid": stages[1], "eye": stages[2], "gather": stages[3],
                           "resolve": stages[4]},

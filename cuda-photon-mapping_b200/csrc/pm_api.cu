@@ -1,6 +1,7 @@
 // pm_api.cu -- context, device memory and the C ABI of include/pm_api.h.
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -11,6 +12,7 @@
 #include "pm_device.cuh"
 #include "pm_gather.cuh"
 #include "pm_grid.cuh"
+#include "pm_lbvh.cuh"
 #include "pm_learned.cuh"
 #include "pm_mlp.cuh"
 #include "pm_render.cuh"
@@ -169,7 +171,8 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws, &ctx->cache_w32,
                       &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
                       &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
-                      &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list};
+                      &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list,
+                      &ctx->bvh_scratch};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -484,23 +487,47 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
         add_angle(ca, sd->materials[12 * i + 9], sd->default_ior);
     }
     float ext = std::max(std::max(aabb[3] - aabb[0], aabb[4] - aabb[1]), aabb[5] - aabb[2]);
+    const float bvh_pad = 1e-4f * std::max(ext, 1.0f);
+    const bool device_bvh = ctx->bvh_builder == PM_BVH_DEVICE_LBVH;
+    if (device_bvh && T >= (1 << 23)) return fail(ctx, PM_ERR_INVALID, "device BVH builder: fewer than 2^23 triangles");
     std::vector<float> nodes;
     std::vector<int> prim;
-    build_bvh(sd->tri_pos, T, 1e-4f * std::max(ext, 1.0f), nodes, prim);
+    if (!device_bvh) {
+        const auto t0 = std::chrono::steady_clock::now();
+        build_bvh(sd->tri_pos, T, bvh_pad, nodes, prim);
+        ctx->bvh_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        ctx->bvh_nodes = (int64_t)(nodes.size() / 16);
+    } else {
+        ctx->bvh_nodes = lbvh_node_count(T);
+    }
 
     ENSURE(ctx->tri, rec.size() * 4);
     ENSURE(ctx->tri_pos, 9 * (size_t)T * 4);
     ENSURE(ctx->tri_nrm, 9 * (size_t)T * 4);
-    ENSURE(ctx->nodes, nodes.size() * 4);
-    ENSURE(ctx->prim, prim.size() * 4);
+    ENSURE(ctx->nodes, (size_t)ctx->bvh_nodes * 64);
+    ENSURE(ctx->prim, (size_t)T * 4);
     ENSURE(ctx->maabb, maabb.size() * 4);
     ENSURE(ctx->mats, 12 * (size_t)M * 4);
     ENSURE(ctx->ca, std::max<size_t>(ca.size(), 3) * 4);
     CK(cudaMemcpyAsync(ctx->tri.p, rec.data(), rec.size() * 4, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->tri_pos.p, sd->tri_pos, 9 * (size_t)T * 4, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->tri_nrm.p, sd->tri_nrm, 9 * (size_t)T * 4, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->nodes.p, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->prim.p, prim.data(), prim.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    if (!device_bvh) {
+        CK(cudaMemcpyAsync(ctx->nodes.p, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->prim.p, prim.data(), prim.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+    } else {
+        ENSURE(ctx->bvh_scratch, lbvh_scratch_bytes(T));
+        int launches = 0;
+        CK(cudaEventRecord(ctx->ev[9], ctx->st));
+        CK(lbvh_build(P<float>(ctx->tri_pos), T, bvh_pad, P<float4>(ctx->nodes), P<int>(ctx->prim), ctx->bvh_scratch.p,
+                      P<unsigned>(ctx->status), &launches, ctx->st));
+        CK(cudaEventRecord(ctx->ev[10], ctx->st));
+        CK(cudaEventSynchronize(ctx->ev[10]));
+        ctx->bvh_ms = elapsed(ctx->ev[9], ctx->ev[10]);
+        ctx->launches += launches;
+        release(ctx->bvh_scratch);
+        if (int rc = check_status(ctx, "device BVH build")) return rc;
+    }
     CK(cudaMemcpyAsync(ctx->maabb.p, maabb.data(), maabb.size() * 4, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->mats.p, sd->materials, 12 * (size_t)M * 4, cudaMemcpyHostToDevice, ctx->st));
     if (!ca.empty()) CK(cudaMemcpyAsync(ctx->ca.p, ca.data(), ca.size() * 4, cudaMemcpyHostToDevice, ctx->st));
@@ -520,9 +547,27 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
     ctx->default_ior = sd->default_ior;
     std::memcpy(ctx->aabb, aabb, sizeof aabb);
     ctx->has_scene = true;
+    ctx->scene_bvh_builder = device_bvh ? PM_BVH_DEVICE_LBVH : PM_BVH_HOST_SAH;
     ctx->yield_g = ctx->yield_c = 0.0;
     ctx->yield_bounces = 0;
     for (auto& m : ctx->maps) { m.built = false; m.n = 0; }
+    return PM_OK;
+}
+
+int pm_set_bvh_builder(pm_ctx* ctx, int builder) {
+    if (!ctx) return PM_ERR_INVALID;
+    if (builder != PM_BVH_HOST_SAH && builder != PM_BVH_DEVICE_LBVH)
+        return fail(ctx, PM_ERR_INVALID, "bvh builder: PM_BVH_HOST_SAH or PM_BVH_DEVICE_LBVH");
+    ctx->bvh_builder = builder;
+    return PM_OK;
+}
+
+int pm_bvh_info(pm_ctx* ctx, int32_t* out_builder, int64_t* out_nodes, float* out_build_ms) {
+    if (!ctx) return PM_ERR_INVALID;
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
+    if (out_builder) *out_builder = ctx->scene_bvh_builder;
+    if (out_nodes) *out_nodes = ctx->bvh_nodes;
+    if (out_build_ms) *out_build_ms = ctx->bvh_ms;
     return PM_OK;
 }
 

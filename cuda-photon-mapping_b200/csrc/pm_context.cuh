@@ -54,6 +54,11 @@ struct pm_ctx {
     // learned radiance cache
     bool has_cache = false;
     pm::DevBuf cache_w32, cache_w16, cache_m, cache_v, cache_grad, cache_loss;
+    // BVH: builder for the next pm_set_scene; the current scene's builder, size, build time
+    int bvh_builder = 0, scene_bvh_builder = 0;
+    int64_t bvh_nodes = 0;
+    float bvh_ms = 0.f;
+    pm::DevBuf bvh_scratch;
     pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts, fallback_list;
     pm_cache_opts cache_opts = {};
     float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};

@@ -470,25 +470,29 @@ cudaError_t grid_sort(GridBuffers& B, const float aabb[6], GridPlan& plan, int S
     return e;
 }
 
-// LSD radix sort of B.cid (keys < key_space, stable), carrying the photon
-// index; digits of equal width <= 9 bits; then the sorted records.
-cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* launches, cudaStream_t st) {
+size_t radix_hist_elems(int64_t n) {
+    return (size_t)RADIX_MAX_BINS * (size_t)std::max<int64_t>(1, (n + RADIX_TILE - 1) / RADIX_TILE);
+}
+
+// Stable LSD radix sort of n keys below 2^key_bits, digits of equal width <= 9 bits.
+cudaError_t radix_sort_u32(const RadixBuffers& B, const uint32_t* keys_in, const uint32_t* vals_in, int64_t n,
+                           int key_bits, bool want_keys, const uint32_t** keys_sorted, const uint32_t** vals_sorted,
+                           int* launches, cudaStream_t st) {
     cudaError_t e;
-    int bits = 1;
-    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)key_space) bits++;
+    const int bits = std::min(std::max(key_bits, 1), 32);
     const int passes = (bits + RADIX_MAX_BITS - 1) / RADIX_MAX_BITS;
     const int width = (bits + passes - 1) / passes;
     const int tiles = (int)((n + RADIX_TILE - 1) / RADIX_TILE);
     const int64_t hist_n = ((int64_t)1 << width) * tiles;
-    const uint32_t* kin = B.cid;
-    const uint32_t* vin = nullptr;
+    const uint32_t* kin = keys_in;
+    const uint32_t* vin = vals_in;
     if ((e = cudaFuncSetAttribute(k_radix_downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RadixSmem))) !=
         cudaSuccess)
         return e;
     for (int p = 0; p < passes; p++) {
         const int shift = width * p;
         const bool last = p == passes - 1;
-        uint32_t* kout = last ? nullptr : B.keys[p & 1];
+        uint32_t* kout = (last && !want_keys) ? nullptr : B.keys[p & 1];
         uint32_t* vout = B.vals[p & 1];
         k_radix_upsweep<<<tiles, RADIX_THREADS, 0, st>>>(kin, n, shift, width, B.hist, tiles);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -499,8 +503,23 @@ cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* 
         kin = kout;
         vin = vout;
     }
-    k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(vin, n, B.pos, B.dir, B.pow, B.gpos, B.gdir, B.gpow, B.status);
-    *launches += 3 * passes + 1;
+    if (keys_sorted) *keys_sorted = kin;
+    if (vals_sorted) *vals_sorted = vin;
+    *launches += 3 * passes;
+    return cudaSuccess;
+}
+
+// LSD radix sort of B.cid (keys < key_space, stable), carrying the photon
+// index; then the sorted records.
+cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* launches, cudaStream_t st) {
+    int bits = 1;
+    while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)key_space) bits++;
+    RadixBuffers RB{{B.keys[0], B.keys[1]}, {B.vals[0], B.vals[1]}, B.hist, B.scan_ws, B.status};
+    const uint32_t* order = nullptr;
+    cudaError_t e = radix_sort_u32(RB, B.cid, nullptr, n, bits, false, nullptr, &order, launches, st);
+    if (e != cudaSuccess) return e;
+    k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(order, n, B.pos, B.dir, B.pow, B.gpos, B.gdir, B.gpow, B.status);
+    *launches += 1;
     return cudaGetLastError();
 }
 

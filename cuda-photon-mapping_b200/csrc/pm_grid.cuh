@@ -80,6 +80,23 @@ struct GridMulti {
 cudaError_t grid_multi(GridBuffers& B, const GridMulti& M, int* launches, cudaStream_t st);
 cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* launches, cudaStream_t st);
 
+// Scratch of a stand-alone radix sort: keys / vals ping-pong buffers (n each),
+// hist (radix_hist_elems(n)), scan workspace (scan_workspace_bytes(hist elems)).
+struct RadixBuffers {
+    uint32_t* keys[2];
+    uint32_t* vals[2];
+    uint32_t* hist;
+    void* scan_ws;
+    unsigned* status;
+};
+size_t radix_hist_elems(int64_t n);
+// Stable LSD radix sort of n keys below 2^key_bits carrying values (vals_in
+// null: the input index).  *vals_sorted (and *keys_sorted when want_keys)
+// point into B's buffers.
+cudaError_t radix_sort_u32(const RadixBuffers& B, const uint32_t* keys_in, const uint32_t* vals_in, int64_t n,
+                           int key_bits, bool want_keys, const uint32_t** keys_sorted, const uint32_t** vals_sorted,
+                           int* launches, cudaStream_t st);
+
 // sub-cell division for a grid whose fullest cell holds max_count photons:
 // about 2k photons per sub-cell slab of a surface crossing the cell
 int grid_auto_subdiv(uint32_t max_count, int k_hint);

@@ -150,6 +150,8 @@ def library():
         "pm_cache_init": ([vp, C.POINTER(_CacheOpts)], C.c_int),
         "pm_cache_train_step": ([vp, vp, vp, vp, vp, i64, vp], C.c_int),
         "pm_cache_train_steps": ([vp, vp, vp, vp, vp, i64, i64, C.c_int, vp, vp], C.c_int),
+        "pm_set_bvh_builder": ([vp, C.c_int], C.c_int),
+        "pm_bvh_info": ([vp, vp, vp, vp], C.c_int),
         "pm_cache_gradient": ([vp, vp, vp, vp, vp, i64, vp, vp], C.c_int),
         "pm_cache_infer": ([vp, vp, vp, i64, vp], C.c_int),
         "pm_cache_get_params": ([vp, vp], C.c_int),
@@ -235,6 +237,16 @@ class Context:
             raise PMError(rc, f"{what}: {self.L.pm_last_error(self.h).decode()}")
 
     # ------------------------------------------------------------ scene
+    def set_bvh_builder(self, builder):
+        """'host_sah' (default) or 'device_lbvh': the BVH builder of the next set_scene."""
+        code = {"host_sah": 0, "device_lbvh": 1}[builder]
+        self._check(self.L.pm_set_bvh_builder(self.h, code), "pm_set_bvh_builder")
+
+    def bvh_info(self):
+        b, n, ms = C.c_int32(), C.c_int64(), C.c_float()
+        self._check(self.L.pm_bvh_info(self.h, C.byref(b), C.byref(n), C.byref(ms)), "pm_bvh_info")
+        return dict(builder=("host_sah", "device_lbvh")[b.value], nodes=n.value, build_ms=ms.value)
+
     def set_scene(self, sc):
         d, _keep = _scene_desc(sc)
         self._check(self.L.pm_set_scene(self.h, C.byref(d)), "pm_set_scene")

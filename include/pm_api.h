@@ -131,6 +131,14 @@ int pm_sync(pm_ctx* ctx);
 int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* scene);
 int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]);
 
+/* BVH builder used by the next pm_set_scene (the closest-hit answers, and so
+ * every photon map and image, are the same with either; only speed differs). */
+#define PM_BVH_HOST_SAH 0     /* binned SAH on the host (default): the faster tree to trace */
+#define PM_BVH_DEVICE_LBVH 1  /* linear BVH over Morton codes, built on the device in ~1 ms */
+int pm_set_bvh_builder(pm_ctx* ctx, int builder);
+/* The current scene's BVH: its builder, interior nodes, build time in ms. */
+int pm_bvh_info(pm_ctx* ctx, int32_t* out_builder, int64_t* out_nodes, float* out_build_ms);
+
 /* Photon pass.  Replaces trace_photons(gpu_scene, cpu_scene, diffuse_num,
  * specular_num) (PhotonTracing.cu:379-422): fills both maps' photon lists to
  * capacity in canonical order (path index, then bounce). out_paths (optional)

@@ -118,6 +118,37 @@ def test_trace_paths_heightfield_subset(ctx, orc):
     assert np.array_equal(_np(out["c_pos"]), ref["c_pos"])
 
 
+@pytest.mark.parametrize("which", ["cornell_small", "heightfield", "cornell_stress_4k"])
+def test_device_bvh_gives_the_same_photons_and_image(ctx, which):
+    """The device LBVH and the host SAH tree answer every closest-hit query the
+    same (smallest (t, triangle index)), so the photon lists, the caustic map
+    and the image are bit-identical; only the tree (and its speed) differs."""
+    import photonmap
+    if which == "heightfield":
+        sc = scenes.cornell(sphere_level=3, heightfield_n=256, seed=0)
+    else:
+        sc = scenes.workload(which)[0]
+    cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, 160, 90)
+    out = {}
+    for builder in ("host_sah", "device_lbvh"):
+        ctx.set_bvh_builder(builder)
+        ctx.set_scene(sc)
+        info = ctx.bvh_info()
+        assert info["builder"] == builder and info["nodes"] >= 1 and info["build_ms"] >= 0.0
+        ctx.trace_photons(3, 12, 40_000, 8_000)
+        g = ctx.photons(0, sorted_=False)
+        c = ctx.photons(1, sorted_=False)
+        ctx.build_grid(0)
+        ctx.build_grid(1)
+        rgb, rad = ctx.render(cam, 64, 0.1, 4, k_caustic=32, r_caustic=0.1)
+        out[builder] = [_np(t) for t in (g["list_pos"], g["list_dir"], g["list_power"], c["list_pos"],
+                                         c["list_dir"], rgb, rad)]
+        assert ctx.status() == 0
+    ctx.set_bvh_builder("host_sah")
+    for a, b in zip(out["host_sah"], out["device_lbvh"]):
+        assert np.array_equal(a, b)
+
+
 def test_heightfield_render_matches_oracle(ctx, orc):
     # eye rays through the BVH of the 130k-triangle scene, small photon map
     sc = scenes.cornell(sphere_level=3, heightfield_n=256, seed=0)
