@@ -151,6 +151,12 @@ def library():
         "pm_cache_train_step": ([vp, vp, vp, vp, vp, i64, vp], C.c_int),
         "pm_cache_train_steps": ([vp, vp, vp, vp, vp, i64, i64, C.c_int, vp, vp], C.c_int),
         "pm_set_bvh_builder": ([vp, C.c_int], C.c_int),
+        "pm_obj_load": ([C.c_char_p, C.c_char_p, vp, C.c_char_p, C.c_int], C.c_int),
+        "pm_obj_desc": ([vp, C.c_float, vp], C.c_int),
+        "pm_obj_model_count": ([vp], C.c_int32),
+        "pm_obj_model_name": ([vp, C.c_int32], C.c_char_p),
+        "pm_obj_light_model": ([vp], C.c_int32),
+        "pm_obj_free": ([vp], None),
         "pm_bvh_info": ([vp, vp, vp, vp], C.c_int),
         "pm_cache_gradient": ([vp, vp, vp, vp, vp, i64, vp, vp], C.c_int),
         "pm_cache_infer": ([vp, vp, vp, i64, vp], C.c_int),
@@ -172,6 +178,41 @@ def library():
         fn.restype = res
     _LIB = L
     return L
+
+
+def load_obj(path, default_ior=1.0):
+    """Scene of an OBJ file (and its mtllib) through the library's loader
+    (pm_obj_load): a photonmap.scenes.Scene with the model names; the model
+    named "light" emits (intensity 1)."""
+    from . import scenes
+    L = library()
+    d, f = os.path.split(os.path.abspath(str(path)))
+    h = C.c_void_p()
+    err = C.create_string_buffer(512)
+    rc = L.pm_obj_load(d.encode(), f.encode(), C.byref(h), err, len(err))
+    if rc:
+        raise PMError(rc, f"pm_obj_load: {err.value.decode()}")
+    try:
+        names = tuple(L.pm_obj_model_name(h, m).decode() for m in range(L.pm_obj_model_count(h)))
+        if L.pm_obj_light_model(h) < 0:
+            raise PMError(-1, f"pm_obj_load: no model named 'light' in {path} (models: {names})")
+        desc = _SceneDesc()
+        rc = L.pm_obj_desc(h, float(default_ior), C.byref(desc))
+        if rc:
+            raise PMError(rc, "pm_obj_desc")
+        T, M = desc.ntri, desc.nmodel
+
+        def arr(ptr, n, ctype):
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,)).copy()
+        return scenes.Scene(tri_pos=arr(desc.tri_pos, 9 * T, C.c_float).reshape(T, 3, 3),
+                            tri_nrm=arr(desc.tri_nrm, 9 * T, C.c_float).reshape(T, 3, 3),
+                            tri_model=arr(desc.tri_model, T, C.c_int32),
+                            materials=arr(desc.materials, 12 * M, C.c_float).reshape(M, 12),
+                            light_model=int(desc.light_model),
+                            light_intensity=np.array(list(desc.light_intensity), np.float32),
+                            default_ior=float(desc.default_ior), names=names)
+    finally:
+        L.pm_obj_free(h)
 
 
 def camera_setup(position, direction, up, fov_deg, width, height) -> Camera:

@@ -129,6 +129,23 @@ int pm_sync(pm_ctx* ctx);
  * initialize_scene_and_photon_maps (Initializer.cu:180-205): models, lights,
  * scene AABB, critical-angle table (PhotonTracing.cu:79-125). */
 int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* scene);
+
+/* OBJ / MTL import (host only, no context).  Replaces loadOBJ
+ * (ObjLoader.cpp:18-320) with the light convention of
+ * initialize_light_sources (Initializer.cu:62-100): models are runs of
+ * consecutive face lines named by the last g / o line, materials come from
+ * usemtl + the mtllib file (Material() defaults for what it omits), quads
+ * split as (v0 v1 v3), (v1 v2 v3), the model named "light" emits.  Errors:
+ * PM_ERR_IO (file), PM_ERR_INVALID (syntax, indices), message in err. */
+typedef struct pm_obj_scene pm_obj_scene;
+int pm_obj_load(const char* dir, const char* file, pm_obj_scene** out, char* err, int err_len);
+/* A pm_scene_desc pointing into s (valid while s lives): light intensity 1,
+ * the given default refractive index.  PM_ERR_INVALID if no model is named "light". */
+int pm_obj_desc(const pm_obj_scene* s, float default_ior, pm_scene_desc* out);
+int32_t pm_obj_model_count(const pm_obj_scene* s);
+const char* pm_obj_model_name(const pm_obj_scene* s, int32_t model);
+int32_t pm_obj_light_model(const pm_obj_scene* s);   /* -1: none */
+void pm_obj_free(pm_obj_scene* s);
 int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]);
 
 /* BVH builder used by the next pm_set_scene (the closest-hit answers, and so

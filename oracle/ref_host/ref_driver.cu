@@ -32,6 +32,8 @@
 #include "MMInnerStack.cu"
 #include "RayPlan.cu"
 #include "MathFunctions.cu"
+#include "ModelConstructInfo.cu"
+#include "ObjLoader.cpp"
 #undef private
 #undef protected
 
@@ -292,6 +294,60 @@ void ref_render(void* h, const float* position, const float* direction, const fl
             }
         }
     }
+}
+
+// The reference's OBJ loader (CPM/ObjLoader.cpp loadOBJ) on dir/file, its
+// ModelConstructInfo list flattened: per model the type (0 triangle, 1 quad,
+// 2 polygon), vertex count, material (diffuse, specular, emission, index,
+// opaque, shininess) and name; all models' vertex positions and normals
+// concatenated.  Null when the loader throws.
+struct RefObj {
+    std::vector<ModelConstructInfo> models;
+    std::vector<std::string> names;
+};
+
+void* ref_obj_load(const char* dir, const char* file, int* out_models, int* out_vertices) {
+    try {
+        auto r = loadOBJ(dir, file);
+        RefObj* o = new RefObj();
+        o->models = std::move(r.first);
+        o->names = std::move(r.second);
+        int nv = 0;
+        for (auto& m : o->models) nv += m.size;
+        *out_models = (int)o->models.size();
+        *out_vertices = nv;
+        return o;
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+void ref_obj_model(void* h, int m, int* type, int* size, float* mat12, char* name, int name_len) {
+    const RefObj* o = (const RefObj*)h;
+    const ModelConstructInfo& mi = o->models[m];
+    *type = (int)mi.type;
+    *size = mi.size;
+    const Material& t = mi.material;
+    const float v[12] = {t.diffuse.x, t.diffuse.y, t.diffuse.z, t.specular.x, t.specular.y, t.specular.z,
+                         t.emission.x, t.emission.y, t.emission.z, t.refr_index, t.opaque, t.shininess};
+    std::memcpy(mat12, v, sizeof v);
+    std::snprintf(name, (size_t)name_len, "%s", o->names[m].c_str());
+}
+
+void ref_obj_vertices(void* h, float* pos, float* nrm) {
+    const RefObj* o = (const RefObj*)h;
+    size_t k = 0;
+    for (auto& m : o->models)
+        for (int i = 0; i < m.size; i++, k++) {
+            pos[3 * k] = m.positions[i].x; pos[3 * k + 1] = m.positions[i].y; pos[3 * k + 2] = m.positions[i].z;
+            nrm[3 * k] = m.normals[i].x; nrm[3 * k + 1] = m.normals[i].y; nrm[3 * k + 2] = m.normals[i].z;
+        }
+}
+
+void ref_obj_free(void* h) {
+    RefObj* o = (RefObj*)h;
+    for (auto& m : o->models) { free(m.positions); free(m.texcoords); free(m.normals); }
+    delete o;
 }
 
 }  // extern "C"
