@@ -241,13 +241,48 @@ struct WarpWalk {
     unsigned long long T;     // a candidate enters when its key < T
     float lim, lim2;          // distance bound for pruning; squared pre-filter bound
     float bscale;             // DBINS / r: distance histogram bin of d = min(DBINS - 1, (int)(d * bscale))
+    bool guessed;             // the first ring ran with a density guess of the bound
+    bool failed;              // ... and found fewer than k photons within it: walk again without
 
     __device__ WarpWalk(const GatherGrid& g, WarpStore<UCAP>& u, V3 qq, float rr, int kk, int ln)
         : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), qn(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f),
-          bscale((float)DBINS / rr) {
+          bscale((float)DBINS / rr), guessed(false), failed(false) {
 #pragma unroll
         for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
         __syncwarp();
+    }
+
+    // back to the empty store and the bound r
+    __device__ void reset() {
+        n = 0;
+        qn = 0;
+        T = ~0ull;
+        lim = r;
+        lim2 = r * r * 1.000001f;
+        guessed = failed = false;
+        __syncwarp();
+#pragma unroll
+        for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+        __syncwarp();
+    }
+
+    // Density guess of the bound before the first ring's photons are scanned:
+    // its N photons lie in the 3 x 3 x 3 block of sub-cells of edge sc around
+    // the query; spread over a plane through the block (area 9 sc^2) they give
+    // about 2k photons within g = 3 sc sqrt(2k / (pi N)).  The guess only
+    // filters which candidates enter the store; when fewer than k lie within
+    // it, the walk starts again with the bound r, so the answer is unchanged.
+    __device__ void guess_bound(float sc) {
+        uint32_t c = lane < qn ? U.qc[lane] : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (c <= (uint32_t)k) return;   // too few photons in the block to gain anything
+        const float g = 3.f * sc * sqrtf((float)(2 * k) / (3.14159265f * (float)c));
+        if (g < lim) {
+            lim = g;
+            lim2 = g * g * 1.000001f;
+            guessed = true;
+        }
     }
 
     __device__ __forceinline__ uint32_t bin_of(float d) const {
@@ -334,8 +369,9 @@ struct WarpWalk {
         }
     }
 
-    // keep the k best keys of the store, tighten the threshold
-    __device__ void merge() {
+    // keep the k best keys of the store, tighten the threshold (last: the
+    // walk is over, so the histogram need not count the kept keys again)
+    __device__ void merge(bool last = false) {
         __syncwarp();
         if (n > k) {
             T = kth_key();
@@ -356,11 +392,13 @@ struct WarpWalk {
                 __syncwarp();
             }
             n = w;
-            // the histogram counts the store's keys again
+            if (!last) {
+                // the histogram counts the store's keys again
 #pragma unroll
-            for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
-            __syncwarp();
-            for (int i = lane; i < n; i += 32) atomicAdd(&U.dh[bin_of(__uint_as_float((uint32_t)(U.key[i] >> 32)))], 1u);
+                for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+                __syncwarp();
+                for (int i = lane; i < n; i += 32) atomicAdd(&U.dh[bin_of(__uint_as_float((uint32_t)(U.key[i] >> 32)))], 1u);
+            }
         } else if (n == k) {
             T = warp_max_key(U, n, lane);
         }
@@ -476,7 +514,7 @@ struct WarpWalk {
     // bound, non-empty photon range); the survivors are queued and scanned
     // together.  After each shell the distance histogram tightens the bound; a
     // shell whose nearest possible point is farther than the bound ends the walk.
-    __device__ void walk(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz) {
+    __device__ void walk(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz, bool use_guess) {
         constexpr int NM = 1;
         const int S = G.S, sh = __ffs(S) - 1;
         const float sc = G.cell / (float)S, pad = G.cell * 1e-4f;
@@ -535,7 +573,12 @@ struct WarpWalk {
                 for (int u = 0; u < NM; u++)
                     if (base + 32 * u < total) enqueue(b[u] > a[u], a[u], b[u] - a[u]);
             }
+            if (R == 1 && use_guess) guess_bound(sc);   // ring 1 (27 sub-cells) is all still queued
             flush();
+            if (R == 1 && guessed && n < k) {
+                failed = true;
+                return;
+            }
             if (n >= k) bound();
         }
         flush();
@@ -603,11 +646,17 @@ __device__ __forceinline__ void gather_query(const GatherGrid& G, WarpStore<UCAP
     const int rc = (int)ceilf(r / G.cell);
     const int x0 = max(0, hx - rc), y0 = max(0, hy - rc), z0 = max(0, hz - rc);
     const int x1 = min(G.gx - 1, hx + rc), y1 = min(G.gy - 1, hy + rc), z1 = min(G.gz - 1, hz + rc);
-    W.walk(hx * S + sx, hy * S + sy, hz * S + sz, x0 * S, y0 * S, z0 * S, x1 * S + S - 1, y1 * S + S - 1,
-           z1 * S + S - 1);
-    W.merge();
+    for (int pass = 0; pass < 2; pass++) {
+        W.walk(hx * S + sx, hy * S + sy, hz * S + sz, x0 * S, y0 * S, z0 * S, x1 * S + S - 1, y1 * S + S - 1,
+               z1 * S + S - 1, pass == 0);
+        if (!W.failed) break;
+        W.reset();
+    }
+    W.merge(!O.ids);
     const int cnt = W.n;
-    const float rk = cnt ? __uint_as_float((uint32_t)(warp_max_key(U, cnt, lane) >> 32)) : 0.f;
+    // after the merge a full store holds exactly the k best keys, the largest being T
+    const unsigned long long kmax = cnt >= k ? W.T : (cnt ? warp_max_key(U, cnt, lane) : 0ull);
+    const float rk = cnt ? __uint_as_float((uint32_t)(kmax >> 32)) : 0.f;
 
     // estimate (Raytracer.cuh:110-138): lanes take entries, then a fixed-order reduction
     V3 res = v3(0.f, 0.f, 0.f);
