@@ -140,6 +140,28 @@ constexpr int TRAV_SENTINEL = 0x76543210;
 constexpr int TRAV_STACK = 64;
 constexpr int TRAV_NONE = 0x7fffffff;
 
+// Traversal stacks.  LocalStack: the whole stack in per-thread local memory.
+// SplitStack: entries [0, H) in a shared-memory column of the block (entry i of
+// thread t at column[i * STRIDE], so the 32 lanes of a warp always use 32
+// different banks whatever their depths) and the deeper entries in local
+// memory.  Lanes of a warp sit at different depths, so a local-memory stack
+// touches a different 128-byte line per lane; the shared column does not.
+struct LocalStack {
+    int a[TRAV_STACK];
+    __device__ __forceinline__ int get(int i) const { return a[i]; }
+    __device__ __forceinline__ void set(int i, int v) { a[i] = v; }
+};
+template <int H, int STRIDE>
+struct SplitStack {
+    int* col;                    // this thread's column of the block's shared stack
+    int deep[TRAV_STACK - H];
+    __device__ __forceinline__ int get(int i) const { return i < H ? col[i * STRIDE] : deep[i - H]; }
+    __device__ __forceinline__ void set(int i, int v) {
+        if (i < H) col[i * STRIDE] = v;
+        else deep[i - H] = v;
+    }
+};
+
 struct Trav {
     float ix, iy, iz, ox, oy, oz;      // slab terms: 1/d and o/d
     float best_t;
@@ -151,7 +173,8 @@ struct Trav {
     int node, leaf, sp, min_model;
 };
 
-__device__ __forceinline__ void trav_pass(Trav& T, int min_model, int* stack) {
+template <class Stk>
+__device__ __forceinline__ void trav_pass(Trav& T, int min_model, Stk& stack) {
     T.best_t = __int_as_float(0x7f800000);
     T.best_tri = TRAV_NONE;
     T.best_uvw = v3(0.f, 0.f, 0.f);
@@ -159,10 +182,11 @@ __device__ __forceinline__ void trav_pass(Trav& T, int min_model, int* stack) {
     T.node = 0;
     T.leaf = 0;
     T.sp = 0;
-    stack[0] = TRAV_SENTINEL;
+    stack.set(0, TRAV_SENTINEL);
 }
 
-__device__ __forceinline__ void trav_init(Trav& T, V3 o, V3 d, int* stack) {
+template <class Stk>
+__device__ __forceinline__ void trav_init(Trav& T, V3 o, V3 d, Stk& stack) {
     T.ix = safe_inv(d.x); T.iy = safe_inv(d.y); T.iz = safe_inv(d.z);
     T.ox = o.x * T.ix; T.oy = o.y * T.iy; T.oz = o.z * T.iz;
     T.zmodel = -1;
@@ -175,7 +199,8 @@ __device__ __forceinline__ void trav_init(Trav& T, V3 o, V3 d, int* stack) {
 
 // One round: descend until this lane holds a leaf (or every active lane does),
 // then test the held leaves.  Returns true when the pass is complete.
-__device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, int* stack) {
+template <class Stk>
+__device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, Stk& stack) {
     int node = T.node, leaf = T.leaf, sp = T.sp;
     const float ix = T.ix, iy = T.iy, iz = T.iz, ox = T.ox, oy = T.oy, oz = T.oz;
     while ((unsigned)node < (unsigned)TRAV_SENTINEL) {
@@ -194,19 +219,19 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
         const float c1max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
         const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
         if (!h0 && !h1) {
-            node = stack[sp--];
+            node = stack.get(sp--);
         } else {
             const int r0 = __float_as_int(a0.w), r1 = __float_as_int(a1.w);
             node = h0 ? r0 : r1;
             if (h0 && h1) {
                 int other = r1;
                 if (c1min < c0min) { node = r1; other = r0; }
-                if (sp < TRAV_STACK - 1) stack[++sp] = other;
+                if (sp < TRAV_STACK - 1) stack.set(++sp, other);
             }
         }
         if (node < 0 && leaf >= 0) {   // first leaf: postpone it, keep descending
             leaf = node;
-            node = stack[sp--];
+            node = stack.get(sp--);
         }
         if (!__any_sync(__activemask(), leaf >= 0)) break;   // every lane holds a leaf
     }
@@ -238,7 +263,7 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
             else { T.best_t = t; T.best_tri = tri; T.best_uvw = uvw; }
         }
         leaf = node;                    // another postponed leaf: process it as well
-        if (node < 0) node = stack[sp--];
+        if (node < 0) node = stack.get(sp--);
     }
     T.node = node; T.leaf = leaf; T.sp = sp;
     return node == TRAV_SENTINEL;
@@ -252,7 +277,8 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
 // models after z, else z's hit.  Returns TRAV_AGAIN after starting the second
 // pass (models > z), TRAV_HIT with h filled, or TRAV_MISS.
 enum { TRAV_HIT = 0, TRAV_MISS = 1, TRAV_AGAIN = 2 };
-__device__ __forceinline__ int trav_resolve(const DevScene& S, Trav& T, Hit& h, int* stack) {
+template <class Stk>
+__device__ __forceinline__ int trav_resolve(const DevScene& S, Trav& T, Hit& h, Stk& stack) {
     if (T.best_tri != TRAV_NONE &&
         (T.min_model != 0 || T.zmodel < 0 || hit_model_raw(S, T.best_tri) > T.zmodel)) {
         h.t = T.best_t; h.tri = T.best_tri; h.uvw = T.best_uvw;
@@ -269,7 +295,7 @@ __device__ __forceinline__ int trav_resolve(const DevScene& S, Trav& T, Hit& h, 
 
 // Closest hit of one ray, both passes run to completion.
 static __device__ __noinline__ bool intersect(const DevScene& S, V3 o, V3 d, Hit& h) {
-    int stack[TRAV_STACK];
+    LocalStack stack;
     Trav T;
     trav_init(T, o, d, stack);
     while (true) {

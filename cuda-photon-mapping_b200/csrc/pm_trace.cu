@@ -32,6 +32,11 @@ constexpr int TRACE_THREADS = 128;
 // bound by the latency of its node and triangle loads, and twice the resident
 // warps hide more of it than the spills cost (10M photons: 5.77 -> 5.10 ms).
 constexpr int TRACE_MIN_BLOCKS = 8;
+// top TRACE_SMEM_STACK entries of each lane's traversal stack in shared memory
+// (8: 5.13 -> 4.92 ms per 10M photons; 16 and 32 entries take L1 from the
+// node and triangle loads: 4.98 and 5.08 ms)
+constexpr int TRACE_SMEM_STACK = 8;
+using TraceStack = SplitStack<TRACE_SMEM_STACK, TRACE_THREADS>;
 constexpr int MAX_STACK = 32;
 constexpr int REJECT_LIMIT = 1 << 16;
 constexpr int TRACE_REFILL = 8;          // default for KParams::refill   // emission rejection loop bound (acceptance ~1/2 on valid lights)
@@ -230,7 +235,9 @@ k_trace(KParams P) {
     const int lane = threadIdx.x & 31;
     Lane L;
     Trav T;
-    int stack[TRAV_STACK];
+    __shared__ int stack_cols[TRACE_SMEM_STACK * TRACE_THREADS];
+    TraceStack stack;
+    stack.col = stack_cols + threadIdx.x;
     float sior[MAX_STACK];
     int sid[MAX_STACK];
     int64_t j = -1;          // batch-local path index of this lane
@@ -308,7 +315,9 @@ k_trace_multi(const KParams* __restrict__ tab, const int64_t* __restrict__ off, 
     const int lane = threadIdx.x & 31;
     Lane L;
     Trav T;
-    int stack[TRAV_STACK];
+    __shared__ int stack_cols[TRACE_SMEM_STACK * TRACE_THREADS];
+    TraceStack stack;
+    stack.col = stack_cols + threadIdx.x;
     float sior[MAX_STACK];
     int sid[MAX_STACK];
     int64_t j = -1;          // global path index of this lane
