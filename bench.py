@@ -442,6 +442,8 @@ def run_ours(args):
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
     # end to end through the public API with the frame read back to pinned host memory
+    # (one untimed step first: new seeds, so the photon pass re-sizes its batches)
+    step(9_999, e2e=True)
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
