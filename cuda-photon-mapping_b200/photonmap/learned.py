@@ -13,11 +13,11 @@ from __future__ import annotations
 import dataclasses
 
 # Settings of the learned frame that is timed and quality-checked: 16x16
-# tiles, 16 exact probes per tile, a tile falls back to the exact gather when
+# tiles, 8 exact probes per tile, a tile falls back to the exact gather when
 # its cache bias exceeds 5 % of the probes' estimate by more than two standard
 # errors of the probe differences (so the probes' own kNN noise does not
 # flag it).  render_learned(**FRAME_SETTINGS, ...).
-FRAME_SETTINGS = dict(tile=16, probes=16, max_rel_err=0.05, noise_z=2.0)
+FRAME_SETTINGS = dict(tile=16, probes=8, max_rel_err=0.05, noise_z=2.0)
 
 
 @dataclasses.dataclass
