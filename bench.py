@@ -358,6 +358,17 @@ def learned_frames(ctx, cam, w, rgb, args, world):
 
     ms_plain = timed(plain)
     ms_learned = timed(learned_frame)
+    # the same frame captured once and replayed as one CUDA graph per frame
+    graph = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=TRAIN_PER_FRAME // BATCH,
+                              batch=BATCH, offset=off[0], out_rgb8=rgb, **learned.FRAME_SETTINGS)
+    gstats = {}
+
+    def graph_frame():
+        graph.run()
+
+    ms_graph = timed(graph_frame)
+    gstats.update(graph.run(stats=True)[2])
+    graph.close()
     # tensor-core throughput of the cache kernels (forward 32,640 flop per sample, backward ~2x)
     fwd = 2 * (60 * 64 + 3 * 64 * 64 + 64 * 3)
     n = min(pool.n, 1 << 20)
@@ -375,6 +386,8 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     inf_tf = fwd * n / (ms_inf * 1e-3) / 1e12
     tr_tf = 3 * fwd * min(BATCH * 4, pool.n) / (ms_tr * 1e-3) / 1e12
     return {"ms_per_frame_plain": ms_plain, "ms_per_frame_learned": ms_learned, "speedup": ms_plain / ms_learned,
+            "ms_per_frame_learned_graph": ms_graph, "speedup_graph": ms_plain / ms_graph,
+            "graph_fallback_requests_frac": gstats["fallback_requests"] / max(gstats["requests"], 1),
             "frame": "eye pass + global estimate + resolve, photon map resident",
             "train_samples_per_frame": TRAIN_PER_FRAME, "pool": pool.n, "warmup_steps": WARM_STEPS,
             "check": dict(learned.FRAME_SETTINGS), "fallback_tiles_frac": stats["fallback_tiles"] / max(stats["tiles"], 1),

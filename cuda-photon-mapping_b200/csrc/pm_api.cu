@@ -127,6 +127,38 @@ GatherGrid grid_of(MapState& m, MapState& est_src) {
     return G;
 }
 
+MlpNet cache_net(pm_ctx* ctx) {
+    MlpNet net;
+    net.w = P<__nv_bfloat16>(ctx->cache_w16);
+    for (int a = 0; a < 3; a++) { net.lo[a] = ctx->cache_lo[a]; net.inv[a] = ctx->cache_inv[a]; }
+    net.out_scale = ctx->cache_opts.out_scale;
+    net.freq0 = (float)(1 << ctx->cache_opts.octave0);
+    return net;
+}
+
+int learned_checks(pm_ctx* ctx, const pm_learned_opts* lo) {
+    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
+    if (lo->tile < 1 || lo->tile > 256 || lo->probes < 1 || lo->probes > 64 || lo->max_rel_err != lo->max_rel_err ||
+        !(lo->noise_z >= 0.f && lo->noise_z <= 100.f))
+        return fail(ctx, PM_ERR_INVALID, "learned options: tile 1..256, probes 1..64, max_rel_err not NaN, noise_z 0..100");
+    return PM_OK;
+}
+
+int render_checks(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o) {
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
+    if (o->max_depth < 0 || o->max_depth > RENDER_MAX_DEPTH) return fail(ctx, PM_ERR_INVALID, "max_depth must be 0..5");
+    if (o->k_global < 0 || o->k_global > 256 || o->k_caustic < 0 || o->k_caustic > 256)
+        return fail(ctx, PM_ERR_INVALID, "k must be 0..256");
+    if (cam->width <= 0 || cam->height <= 0) return fail(ctx, PM_ERR_INVALID, "bad camera size");
+    MapState& G = ctx->maps[PM_MAP_GLOBAL];
+    MapState& C = ctx->maps[PM_MAP_CAUSTIC];
+    if (!G.built) return fail(ctx, PM_ERR_INVALID, "global map grid not built");
+    if (C.built && o->faithful_caustic && C.n > G.n)
+        return fail(ctx, PM_ERR_INVALID, "faithful caustic estimate reads the global map with caustic indices: "
+                                         "the caustic map must not be larger than the global map");
+    return PM_OK;
+}
+
 }  // namespace pm
 
 extern "C" {
@@ -208,15 +240,6 @@ int pm_launch_count(pm_ctx* ctx, int64_t* out) {
 }
 
 namespace {
-
-MlpNet cache_net(pm_ctx* ctx) {
-    MlpNet net;
-    net.w = P<__nv_bfloat16>(ctx->cache_w16);
-    for (int a = 0; a < 3; a++) { net.lo[a] = ctx->cache_lo[a]; net.inv[a] = ctx->cache_inv[a]; }
-    net.out_scale = ctx->cache_opts.out_scale;
-    net.freq0 = (float)(1 << ctx->cache_opts.octave0);
-    return net;
-}
 
 MlpInputs cache_inputs(const float* pos, const float* nrm, int64_t n) {
     MlpInputs in{};
@@ -944,20 +967,6 @@ struct FrameSetup {
     bool caustic = false;
 };
 
-int render_checks(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o) {
-    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
-    if (o->max_depth < 0 || o->max_depth > RENDER_MAX_DEPTH) return fail(ctx, PM_ERR_INVALID, "max_depth must be 0..5");
-    if (o->k_global < 0 || o->k_global > 256 || o->k_caustic < 0 || o->k_caustic > 256)
-        return fail(ctx, PM_ERR_INVALID, "k must be 0..256");
-    if (cam->width <= 0 || cam->height <= 0) return fail(ctx, PM_ERR_INVALID, "bad camera size");
-    MapState& G = ctx->maps[PM_MAP_GLOBAL];
-    MapState& C = ctx->maps[PM_MAP_CAUSTIC];
-    if (!G.built) return fail(ctx, PM_ERR_INVALID, "global map grid not built");
-    if (C.built && o->faithful_caustic && C.n > G.n)
-        return fail(ctx, PM_ERR_INVALID, "faithful caustic estimate reads the global map with caustic indices: "
-                                         "the caustic map must not be larger than the global map");
-    return PM_OK;
-}
 
 // buffers, eye pass (timed into ev[4] .. ev[5]) and the request count
 int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F) {
@@ -1046,10 +1055,7 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_
 int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, const pm_learned_opts* lo,
                       uint8_t* out_rgb8, float* out_radiance, pm_learned_stats* out_stats) {
     if (!ctx || !cam || !o || !lo || !out_rgb8) return PM_ERR_INVALID;
-    if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
-    if (lo->tile < 1 || lo->tile > 256 || lo->probes < 1 || lo->probes > 64 || lo->max_rel_err != lo->max_rel_err ||
-        !(lo->noise_z >= 0.f && lo->noise_z <= 100.f))
-        return fail(ctx, PM_ERR_INVALID, "learned options: tile 1..256, probes 1..64, max_rel_err not NaN, noise_z 0..100");
+    if (int rc = learned_checks(ctx, lo)) return rc;
     if (int rc = render_checks(ctx, cam, o)) return rc;
     CK(cudaSetDevice(ctx->device));
     FrameSetup F;
@@ -1080,9 +1086,10 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     GatherOut PO{P<float>(ctx->probe_est), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), PQ, o->r_global, o->k_global, 0, PO, P<unsigned>(ctx->status), ctx->st));
     CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 32, ctx->st));
-    CK(learned_select(F.cd, F.R, F.nreq, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
+    CK(learned_select(F.cd, F.R, F.nreq, nullptr, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
                       P<float>(ctx->est_mlp), lo->max_rel_err, lo->noise_z, P<uint8_t>(ctx->tile_flag),
-                      P<unsigned long long>(ctx->learned_counts), P<uint32_t>(ctx->fallback_list), ctx->st));
+                      P<unsigned long long>(ctx->learned_counts), P<uint32_t>(ctx->fallback_list), ctx->sm_count,
+                      ctx->st));
     // the exact gather for the listed fallback requests only (count read on the device)
     GatherQueries Q{};
     Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = LEARNED_FALLBACK;
@@ -1090,7 +1097,8 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     GatherOut OF{P<float>(ctx->est_fb), nullptr, nullptr, nullptr};
     unsigned long long* counts = P<unsigned long long>(ctx->learned_counts);
     CK(gather_listed(grid_of(G, G), Q, counts + 1, counts + 2, o->r_global, o->k_global, OF, ctx->sm_count, ctx->st));
-    CK(learned_merge(F.R, F.nreq, P<float>(ctx->est_mlp), P<float>(ctx->est_fb), P<float>(ctx->est_g), ctx->st));
+    CK(learned_merge(F.R, F.nreq, nullptr, P<float>(ctx->est_mlp), P<float>(ctx->est_fb), P<float>(ctx->est_g),
+                     ctx->sm_count, ctx->st));
     ctx->launches += (F.nreq > 0 ? 1 : 0) + 1 + 1 + 1 + (F.nreq > 0 ? 1 : 0) + 1 + (F.nreq > 0 ? 1 : 0);
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
     if (out_stats) {

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include "../../include/pm_api.h"
 #include "pm_gather.cuh"
+#include "pm_mlp.cuh"
 #include "pm_scene.cuh"
 
 namespace pm {
@@ -88,6 +89,12 @@ int check_status(pm_ctx* ctx, const char* what);
 float elapsed(cudaEvent_t a, cudaEvent_t b);
 // gather view of map m, estimates read from est_src's direction / power arrays
 GatherGrid grid_of(MapState& m, MapState& est_src);
+// the radiance cache's network as the kernels read it
+MlpNet cache_net(pm_ctx* ctx);
+// a frame's checks: scene, grid, camera size, depth and k ranges
+int render_checks(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o);
+// the learned render's option checks (PM_OK or the failure recorded on ctx)
+int learned_checks(pm_ctx* ctx, const pm_learned_opts* lo);
 
 }  // namespace pm
 

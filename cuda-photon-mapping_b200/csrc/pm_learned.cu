@@ -7,6 +7,7 @@
 // over its probes exceeds a threshold takes the exact gather for all of its
 // requests.  Probe slots are fixed per (tile, probe), so the result
 // does not depend on scheduling.
+#include <algorithm>
 #include "pm_learned.cuh"
 #include "pm_device.cuh"
 
@@ -90,12 +91,10 @@ __global__ void k_tile_flags(int64_t ntiles, int P, const uint32_t* __restrict__
     if (f) atomicAdd(nflag, 1ull);
 }
 
-// requests of flagged tiles that need the global estimate get flag bit 2 and
-// join the list of fallback requests (list order is immaterial: every answer
-// is written at its request's index)
-__global__ void k_mark_fallback(int64_t nreq, Requests R, int W, int tile, int tiles_x, const uint8_t* __restrict__ flag,
-                                unsigned long long* __restrict__ nfb, uint32_t* __restrict__ list) {
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// request q (of nreq): flag bit 2 and a list entry when its tile is flagged (all lanes of the warp call this)
+__device__ __forceinline__ void mark_one(int64_t q, int64_t nreq, Requests& R, int W, int tile, int tiles_x,
+                                         const uint8_t* __restrict__ flag, unsigned long long* __restrict__ nfb,
+                                         uint32_t* __restrict__ list) {
     bool fb = false;
     if (q < nreq) {
         float4 b = R.b[q];
@@ -117,19 +116,38 @@ __global__ void k_mark_fallback(int64_t nreq, Requests R, int W, int tile, int t
     if (fb) list[base + __popc(m & lanemask_lt())] = (uint32_t)q;
 }
 
+// requests of flagged tiles that need the global estimate get flag bit 2 and
+// join the list of fallback requests (list order is immaterial: every answer
+// is written at its request's index)
+__global__ void k_mark_fallback(int64_t cap, const unsigned long long* __restrict__ n_dev, Requests R, int W, int tile,
+                                int tiles_x, const uint8_t* __restrict__ flag, unsigned long long* __restrict__ nfb,
+                                uint32_t* __restrict__ list) {
+    const int64_t nreq = n_dev ? (int64_t)min(*n_dev, (unsigned long long)cap) : cap;
+    for (int64_t b0 = (int64_t)blockIdx.x * blockDim.x; b0 < nreq; b0 += (int64_t)gridDim.x * blockDim.x)
+        mark_one(b0 + threadIdx.x, nreq, R, W, tile, tiles_x, flag, nfb, list);
+}
+
 // est = exact for fallback requests, else the cache
-__global__ void k_merge(int64_t nreq, Requests R, const float* __restrict__ cached, const float* __restrict__ exact,
-                        float* __restrict__ est) {
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nreq) return;
-    const bool fb = (__float_as_uint(R.b[q].w) & LEARNED_FALLBACK) != 0u;
-    const float* src = fb ? exact : cached;
-    est[3 * q] = src[3 * q];
-    est[3 * q + 1] = src[3 * q + 1];
-    est[3 * q + 2] = src[3 * q + 2];
+__global__ void k_merge(int64_t cap, const unsigned long long* __restrict__ n_dev, Requests R,
+                        const float* __restrict__ cached, const float* __restrict__ exact, float* __restrict__ est) {
+    const int64_t nreq = n_dev ? (int64_t)min(*n_dev, (unsigned long long)cap) : cap;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nreq; q += (int64_t)gridDim.x * blockDim.x) {
+        const bool fb = (__float_as_uint(R.b[q].w) & LEARNED_FALLBACK) != 0u;
+        const float* src = fb ? exact : cached;
+        est[3 * q] = src[3 * q];
+        est[3 * q + 1] = src[3 * q + 1];
+        est[3 * q + 2] = src[3 * q + 2];
+    }
 }
 
 inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// one thread per request when the count is known on the host, else a
+// grid-stride launch of (at most) 8 blocks of 256 per SM over the capacity
+inline unsigned req_blocks(int64_t cap, bool on_device, int sm_count) {
+    const unsigned b = blocks(cap, 256);
+    return on_device ? std::min<unsigned>(b, (unsigned)(8 * std::max(sm_count, 1))) : b;
+}
 
 }  // namespace
 
@@ -141,23 +159,25 @@ cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, in
     return cudaGetLastError();
 }
 
-cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
-                           const float* probe_exact, const float* cached, float max_rel_err, float noise_z,
-                           uint8_t* tile_flag, unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st) {
+cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, const unsigned long long* nreq_dev,
+                           int tile, int P, const uint32_t* preq, const float* probe_exact, const float* cached,
+                           float max_rel_err, float noise_z, uint8_t* tile_flag, unsigned long long* counts,
+                           uint32_t* fallback_list, int sm_count, cudaStream_t st) {
     const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
     const int64_t ntiles = (int64_t)tx * ty;
     k_tile_flags<<<blocks(ntiles, 256), 256, 0, st>>>(ntiles, P, preq, probe_exact, cached, max_rel_err, noise_z, tile_flag,
                                                       counts);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || nreq <= 0) return e;
-    k_mark_fallback<<<blocks(nreq, 256), 256, 0, st>>>(nreq, R, cam.W, tile, tx, tile_flag, counts + 1, fallback_list);
+    k_mark_fallback<<<req_blocks(nreq, nreq_dev != nullptr, sm_count), 256, 0, st>>>(nreq, nreq_dev, R, cam.W, tile, tx,
+                                                                                    tile_flag, counts + 1, fallback_list);
     return cudaGetLastError();
 }
 
-cudaError_t learned_merge(const Requests& R, int64_t nreq, const float* cached, const float* exact, float* est,
-                          cudaStream_t st) {
+cudaError_t learned_merge(const Requests& R, int64_t nreq, const unsigned long long* nreq_dev, const float* cached,
+                          const float* exact, float* est, int sm_count, cudaStream_t st) {
     if (nreq <= 0) return cudaSuccess;
-    k_merge<<<blocks(nreq, 256), 256, 0, st>>>(nreq, R, cached, exact, est);
+    k_merge<<<req_blocks(nreq, nreq_dev != nullptr, sm_count), 256, 0, st>>>(nreq, nreq_dev, R, cached, exact, est);
     return cudaGetLastError();
 }
 

@@ -19,12 +19,14 @@ cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, in
 // LEARNED_FALLBACK on every global request of a flagged tile, whose index also
 // goes to fallback_list (nreq entries of room, any order).
 // counts[0] += flagged tiles, counts[1] += fallback requests (= list length).
-cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, int tile, int P, const uint32_t* preq,
-                           const float* probe_exact, const float* cached, float max_rel_err, float noise_z,
-                           uint8_t* tile_flag, unsigned long long* counts, uint32_t* fallback_list, cudaStream_t st);
+// nreq_dev (optional): the request count on the device, nreq then a capacity.
+cudaError_t learned_select(const CameraDev& cam, const Requests& R, int64_t nreq, const unsigned long long* nreq_dev,
+                           int tile, int P, const uint32_t* preq, const float* probe_exact, const float* cached,
+                           float max_rel_err, float noise_z, uint8_t* tile_flag, unsigned long long* counts,
+                           uint32_t* fallback_list, int sm_count, cudaStream_t st);
 
 // est = exact estimate for fallback requests, the cache's otherwise
-cudaError_t learned_merge(const Requests& R, int64_t nreq, const float* cached, const float* exact, float* est,
-                          cudaStream_t st);
+cudaError_t learned_merge(const Requests& R, int64_t nreq, const unsigned long long* nreq_dev, const float* cached,
+                          const float* exact, float* est, int sm_count, cudaStream_t st);
 
 }  // namespace pm

@@ -159,13 +159,14 @@ __device__ void load_weights(const __nv_bfloat16* __restrict__ w, unsigned char*
 }
 
 // one input sample: position, normal, whether it is used
-__device__ __forceinline__ bool load_sample(const MlpInputs& in, int64_t i, V3& p, V3& n) {
+// (sample i of cnt; base: array offset of sample 0 in pos3 / nrm3)
+__device__ __forceinline__ bool load_sample(const MlpInputs& in, int64_t cnt, int64_t base, int64_t i, V3& p, V3& n) {
     p = v3(0.f, 0.f, 0.f);
     n = v3(0.f, 0.f, 1.f);
-    if (i >= in.n) return false;
+    if (i >= cnt) return false;
     if (in.pos3) {
-        p = ld3(in.pos3 + 3 * i);
-        n = ld3(in.nrm3 + 3 * i);
+        p = ld3(in.pos3 + 3 * (base + i));
+        n = ld3(in.nrm3 + 3 * (base + i));
         return true;
     }
     const float4 a = in.rec_pos[i], b = in.rec_nrm[i];
@@ -275,13 +276,14 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
     bool ok = true, any = false;
     float loss = 0.f;
     const int64_t tiles = (in.n + TILE - 1) / TILE;
+    const int64_t base = in.base_dev ? *in.base_dev : 0;
     int iter = 0;
     for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, iter++) {
         const int64_t i = tile * TILE + tid;
         V3 p, n;
-        const bool use = load_sample(in, i, p, n);
-        const float wgt = use ? (weight ? weight[i] : 1.f) : 0.f;
-        const V3 t = use ? ld3(target + 3 * i) : v3(0.f, 0.f, 0.f);
+        const bool use = load_sample(in, in.n, base, i, p, n);
+        const float wgt = use ? (weight ? weight[base + i] : 1.f) : 0.f;
+        const V3 t = use ? ld3(target + 3 * (base + i)) : v3(0.f, 0.f, 0.f);
         write_features(sX, tid, net, p, n);
         fence_async_smem();
         tc_before();
@@ -434,16 +436,17 @@ k_mlp_infer(MlpNet net, MlpInputs in, float* __restrict__ out, unsigned* status)
     const int bar_id = 1 + g;
     uint32_t phase = 0;
     bool ok = true;
-    const int64_t tiles = (in.n + TILE - 1) / TILE;
+    const int64_t cnt = in.n_dev ? (int64_t)min(*in.n_dev, (unsigned long long)in.n) : in.n;
+    const int64_t tiles = (cnt + TILE - 1) / TILE;
     const int64_t stride = (int64_t)gridDim.x * INFER_GROUPS;
     int64_t tile = (int64_t)blockIdx.x * INFER_GROUPS + g;
     V3 p, n;
-    bool use = load_sample(in, tile * TILE + row, p, n);
+    bool use = load_sample(in, cnt, 0, tile * TILE + row, p, n);
     for (; tile < tiles && ok; tile += stride) {
         const int64_t i = tile * TILE + row;
         write_features(sX, row, net, p, n);
         const bool use_cur = use;
-        use = load_sample(in, (tile + stride) * TILE + row, p, n);   // next tile's sample, in flight
+        use = load_sample(in, cnt, 0, (tile + stride) * TILE + row, p, n);   // next tile's sample, in flight
         fence_async_smem();
         tc_before();
         wg_sync_and(bar_id, true);
@@ -472,7 +475,7 @@ k_mlp_infer(MlpNet net, MlpInputs in, float* __restrict__ out, unsigned* status)
             tc_after();
         }
         if (!ok) break;
-        if (i < in.n) {
+        if (i < cnt) {
             const float sc = use_cur ? net.out_scale : 0.f;
             out[3 * i] = y[0] * sc;
             out[3 * i + 1] = y[1] * sc;
@@ -489,11 +492,9 @@ k_mlp_infer(MlpNet net, MlpInputs in, float* __restrict__ out, unsigned* status)
     if (warp == 0) tmem_dealloc(*tslot, TMEM_COLS_INFER);
 }
 
-__global__ void k_adam(float* __restrict__ w32, __nv_bfloat16* __restrict__ w16, float* __restrict__ grad,
-                       float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
-                       float c1, float c2) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= MLP_PARAMS) return;
+__device__ __forceinline__ void adam_update(int i, float* __restrict__ w32, __nv_bfloat16* __restrict__ w16,
+                                            float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
+                                            float lr, float b1, float b2, float eps, float c1, float c2) {
     const float g = grad[i];
     const float mi = b1 * m[i] + (1.f - b1) * g;
     const float vi = b2 * v[i] + (1.f - b2) * g * g;
@@ -503,6 +504,27 @@ __global__ void k_adam(float* __restrict__ w32, __nv_bfloat16* __restrict__ w16,
     w32[i] = w;
     w16[i] = __float2bfloat16_rn(w);
     grad[i] = 0.f;
+}
+
+__global__ void k_adam(float* __restrict__ w32, __nv_bfloat16* __restrict__ w16, float* __restrict__ grad,
+                       float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < MLP_PARAMS) adam_update(i, w32, w16, grad, m, v, lr, b1, b2, eps, c1, c2);
+}
+
+__global__ void k_step_inc(int* step) { *step += 1; }
+
+// k_adam with the bias corrections 1 / (1 - beta^step) formed on the device
+__global__ void k_adam_dev(float* __restrict__ w32, __nv_bfloat16* __restrict__ w16, float* __restrict__ grad,
+                           float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
+                           const int* __restrict__ step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MLP_PARAMS) return;
+    const int s = *step;
+    const float c1 = (float)(1.0 / (1.0 - pow((double)b1, (double)s)));
+    const float c2 = (float)(1.0 / (1.0 - pow((double)b2, (double)s)));
+    adam_update(i, w32, w16, grad, m, v, lr, b1, b2, eps, c1, c2);
 }
 
 __global__ void k_to_bf16(const float* __restrict__ w32, __nv_bfloat16* __restrict__ w16) {
@@ -545,6 +567,13 @@ cudaError_t mlp_adam(float* w32, __nv_bfloat16* w16, float* grad, float* m, floa
     const float c1 = (float)(1.0 / (1.0 - std::pow((double)beta1, step)));
     const float c2 = (float)(1.0 / (1.0 - std::pow((double)beta2, step)));
     k_adam<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(w32, w16, grad, m, v, lr, beta1, beta2, eps, c1, c2);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_adam_dev(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int* step_dev, float lr,
+                         float beta1, float beta2, float eps, cudaStream_t st) {
+    k_step_inc<<<1, 1, 0, st>>>(step_dev);
+    k_adam_dev<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(w32, w16, grad, m, v, lr, beta1, beta2, eps, step_dev);
     return cudaGetLastError();
 }
 

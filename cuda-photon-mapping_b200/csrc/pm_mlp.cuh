@@ -41,6 +41,9 @@ struct MlpInputs {
     const float4* rec_pos;
     const float4* rec_nrm;
     uint32_t flag_mask;
+    // optional, for launches whose sizes live on the device (graph replay):
+    const unsigned long long* n_dev;   // inference: min(*n_dev, n) samples (n a capacity)
+    const int64_t* base_dev;           // training on pos3 / nrm3: sample i is array entry *base_dev + i
 };
 
 // One training pass over n samples: accumulates d(loss)/d(weights) into grad
@@ -59,6 +62,11 @@ cudaError_t mlp_infer(const MlpNet& net, const MlpInputs& in, float* out, unsign
 // Adam step on the FP32 master weights; refreshes the BF16 copies and zeroes grad.
 cudaError_t mlp_adam(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int step, float lr,
                      float beta1, float beta2, float eps, cudaStream_t st);
+
+// The same with the step number on the device: *step_dev += 1, then the step
+// uses it for the bias corrections (a replayed graph advances it itself).
+cudaError_t mlp_adam_dev(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int* step_dev, float lr,
+                         float beta1, float beta2, float eps, cudaStream_t st);
 
 // BF16 copies of FP32 weights.
 cudaError_t mlp_to_bf16(const float* w32, __nv_bfloat16* w16, cudaStream_t st);

@@ -164,6 +164,10 @@ def library():
         "pm_cache_set_params": ([vp, vp], C.c_int),
         "pm_cache_sample_points": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
         "pm_render_learned": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "pm_learned_graph_create": ([vp, vp, vp, vp, vp, vp, vp, i64, i64, i32, i64, vp, vp, vp], C.c_int),
+        "pm_learned_graph_run": ([vp, vp], C.c_int),
+        "pm_learned_graph_offset": ([vp, vp], C.c_int),
+        "pm_learned_graph_destroy": ([vp], None),
         "pm_get_requests": ([vp, C.POINTER(_RequestView)], C.c_int),
         "pm_batch_create": ([C.POINTER(C.c_void_p), vp, C.c_int32, C.POINTER(_BatchOpts)], C.c_int),
         "pm_batch_destroy": ([vp], None),
@@ -464,6 +468,32 @@ class Context:
         return rgb, rad, dict(tiles=st.tiles, fallback_tiles=st.fallback_tiles, requests=st.requests,
                               fallback_requests=st.fallback_requests)
 
+    def learned_graph(self, cam: Camera, k_global, r_global, max_depth=4, pool=None, steps=4, batch=65536, offset=0,
+                      tile=16, probes=16, max_rel_err=0.05, noise_z=0.0, radiance=False, out_rgb8=None,
+                      out_radiance=None):
+        """The learned frame (`steps` Adam steps on the pool + render_learned) as one
+        replayable CUDA graph (pm_learned_graph_create); `pool` a photonmap.learned.Pool
+        (or None with steps=0).  Returns a LearnedGraph: .run(stats=False) -> (rgb, radiance, stats)."""
+        torch = self.torch
+        W, H = cam.width, cam.height
+        rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
+        rad = out_radiance
+        if rad is None and radiance:
+            rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
+        o = _RenderOpts(max_depth, k_global, r_global, 0, 0.2, 1)
+        lo = _LearnedOpts(int(tile), int(probes), float(max_rel_err), float(noise_z))
+        if pool is not None:
+            pos, nrm, tgt = self._samples(pool.pos, pool.nrm, pool.target)
+            n = pos.shape[0]
+        else:
+            pos = nrm = tgt = None
+            n = 0
+        h = C.c_void_p()
+        self._check(self.L.pm_learned_graph_create(self.h, C.byref(cam), C.byref(o), C.byref(lo), _ptr(pos), _ptr(nrm),
+                                                   _ptr(tgt), int(n), int(batch), int(steps), int(offset), _ptr(rgb),
+                                                   _ptr(rad), C.byref(h)), "pm_learned_graph_create")
+        return LearnedGraph(self, h, rgb, rad, (pos, nrm, tgt))
+
     # ------------------------------------------------------------ render
     def render(self, cam: Camera, k_global, r_global, max_depth=4, k_caustic=0, r_caustic=0.2,
                faithful_caustic=True, radiance=True, out_rgb8=None, out_radiance=None):
@@ -534,6 +564,36 @@ class _DeviceArray:
     def __init__(self, ptr, shape, dtype):
         self.__cuda_array_interface__ = {"shape": tuple(int(x) for x in shape), "typestr": self._TYPESTR[str(dtype)],
                                          "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+class LearnedGraph:
+    """A captured learned frame (Context.learned_graph); keeps its pool and outputs alive."""
+
+    def __init__(self, ctx, h, rgb, rad, keep):
+        self.ctx, self.h, self.rgb, self.rad, self._keep = ctx, h, rgb, rad, keep
+
+    def run(self, stats=False):
+        st = _LearnedStats() if stats else None
+        self.ctx._check(self.ctx.L.pm_learned_graph_run(self.h, C.byref(st) if stats else None), "pm_learned_graph_run")
+        d = None if st is None else dict(tiles=st.tiles, fallback_tiles=st.fallback_tiles, requests=st.requests,
+                                         fallback_requests=st.fallback_requests)
+        return self.rgb, self.rad, d
+
+    def offset(self):
+        o = C.c_int64()
+        self.ctx._check(self.ctx.L.pm_learned_graph_offset(self.h, C.byref(o)), "pm_learned_graph_offset")
+        return o.value
+
+    def close(self):
+        if self.h:
+            self.ctx.L.pm_learned_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

@@ -311,6 +311,28 @@ typedef struct pm_learned_stats {
 int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, const pm_learned_opts* lopts,
                       uint8_t* out_rgb8, float* out_radiance, pm_learned_stats* out_stats);
 
+/* The learned frame as one replayable CUDA graph (no counterpart in the
+ * reference, whose frame is Drawer::draw_in_gpu, Drawer.cu:22-41): `steps`
+ * Adam steps on consecutive `batch`-sample slices of the training pool
+ * (device arrays, 3 floats per sample, the slicing of pm_cache_train_steps
+ * from pool_offset), then pm_render_learned's frame into out_rgb8 /
+ * out_radiance (device, fixed at creation; radiance optional).  The global
+ * map only (k_caustic must be 0 when a caustic map is built).  Creation runs
+ * one frame eagerly to load its kernels and puts the cache back as it was,
+ * then captures on the context's stream (which must not be the legacy default
+ * stream).  The graph reads the context's scene, photon map and cache: create
+ * it again after pm_set_scene, pm_build_grid or pm_cache_init.  Each run is
+ * one graph launch and one status check; out_stats optional. */
+typedef struct pm_learned_graph pm_learned_graph;
+int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, const pm_learned_opts* lopts,
+                            const float* pool_pos, const float* pool_nrm, const float* pool_target, int64_t pool_n,
+                            int64_t batch, int32_t steps, int64_t pool_offset, uint8_t* out_rgb8, float* out_radiance,
+                            pm_learned_graph** out);
+int pm_learned_graph_run(pm_learned_graph* graph, pm_learned_stats* out_stats);
+/* The pool offset the next frame's training starts at. */
+int pm_learned_graph_offset(pm_learned_graph* graph, int64_t* out_offset);
+void pm_learned_graph_destroy(pm_learned_graph* graph);
+
 /* Host copies of the FP32 master parameters (get / set, PM_CACHE_PARAMS floats). */
 int pm_cache_get_params(pm_ctx* ctx, float* out_params_host);
 int pm_cache_set_params(pm_ctx* ctx, const float* params_host);

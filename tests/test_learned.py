@@ -143,3 +143,56 @@ def test_rmse_against_fp64_oracle():
         print(f"\nrelative RMSE vs FP64 4-map reference: plain {rmse_plain:.4f} learned {rmse_learned:.4f} "
               f"({settings}); fidelity of plain to the FP64 same-map oracle {fidelity:.2e}; fallback {st}")
         assert rmse_learned <= rmse_plain, (settings, rmse_plain, rmse_learned, st)
+
+
+@pytest.mark.gpu
+def test_learned_graph_render_equals_learned_render(setup):
+    """The captured frame without training is pm_render_learned bit for bit."""
+    from photonmap import learned
+    ctx, cam, w = setup
+    _train(ctx, cam, w, 300)
+    S = learned.FRAME_SETTINGS
+    rgb, rad, st = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], **S)
+    g = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=None, steps=0, radiance=True, **S)
+    try:
+        for _ in range(2):                      # replays are identical
+            rgb_g, rad_g, st_g = g.run(stats=True)
+            assert st_g == st
+            assert torch.equal(rgb_g, rgb)
+            assert torch.equal(rad_g, rad)
+    finally:
+        g.close()
+
+
+@pytest.mark.gpu
+def test_learned_graph_training_follows_eager_training(setup):
+    """Frames of the graph train like cache_train_steps + render_learned: the
+    same pool slices, the same weights up to the order of the gradient sums."""
+    from photonmap import learned
+    ctx, cam, w = setup
+    pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=1 << 16, seed=2)
+    S = learned.FRAME_SETTINGS
+    frames, steps, batch = 3, 2, 16384
+    ctx.cache_init(seed=3, lr=1e-3, out_scale=pool.scale)
+    w0 = ctx.cache_params()
+    g = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=steps, batch=batch, offset=5000,
+                          radiance=True, **S)
+    try:
+        assert np.array_equal(ctx.cache_params(), w0)   # creating the graph leaves the cache as it was
+        for _ in range(frames):
+            _, rad_g, _ = g.run()
+        off_g = g.offset()
+        w_g = ctx.cache_params()
+        rad_g = rad_g.clone()
+    finally:
+        g.close()
+    ctx.cache_init(seed=3, lr=1e-3, out_scale=pool.scale)
+    assert np.array_equal(ctx.cache_params(), w0)
+    off = 5000
+    for _ in range(frames):
+        _, off = learned.cache_fit(ctx, pool, steps, batch=batch, offset=off, want_loss=False)
+        _, rad_e, _ = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], **S)
+    assert off_g == off
+    np.testing.assert_allclose(w_g, ctx.cache_params(), rtol=0, atol=5e-5)
+    a, b = rad_g.cpu().numpy(), rad_e.cpu().numpy()
+    assert np.abs(a - b).mean() <= 1e-3 * np.abs(b).mean()
