@@ -1,9 +1,11 @@
 // pm_learned_graph.cu -- the learned frame (online training + learned render)
 // captured once and replayed as one CUDA graph.
 //
-// One frame = `steps` Adam steps on consecutive batches of a training pool,
-// then the learned render of pm_render_learned (eye pass, cache inference,
-// exact probes, tile check, listed fallback gather, merge, resolve).  Every
+// One frame = `steps` Adam steps on consecutive batches of a training pool
+// and the learned render of pm_render_learned (eye pass, cache inference,
+// exact probes, tile check, listed fallback gather, merge, resolve); the
+// training runs on a second stream beside the eye pass and the probe gathers,
+// and inference waits for it.  Every
 // size that the host-driven path reads back between launches lives on the
 // device here: the eye pass's request count drives inference, the fallback
 // marking, the listed gather and the merge (persistent or grid-stride
@@ -44,6 +46,10 @@ struct pm_learned_graph {
     DevBuf req_a, req_b, req_c, counter, px_base, px_count, est_mlp, est_fb, est_g;
     DevBuf probe_pos, probe_nrm, probe_req, probe_est, tile_flag, counts, fb_list, state;
     int launches_per_frame = 0;
+    // training runs on a second stream beside the eye pass and the probe
+    // gathers (it needs neither; inference waits for it)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -70,12 +76,16 @@ Requests requests_of(pm_learned_graph* g) {
 // every launch of one frame, on ctx->st (captured or eager)
 int enqueue_frame(pm_learned_graph* g) {
     pm_ctx* ctx = g->ctx;
-    cudaStream_t st = ctx->st;
+    const cudaStream_t main_st = ctx->st;
     unsigned* status = P<unsigned>(ctx->status);
     const MlpNet net = cache_net(ctx);
     const pm_cache_opts& co = ctx->cache_opts;
     int launches = 0;
-    // online training on the pool
+    // online training on the pool, on the side stream: the eye pass leaves
+    // most SMs idle while its slowest pixels finish, and training fills them
+    CK(cudaEventRecord(g->fork, main_st));
+    CK(cudaStreamWaitEvent(g->side, g->fork, 0));
+    cudaStream_t st = g->side;
     for (int s = 0; s < g->steps; s++) {
         k_pool_wrap<<<1, 1, 0, st>>>(state_offset(g), g->pool_n, g->batch);
         CK(cudaGetLastError());
@@ -95,18 +105,13 @@ int enqueue_frame(pm_learned_graph* g) {
         CK(cudaGetLastError());
         launches += 5;
     }
+    CK(cudaEventRecord(g->join, st));
+    st = main_st;
     // the learned render
     const DevScene S = dev_scene(ctx);
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     const Requests R = requests_of(g);
     CK(eye_pass(S, g->cd, g->ro.max_depth, R, status, st));
-    MlpInputs in{};
-    in.n = g->cap;
-    in.rec_pos = R.a;
-    in.rec_nrm = R.b;
-    in.flag_mask = 1u;
-    in.n_dev = R.counter;
-    CK(mlp_infer(net, in, P<float>(g->est_mlp), status, ctx->sm_count, st));
     const int T = g->lo.tile, Pn = g->lo.probes;
     CK(learned_probes(g->cd, R, T, Pn, P<float4>(g->probe_pos), P<float4>(g->probe_nrm), P<uint32_t>(g->probe_req), st));
     GatherQueries PQ{};
@@ -116,6 +121,14 @@ int enqueue_frame(pm_learned_graph* g) {
     PQ.flag_mask = 1u;
     GatherOut PO{P<float>(g->probe_est), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), PQ, g->ro.r_global, g->ro.k_global, 0, PO, status, st));
+    CK(cudaStreamWaitEvent(st, g->join, 0));   // the trained weights for inference
+    MlpInputs in{};
+    in.n = g->cap;
+    in.rec_pos = R.a;
+    in.rec_nrm = R.b;
+    in.flag_mask = 1u;
+    in.n_dev = R.counter;
+    CK(mlp_infer(net, in, P<float>(g->est_mlp), status, ctx->sm_count, st));
     unsigned long long* counts = P<unsigned long long>(g->counts);
     CK(cudaMemsetAsync(counts, 0, 32, st));
     CK(learned_select(g->cd, R, g->cap, R.counter, T, Pn, P<uint32_t>(g->probe_req), P<float>(g->probe_est),
@@ -141,6 +154,9 @@ int enqueue_frame(pm_learned_graph* g) {
 void free_graph(pm_learned_graph* g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->fork) cudaEventDestroy(g->fork);
+    if (g->join) cudaEventDestroy(g->join);
+    if (g->side) cudaStreamDestroy(g->side);
     DevBuf* bufs[] = {&g->req_a, &g->req_b, &g->req_c, &g->counter, &g->px_base, &g->px_count, &g->est_mlp, &g->est_fb,
                       &g->est_g, &g->probe_pos, &g->probe_nrm, &g->probe_req, &g->probe_est, &g->tile_flag,
                       &g->counts, &g->fb_list, &g->state};
@@ -202,6 +218,10 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
         {&g->tile_flag, (size_t)g->ntiles}, {&g->counts, 32}, {&g->fb_list, (size_t)g->cap * 4}, {&g->state, 16}};
     for (const auto& a : allocs)
         if ((e = need(*a.b, a.bytes)) != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph buffers"));
+    if ((e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(cuda_fail(ctx, e, "learned graph streams"));
     // training state: the pool offset and the Adam step number
     const int64_t st_host[2] = {std::max<int64_t>(pool_offset, 0), 0};
     if ((e = cudaMemcpyAsync(g->state.p, st_host, 16, cudaMemcpyHostToDevice, ctx->st)) != cudaSuccess ||
