@@ -524,6 +524,7 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
         ctx->bvh_nodes = lbvh_node_count(T);
     }
 
+    ctx->has_scene = false;   // until the new scene is complete
     ENSURE(ctx->tri, rec.size() * 4);
     ENSURE(ctx->tri_pos, 9 * (size_t)T * 4);
     ENSURE(ctx->tri_nrm, 9 * (size_t)T * 4);
