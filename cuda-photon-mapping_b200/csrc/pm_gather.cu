@@ -328,10 +328,14 @@ struct WarpWalk {
             got += __popc(bm);
         }
         __syncwarp();
-        unsigned long long v = lane < got ? U.sel[lane] : ~0ull;
+        // the bin holds a handful of keys (unique): rank each against the
+        // others instead of sorting 32 lanes
+        const unsigned long long mine = lane < got ? U.sel[lane] : ~0ull;
         __syncwarp();
-        v = warp_sort32(v, lane);
-        return shfl_u64(v, k - (int)before - 1);
+        int rank = 0;
+        for (int j = 0; j < got; j++) rank += shfl_u64(mine, j) < mine ? 1 : 0;
+        const unsigned hit = __ballot_sync(0xffffffffu, lane < got && rank == k - (int)before - 1);
+        return shfl_u64(mine, __ffs(hit) - 1);
     }
 
     // Tighten the distance bound from the histogram alone (n > k): the k-th
