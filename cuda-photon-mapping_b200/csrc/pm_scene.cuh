@@ -15,8 +15,8 @@
 //     AABB passes for the ray (evaluated lazily, once per model per ray);
 //   * BVH node boxes are padded, and a node is skipped only when its entry
 //     distance is strictly larger than the best t, so no candidate that could
-//     win (including exact ties) is culled.  (The slab arithmetic uses
-//     box * (1/d) - o * (1/d); the padding dwarfs its rounding.)
+//     win (including exact ties) is culled.  (The slab arithmetic is
+//     fma(box, 1/d, -o/d); the padding dwarfs its rounding.)
 #pragma once
 #include "pm_device.cuh"
 
@@ -202,19 +202,23 @@ __device__ __forceinline__ void trav_init(Trav& T, V3 o, V3 d, Stk& stack) {
 template <class Stk>
 __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, Stk& stack) {
     int node = T.node, leaf = T.leaf, sp = T.sp;
-    const float ix = T.ix, iy = T.iy, iz = T.iz, ox = T.ox, oy = T.oy, oz = T.oz;
+    // Box slabs as fused multiply-adds: the boxes are padded far beyond the
+    // rounding of either form, so culling stays conservative and the answer
+    // (decided by the exact triangle tests) is the same; the fused form is
+    // half the instructions of the node test.
+    const float ix = T.ix, iy = T.iy, iz = T.iz, nox = -T.ox, noy = -T.oy, noz = -T.oz;
     while ((unsigned)node < (unsigned)TRAV_SENTINEL) {
         const float4* N = S.nodes + 4 * (size_t)node;
         const float4 a0 = __ldg(N), b0 = __ldg(N + 1), a1 = __ldg(N + 2), b1 = __ldg(N + 3);
         const float best_t = T.best_t;
-        float t0x = a0.x * ix - ox, t1x = b0.x * ix - ox;
-        float t0y = a0.y * iy - oy, t1y = b0.y * iy - oy;
-        float t0z = a0.z * iz - oz, t1z = b0.z * iz - oz;
+        float t0x = __fmaf_rn(a0.x, ix, nox), t1x = __fmaf_rn(b0.x, ix, nox);
+        float t0y = __fmaf_rn(a0.y, iy, noy), t1y = __fmaf_rn(b0.y, iy, noy);
+        float t0z = __fmaf_rn(a0.z, iz, noz), t1z = __fmaf_rn(b0.z, iz, noz);
         const float c0min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
         const float c0max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
-        t0x = a1.x * ix - ox; t1x = b1.x * ix - ox;
-        t0y = a1.y * iy - oy; t1y = b1.y * iy - oy;
-        t0z = a1.z * iz - oz; t1z = b1.z * iz - oz;
+        t0x = __fmaf_rn(a1.x, ix, nox); t1x = __fmaf_rn(b1.x, ix, nox);
+        t0y = __fmaf_rn(a1.y, iy, noy); t1y = __fmaf_rn(b1.y, iy, noy);
+        t0z = __fmaf_rn(a1.z, iz, noz); t1z = __fmaf_rn(b1.z, iz, noz);
         const float c1min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
         const float c1max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
         const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
