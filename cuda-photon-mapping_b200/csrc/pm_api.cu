@@ -64,6 +64,7 @@ DevScene dev_scene(pm_ctx* c) {
     S.tri_diffuse = c->has_tri_diffuse ? P<float>(c->tri_diffuse) : nullptr;
     S.nodes = P<float4>(c->nodes);
     S.prim = P<int>(c->prim);
+    S.tri_leaf = P<float4>(c->tri_leaf);
     S.maabb = P<float>(c->maabb);
     S.mats = P<float>(c->mats);
     S.ca = P<float>(c->ca);
@@ -204,7 +205,7 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
                       &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
                       &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list,
-                      &ctx->bvh_scratch};
+                      &ctx->bvh_scratch, &ctx->tri_leaf};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -552,6 +553,9 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
         release(ctx->bvh_scratch);
         if (int rc = check_status(ctx, "device BVH build")) return rc;
     }
+    ENSURE(ctx->tri_leaf, 80 * (size_t)T);
+    CK(bvh_leaf_records(P<float4>(ctx->tri), P<int>(ctx->prim), T, P<float4>(ctx->tri_leaf), ctx->st));
+    ctx->launches += 1;
     CK(cudaMemcpyAsync(ctx->maabb.p, maabb.data(), maabb.size() * 4, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->mats.p, sd->materials, 12 * (size_t)M * 4, cudaMemcpyHostToDevice, ctx->st));
     if (!ca.empty()) CK(cudaMemcpyAsync(ctx->ca.p, ca.data(), ca.size() * 4, cudaMemcpyHostToDevice, ctx->st));

@@ -59,7 +59,7 @@ struct pm_ctx {
     int bvh_builder = 0, scene_bvh_builder = 0;
     int64_t bvh_nodes = 0;
     float bvh_ms = 0.f;
-    pm::DevBuf bvh_scratch;
+    pm::DevBuf bvh_scratch, tri_leaf;
     pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts, fallback_list;
     pm_cache_opts cache_opts = {};
     float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};

@@ -250,7 +250,26 @@ Layout layout(int n) {
     return L;
 }
 
+__global__ void k_leaf_records(const float4* __restrict__ tri, const int* __restrict__ prim, int n,
+                               float4* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int t = prim[j];
+    if (t < 0 || t >= n) return;
+    const float4* src = tri + 5 * (size_t)t;
+    float4* dst = out + 5 * (size_t)j;
+    dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+    const float4 q4 = src[4];
+    dst[4] = make_float4(q4.x, q4.y, q4.z, __int_as_float(t));
+}
+
 }  // namespace
+
+cudaError_t bvh_leaf_records(const float4* tri, const int* prim, int ntri, float4* out, cudaStream_t st) {
+    if (ntri <= 0) return cudaSuccess;
+    k_leaf_records<<<blocks_of(ntri, 256), 256, 0, st>>>(tri, prim, ntri, out);
+    return cudaGetLastError();
+}
 
 size_t lbvh_scratch_bytes(int ntri) { return layout(ntri).total; }
 

@@ -24,7 +24,7 @@ namespace pm {
 
 // Triangle record: 5 float4 = 80 bytes
 //   q0 = (v0, n.v0)   q1 = (v1 - v0, 1/(n.n))   q2 = (v2, model bits)
-//   q3 = (v0 - v2, 0) q4 = (n, 0)             n = cross(v1 - v0, v2 - v0)
+//   q3 = (v0 - v2, 0) q4 = (n, 0 / in tri_leaf: the triangle index bits)   n = cross(v1 - v0, v2 - v0)
 struct DevScene {
     const float4* tri;        // 5 per triangle
     const float* tri_pos;     // 9 per triangle (vertex positions, as given)
@@ -32,6 +32,8 @@ struct DevScene {
     const float* tri_diffuse; // 3 per triangle or null
     const float4* nodes;      // 4 per interior node: both children's (lo, ref), (hi, -)
     const int* prim;          // leaf triangle indices
+    const float4* tri_leaf;   // the triangle records again in leaf order (record j = triangle prim[j],
+                              // its index in q4.w), so a leaf's triangles are contiguous
     const float* maabb;       // 6 per model (min xyz, max xyz)
     const float* mats;        // 12 per model
     const float* ca;          // critical angle table: (n1, n2, cos) triples
@@ -243,10 +245,10 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
         const int packed = ~leaf;
         const int first = packed >> 8, count = packed & 255;
         for (int i = 0; i < count; i++) {
-            const int tri = __ldg(S.prim + first + i);
-            const float4* Q = S.tri + 5 * (size_t)tri;
+            const float4* Q = S.tri_leaf + 5 * (size_t)(first + i);
             const int m = __float_as_int(__ldg(&Q[2].w));
             if (m < T.min_model) continue;
+            const int tri = __float_as_int(__ldg(&Q[4].w));
             float t; V3 uvw;
             if (!tri_test(Q, o, d, T.best_t, tri, T.best_tri, t, uvw)) continue;
             const bool zero = t == 0.0f;
