@@ -4,8 +4,8 @@
 // One frame = `steps` Adam steps on consecutive batches of a training pool
 // and the learned render of pm_render_learned (eye pass, cache inference,
 // exact probes, tile check, listed fallback gather, merge, resolve); the
-// training runs on a second stream beside the eye pass and the probe gathers,
-// and inference waits for it.  Every
+// training, then the cache inference (once the eye pass is done) run on a
+// second stream beside the eye pass and the probe gathers.  Every
 // size that the host-driven path reads back between launches lives on the
 // device here: the eye pass's request count drives inference, the fallback
 // marking, the listed gather and the merge (persistent or grid-stride
@@ -49,7 +49,7 @@ struct pm_learned_graph {
     // training runs on a second stream beside the eye pass and the probe
     // gathers (it needs neither; inference waits for it)
     cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr;
 };
 
 namespace {
@@ -105,13 +105,23 @@ int enqueue_frame(pm_learned_graph* g) {
         CK(cudaGetLastError());
         launches += 5;
     }
-    CK(cudaEventRecord(g->join, st));
     st = main_st;
-    // the learned render
+    // the learned render: eye pass, then the probe gathers here while the side
+    // stream (after its training) answers every request with the cache
     const DevScene S = dev_scene(ctx);
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     const Requests R = requests_of(g);
     CK(eye_pass(S, g->cd, g->ro.max_depth, R, status, st));
+    CK(cudaEventRecord(g->eye_done, st));
+    CK(cudaStreamWaitEvent(g->side, g->eye_done, 0));
+    MlpInputs in{};
+    in.n = g->cap;
+    in.rec_pos = R.a;
+    in.rec_nrm = R.b;
+    in.flag_mask = 1u;
+    in.n_dev = R.counter;
+    CK(mlp_infer(net, in, P<float>(g->est_mlp), status, ctx->sm_count, g->side));
+    CK(cudaEventRecord(g->join, g->side));
     const int T = g->lo.tile, Pn = g->lo.probes;
     CK(learned_probes(g->cd, R, T, Pn, P<float4>(g->probe_pos), P<float4>(g->probe_nrm), P<uint32_t>(g->probe_req), st));
     GatherQueries PQ{};
@@ -121,14 +131,7 @@ int enqueue_frame(pm_learned_graph* g) {
     PQ.flag_mask = 1u;
     GatherOut PO{P<float>(g->probe_est), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), PQ, g->ro.r_global, g->ro.k_global, 0, PO, status, st));
-    CK(cudaStreamWaitEvent(st, g->join, 0));   // the trained weights for inference
-    MlpInputs in{};
-    in.n = g->cap;
-    in.rec_pos = R.a;
-    in.rec_nrm = R.b;
-    in.flag_mask = 1u;
-    in.n_dev = R.counter;
-    CK(mlp_infer(net, in, P<float>(g->est_mlp), status, ctx->sm_count, st));
+    CK(cudaStreamWaitEvent(st, g->join, 0));   // the cache's answers
     unsigned long long* counts = P<unsigned long long>(g->counts);
     CK(cudaMemsetAsync(counts, 0, 32, st));
     CK(learned_select(g->cd, R, g->cap, R.counter, T, Pn, P<uint32_t>(g->probe_req), P<float>(g->probe_est),
@@ -156,6 +159,7 @@ void free_graph(pm_learned_graph* g) {
     if (g->graph) cudaGraphDestroy(g->graph);
     if (g->fork) cudaEventDestroy(g->fork);
     if (g->join) cudaEventDestroy(g->join);
+    if (g->eye_done) cudaEventDestroy(g->eye_done);
     if (g->side) cudaStreamDestroy(g->side);
     DevBuf* bufs[] = {&g->req_a, &g->req_b, &g->req_c, &g->counter, &g->px_base, &g->px_count, &g->est_mlp, &g->est_fb,
                       &g->est_g, &g->probe_pos, &g->probe_nrm, &g->probe_req, &g->probe_est, &g->tile_flag,
@@ -220,7 +224,8 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
         if ((e = need(*a.b, a.bytes)) != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph buffers"));
     if ((e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess)
+        (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g->eye_done, cudaEventDisableTiming)) != cudaSuccess)
         return bail(cuda_fail(ctx, e, "learned graph streams"));
     // training state: the pool offset and the Adam step number
     const int64_t st_host[2] = {std::max<int64_t>(pool_offset, 0), 0};
