@@ -160,6 +160,78 @@ int render_checks(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o) {
     return PM_OK;
 }
 
+int64_t eye_block_order(const pm_ctx* ctx, const pm_camera* cam, std::vector<int>& order) {
+    const int W = cam->width, H = cam->height;
+    const int64_t npx = (int64_t)W * H, nb = eye_blocks(npx), T = eye_threads();
+    // the kernel's camera: direction(u, v) = A + hor u + ver v, A = llc - pos
+    double pos[3], hor[3], ver[3], A[3];
+    for (int a = 0; a < 3; a++) {
+        pos[a] = cam->position[a];
+        hor[a] = (double)cam->right[a] * cam->viewport_w;
+        ver[a] = (double)cam->up[a] * cam->viewport_h;
+        A[a] = (pos[a] + cam->forward[a]) * cam->focal - 0.5 * hor[a] - 0.5 * ver[a] - pos[a];
+    }
+    auto cross = [](const double* x, const double* y, double* z) {
+        z[0] = x[1] * y[2] - x[2] * y[1]; z[1] = x[2] * y[0] - x[0] * y[2]; z[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    auto dot = [](const double* x, const double* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    double hv[3];
+    cross(hor, ver, hv);
+    struct Rect { int x0, x1, y0, y1; };
+    std::vector<Rect> rects;
+    const int M = (int)ctx->h_mats.size() / 12;
+    for (int m = 0; m < M; m++) {
+        const float* mt = &ctx->h_mats[12 * (size_t)m];
+        const bool deep = mt[3] > 0.f || mt[4] > 0.f || mt[5] > 0.f || mt[10] < 1.f;
+        if (!deep) continue;
+        const float* bx = &ctx->h_maabb[6 * (size_t)m];
+        if (bx[0] > bx[3]) continue;   // a model without triangles
+        double u0 = 1e30, u1 = -1e30, v0 = 1e30, v1 = -1e30;
+        bool whole = false;
+        for (int c = 0; c < 8 && !whole; c++) {
+            double D[3] = {(c & 1 ? bx[3] : bx[0]) - pos[0], (c & 2 ? bx[4] : bx[1]) - pos[1],
+                           (c & 4 ? bx[5] : bx[2]) - pos[2]};
+            // s D - u hor - v ver = A  (Cramer's rule)
+            const double det = dot(D, hv);
+            if (!(std::fabs(det) > 1e-12)) { whole = true; break; }
+            const double sc = dot(A, hv) / det;
+            double t[3];
+            cross(A, ver, t);
+            const double u = -dot(D, t) / det;   // det[D, A, -ver] / det
+            cross(hor, A, t);
+            const double v = -dot(D, t) / det;   // det[D, -hor, A] / det
+            if (!(sc > 0.0)) { whole = true; break; }
+            u0 = std::min(u0, u); u1 = std::max(u1, u); v0 = std::min(v0, v); v1 = std::max(v1, v);
+        }
+        if (whole) { order.resize((size_t)nb); for (int64_t b = 0; b < nb; b++) order[(size_t)b] = (int)b; return nb; }
+        Rect r;
+        r.x0 = (int)std::max(0.0, std::floor(u0 * W - 0.5) - 1.0);
+        r.x1 = (int)std::min((double)W - 1, std::ceil(u1 * W - 0.5) + 1.0);
+        r.y0 = (int)std::max(0.0, std::floor(v0 * H - 0.5) - 1.0);
+        r.y1 = (int)std::min((double)H - 1, std::ceil(v1 * H - 0.5) + 1.0);
+        if (r.x0 <= r.x1 && r.y0 <= r.y1) rects.push_back(r);
+    }
+    order.clear();
+    order.reserve((size_t)nb);
+    std::vector<int> rest;
+    rest.reserve((size_t)nb);
+    for (int64_t b = 0; b < nb; b++) {
+        const int64_t p0 = b * T, p1 = std::min(p0 + T - 1, npx - 1);
+        const int r0 = (int)(p0 / W), r1 = (int)(p1 / W);
+        bool hot = false;
+        for (const Rect& r : rects) {
+            if (r1 < r.y0 || r0 > r.y1) continue;
+            if (r0 != r1) { hot = true; break; }
+            const int c0 = (int)(p0 % W), c1 = (int)(p1 % W);
+            if (c1 >= r.x0 && c0 <= r.x1) { hot = true; break; }
+        }
+        (hot ? order : rest).push_back((int)b);
+    }
+    const int64_t first = (int64_t)order.size();
+    order.insert(order.end(), rest.begin(), rest.end());
+    return first;
+}
+
 }  // namespace pm
 
 extern "C" {
@@ -205,7 +277,7 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
                       &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
                       &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list,
-                      &ctx->bvh_scratch, &ctx->tri_leaf};
+                      &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -576,6 +648,9 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
     std::memcpy(ctx->aabb, aabb, sizeof aabb);
     ctx->has_scene = true;
     ctx->scene_bvh_builder = device_bvh ? PM_BVH_DEVICE_LBVH : PM_BVH_HOST_SAH;
+    ctx->h_maabb = maabb;
+    ctx->eye_order_valid = false;
+    ctx->h_mats.assign(sd->materials, sd->materials + 12 * (size_t)M);
     ctx->yield_g = ctx->yield_c = 0.0;
     ctx->yield_bounces = 0;
     for (auto& m : ctx->maps) { m.built = false; m.n = 0; }
@@ -1000,8 +1075,16 @@ int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, Frame
     R.counter = P<unsigned long long>(ctx->req_counter);
     R.px_base = P<uint32_t>(ctx->px_base);
     R.px_count = P<uint32_t>(ctx->px_count);
+    if (!ctx->eye_order_valid || std::memcmp(&ctx->eye_order_cam, cam, sizeof *cam) != 0) {
+        std::vector<int> order;
+        eye_block_order(ctx, cam, order);
+        ENSURE(ctx->eye_order, order.size() * 4);
+        CK(cudaMemcpyAsync(ctx->eye_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+        ctx->eye_order_cam = *cam;
+        ctx->eye_order_valid = true;
+    }
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
-    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), ctx->st));
+    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), ctx->st, P<int>(ctx->eye_order)));
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
     unsigned long long nreq = 0;
     CK(cudaMemcpyAsync(&nreq, R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));

@@ -3,6 +3,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <vector>
 #include <cuda_runtime.h>
 #include "../../include/pm_api.h"
 #include "pm_gather.cuh"
@@ -60,6 +61,11 @@ struct pm_ctx {
     int64_t bvh_nodes = 0;
     float bvh_ms = 0.f;
     pm::DevBuf bvh_scratch, tri_leaf;
+    // host copies for the eye pass's block order: 6 AABB floats and 12 material floats per model
+    std::vector<float> h_maabb, h_mats;
+    pm::DevBuf eye_order;
+    bool eye_order_valid = false;   // eye_order holds the order for eye_order_cam on this scene
+    pm_camera eye_order_cam = {};
     pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts, fallback_list;
     pm_cache_opts cache_opts = {};
     float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};
@@ -93,6 +99,12 @@ GatherGrid grid_of(MapState& m, MapState& est_src);
 MlpNet cache_net(pm_ctx* ctx);
 // a frame's checks: scene, grid, camera size, depth and k ranges
 int render_checks(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o);
+// Launch order of the eye pass's pixel blocks (eye_blocks entries): first the
+// blocks that overlap the screen rectangle of a specular or refractive model
+// (their pixels spawn chains of reflected / refracted rays, the longest jobs
+// of the pass), then the others, each part in image order.  Returns the
+// number of blocks put first.
+int64_t eye_block_order(const pm_ctx* ctx, const pm_camera* cam, std::vector<int>& order);
 // the learned render's option checks (PM_OK or the failure recorded on ctx)
 int learned_checks(pm_ctx* ctx, const pm_learned_opts* lo);
 

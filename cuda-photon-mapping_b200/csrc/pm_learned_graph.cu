@@ -44,7 +44,7 @@ struct pm_learned_graph {
     int steps = 0;
     // device buffers owned by the graph
     DevBuf req_a, req_b, req_c, counter, px_base, px_count, est_mlp, est_fb, est_g;
-    DevBuf probe_pos, probe_nrm, probe_req, probe_est, tile_flag, counts, fb_list, state;
+    DevBuf probe_pos, probe_nrm, probe_req, probe_est, tile_flag, counts, fb_list, state, eye_order;
     int launches_per_frame = 0;
     // training runs on a second stream beside the eye pass and the probe
     // gathers (it needs neither; inference waits for it)
@@ -111,7 +111,7 @@ int enqueue_frame(pm_learned_graph* g) {
     const DevScene S = dev_scene(ctx);
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     const Requests R = requests_of(g);
-    CK(eye_pass(S, g->cd, g->ro.max_depth, R, status, st));
+    CK(eye_pass(S, g->cd, g->ro.max_depth, R, status, st, P<int>(g->eye_order)));
     CK(cudaEventRecord(g->eye_done, st));
     CK(cudaStreamWaitEvent(g->side, g->eye_done, 0));
     MlpInputs in{};
@@ -163,7 +163,7 @@ void free_graph(pm_learned_graph* g) {
     if (g->side) cudaStreamDestroy(g->side);
     DevBuf* bufs[] = {&g->req_a, &g->req_b, &g->req_c, &g->counter, &g->px_base, &g->px_count, &g->est_mlp, &g->est_fb,
                       &g->est_g, &g->probe_pos, &g->probe_nrm, &g->probe_req, &g->probe_est, &g->tile_flag,
-                      &g->counts, &g->fb_list, &g->state};
+                      &g->counts, &g->fb_list, &g->state, &g->eye_order};
     for (DevBuf* b : bufs) release(*b);
     delete g;
 }
@@ -227,6 +227,14 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
         (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->eye_done, cudaEventDisableTiming)) != cudaSuccess)
         return bail(cuda_fail(ctx, e, "learned graph streams"));
+    // the eye pass's block order (slow blocks first), fixed with the camera
+    std::vector<int> order;
+    eye_block_order(ctx, cam, order);
+    if ((e = need(g->eye_order, order.size() * 4)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(g->eye_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, ctx->st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->st)) != cudaSuccess)
+        return bail(cuda_fail(ctx, e, "learned graph eye order"));
     // training state: the pool offset and the Adam step number
     const int64_t st_host[2] = {std::max<int64_t>(pool_offset, 0), 0};
     if ((e = cudaMemcpyAsync(g->state.p, st_host, 16, cudaMemcpyHostToDevice, ctx->st)) != cudaSuccess ||

@@ -254,9 +254,10 @@ __device__ __forceinline__ void eye_emit(Requests& R, bool valid, int64_t gi, in
 }
 
 __global__ void __launch_bounds__(EYE_THREADS)
-k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status) {
+k_eye(DevScene S, CameraDev cam, int D, Requests R, unsigned* status, const int* __restrict__ order) {
     const int64_t npx = (int64_t)cam.W * cam.H;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t blk = order ? (int64_t)order[blockIdx.x] : (int64_t)blockIdx.x;
+    const int64_t i = blk * blockDim.x + threadIdx.x;
     const bool valid = i < npx;
     float4 ha[RENDER_MAX_HITS], hb[RENDER_MAX_HITS], hc[RENDER_MAX_HITS];
     const int nh = valid ? eye_hits(S, cam, D, i, (uint32_t)i, ha, hb, hc, status) : 0;
@@ -341,13 +342,16 @@ __global__ void k_resolve_multi(const RenderInstDev* __restrict__ tab, const int
 
 }  // namespace
 
+int64_t eye_blocks(int64_t npx) { return (npx + EYE_THREADS - 1) / EYE_THREADS; }
+int eye_threads() { return EYE_THREADS; }
+
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
-                     cudaStream_t st) {
+                     cudaStream_t st, const int* block_order) {
     if (max_depth < 0 || max_depth > RENDER_MAX_DEPTH) return cudaErrorInvalidValue;
     const int64_t npx = (int64_t)cam.W * cam.H;
     cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
     if (e != cudaSuccess) return e;
-    k_eye<<<(unsigned)((npx + EYE_THREADS - 1) / EYE_THREADS), EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status);
+    k_eye<<<(unsigned)eye_blocks(npx), EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status, block_order);
     return cudaGetLastError();
 }
 

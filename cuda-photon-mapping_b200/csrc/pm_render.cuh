@@ -28,8 +28,13 @@ struct Requests {
     uint32_t* px_count;            // requests of each pixel (hit order)
 };
 
+// block_order (optional, eye_blocks(cam) entries): the pixel block each thread
+// block of the launch takes (a permutation), e.g. the slow ones first.
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
-                     cudaStream_t st);
+                     cudaStream_t st, const int* block_order = nullptr);
+// pixel blocks of the eye pass (EYE_THREADS consecutive pixels each)
+int64_t eye_blocks(int64_t npx);
+int eye_threads();
 
 // ---- several instances in one launch: global pixel g of instance i lies in
 // [px_off[i], px_off[i+1]); requests and outputs are indexed by global pixel ----
