@@ -63,15 +63,17 @@ constexpr int COUNT_THREADS = 1024;
 constexpr int COUNT_CHUNK = 65535;
 constexpr int COUNT_SMEM_WORDS = 56 * 1024;   // 224 KB: 114,688 16-bit counters
 
+// Photons [blockIdx.x * chunk, ... + chunk) (chunk <= COUNT_CHUNK, so no
+// 16-bit counter can overflow).
 __global__ void __launch_bounds__(COUNT_THREADS)
-k_count_cells_smem(const float* __restrict__ pos, int64_t n, GridGeom ga, GridGeom gb, int two, int cells_a,
-                   int cells_b, uint32_t* __restrict__ ca, uint32_t* __restrict__ cb) {
+k_count_cells_smem(const float* __restrict__ pos, int64_t n, int64_t chunk, GridGeom ga, GridGeom gb, int two,
+                   int cells_a, int cells_b, uint32_t* __restrict__ ca, uint32_t* __restrict__ cb) {
     extern __shared__ uint32_t h16[];
     const int words_a = (cells_a + 1) >> 1, words = words_a + (two ? (cells_b + 1) >> 1 : 0);
     for (int i = threadIdx.x; i < words; i += COUNT_THREADS) h16[i] = 0u;
     __syncthreads();
-    const int64_t first = (int64_t)blockIdx.x * COUNT_CHUNK;
-    const int64_t last = min(first + (int64_t)COUNT_CHUNK, n);
+    const int64_t first = (int64_t)blockIdx.x * chunk;
+    const int64_t last = min(first + chunk, n);
     for (int64_t i = first + threadIdx.x; i < last; i += COUNT_THREADS) {
         const float* p = pos + 3 * i;
         const float x = p[0], y = p[1], z = p[2];
@@ -419,8 +421,15 @@ cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int reg
         const int smem = (int)smem_words * 4;
         if ((e = cudaFuncSetAttribute(k_count_cells_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
             return e;
-        k_count_cells_smem<<<blocks_for(n, COUNT_CHUNK), COUNT_THREADS, smem, st>>>(
-            B.pos, n, geom(pa), geom(pb), two ? 1 : 0, (int)pa.cells, (int)pb.cells, B.cell_sizes, B.counts2);
+        // one block per SM at this shared-memory size: whole waves of equal chunks
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t least = blocks_for(n, COUNT_CHUNK);
+        const int64_t nblk = (least + sms - 1) / sms * sms;
+        const int64_t chunk = (n + nblk - 1) / nblk;
+        k_count_cells_smem<<<(unsigned)blocks_for(n, (int)chunk), COUNT_THREADS, smem, st>>>(
+            B.pos, n, chunk, geom(pa), geom(pb), two ? 1 : 0, (int)pa.cells, (int)pb.cells, B.cell_sizes, B.counts2);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         k_count_max<<<std::min<int64_t>(blocks_for(std::max(pa.cells, pb.cells), 256), 296), 256, 0, st>>>(
             B.cell_sizes, pa.cells, B.counts2, two ? pb.cells : 0, B.small);
