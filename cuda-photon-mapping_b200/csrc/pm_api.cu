@@ -78,6 +78,7 @@ DevScene dev_scene(pm_ctx* c) {
 }
 
 int check_status(pm_ctx* ctx, const char* what) {
+    if (int rc = cache_fence(ctx)) return rc;
     uint32_t bits = 0;
     CK(cudaMemcpyAsync(&bits, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -126,6 +127,14 @@ GatherGrid grid_of(MapState& m, MapState& est_src) {
     G.cell = m.cell;
     G.S = m.S;
     return G;
+}
+
+int cache_fence(pm_ctx* ctx) {
+    if (ctx->train_pending) {
+        CK(cudaStreamWaitEvent(ctx->st, ctx->train_done, 0));
+        ctx->train_pending = false;
+    }
+    return PM_OK;
 }
 
 MlpNet cache_net(pm_ctx* ctx) {
@@ -269,6 +278,12 @@ void pm_destroy(pm_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
+    if (ctx->train_st) {
+        cudaStreamSynchronize(ctx->train_st);
+        cudaStreamDestroy(ctx->train_st);
+    }
+    if (ctx->train_fork) cudaEventDestroy(ctx->train_fork);
+    if (ctx->train_done) cudaEventDestroy(ctx->train_done);
     DevBuf* bufs[] = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
                       &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage_pos, &ctx->stage_dir,
                       &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
@@ -294,6 +309,7 @@ const char* pm_last_error(const pm_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 
 int pm_sync(pm_ctx* ctx) {
     if (!ctx) return PM_ERR_INVALID;
+    if (int rc = cache_fence(ctx)) return rc;
     CK(cudaStreamSynchronize(ctx->st));
     return PM_OK;
 }
@@ -324,17 +340,17 @@ MlpInputs cache_inputs(const float* pos, const float* nrm, int64_t n) {
 
 // loss and gradient of n samples into ctx->cache_grad (zeroed first); loss_out: mean squared error
 int cache_backprop(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
-                   int64_t n, float* loss_out) {
-    CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
-    CK(cudaMemsetAsync(ctx->cache_loss.p, 0, 4, ctx->st));
+                   int64_t n, float* loss_out, cudaStream_t st) {
+    CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, st));
+    CK(cudaMemsetAsync(ctx->cache_loss.p, 0, 4, st));
     const float grad_scale = 2.f / (3.f * (float)n);
     CK(mlp_train(cache_net(ctx), cache_inputs(pos, nrm, n), target, weight, grad_scale, P<float>(ctx->cache_grad),
-                 P<float>(ctx->cache_loss), P<unsigned>(ctx->status), ctx->sm_count, ctx->st));
+                 P<float>(ctx->cache_loss), P<unsigned>(ctx->status), ctx->sm_count, st));
     ctx->launches += 1;
     if (loss_out) {
         float l = 0.f;
-        CK(cudaMemcpyAsync(&l, ctx->cache_loss.p, 4, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        CK(cudaMemcpyAsync(&l, ctx->cache_loss.p, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
         *loss_out = l / (3.f * (float)n);
     }
     return PM_OK;
@@ -355,6 +371,7 @@ int pm_cache_init(pm_ctx* ctx, const pm_cache_opts* o) {
         !(o->eps > 0.f) || !(o->out_scale > 0.f) || o->octave0 < 0 || o->octave0 > 8)
         return fail(ctx, PM_ERR_INVALID, "cache options: lr >= 0, 0 <= beta < 1, eps > 0, out_scale > 0, octave0 0..8");
     CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_fence(ctx)) return rc;
     const float* box = o->aabb;
     bool zero = true;
     for (int a = 0; a < 6; a++) zero = zero && box[a] == 0.f;
@@ -405,7 +422,8 @@ int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const f
     if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
     if (n <= 0 || !pos || !nrm || !target) return fail(ctx, PM_ERR_INVALID, "cache train: n > 0 and sample arrays required");
     CK(cudaSetDevice(ctx->device));
-    if (int rc = cache_backprop(ctx, pos, nrm, target, weight, n, out_loss)) return rc;
+    if (int rc = cache_fence(ctx)) return rc;
+    if (int rc = cache_backprop(ctx, pos, nrm, target, weight, n, out_loss, ctx->st)) return rc;
     ctx->cache_step++;
     const pm_cache_opts& o = ctx->cache_opts;
     CK(mlp_adam(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), P<float>(ctx->cache_grad),
@@ -424,21 +442,42 @@ int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const 
     const int64_t b = std::min(batch, n);
     int64_t off = inout_offset ? std::max<int64_t>(*inout_offset, 0) : 0;
     const pm_cache_opts& o = ctx->cache_opts;
+    // Without a loss to report, the steps go to the context's training stream
+    // (after everything queued so far) and the call returns: work issued next
+    // that does not touch the cache (an eye pass, a photon pass) runs beside
+    // them, and whatever touches the cache or synchronises waits for them.
+    cudaStream_t st = ctx->st;
+    if (!out_loss && steps > 0) {
+        if (!ctx->train_st) {
+            CK(cudaStreamCreateWithFlags(&ctx->train_st, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ctx->train_fork, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->train_done, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(ctx->train_fork, ctx->st));
+        CK(cudaStreamWaitEvent(ctx->train_st, ctx->train_fork, 0));
+        st = ctx->train_st;
+    } else if (int rc = cache_fence(ctx)) {
+        return rc;
+    }
     for (int s = 0; s < steps; ++s) {
         if (off + b > n) off = 0;
         if (int rc = cache_backprop(ctx, pos + off * 3, nrm + off * 3, target + off * 3, weight ? weight + off : nullptr,
-                                    b, s + 1 == steps ? out_loss : nullptr))
+                                    b, s + 1 == steps ? out_loss : nullptr, st))
             return rc;
         ctx->cache_step++;
         CK(mlp_adam(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), P<float>(ctx->cache_grad),
                     P<float>(ctx->cache_m), P<float>(ctx->cache_v), ctx->cache_step, o.lr, o.beta1, o.beta2, o.eps,
-                    ctx->st));
+                    st));
         ctx->launches += 1;
         off += b;
     }
     if (inout_offset) *inout_offset = off;
-    // without a loss to report the steps stay queued: their device status is
-    // reported by the next call on the context that synchronises
+    if (st != ctx->st) {
+        CK(cudaEventRecord(ctx->train_done, st));
+        ctx->train_pending = true;
+        // the steps' device status is reported by the next call that synchronises
+        return PM_OK;
+    }
     return out_loss ? check_status(ctx, "cache train steps") : PM_OK;
 }
 
@@ -448,7 +487,8 @@ int pm_cache_gradient(pm_ctx* ctx, const float* pos, const float* nrm, const flo
     if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
     if (n <= 0 || !pos || !nrm || !target) return fail(ctx, PM_ERR_INVALID, "cache gradient: n > 0 and sample arrays required");
     CK(cudaSetDevice(ctx->device));
-    if (int rc = cache_backprop(ctx, pos, nrm, target, weight, n, out_loss)) return rc;
+    if (int rc = cache_fence(ctx)) return rc;
+    if (int rc = cache_backprop(ctx, pos, nrm, target, weight, n, out_loss, ctx->st)) return rc;
     CK(cudaMemcpyAsync(out_grad_host, ctx->cache_grad.p, (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -460,6 +500,7 @@ int pm_cache_infer(pm_ctx* ctx, const float* pos, const float* nrm, int64_t n, f
     if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
     if (n < 0 || (n > 0 && (!pos || !nrm || !out_rgb))) return fail(ctx, PM_ERR_INVALID, "cache infer: bad arguments");
     CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_fence(ctx)) return rc;
     CK(mlp_infer(cache_net(ctx), cache_inputs(pos, nrm, n), out_rgb, P<unsigned>(ctx->status), ctx->sm_count, ctx->st));
     if (n > 0) ctx->launches += 1;
     return check_status(ctx, "cache infer");
@@ -469,6 +510,7 @@ int pm_cache_get_params(pm_ctx* ctx, float* out) {
     if (!ctx || !out) return PM_ERR_INVALID;
     if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
     CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_fence(ctx)) return rc;
     CK(cudaMemcpyAsync(out, ctx->cache_w32.p, (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return PM_OK;
@@ -478,6 +520,7 @@ int pm_cache_set_params(pm_ctx* ctx, const float* in) {
     if (!ctx || !in) return PM_ERR_INVALID;
     if (!ctx->has_cache) return fail(ctx, PM_ERR_INVALID, "cache not initialised");
     CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_fence(ctx)) return rc;
     CK(cudaMemcpyAsync(ctx->cache_w32.p, in, (size_t)PM_CACHE_PARAMS * 4, cudaMemcpyHostToDevice, ctx->st));
     CK(mlp_to_bf16(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -1162,7 +1205,8 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     ENSURE(ctx->learned_counts, 32);   // flagged tiles, fallback requests, gather work counter
     ENSURE(ctx->fallback_list, (size_t)std::max<int64_t>(F.nreq, 1) * 4);
     CK(cudaEventRecord(ctx->ev[6], ctx->st));
-    // the cache answers every global request
+    // the cache answers every global request (after training still queued)
+    if (int rc = cache_fence(ctx)) return rc;
     MlpInputs in{};
     in.n = F.nreq; in.rec_pos = F.R.a; in.rec_nrm = F.R.b; in.flag_mask = 1u;
     CK(mlp_infer(cache_net(ctx), in, P<float>(ctx->est_mlp), P<unsigned>(ctx->status), ctx->sm_count, ctx->st));

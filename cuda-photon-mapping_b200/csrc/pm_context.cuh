@@ -64,6 +64,11 @@ struct pm_ctx {
     // host copies for the eye pass's block order: 6 AABB floats and 12 material floats per model
     std::vector<float> h_maabb, h_mats;
     pm::DevBuf eye_order;
+    // training steps queued without a loss run on their own stream; whatever
+    // reads or writes the cache (or synchronises the context) waits for them
+    cudaStream_t train_st = nullptr;
+    cudaEvent_t train_fork = nullptr, train_done = nullptr;
+    bool train_pending = false;
     bool eye_order_valid = false;   // eye_order holds the order for eye_order_cam on this scene
     pm_camera eye_order_cam = {};
     pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts, fallback_list;
@@ -95,6 +100,8 @@ int check_status(pm_ctx* ctx, const char* what);
 float elapsed(cudaEvent_t a, cudaEvent_t b);
 // gather view of map m, estimates read from est_src's direction / power arrays
 GatherGrid grid_of(MapState& m, MapState& est_src);
+// order the context's stream after the training steps still queued on the training stream
+int cache_fence(pm_ctx* ctx);
 // the radiance cache's network as the kernels read it
 MlpNet cache_net(pm_ctx* ctx);
 // a frame's checks: scene, grid, camera size, depth and k ranges

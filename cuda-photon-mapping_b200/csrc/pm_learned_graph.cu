@@ -190,6 +190,7 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
     if (steps < 0 || (steps > 0 && (!pool_pos || !pool_nrm || !pool_target || pool_n <= 0 || batch <= 0)))
         return fail(ctx, PM_ERR_INVALID, "learned graph: steps >= 0; with steps, a pool (n > 0) and batch > 0");
     CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_fence(ctx)) return rc;
     pm_learned_graph* g = new pm_learned_graph();
     g->ctx = ctx;
     g->ro = *o;
@@ -283,6 +284,7 @@ int pm_learned_graph_run(pm_learned_graph* g, pm_learned_stats* out_stats) {
     if (!g) return PM_ERR_INVALID;
     pm_ctx* ctx = g->ctx;
     CK(cudaSetDevice(ctx->device));
+    if (int rc = cache_fence(ctx)) return rc;
     // the step number follows the context's (training calls between frames count too)
     CK(cudaMemcpyAsync(state_step(g), &ctx->cache_step, 4, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaGraphLaunch(g->exec, ctx->st));

@@ -267,9 +267,13 @@ int pm_cache_train_step(pm_ctx* ctx, const float* pos, const float* nrm, const f
  * would run past n; *inout_offset receives the next offset.  No host
  * synchronisation between steps.  With out_loss set, the call waits for the
  * steps, checks their device status and stores the last step's loss (as
- * pm_cache_train_step reports it); with out_loss null it returns once the
- * steps are queued on the context's stream, and a device-side failure of
- * theirs is reported by the next synchronising call on the context. */
+ * pm_cache_train_step reports it).  With out_loss null it returns once the
+ * steps are queued, on the context's own training stream after everything
+ * queued so far: work issued next that does not touch the cache (a photon
+ * pass, the eye pass of pm_render_learned) runs beside them, every call that
+ * reads or writes the cache or synchronises the context waits for them, and
+ * a device-side failure of theirs is reported by the next synchronising call.
+ * The sample arrays must stay valid until then. */
 int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const float* target, const float* weight,
                          int64_t n, int64_t batch, int steps, int64_t* inout_offset, float* out_loss);
 
