@@ -427,9 +427,11 @@ def run_ours(args):
     host_rgb = torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True)
 
     def step(i, e2e=False):
-        ctx.trace_photons(w["seed"] + 1000 * rank + i, w["max_bounces"], w["photons"])
-        ctx.build_grid(0)
-        ctx.render(cam, w["k"], w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb)
+        # pm_frame: photon pass, grid build and frame in one call (the eye pass
+        # runs beside the grid build); same photons and image as
+        # trace_photons + build_grid + render
+        ctx.frame(w["seed"] + 1000 * rank + i, w["max_bounces"], w["photons"], cam, w["k"], w["radius"],
+                  w["max_depth"], radiance=False, out_rgb8=rgb)
         if e2e:
             host_rgb.copy_(rgb, non_blocking=True)
 
@@ -499,7 +501,8 @@ def run_ours(args):
             "data": "synthetic (seeded procedural scene, seeded Philox photon streams)",
             "config": {"workload": args.workload, "photons": w["photons"], "max_bounces": w["max_bounces"],
                        "image": f"{W}x{H}", "k": w["k"], "radius": w["radius"], "eye_depth": w["max_depth"],
-                       "triangles": sc.ntri, "bvh": bvh, "l2": "inputs larger than L2 (photon map ~0.5 GB)",
+                       "triangles": sc.ntri, "bvh": bvh, "api": "pm_frame (photon pass + grid + frame)",
+                       "l2": "inputs larger than L2 (photon map ~0.5 GB)",
                        "parallelism": f"replicas{world}"},
             "stages_ms": {"trace": stages[0], "grid": stages[1], "eye": stages[2], "gather": stages[3],
                           "resolve": stages[4]},

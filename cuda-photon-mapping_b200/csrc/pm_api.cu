@@ -282,6 +282,12 @@ void pm_destroy(pm_ctx* ctx) {
         cudaStreamSynchronize(ctx->train_st);
         cudaStreamDestroy(ctx->train_st);
     }
+    if (ctx->frame_st) {
+        cudaStreamSynchronize(ctx->frame_st);
+        cudaStreamDestroy(ctx->frame_st);
+    }
+    if (ctx->frame_fork) cudaEventDestroy(ctx->frame_fork);
+    if (ctx->frame_done) cudaEventDestroy(ctx->frame_done);
     if (ctx->train_fork) cudaEventDestroy(ctx->train_fork);
     if (ctx->train_done) cudaEventDestroy(ctx->train_done);
     DevBuf* bufs[] = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
@@ -1091,8 +1097,8 @@ struct FrameSetup {
 };
 
 
-// buffers, eye pass (timed into ev[4] .. ev[5]) and the request count
-int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F) {
+// buffers and the eye pass on stream st (timed into ev[4] .. ev[5])
+int render_eye_launch(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F, cudaStream_t st) {
     MapState& C = ctx->maps[PM_MAP_CAUSTIC];
     F.npx = (int64_t)cam->width * cam->height;
     const int64_t per_px = ((int64_t)1 << std::max(o->max_depth, 1)) - 1;
@@ -1122,21 +1128,32 @@ int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, Frame
         std::vector<int> order;
         eye_block_order(ctx, cam, order);
         ENSURE(ctx->eye_order, order.size() * 4);
-        CK(cudaMemcpyAsync(ctx->eye_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->eye_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
         ctx->eye_order_cam = *cam;
         ctx->eye_order_valid = true;
     }
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
-    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), ctx->st, P<int>(ctx->eye_order)));
-    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    CK(cudaEventRecord(ctx->ev[4], st));
+    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), st, P<int>(ctx->eye_order)));
+    CK(cudaEventRecord(ctx->ev[5], st));
+    ctx->launches += 1;
+    return PM_OK;
+}
+
+// the request count of the eye pass (ordered on ctx->st)
+int render_eye_count(pm_ctx* ctx, FrameSetup& F) {
     unsigned long long nreq = 0;
-    CK(cudaMemcpyAsync(&nreq, R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&nreq, F.R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     F.nreq = (int64_t)std::min<unsigned long long>(nreq, (unsigned long long)F.cap);
     ctx->last_requests = F.nreq;
     ctx->last_pixels = F.npx;
-    ctx->launches += 1;
     return PM_OK;
+}
+
+// buffers, eye pass and the request count
+int render_eye(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F) {
+    if (int rc = render_eye_launch(ctx, cam, o, F, ctx->st)) return rc;
+    return render_eye_count(ctx, F);
 }
 
 // caustic gather, resolve (ev[7] .. ev[8]) and the stage times
@@ -1166,12 +1183,10 @@ int render_finish(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* 
 
 }  // namespace
 
-int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance) {
-    if (!ctx || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
-    if (int rc = render_checks(ctx, cam, o)) return rc;
-    CK(cudaSetDevice(ctx->device));
-    FrameSetup F;
-    if (int rc = render_eye(ctx, cam, o, F)) return rc;
+namespace {
+
+// global gather, caustic gather, resolve and the status check of a frame whose requests are counted
+int render_rest(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* out_rgb8, float* out_radiance) {
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     GatherQueries Q{};
     Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = 1u;
@@ -1181,6 +1196,55 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_
     ctx->launches += 1;
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
     return check_status(ctx, "render");
+}
+
+}  // namespace
+
+int pm_frame(pm_ctx* ctx, const pm_trace_opts* to, const pm_grid_opts* go, const pm_camera* cam,
+             const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance, int64_t* out_paths) {
+    if (!ctx || !to || !go || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
+    if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "no scene");
+    if (o->max_depth < 0 || o->max_depth > RENDER_MAX_DEPTH) return fail(ctx, PM_ERR_INVALID, "max_depth must be 0..5");
+    if (o->k_global < 0 || o->k_global > 256 || o->k_caustic < 0 || o->k_caustic > 256)
+        return fail(ctx, PM_ERR_INVALID, "k must be 0..256");
+    if (cam->width <= 0 || cam->height <= 0) return fail(ctx, PM_ERR_INVALID, "bad camera size");
+    CK(cudaSetDevice(ctx->device));
+    if (int rc = pm_trace_photons(ctx, to, out_paths)) return rc;
+    // the eye pass needs neither the photons nor the grid: it runs on the
+    // frame stream beside the grid build
+    if (!ctx->frame_st) {
+        CK(cudaStreamCreateWithFlags(&ctx->frame_st, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->frame_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->frame_done, cudaEventDisableTiming));
+    }
+    FrameSetup F;
+    CK(cudaEventRecord(ctx->frame_fork, ctx->st));
+    CK(cudaStreamWaitEvent(ctx->frame_st, ctx->frame_fork, 0));
+    int rc = render_eye_launch(ctx, cam, o, F, ctx->frame_st);
+    if (rc == PM_OK) {
+        if (cudaEventRecord(ctx->frame_done, ctx->frame_st) != cudaSuccess) rc = cuda_fail(ctx, cudaErrorUnknown, "frame event");
+    }
+    if (rc == PM_OK) rc = pm_build_grid(ctx, PM_MAP_GLOBAL, go, nullptr);
+    if (rc == PM_OK && to->caustic_capacity > 0 && o->k_caustic > 0) rc = pm_build_grid(ctx, PM_MAP_CAUSTIC, go, nullptr);
+    if (rc != PM_OK) {
+        cudaStreamSynchronize(ctx->frame_st);   // the eye pass's buffers stay in use until it ends
+        return rc;
+    }
+    CK(cudaStreamWaitEvent(ctx->st, ctx->frame_done, 0));
+    if (int rc2 = render_checks(ctx, cam, o)) return rc2;
+    F.caustic = ctx->maps[PM_MAP_CAUSTIC].built;
+    if (F.caustic) ENSURE(ctx->est_c, (size_t)F.cap * 12);
+    if (int rc2 = render_eye_count(ctx, F)) return rc2;
+    return render_rest(ctx, o, F, out_rgb8, out_radiance);
+}
+
+int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance) {
+    if (!ctx || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
+    if (int rc = render_checks(ctx, cam, o)) return rc;
+    CK(cudaSetDevice(ctx->device));
+    FrameSetup F;
+    if (int rc = render_eye(ctx, cam, o, F)) return rc;
+    return render_rest(ctx, o, F, out_rgb8, out_radiance);
 }
 
 int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, const pm_learned_opts* lo,

@@ -69,6 +69,9 @@ struct pm_ctx {
     cudaStream_t train_st = nullptr;
     cudaEvent_t train_fork = nullptr, train_done = nullptr;
     bool train_pending = false;
+    // pm_frame's eye pass runs on its own stream beside the grid build
+    cudaStream_t frame_st = nullptr;
+    cudaEvent_t frame_fork = nullptr, frame_done = nullptr;
     bool eye_order_valid = false;   // eye_order holds the order for eye_order_cam on this scene
     pm_camera eye_order_cam = {};
     pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts, fallback_list;

@@ -164,6 +164,7 @@ def library():
         "pm_cache_set_params": ([vp, vp], C.c_int),
         "pm_cache_sample_points": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
         "pm_render_learned": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "pm_frame": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "pm_learned_graph_create": ([vp, vp, vp, vp, vp, vp, vp, i64, i64, i32, i64, vp, vp, vp], C.c_int),
         "pm_learned_graph_run": ([vp, vp], C.c_int),
         "pm_learned_graph_offset": ([vp, vp], C.c_int),
@@ -493,6 +494,25 @@ class Context:
                                                    _ptr(tgt), int(n), int(batch), int(steps), int(offset), _ptr(rgb),
                                                    _ptr(rad), C.byref(h)), "pm_learned_graph_create")
         return LearnedGraph(self, h, rgb, rad, (pos, nrm, tgt))
+
+    def frame(self, seed, max_bounces, global_capacity, cam: Camera, k_global, r_global, max_depth=4,
+              caustic_capacity=0, k_caustic=0, r_caustic=0.2, faithful_caustic=True, desired=1000, sub_div=0,
+              radiance=True, out_rgb8=None, out_radiance=None):
+        """Photon pass + grid build(s) + frame in one call (pm_frame; the eye pass
+        runs beside the grid build).  Returns (rgb8, radiance, paths traced)."""
+        torch = self.torch
+        W, H = cam.width, cam.height
+        rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
+        rad = out_radiance
+        if rad is None and radiance:
+            rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
+        to = _TraceOpts(seed, 0, max_bounces, global_capacity, caustic_capacity, 0)
+        go = _GridOpts(desired, 5, 5, sub_div, 0)
+        ro = _RenderOpts(max_depth, k_global, r_global, k_caustic, r_caustic, int(faithful_caustic))
+        paths = C.c_int64()
+        self._check(self.L.pm_frame(self.h, C.byref(to), C.byref(go), C.byref(cam), C.byref(ro), _ptr(rgb), _ptr(rad),
+                                    C.byref(paths)), "pm_frame")
+        return rgb, rad, paths.value
 
     # ------------------------------------------------------------ render
     def render(self, cam: Camera, k_global, r_global, max_depth=4, k_caustic=0, r_caustic=0.2,

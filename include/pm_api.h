@@ -206,6 +206,15 @@ int pm_camera_setup(const float position[3], const float direction[3], const flo
  * The global map must be built; the caustic map is used when built. */
 int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, uint8_t* out_rgb8, float* out_radiance);
 
+/* A whole frame in one call: pm_trace_photons(trace), pm_build_grid of the
+ * global map (and of the caustic map when trace fills one and k_caustic > 0)
+ * with grid, then pm_render's frame.  The eye pass needs neither the photons
+ * nor the grid, so it runs on a second stream of the context beside the grid
+ * build.  Results are pm_trace_photons + pm_build_grid + pm_render's
+ * (Initializer.cu:142-177 followed by Drawer::draw_in_gpu, Drawer.cu:22-41). */
+int pm_frame(pm_ctx* ctx, const pm_trace_opts* trace, const pm_grid_opts* grid, const pm_camera* cam,
+             const pm_render_opts* opts, uint8_t* out_rgb8, float* out_radiance, int64_t* out_paths);
+
 /* Device prefix sum used by the grid build (exposed for known-answer tests):
  * exclusive (inclusive = 0) or inclusive scan of n u32 device values. */
 int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive);

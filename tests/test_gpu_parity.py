@@ -355,3 +355,27 @@ def test_full_size_photon_pass_properties(ctx):
     same = slot_key[1:] == slot_key[:-1]
     assert bool((ids[1:][same] > ids[:-1][same]).all())
     assert np.array_equal(_np(ph["list_pos"])[_np(ids)[:1000]], _np(sp[:1000, :3]))
+
+
+def test_frame_call_equals_the_three_calls(ctx):
+    """pm_frame (eye pass beside the grid build) gives the photons and the image
+    of pm_trace_photons + pm_build_grid + pm_render, with and without a caustic map."""
+    import photonmap
+    sc, cs, w = scenes.workload("cornell_small")
+    ctx.set_scene(sc)
+    cam = photonmap.camera_setup((0, 0, 3.5), (0, 0, -1), (0, 1, 0), 45.0, 128, 96)
+    for caustic, kc in ((0, 0), (8_000, 32)):
+        ctx.trace_photons(7, 8, 60_000, caustic)
+        ctx.build_grid(0)
+        if caustic:
+            ctx.build_grid(1)
+        rgb_a, rad_a = ctx.render(cam, 64, 0.1, 4, k_caustic=kc, r_caustic=0.1)
+        rgb_a, rad_a = rgb_a.clone(), rad_a.clone()
+        pos_a = _np(ctx.photons(0, sorted_=False)["list_pos"])
+        rgb_b, rad_b, paths = ctx.frame(7, 8, 60_000, cam, 64, 0.1, 4, caustic_capacity=caustic, k_caustic=kc,
+                                        r_caustic=0.1)
+        assert paths > 0
+        assert np.array_equal(_np(ctx.photons(0, sorted_=False)["list_pos"]), pos_a)
+        assert torch.equal(rgb_b, rgb_a)
+        assert torch.equal(rad_b, rad_a)
+        assert ctx.status() == 0
