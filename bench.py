@@ -539,7 +539,10 @@ def run_reference(args):
     return {"metric": METRIC, "value": v, "unit": "Mphotons/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1000, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "photons": w["photons"], "image": f"{w['width']}x{w['height']}"},
+            "config": {"workload": args.workload, "photons": w["photons"], "max_bounces": w["max_bounces"],
+                       "image": f"{w['width']}x{w['height']}", "k": w["k"], "radius": w["radius"],
+                       "eye_depth": w["max_depth"], "triangles": sc.ntri, "parallelism": "replicas1",
+                       "api": "the reference's CPU mode (render_cpu) + the oracle's CPU photon pass and grid"},
             "cpu_baseline": {"value": v, "unit": "Mphotons/s", "cores": est["cores"], "kind": "reference",
                              "sample": est["sample"]},
             "e2e": {"value": v, "unit": "Mphotons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
