@@ -31,6 +31,30 @@ METRIC = "Mphotons/s + ms/frame @10M,1080p"
 WORKLOAD = "cornell_hf_1080p"
 
 
+def max_over_ranks(values, world):
+    """Each value's maximum over the ranks (the slowest rank times the job);
+    the tensor lives where the process group's backend works (CUDA for nccl)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def step_seed(seed, rank, step):
+    """Photon-stream key of a rank's step: every rank traces its own
+    independent photons (replicas, weak scaling), every step new ones."""
+    return seed + (rank << 32) + step   # 64-bit stream keys: 2^32 steps per rank
+
+
+def job_mphotons(world, photons_per_rank, ms):
+    """Whole-job throughput: all ranks' photons over the (max-over-ranks) step time."""
+    return world * photons_per_rank / (ms * 1e-3) / 1e6
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -350,11 +374,7 @@ def learned_frames(ctx, cam, w, rgb, args, world):
         b.record()
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / K
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t[0])
-        return ms
+        return max_over_ranks([ms], world)[0]
 
     ms_plain = timed(plain)
     ms_learned = timed(learned_frame)
@@ -430,7 +450,7 @@ def run_ours(args):
         # pm_frame: photon pass, grid build and frame in one call (the eye pass
         # runs beside the grid build); same photons and image as
         # trace_photons + build_grid + render
-        ctx.frame(w["seed"] + 1000 * rank + i, w["max_bounces"], w["photons"], cam, w["k"], w["radius"],
+        ctx.frame(step_seed(w["seed"], rank, i), w["max_bounces"], w["photons"], cam, w["k"], w["radius"],
                   w["max_depth"], radiance=False, out_rgb8=rgb)
         if e2e:
             host_rgb.copy_(rgb, non_blocking=True)
@@ -466,10 +486,7 @@ def run_ours(args):
         step(10_000 + i, e2e=True)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1000 / args.steps
-    if world > 1:
-        t = torch.tensor([ms, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], world)
     stages = stage_sum / args.steps
 
     # gather kernel roofline: compulsory bytes per query = k neighbours x (16 B position
@@ -495,7 +512,7 @@ def run_ours(args):
                    "kind": "reference", "sample": est["sample"],
                    "ms_per_frame": est["step_s"] * 1000, "stages_s": {k: est[k] for k in ("trace_s", "grid_s", "frame_s")}}
         line = {
-            "metric": METRIC, "value": world * w["photons"] / (ms * 1e-3) / 1e6, "unit": "Mphotons/s",
+            "metric": METRIC, "value": job_mphotons(world, w["photons"], ms), "unit": "Mphotons/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene, seeded Philox photon streams)",
@@ -509,7 +526,7 @@ def run_ours(args):
             "roofline": {"kernel": "k_gather (kNN + estimate)", "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": None,
                          "algorithmic_bytes_per_launch": gather_bytes, "queries_per_launch": nreq},
-            "e2e": {"value": world * w["photons"] / (e2e_ms * 1e-3) / 1e6, "unit": "Mphotons/s",
+            "e2e": {"value": job_mphotons(world, w["photons"], e2e_ms), "unit": "Mphotons/s",
                     "ms_per_step": e2e_ms, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3},
             "gpu_launches": launches,
             "clocks": clocks,
