@@ -298,7 +298,8 @@ void pm_destroy(pm_ctx* ctx) {
                       &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
                       &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
                       &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list,
-                      &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order};
+                      &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order, &ctx->rq_keys,
+                      &ctx->rq_k0, &ctx->rq_k1, &ctx->rq_v0, &ctx->rq_v1, &ctx->rq_hist, &ctx->rq_ws};
     for (DevBuf* b : bufs) release(*b);
     for (auto& m : ctx->maps) {
         DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
@@ -1190,8 +1191,26 @@ int render_rest(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* ou
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     GatherQueries Q{};
     Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = 1u;
+    // the gather visits the requests in Morton order of their hit points
+    const uint32_t* order = nullptr;
+    if (F.nreq > 0) {
+        const int64_t n = F.nreq;
+        ENSURE(ctx->rq_keys, (size_t)n * 4);
+        ENSURE(ctx->rq_k0, (size_t)n * 4); ENSURE(ctx->rq_k1, (size_t)n * 4);
+        ENSURE(ctx->rq_v0, (size_t)n * 4); ENSURE(ctx->rq_v1, (size_t)n * 4);
+        ENSURE(ctx->rq_hist, radix_hist_elems(n) * 4);
+        ENSURE(ctx->rq_ws, scan_workspace_bytes((int64_t)radix_hist_elems(n)));
+        CK(cudaEventRecord(ctx->ev[6], ctx->st));
+        CK(request_keys(F.R.a, n, ctx->aabb, P<uint32_t>(ctx->rq_keys), ctx->st));
+        RadixBuffers RB{{P<uint32_t>(ctx->rq_k0), P<uint32_t>(ctx->rq_k1)}, {P<uint32_t>(ctx->rq_v0), P<uint32_t>(ctx->rq_v1)},
+                        P<uint32_t>(ctx->rq_hist), ctx->rq_ws.p, P<unsigned>(ctx->status)};
+        int launches = 0;
+        CK(radix_sort_u32(RB, P<uint32_t>(ctx->rq_keys), nullptr, n, 30, false, nullptr, &order, &launches, ctx->st));
+        ctx->launches += launches + 1;
+        Q.idx = order;
+    }
     GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};
-    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    if (F.nreq <= 0) CK(cudaEventRecord(ctx->ev[6], ctx->st));
     CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OG, P<unsigned>(ctx->status), ctx->st));
     ctx->launches += 1;
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;

@@ -64,6 +64,7 @@ struct pm_ctx {
     // host copies for the eye pass's block order: 6 AABB floats and 12 material floats per model
     std::vector<float> h_maabb, h_mats;
     pm::DevBuf eye_order;
+    pm::DevBuf rq_keys, rq_k0, rq_k1, rq_v0, rq_v1, rq_hist, rq_ws;   // the gather's request order
     // training steps queued without a loss run on their own stream; whatever
     // reads or writes the cache (or synchronises the context) waits for them
     cudaStream_t train_st = nullptr;

@@ -342,6 +342,38 @@ __global__ void k_resolve_multi(const RenderInstDev* __restrict__ tab, const int
 
 }  // namespace
 
+namespace {
+__device__ __forceinline__ uint32_t spread10r(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+__global__ void k_request_keys(const float4* __restrict__ a, int64_t n, float lx, float ly, float lz, float sx,
+                               float sy, float sz, uint32_t* __restrict__ keys) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = a[i];
+    const uint32_t x = (uint32_t)min(max((int)((p.x - lx) * sx), 0), 1023);
+    const uint32_t y = (uint32_t)min(max((int)((p.y - ly) * sy), 0), 1023);
+    const uint32_t z = (uint32_t)min(max((int)((p.z - lz) * sz), 0), 1023);
+    keys[i] = (spread10r(x) << 2) | (spread10r(y) << 1) | spread10r(z);
+}
+}  // namespace
+
+cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32_t* keys, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    float sc[3];
+    for (int k = 0; k < 3; k++) {
+        const float ext = aabb[3 + k] - aabb[k];
+        sc[k] = ext > 0.f ? 1024.f / ext : 0.f;
+    }
+    k_request_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, n, aabb[0], aabb[1], aabb[2], sc[0], sc[1], sc[2],
+                                                                 keys);
+    return cudaGetLastError();
+}
+
 int64_t eye_blocks(int64_t npx) { return (npx + EYE_THREADS - 1) / EYE_THREADS; }
 int eye_threads() { return EYE_THREADS; }
 

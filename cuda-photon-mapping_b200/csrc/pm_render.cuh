@@ -32,6 +32,8 @@ struct Requests {
 // block of the launch takes (a permutation), e.g. the slow ones first.
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
                      cudaStream_t st, const int* block_order = nullptr);
+// 30-bit Morton code of each request's hit point in the box aabb (10 bits per axis)
+cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32_t* keys, cudaStream_t st);
 // pixel blocks of the eye pass (EYE_THREADS consecutive pixels each)
 int64_t eye_blocks(int64_t npx);
 int eye_threads();
