@@ -417,6 +417,38 @@ def learned_frames(ctx, cam, w, rgb, args, world):
                     "flop_per_sample_forward": fwd}}
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# default workload's kernels, from one ncu capture of the timed step's launches
+# (profiles/dram_traffic_cornell_hf_1080p.md gives the command and the figures)
+DRAM_TRAFFIC = {"k_trace": 161_125_120 + 443_799_552, "k_gather": 451_488_256 + 14_518_272}
+
+
+def rooflines(w, sc, bvh, nreq, paths, k_trace_ms, k_gather_ms, hbm, src, default_workload):
+    """HBM rooflines of the step's two large kernels, each timed alone with CUDA
+    events on the context stream (k_trace summed over the photon pass's batches).
+
+    k_trace algorithmic bytes: 32 B stage record per stored photon (at least the
+    photon budget) + 8 B per-path photon counts + the scene read once (64 B per
+    BVH node, 80 B leaf-ordered triangle record + 36 B vertex normals per
+    triangle).  k_gather: per kNN query k neighbours x (16 B position + 12 B
+    direction + 12 B power) + 32 B request (point, normal) + 12 B estimate.
+    """
+    scene_bytes = bvh["nodes"] * 64 + sc.ntri * (80 + 36)
+    units = {
+        "k_trace": (w["photons"] * 32 + paths * 8 + scene_bytes, k_trace_ms, "BVH traversal: latency / issue bound",
+                    {"paths_per_launch": paths, "photons_per_launch": w["photons"]}),
+        "k_gather": (nreq * (w["k"] * 40 + 44), k_gather_ms, "kNN walk: issue / L1-L2 latency bound",
+                     {"queries_per_launch": nreq}),
+    }
+    out = {}
+    for name, (alg, ms, note, extra) in units.items():
+        achieved = alg / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        out[name] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": src, "traffic": DRAM_TRAFFIC.get(name) if default_workload else None,
+                     "algorithmic_bytes_per_launch": int(alg), "ms_per_launch": ms, "note": note, **extra}
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -446,19 +478,21 @@ def run_ours(args):
     rgb = torch.empty(W * H * 3, dtype=torch.uint8, device="cuda")
     host_rgb = torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True)
 
+    paths = [0]
+
     def step(i, e2e=False):
         # pm_frame: photon pass, grid build and frame in one call (the eye pass
         # runs beside the grid build); same photons and image as
         # trace_photons + build_grid + render
-        ctx.frame(step_seed(w["seed"], rank, i), w["max_bounces"], w["photons"], cam, w["k"], w["radius"],
-                  w["max_depth"], radiance=False, out_rgb8=rgb)
+        _, _, paths[0] = ctx.frame(step_seed(w["seed"], rank, i), w["max_bounces"], w["photons"], cam, w["k"],
+                                   w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb)
         if e2e:
             host_rgb.copy_(rgb, non_blocking=True)
 
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
-    stage_sum = np.zeros(5)
+    stage_sum = np.zeros(7)
     sampler = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
@@ -469,7 +503,9 @@ def run_ours(args):
     for i in range(args.steps):
         step(args.warmup + i)
         st = ctx.stage_times()
-        stage_sum += np.array([st["trace_ms"], st["grid_ms"], st["eye_ms"], st["gather_ms"], st["resolve_ms"]])
+        stage_sum += np.array([st["trace_ms"], st["grid_ms"], st["eye_ms"], st["gather_ms"], st["resolve_ms"],
+                               st["k_trace_ms"], st["k_gather_ms"]])
+    paths_timed = paths[0]
     ev1.record()
     torch.cuda.synchronize()
     launches = ctx.launch_count() - launches0
@@ -489,8 +525,6 @@ def run_ours(args):
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], world)
     stages = stage_sum / args.steps
 
-    # gather kernel roofline: compulsory bytes per query = k neighbours x (16 B position
-    # + 12 B direction + 12 B power) + 32 B request (point, normal) + 12 B estimate
     learned_block = None
     if not args.no_learned:
         learned_block = learned_frames(ctx, cam, w, rgb, args, world)
@@ -502,9 +536,10 @@ def run_ours(args):
     line = None
     if rank == 0:
         nreq = ctx.render_requests()   # kNN queries of the frame's gather
-        gather_bytes = nreq * (w["k"] * 40 + 44)
-        gather_ms = stages[3]
-        achieved = gather_bytes / (gather_ms * 1e-3) / 1e9 if gather_ms > 0 else 0.0
+        kernels = rooflines(w, sc, bvh, nreq, paths_timed, stages[5], stages[6], hbm, src,
+                            default_workload=(args.workload == WORKLOAD and not (args.photons or args.width
+                                                                                  or args.height)))
+        dominant = max(kernels, key=lambda k: kernels[k]["ms_per_launch"])
         cpu = None
         if not args.no_cpu_baseline:
             est = cpu_reference_estimate(sc, w)
@@ -523,9 +558,8 @@ def run_ours(args):
                        "parallelism": f"replicas{world}"},
             "stages_ms": {"trace": stages[0], "grid": stages[1], "eye": stages[2], "gather": stages[3],
                           "resolve": stages[4]},
-            "roofline": {"kernel": "k_gather (kNN + estimate)", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": None,
-                         "algorithmic_bytes_per_launch": gather_bytes, "queries_per_launch": nreq},
+            "roofline": dict(kernel=dominant, **kernels[dominant]),
+            "roofline_kernels": kernels,
             "e2e": {"value": job_mphotons(world, w["photons"], e2e_ms), "unit": "Mphotons/s",
                     "ms_per_step": e2e_ms, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3},
             "gpu_launches": launches,

@@ -291,7 +291,7 @@ void pm_destroy(pm_ctx* ctx) {
     if (ctx->train_fork) cudaEventDestroy(ctx->train_fork);
     if (ctx->train_done) cudaEventDestroy(ctx->train_done);
     DevBuf* bufs[] = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
-                      &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage_pos, &ctx->stage_dir,
+                      &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage,
                       &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
                       &ctx->scratch_pow, &ctx->req_a, &ctx->req_b, &ctx->req_c, &ctx->req_counter, &ctx->px_base,
                       &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws, &ctx->cache_w32,
@@ -734,10 +734,9 @@ int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]) {
 static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, TraceBatch& B) {
     if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "pm_set_scene first");
     if (o->max_bounces < 1 || o->max_bounces > 32) return fail(ctx, PM_ERR_INVALID, "max_bounces must be 1..32");
-    const size_t stage = (size_t)o->max_bounces * (size_t)npaths * 16;
+    const size_t stage = (size_t)o->max_bounces * (size_t)npaths * 32;
     ENSURE(ctx->counter, 8);
-    ENSURE(ctx->stage_pos, stage);
-    ENSURE(ctx->stage_dir, stage);
+    ENSURE(ctx->stage, stage);
     ENSURE(ctx->cnt_g, (size_t)npaths * 4);
     ENSURE(ctx->cnt_c, (size_t)npaths * 4);
     ENSURE(ctx->scan_g, (size_t)npaths * 4);
@@ -749,8 +748,7 @@ static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, Tr
     B.tag = o->stream_tag;
     B.max_bounces = o->max_bounces;
     B.path_counter = P<unsigned long long>(ctx->counter);
-    B.stage_pos = P<float4>(ctx->stage_pos);
-    B.stage_dir = P<float4>(ctx->stage_dir);
+    B.stage = P<float4>(ctx->stage);
     B.cnt_g = P<uint32_t>(ctx->cnt_g);
     B.cnt_c = P<uint32_t>(ctx->cnt_c);
     B.scan_g = P<uint32_t>(ctx->scan_g);
@@ -797,6 +795,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     int64_t fg = 0, fc = 0, p0 = 0;
     double yg = 0.0, yc = 0.0;   // photons per path so far
     int64_t got_g = 0, got_c = 0;
+    float k_trace_ms = 0.f;
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     while ((fg < cg || fc < cc) && p0 < max_paths) {
         nb = std::min(nb, max_paths - p0);
@@ -806,6 +805,8 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         B.p0 = p0;
         B.npaths = nb;
         for (int a = 0; a < 3; a++) B.power[a] = power[a];
+        B.k_begin = ctx->ev[12];
+        B.k_end = ctx->ev[13];
         PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg};
         PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc};
         CK(trace_batch(B, LG, LC, ctx->st));
@@ -813,6 +814,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         uint32_t tot[2] = {0, 0};
         CK(cudaMemcpyAsync(tot, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
+        k_trace_ms += elapsed(ctx->ev[12], ctx->ev[13]);
         got_g += tot[0];
         got_c += tot[1];
         fg = std::min(cg, fg + (int64_t)tot[0]);
@@ -830,6 +832,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(cudaEventSynchronize(ctx->ev[1]));
     ctx->stage_ms[0] = elapsed(ctx->ev[0], ctx->ev[1]);
+    ctx->stage_ms[5] = k_trace_ms;
     G.n = fg;
     C.n = fc;
     if (out_paths) *out_paths = p0;
@@ -1211,9 +1214,12 @@ int render_rest(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* ou
     }
     GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};
     if (F.nreq <= 0) CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    CK(cudaEventRecord(ctx->ev[11], ctx->st));
     CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OG, P<unsigned>(ctx->status), ctx->st));
+    CK(cudaEventRecord(ctx->ev[12], ctx->st));
     ctx->launches += 1;
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
+    ctx->stage_ms[6] = elapsed(ctx->ev[11], ctx->ev[12]);
     return check_status(ctx, "render");
 }
 

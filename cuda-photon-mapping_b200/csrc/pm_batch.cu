@@ -53,7 +53,7 @@ struct pm_batch {
     // device tables
     DevBuf t_trace, t_outs, t_path_off, t_grid, t_ph_off, t_cell_off, t_render, t_px_off, t_gather;
     // trace
-    DevBuf counter, stage_pos, stage_dir, cnt_g, cnt_c, scan_g, totals, trace_ws, inst_total;
+    DevBuf counter, stage, cnt_g, cnt_c, scan_g, totals, trace_ws, inst_total;
     DevBuf pos, dir, pow;
     // grid
     DevBuf cid, keys0, keys1, vals0, vals1, hist, grid_ws, key_counts, key_starts, cstarts, csizes, gpos, gdir, gpow;
@@ -175,8 +175,7 @@ TraceMulti trace_args(pm_batch* b) {
     M.table = b->t_trace.p;
     M.outs = P<TraceInstOut>(b->t_outs);
     M.path_counter = P<unsigned long long>(b->counter);
-    M.stage_pos = P<float4>(b->stage_pos);
-    M.stage_dir = P<float4>(b->stage_dir);
+    M.stage = P<float4>(b->stage);
     M.cnt_g = P<uint32_t>(b->cnt_g);
     M.cnt_c = P<uint32_t>(b->cnt_c);
     M.scan_g = P<uint32_t>(b->scan_g);
@@ -415,8 +414,7 @@ int create(pm_batch* b, const pm_batch_instance* in, int32_t n, const pm_batch_o
     const int64_t TP = b->total_paths, NS = b->total_slots, NP = b->total_px, RC = b->req_cap;
     const size_t MB = (size_t)b->max_bounces;
     BCK(ensure(b->counter, 16));
-    BCK(ensure(b->stage_pos, MB * TP * 16));
-    BCK(ensure(b->stage_dir, MB * TP * 16));
+    BCK(ensure(b->stage, MB * TP * 32));
     BCK(ensure(b->cnt_g, TP * 4));
     BCK(ensure(b->cnt_c, TP * 4));
     BCK(ensure(b->scan_g, TP * 4));
@@ -486,7 +484,7 @@ void pm_batch_destroy(pm_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     for (pm_ctx* c : b->ctx) pm_destroy(c);
     DevBuf* bufs[] = {&b->t_trace, &b->t_outs, &b->t_path_off, &b->t_grid, &b->t_ph_off, &b->t_cell_off, &b->t_render,
-                      &b->t_px_off, &b->t_gather, &b->counter, &b->stage_pos, &b->stage_dir, &b->cnt_g, &b->cnt_c,
+                      &b->t_px_off, &b->t_gather, &b->counter, &b->stage, &b->cnt_g, &b->cnt_c,
                       &b->scan_g, &b->totals, &b->trace_ws, &b->inst_total, &b->pos, &b->dir, &b->pow, &b->cid,
                       &b->keys0, &b->keys1, &b->vals0, &b->vals1, &b->hist, &b->grid_ws, &b->key_counts,
                       &b->key_starts, &b->cstarts, &b->csizes, &b->gpos, &b->gdir, &b->gpow, &b->req_a, &b->req_b,

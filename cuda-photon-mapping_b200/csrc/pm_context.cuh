@@ -49,7 +49,7 @@ struct pm_ctx {
     pm::DevBuf tri, tri_pos, tri_nrm, tri_diffuse, nodes, prim, maabb, mats, ca;
     pm::MapState maps[2];
     // photon-pass scratch
-    pm::DevBuf counter, stage_pos, stage_dir, cnt_g, cnt_c, scan_g, scan_c, totals, trace_ws, scratch_pow;
+    pm::DevBuf counter, stage, cnt_g, cnt_c, scan_g, scan_c, totals, trace_ws, scratch_pow;
     // render scratch
     pm::DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, est_c;
     pm::DevBuf status, gws;
@@ -79,7 +79,7 @@ struct pm_ctx {
     pm_cache_opts cache_opts = {};
     float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};
     int cache_step = 0;
-    cudaEvent_t ev[12] = {};
+    cudaEvent_t ev[14] = {};
     float stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t launches = 0;      // kernels this context has launched
     int64_t last_requests = 0; // gather requests of the last pm_render

@@ -95,18 +95,25 @@ struct Hit {
     V3 uvw;
 };
 
-// edge-function test with precomputed terms; returns false when the triangle
-// cannot be a better (t, index) candidate than (best_t, best_tri)
-__device__ __forceinline__ bool tri_test(const float4* T, V3 o, V3 d, float best_t, int tri, int best_tri,
-                                         float& t_out, V3& uvw) {
-    float4 q0 = T[0], q4 = T[4];
+// edge-function test with precomputed terms on a leaf-ordered triangle record
+// (q4.w its triangle index, q2.w its model); returns false when the triangle
+// belongs to a model below min_model or cannot be a better (t, index)
+// candidate than (best_t, best_tri).  The record's index and model come with
+// the 16-byte loads the test makes anyway, the model only once the plane test
+// has passed.
+__device__ __forceinline__ bool tri_test(const float4* __restrict__ T, V3 o, V3 d, float best_t, int best_tri,
+                                         int min_model, float& t_out, V3& uvw, int& tri_out, int& m_out) {
+    const float4 q0 = __ldg(T), q4 = __ldg(T + 4);
+    const int tri = __float_as_int(q4.w);
     V3 n = xyz(q4);
     float ndd = vdot(n, d);
     if (fabsf(ndd) < 1e-6f) return false;
     float t = (q0.w - vdot(n, o)) / ndd;
     if (t < 0) return false;
     if (t > best_t || (t == best_t && tri > best_tri)) return false;
-    float4 q1 = T[1], q2 = T[2], q3 = T[3];
+    const float4 q1 = __ldg(T + 1), q2 = __ldg(T + 2), q3 = __ldg(T + 3);
+    const int m = __float_as_int(q2.w);
+    if (m < min_model) return false;
     V3 v0 = xyz(q0);
     V3 P = vadd(o, vscale(d, t));
     float w = vdot(n, vcross(xyz(q1), vsub(P, v0)));
@@ -119,6 +126,8 @@ __device__ __forceinline__ bool tri_test(const float4* T, V3 o, V3 d, float best
     if (u < 0) return false;
     t_out = t;
     uvw = v3(u, v, w);
+    tri_out = tri;
+    m_out = m;
     return true;
 }
 
@@ -246,11 +255,8 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
         const int first = packed >> 8, count = packed & 255;
         for (int i = 0; i < count; i++) {
             const float4* Q = S.tri_leaf + 5 * (size_t)(first + i);
-            const int m = __float_as_int(__ldg(&Q[2].w));
-            if (m < T.min_model) continue;
-            const int tri = __float_as_int(__ldg(&Q[4].w));
-            float t; V3 uvw;
-            if (!tri_test(Q, o, d, T.best_t, tri, T.best_tri, t, uvw)) continue;
+            float t; V3 uvw; int tri, m;
+            if (!tri_test(Q, o, d, T.best_t, T.best_tri, T.min_model, t, uvw, tri, m)) continue;
             const bool zero = t == 0.0f;
             if (zero && (T.min_model != 0 || m < T.zmodel || (m == T.zmodel && tri > T.ztri))) continue;
             bool pass;

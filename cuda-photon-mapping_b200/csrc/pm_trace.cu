@@ -11,8 +11,11 @@
 //  * a persistent grid traces the paths [p0, p0 + npaths) of one batch.  Lanes
 //    whose path ended take the next path indices together (one atomic per
 //    warp, ballot ranks), so SIMD lanes stay busy however long paths are;
-//  * the k-th photon a path stores goes to stage slot [k][path] as two 16-byte
-//    vector stores: (position, map flag) and (direction, 0);
+//  * the k-th photon a path stores goes to stage slot [k][path], a 32-byte
+//    record written as two 16-byte vector stores: (position, map flag) and
+//    (direction, 0); one record fills one DRAM sector, so no sector is left
+//    half written (a half-written sector costs a read of it from DRAM before
+//    its write-back);
 //  * k_compact writes the batch's photons into the global / caustic lists in
 //    canonical order (path, then bounce) after exclusive scans of the per-path
 //    counts, and cuts each list exactly at its capacity.
@@ -61,8 +64,7 @@ struct KParams {
     int64_t p0, npaths;
     V3 power;
     unsigned long long* counter;
-    float4* stage_pos;
-    float4* stage_dir;
+    float4* stage;          // 2 float4 per slot
     uint32_t* cnt_g;
     uint32_t* cnt_c;
     unsigned* status;
@@ -200,8 +202,8 @@ __device__ __forceinline__ bool shade(const KParams& P, Lane& L, const Hit& h, f
         bool caustic = (L.last == SPEC || L.last == REFR) && L.diffuse_surfs == 0;
         int slot = L.ng + L.nc;
         size_t o = (size_t)slot * (size_t)P.npaths + (size_t)j;
-        P.stage_pos[o] = make_float4(ip.x, ip.y, ip.z, __int_as_float(caustic ? 2 : 1));
-        P.stage_dir[o] = make_float4(L.ray.d.x, L.ray.d.y, L.ray.d.z, 0.f);
+        P.stage[2 * o] = make_float4(ip.x, ip.y, ip.z, __int_as_float(caustic ? 2 : 1));
+        P.stage[2 * o + 1] = make_float4(L.ray.d.x, L.ray.d.y, L.ray.d.z, 0.f);
         if (caustic) L.nc++; else L.ng++;
     } else if (dest == SPEC) {
         nr = ray_reflect(L.ray, ip, n);
@@ -382,8 +384,8 @@ k_trace_multi(const KParams* __restrict__ tab, const int64_t* __restrict__ off, 
 // inst_total[i] = global photons the instance produced before the cut.  A
 // batch builds no caustic map: caustic photons are dropped.
 __global__ void k_compact_multi(int64_t total, const int64_t* __restrict__ off, int ninst,
-                                const TraceInstOut* __restrict__ io, const float4* __restrict__ stage_pos,
-                                const float4* __restrict__ stage_dir, const uint32_t* __restrict__ cnt_g,
+                                const TraceInstOut* __restrict__ io, const float4* __restrict__ stage,
+                                const uint32_t* __restrict__ cnt_g,
                                 const uint32_t* __restrict__ cnt_c, const uint32_t* __restrict__ scan_g,
                                 const uint32_t* __restrict__ grand_total, float* gpos, float* gdir, float* gpow,
                                 int64_t* __restrict__ inst_total) {
@@ -401,9 +403,9 @@ __global__ void k_compact_multi(int64_t total, const int64_t* __restrict__ off, 
     const int slots = (int)(cnt_g[g] + cnt_c[g]);
     for (int k = 0; k < slots && og < o.cap; k++) {
         const size_t sidx = (size_t)k * (size_t)total + (size_t)g;
-        const float4 p = stage_pos[sidx];
+        const float4 p = stage[2 * sidx];
         if (__float_as_int(p.w) == 2) continue;
-        const float4 d = stage_dir[sidx];
+        const float4 d = stage[2 * sidx + 1];
         const int64_t idx = o.ph0 + og++;
         gpos[3 * idx] = p.x; gpos[3 * idx + 1] = p.y; gpos[3 * idx + 2] = p.z;
         gdir[3 * idx] = d.x; gdir[3 * idx + 1] = d.y; gdir[3 * idx + 2] = d.z;
@@ -412,7 +414,7 @@ __global__ void k_compact_multi(int64_t total, const int64_t* __restrict__ off, 
 }
 
 // canonical-order append of one batch into the two photon lists
-__global__ void k_compact(int64_t npaths, const float4* __restrict__ stage_pos, const float4* __restrict__ stage_dir,
+__global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
                           const uint32_t* __restrict__ cnt_g, const uint32_t* __restrict__ cnt_c,
                           const uint32_t* __restrict__ scan_g, const uint32_t* __restrict__ scan_c, V3 power,
                           float* gpos, float* gdir, float* gpow, int64_t gcap, int64_t gfilled,
@@ -423,8 +425,8 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage_pos, 
     int64_t og = gfilled + scan_g[j], oc = cfilled + scan_c[j];
     for (int k = 0; k < ng + nc; k++) {
         size_t o = (size_t)k * (size_t)npaths + (size_t)j;
-        float4 p = stage_pos[o];
-        float4 d = stage_dir[o];
+        float4 p = stage[2 * o];
+        float4 d = stage[2 * o + 1];
         bool caustic = __float_as_int(p.w) == 2;
         float *dp, *dd, *dw;
         int64_t idx;
@@ -454,7 +456,7 @@ cudaError_t trace_multi_tables(const TraceMulti& M, const TraceInst* insts, cuda
         P.p0 = I.p0; P.npaths = M.total;
         P.power = v3(I.power[0], I.power[1], I.power[2]);
         P.counter = M.path_counter;
-        P.stage_pos = M.stage_pos; P.stage_dir = M.stage_dir;
+        P.stage = M.stage;
         P.cnt_g = M.cnt_g; P.cnt_c = M.cnt_c;
         P.status = M.status;
         P.refill = M.refill > 0 ? std::min(M.refill, 32) : TRACE_REFILL;
@@ -480,7 +482,7 @@ cudaError_t trace_multi(const TraceMulti& M, cudaStream_t st) {
     if ((e = scan_u32(M.cnt_g, M.scan_g, M.total, 0, M.totals, M.scan_ws, M.status, st)) != cudaSuccess) return e;
     const int64_t n = std::max<int64_t>(M.total, M.ninst);
     k_compact_multi<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
-        M.total, M.path_off, M.ninst, M.outs, M.stage_pos, M.stage_dir, M.cnt_g, M.cnt_c, M.scan_g, M.totals, M.pos,
+        M.total, M.path_off, M.ninst, M.outs, M.stage, M.cnt_g, M.cnt_c, M.scan_g, M.totals, M.pos,
         M.dir, M.pow, M.inst_total);
     return cudaGetLastError();
 }
@@ -494,7 +496,7 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
     P.p0 = B.p0; P.npaths = B.npaths;
     P.power = v3(B.power[0], B.power[1], B.power[2]);
     P.counter = B.path_counter;
-    P.stage_pos = B.stage_pos; P.stage_dir = B.stage_dir;
+    P.stage = B.stage;
     P.cnt_g = B.cnt_g; P.cnt_c = B.cnt_c;
     P.status = B.status;
     P.refill = B.refill > 0 ? std::min(B.refill, 32) : TRACE_REFILL;
@@ -502,12 +504,14 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace, TRACE_THREADS, 0)) != cudaSuccess) return e;
     int64_t want = (B.npaths + TRACE_THREADS - 1) / TRACE_THREADS;
     int64_t grid = std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * B.sm_count);
+    if (B.k_begin && (e = cudaEventRecord(B.k_begin, st)) != cudaSuccess) return e;
     k_trace<<<(unsigned)grid, TRACE_THREADS, 0, st>>>(P);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (B.k_end && (e = cudaEventRecord(B.k_end, st)) != cudaSuccess) return e;
     if ((e = scan_u32(B.cnt_g, B.scan_g, B.npaths, 0, B.totals, B.scan_ws, B.status, st)) != cudaSuccess) return e;
     if ((e = scan_u32(B.cnt_c, B.scan_c, B.npaths, 0, B.totals + 1, B.scan_ws, B.status, st)) != cudaSuccess) return e;
     k_compact<<<(unsigned)((B.npaths + 255) / 256), 256, 0, st>>>(
-        B.npaths, B.stage_pos, B.stage_dir, B.cnt_g, B.cnt_c, B.scan_g, B.scan_c, P.power,
+        B.npaths, B.stage, B.cnt_g, B.cnt_c, B.scan_g, B.scan_c, P.power,
         G.pos, G.dir, G.pow, G.cap, G.filled, C.pos, C.dir, C.pow, C.cap, C.filled);
     return cudaGetLastError();
 }

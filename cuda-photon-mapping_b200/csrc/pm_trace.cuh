@@ -15,8 +15,7 @@ struct TraceBatch {
     float power[3];           // photon power (light intensity / global capacity)
     // scratch sized for npaths (stage: max_bounces * npaths float4 each)
     unsigned long long* path_counter;
-    float4* stage_pos;
-    float4* stage_dir;
+    float4* stage;            // 32-byte photon records: 2 float4 per slot, max_bounces * npaths slots
     uint32_t* cnt_g;
     uint32_t* cnt_c;
     uint32_t* scan_g;
@@ -26,6 +25,7 @@ struct TraceBatch {
     unsigned* status;
     int sm_count;
     int refill;               // k_trace refill threshold in lanes (1..32); 0: the default
+    cudaEvent_t k_begin = nullptr, k_end = nullptr;   // when set: recorded around the k_trace launch
 };
 
 struct PhotonList {
@@ -56,8 +56,7 @@ struct TraceMulti {
     void* table;              // device, trace_multi_table_bytes(ninst): per-instance parameters
     const TraceInstOut* outs; // device, ninst
     unsigned long long* path_counter;
-    float4* stage_pos;        // max_bounces * total each
-    float4* stage_dir;
+    float4* stage;            // 2 float4 per slot, max_bounces * total slots
     uint32_t* cnt_g;          // total each
     uint32_t* cnt_c;
     uint32_t* scan_g;

@@ -538,7 +538,7 @@ class Context:
         out = np.zeros(8, np.float32)
         self._check(self.L.pm_stage_times(self.h, out.ctypes.data), "pm_stage_times")
         return dict(trace_ms=float(out[0]), grid_ms=float(out[1]), eye_ms=float(out[2]), gather_ms=float(out[3]),
-                    resolve_ms=float(out[4]))
+                    resolve_ms=float(out[4]), k_trace_ms=float(out[5]), k_gather_ms=float(out[6]))
 
     def requests(self):
         """Copies of the last render's gather requests (see pm_request_view) as torch tensors."""

@@ -238,7 +238,9 @@ int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclus
 
 /* Per-stage device times of the last pm_trace_photons / pm_build_grid /
  * pm_render calls in milliseconds (CUDA events on the context stream):
- * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather, [4] resolve. */
+ * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather (request
+ * ordering + global gather + caustic gather), [4] resolve, [5] the k_trace
+ * kernels alone, [6] the global gather kernel alone. */
 int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
 
 /* ---------------------------------------------------------------------------

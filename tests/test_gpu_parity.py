@@ -379,3 +379,7 @@ def test_frame_call_equals_the_three_calls(ctx):
         assert torch.equal(rgb_b, rgb_a)
         assert torch.equal(rad_b, rad_a)
         assert ctx.status() == 0
+        # the kernels timed alone lie inside their stages
+        st = ctx.stage_times()
+        assert 0 < st["k_trace_ms"] <= st["trace_ms"]
+        assert 0 < st["k_gather_ms"] <= st["gather_ms"]
