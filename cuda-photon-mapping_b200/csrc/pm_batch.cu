@@ -49,6 +49,7 @@ struct pm_batch {
     std::vector<int64_t> paths, path_off, ph_off, key_off, cell_off, px_off;
     std::vector<TraceInst> trace_host;
     int64_t total_paths = 0, total_slots = 0, total_keys = 0, total_cells = 0, total_px = 0, req_cap = 0;
+    int64_t req_split = 0;    // requests of gather class 0 in [0, req_split), class 1 in [req_split, req_cap)
     int max_bounces = 1;
     // device tables
     DevBuf t_trace, t_outs, t_path_off, t_grid, t_ph_off, t_cell_off, t_render, t_px_off, t_gather;
@@ -247,7 +248,7 @@ int launch_stages(pm_batch* b, int stage, int* launches) {
     Requests R = request_args(b);
     if (stage < 0 || stage == 2) {
         BCK(eye_pass_multi(P<RenderInstDev>(b->t_render), P<int64_t>(b->t_px_off), b->n, b->total_px, R,
-                           P<unsigned>(b->status), b->st));
+                           b->req_split, P<unsigned>(b->status), b->st));
         L += 1;
     }
     if (stage < 0 || stage == 3) {
@@ -255,8 +256,8 @@ int launch_stages(pm_batch* b, int stage, int* launches) {
         Q.n = b->req_cap; Q.pos4 = R.a; Q.nrm4 = R.b; Q.flag_mask = 1u;
         GatherOut O{P<float>(b->est_g), nullptr, nullptr, nullptr};
         BCK(gather_multi(P<GatherInstDev>(b->t_gather), P<int64_t>(b->t_px_off), b->n, Q, R.c, R.counter,
-                         P<unsigned long long>(b->queues), O, b->gather_warps, b->sm_count, b->st));
-        L += 2;
+                         b->req_split, P<unsigned long long>(b->queues), O, b->gather_warps, b->sm_count, b->st));
+        L += (b->req_split > 0 ? 1 : 0) + (b->req_split < b->req_cap ? 1 : 0);
     }
     if (stage < 0 || stage == 4) {
         const float tone_t = (float)std::pow((double)0.6f, -1);
@@ -395,6 +396,7 @@ int create(pm_batch* b, const pm_batch_instance* in, int32_t n, const pm_batch_o
         R.cam.vw = I.camera.viewport_w; R.cam.vh = I.camera.viewport_h; R.cam.focal = I.camera.focal;
         R.cam.W = I.camera.width; R.cam.H = I.camera.height;
         R.max_depth = I.max_depth;
+        R.cls = gather_class(I.k);
     }
     b->path_off = offsets(b->paths);
     b->ph_off = offsets(caps);
@@ -403,6 +405,9 @@ int create(pm_batch* b, const pm_batch_instance* in, int32_t n, const pm_batch_o
     b->total_slots = b->ph_off.back();
     b->total_px = b->px_off.back();
     b->req_cap = offsets(req).back();
+    b->req_split = 0;
+    for (int i = 0; i < n; i++)
+        if (rt[(size_t)i].cls == 0) b->req_split += req[(size_t)i];
     if (b->total_slots >= ((int64_t)1 << 32) || b->total_paths >= ((int64_t)1 << 32) ||
         b->req_cap >= ((int64_t)1 << 32) || b->total_px >= ((int64_t)1 << 32))
         return bfail(b, PM_ERR_INVALID, "batch: more than 2^32 paths, photons, pixels or requests");
@@ -514,9 +519,9 @@ int pm_batch_frame(pm_batch* b, uint64_t frame) {
     }
     BCK(cudaEventRecord(b->ev1, b->st));
     std::vector<int64_t> tot((size_t)b->n);
-    unsigned long long nreq = 0;
+    unsigned long long nreq_cls[2] = {0, 0};   // requests of the two gather classes
     BCK(cudaMemcpyAsync(tot.data(), b->inst_total.p, (size_t)b->n * 8, cudaMemcpyDeviceToHost, b->st));
-    BCK(cudaMemcpyAsync(&nreq, b->req_counter.p, 8, cudaMemcpyDeviceToHost, b->st));
+    BCK(cudaMemcpyAsync(nreq_cls, b->req_counter.p, 16, cudaMemcpyDeviceToHost, b->st));
     BCK(cudaStreamSynchronize(b->st));
     b->ms_last = elapsed(b->ev0, b->ev1);
     b->photons_last = 0;
@@ -526,7 +531,7 @@ int pm_batch_frame(pm_batch* b, uint64_t frame) {
         b->photons_last += std::min(cap, tot[(size_t)i]);
         if (tot[(size_t)i] < cap) b->underfilled++;
     }
-    b->requests_last = (int64_t)nreq;
+    b->requests_last = (int64_t)(nreq_cls[0] + nreq_cls[1]);
     return check_batch_status(b);
 }
 

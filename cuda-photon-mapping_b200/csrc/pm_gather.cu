@@ -814,12 +814,13 @@ __device__ __forceinline__ int find_instance_px(const int64_t* __restrict__ off,
 }
 
 // Requests of several instances, one persistent work queue: warps take
-// request indices from *queue until *n_req (the eye pass's device counter) is
-// reached.  Request q belongs to the instance of its pixel (c.w bits, a
-// global pixel index in [px_off[i], px_off[i+1])) and is answered with that
-// instance's grid, r and k.  Only instances whose store class matches this
-// launch (cls) are answered here; the other requests are left for the other
-// launch.
+// MULTI_CHUNK request indices at a time from *queue until *n_req (the eye
+// pass's device counter of this class) is reached.  Request q belongs to the
+// instance of its pixel (c.w bits, a global pixel index in [px_off[i],
+// px_off[i+1])) and is answered with that instance's grid, r and k.  The eye
+// pass puts every request in its class's range, so an instance of another
+// store class never appears here; the check guards the store size.
+constexpr int MULTI_CHUNK = 4;
 template <int UCAP, int NW>
 __global__ void __launch_bounds__(NW * 32, 32 / NW)
 k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict__ px_off, int ninst,
@@ -831,20 +832,23 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
     const int64_t n = (int64_t)min(*n_req, (unsigned long long)Q.n);
     while (true) {
         unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(queue, 1ull);
-        const int64_t i = (int64_t)__shfl_sync(0xffffffffu, t, 0);
-        if (i >= n) break;
-        const int inst = find_instance_px(px_off, ninst, (int64_t)__float_as_uint(rec_c[i].w));
-        const GatherInstDev& T = tab[inst];
-        if (T.cls != cls) continue;
-        const float4 a = Q.pos4[i], b = Q.nrm4[i];
-        if (!((__float_as_uint(b.w) & Q.flag_mask) != 0u) || T.k <= 0) {
-            gather_zero(i, T.k, O, lane);
-            continue;
+        if (lane == 0) t = atomicAdd(queue, (unsigned long long)MULTI_CHUNK);
+        const int64_t q0 = (int64_t)__shfl_sync(0xffffffffu, t, 0);
+        if (q0 >= n) break;
+        const int64_t q1 = min(q0 + (int64_t)MULTI_CHUNK, n);
+        for (int64_t i = q0; i < q1; i++) {
+            const int inst = find_instance_px(px_off, ninst, (int64_t)__float_as_uint(rec_c[i].w));
+            const GatherInstDev& T = tab[inst];
+            if (T.cls != cls) continue;
+            const float4 a = Q.pos4[i], b = Q.nrm4[i];
+            if (!((__float_as_uint(b.w) & Q.flag_mask) != 0u) || T.k <= 0) {
+                gather_zero(i, T.k, O, lane);
+                continue;
+            }
+            const GatherGrid G = T.G;
+            gather_query<UCAP>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
+            __syncwarp();
         }
-        const GatherGrid G = T.G;
-        gather_query<UCAP>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
-        __syncwarp();
     }
 }
 
@@ -877,17 +881,33 @@ cudaError_t launch_multi(const GatherInstDev* tab, const int64_t* px_off, int ni
 }
 
 cudaError_t gather_multi(const GatherInstDev* tab, const int64_t* px_off, int ninst, const GatherQueries& Q,
-                         const float4* rec_c, const unsigned long long* n_req, unsigned long long* queues,
-                         const GatherOut& O, int warps, int sm_count, cudaStream_t st) {
+                         const float4* rec_c, const unsigned long long* n_req, int64_t split,
+                         unsigned long long* queues, const GatherOut& O, int warps, int sm_count, cudaStream_t st) {
     if (Q.n <= 0) return cudaSuccess;
+    if (split < 0 || split > Q.n || O.ids || O.cnt || O.rk || Q.idx) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(queues, 0, 16, st);
     if (e != cudaSuccess) return e;
+    // class 0: [0, split); class 1: the records from split on, indexed from 0
+    GatherQueries Q0 = Q, Q1 = Q;
+    Q0.n = split;
+    Q1.n = Q.n - split;
+    Q1.pos4 = Q.pos4 + split;
+    Q1.nrm4 = Q.nrm4 + split;
+    GatherOut O1 = O;
+    O1.rad = O.rad + 3 * split;
+    const float4* c1 = rec_c + split;
     if (warps == 4) {
-        if ((e = launch_multi<256, 4>(tab, px_off, ninst, Q, rec_c, n_req, queues, 0, O, sm_count, st)) != cudaSuccess) return e;
-        return launch_multi<512, 4>(tab, px_off, ninst, Q, rec_c, n_req, queues + 1, 1, O, sm_count, st);
+        if (Q0.n > 0 &&
+            (e = launch_multi<256, 4>(tab, px_off, ninst, Q0, rec_c, n_req, queues, 0, O, sm_count, st)) != cudaSuccess)
+            return e;
+        if (Q1.n > 0) e = launch_multi<512, 4>(tab, px_off, ninst, Q1, c1, n_req + 1, queues + 1, 1, O1, sm_count, st);
+        return e;
     }
-    if ((e = launch_multi<256, 8>(tab, px_off, ninst, Q, rec_c, n_req, queues, 0, O, sm_count, st)) != cudaSuccess) return e;
-    return launch_multi<512, 8>(tab, px_off, ninst, Q, rec_c, n_req, queues + 1, 1, O, sm_count, st);
+    if (Q0.n > 0 &&
+        (e = launch_multi<256, 8>(tab, px_off, ninst, Q0, rec_c, n_req, queues, 0, O, sm_count, st)) != cudaSuccess)
+        return e;
+    if (Q1.n > 0) e = launch_multi<512, 8>(tab, px_off, ninst, Q1, c1, n_req + 1, queues + 1, 1, O1, sm_count, st);
+    return e;
 }
 
 int gather_class(int k) { return k <= 96 ? 0 : 1; }

@@ -58,12 +58,14 @@ struct GatherInstDev {
 };
 int gather_class(int k);
 // Q: the request records (pos4 / nrm4 with flag_mask), Q.n = their capacity;
-// rec_c: their third records (global pixel bits in w); n_req: device count of
-// requests; queues: 2 device counters (scratch); px_off: ninst + 1 pixel
-// offsets; warps: block shape, 4 or 8 warps per block.  Two persistent
-// launches (store classes of k <= 96 and k <= 256).
+// rec_c: their third records (global pixel bits in w); the requests of class
+// 0 lie in [0, split), n_req[0] of them, those of class 1 in [split, Q.n),
+// n_req[1] of them (eye_pass_multi's layout); queues: 2 device counters
+// (scratch); px_off: ninst + 1 pixel offsets; warps: block shape, 4 or 8
+// warps per block.  Two persistent launches (store classes of k <= 96 and
+// k <= 256), each over its own range; O.rad only (ids, cnt, rk null).
 cudaError_t gather_multi(const GatherInstDev* tab, const int64_t* px_off, int ninst, const GatherQueries& Q,
-                         const float4* rec_c, const unsigned long long* n_req, unsigned long long* queues,
-                         const GatherOut& O, int warps, int sm_count, cudaStream_t st);
+                         const float4* rec_c, const unsigned long long* n_req, int64_t split,
+                         unsigned long long* queues, const GatherOut& O, int warps, int sm_count, cudaStream_t st);
 
 }  // namespace pm

@@ -274,20 +274,64 @@ __device__ __forceinline__ int find_pixel_instance(const int64_t* __restrict__ o
     return lo;
 }
 
+// eye_emit with the requests of class cls (0 or 1) in their own range:
+// class 0 at [0, split) from R.counter[0], class 1 at [split, R.cap) from
+// R.counter[1]; one scan carries both classes' counts (class 1 in the high 16
+// bits: at most 32 x RENDER_MAX_HITS per warp) and lane 31 reserves both
+__device__ __forceinline__ void eye_emit_split(Requests& R, int64_t split, bool valid, int cls, int64_t gi, int nh,
+                                               const float4* ha, const float4* hb, const float4* hc,
+                                               unsigned* status) {
+    static_assert(32 * RENDER_MAX_HITS < 65536, "per-class warp counts must fit 16 bits");
+    const int lane = threadIdx.x & 31;
+    const unsigned mine = (unsigned)nh << (cls ? 16 : 0);
+    unsigned incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const unsigned wtotal = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long b0 = 0, b1 = 0;
+    if (lane == 31) {
+        if (wtotal & 0xffffu) b0 = atomicAdd(R.counter, (unsigned long long)(wtotal & 0xffffu));
+        if (wtotal >> 16) b1 = atomicAdd(R.counter + 1, (unsigned long long)(wtotal >> 16));
+    }
+    b0 = __shfl_sync(0xffffffffu, b0, 31);
+    b1 = __shfl_sync(0xffffffffu, b1, 31);
+    if (!valid) return;
+    const unsigned excl = incl - mine;
+    const int64_t hi = cls ? R.cap : split;
+    const int64_t base = cls ? split + (int64_t)(b1 + (excl >> 16)) : (int64_t)(b0 + (excl & 0xffffu));
+    if (base + nh > hi) {
+        raise_status(status, ST_OVERFLOW);
+        R.px_base[gi] = 0;
+        R.px_count[gi] = 0;
+        return;
+    }
+    for (int k = 0; k < nh; k++) {
+        R.a[base + k] = ha[k];
+        R.b[base + k] = hb[k];
+        R.c[base + k] = hc[k];
+    }
+    R.px_base[gi] = (uint32_t)base;
+    R.px_count[gi] = (uint32_t)nh;
+}
+
 // all instances' pixels in one launch: global pixel g of instance i (off[i] <= g < off[i+1])
 __global__ void __launch_bounds__(EYE_THREADS)
 k_eye_multi(const RenderInstDev* __restrict__ tab, const int64_t* __restrict__ px_off, int ninst, int64_t npx,
-            Requests R, unsigned* status) {
+            Requests R, int64_t split, unsigned* status) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = g < npx;
     float4 ha[RENDER_MAX_HITS], hb[RENDER_MAX_HITS], hc[RENDER_MAX_HITS];
-    int nh = 0;
+    int nh = 0, cls = 0;
     if (valid) {
         const int i = find_pixel_instance(px_off, ninst, g);
         const RenderInstDev& T = tab[i];
+        cls = T.cls;
         nh = eye_hits(T.S, T.cam, T.max_depth, g - __ldg(px_off + i), (uint32_t)g, ha, hb, hc, status);
     }
-    eye_emit(R, valid, g, nh, ha, hb, hc, status);
+    eye_emit_split(R, split, valid, cls, g, nh, ha, hb, hc, status);
 }
 
 // combine pixel gi's requests with the scene's materials, tone-map, quantise
@@ -388,11 +432,12 @@ cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Req
 }
 
 cudaError_t eye_pass_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
-                           unsigned* status, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
+                           int64_t split, unsigned* status, cudaStream_t st) {
+    if (split < 0 || split > R.cap) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(R.counter, 0, 16, st);
     if (e != cudaSuccess || npx <= 0) return e;
     k_eye_multi<<<(unsigned)((npx + EYE_THREADS - 1) / EYE_THREADS), EYE_THREADS, 0, st>>>(tab, px_off, ninst, npx, R,
-                                                                                          status);
+                                                                                          split, status);
     return cudaGetLastError();
 }
 

@@ -44,9 +44,13 @@ struct RenderInstDev {
     DevScene S;
     CameraDev cam;
     int max_depth;
+    int cls;                  // the gather class of the instance's requests (0 or 1)
 };
+// The requests of class-0 instances go to [0, split) from R.counter[0], those
+// of class-1 instances to [split, R.cap) from R.counter[1] (R.counter: 2
+// device counters, zeroed here), so each gather launch visits its own range.
 cudaError_t eye_pass_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
-                           unsigned* status, cudaStream_t st);
+                           int64_t split, unsigned* status, cudaStream_t st);
 cudaError_t resolve_multi(const RenderInstDev* tab, const int64_t* px_off, int ninst, int64_t npx, Requests R,
                           const float* est_g, float tone_t, uint8_t* rgb8, float* radiance, cudaStream_t st);
 
