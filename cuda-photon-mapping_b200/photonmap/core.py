@@ -158,6 +158,8 @@ def library():
         "pm_obj_light_model": ([vp], C.c_int32),
         "pm_obj_free": ([vp], None),
         "pm_bvh_info": ([vp, vp, vp, vp], C.c_int),
+        "pm_write_ppm": ([C.c_char_p, vp, i32, i32], C.c_int),
+        "pm_write_pfm": ([C.c_char_p, vp, i32, i32], C.c_int),
         "pm_cache_gradient": ([vp, vp, vp, vp, vp, i64, vp, vp], C.c_int),
         "pm_cache_infer": ([vp, vp, vp, i64, vp], C.c_int),
         "pm_cache_get_params": ([vp, vp], C.c_int),
@@ -218,6 +220,38 @@ def load_obj(path, default_ior=1.0):
                             default_ior=float(desc.default_ior), names=names)
     finally:
         L.pm_obj_free(h)
+
+
+def _write_frame(fn, path, frame, itemsize, width, height):
+    """Call fn (pm_write_ppm / pm_write_pfm) on a frame buffer: a torch tensor
+    on any device, or a numpy array, of width * height * 3 contiguous items of
+    itemsize bytes."""
+    want = int(width) * int(height) * 3 * itemsize
+    host = None
+    if hasattr(frame, "data_ptr"):
+        if not frame.is_contiguous() or frame.numel() * frame.element_size() != want:
+            raise PMError(-1, f"{fn}: want {want} contiguous bytes")
+        ptr = C.c_void_p(frame.data_ptr())
+    else:
+        host = np.ascontiguousarray(frame)   # kept alive across the call
+        if host.nbytes != want:
+            raise PMError(-1, f"{fn}: want {want} bytes")
+        ptr = C.c_void_p(host.ctypes.data)
+    rc = getattr(library(), fn)(os.fspath(path).encode(), ptr, int(width), int(height))
+    if rc:
+        raise PMError(rc, fn)
+
+
+def write_ppm(path, rgb8, width, height):
+    """pm_write_ppm: an 8-bit frame in pm_render's layout (row 0 = bottom; uint8
+    tensor on the GPU or host, or numpy) as a binary PPM, top row first."""
+    _write_frame("pm_write_ppm", path, rgb8, 1, width, height)
+
+
+def write_pfm(path, radiance, width, height):
+    """pm_write_pfm: a float32 radiance frame in pm_render's layout as a colour
+    PFM (little-endian, rows bottom to top)."""
+    _write_frame("pm_write_pfm", path, radiance, 4, width, height)
 
 
 def camera_setup(position, direction, up, fov_deg, width, height) -> Camera:

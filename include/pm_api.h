@@ -215,6 +215,20 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, uin
 int pm_frame(pm_ctx* ctx, const pm_trace_opts* trace, const pm_grid_opts* grid, const pm_camera* cam,
              const pm_render_opts* opts, uint8_t* out_rgb8, float* out_radiance, int64_t* out_paths);
 
+/* Headless frame output, in place of the reference's GL pixel-buffer display
+ * (Drawer.cu:22-41, Window.cuh:88-126).  Both take a frame in pm_render's
+ * layout (row 0 = the bottom row, Camera.cuh:67-81) in device or host memory
+ * (device buffers are copied to the host first; the calling thread's current
+ * device must own them) and need no pm_ctx.
+ * pm_write_ppm: rgb8 = width*height*3 bytes, written as a binary PPM (P6,
+ * maxval 255), top row first.
+ * pm_write_pfm: radiance = width*height*3 floats, written as a colour PFM
+ * ("PF", scale -1.0: little-endian), whose rows run bottom to top like the
+ * canvas.  Errors: PM_ERR_INVALID (null, non-positive size), PM_ERR_CUDA (the
+ * device copy), PM_ERR_IO (the file). */
+int pm_write_ppm(const char* path, const uint8_t* rgb8, int32_t width, int32_t height);
+int pm_write_pfm(const char* path, const float* radiance, int32_t width, int32_t height);
+
 /* Device prefix sum used by the grid build (exposed for known-answer tests):
  * exclusive (inclusive = 0) or inclusive scan of n u32 device values. */
 int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive);
