@@ -554,7 +554,8 @@ def run_ours(args):
             "config": {"workload": args.workload, "photons": w["photons"], "max_bounces": w["max_bounces"],
                        "image": f"{W}x{H}", "k": w["k"], "radius": w["radius"], "eye_depth": w["max_depth"],
                        "triangles": sc.ntri, "bvh": bvh, "api": "pm_frame (photon pass + grid + frame)",
-                       "l2": "inputs larger than L2 (photon map ~0.5 GB)",
+                       "l2": f"inputs larger than L2 (grid records of the photon map "
+                             f"~{w['photons'] * 40 / 1e9:.1f} GB)",
                        "parallelism": f"replicas{world}"},
             "stages_ms": {"trace": stages[0], "grid": stages[1], "eye": stages[2], "gather": stages[3],
                           "resolve": stages[4]},
