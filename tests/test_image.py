@@ -55,6 +55,21 @@ def test_pfm_rows_bottom_first(tmp_path):
     assert np.array_equal(img, rad)
 
 
+def test_host_torch_tensors(tmp_path):
+    torch = pytest.importorskip("torch")
+    W, H = 3, 2
+    canvas = torch.arange(W * H * 3, dtype=torch.uint8)
+    photonmap.write_ppm(tmp_path / "t.ppm", canvas, W, H)
+    _, _, img = _read_ppm(tmp_path / "t.ppm")
+    assert np.array_equal(img, canvas.numpy().reshape(H, W, 3)[::-1])
+    rad = torch.linspace(0, 1, W * H * 3, dtype=torch.float32).reshape(W * H, 3)
+    photonmap.write_pfm(tmp_path / "t.pfm", rad, W, H)
+    _, _, fimg = _read_pfm(tmp_path / "t.pfm")
+    assert np.array_equal(fimg, rad.numpy().reshape(H, W, 3))
+    with pytest.raises(PMError):
+        photonmap.write_ppm(tmp_path / "t.ppm", canvas[::2], W, H)   # not contiguous
+
+
 def test_errors(tmp_path):
     canvas = np.zeros(4 * 2 * 3, np.uint8)
     with pytest.raises(PMError):
