@@ -36,7 +36,11 @@ newmtl lamp
 # faces in the forms the reference parses (v/vt/vn, v//vn), a quad model, a
 # triangle model with negative indices, a run split by an 's' line (the name
 # repeats: the second copy becomes "wall1"), a material without Ks (specular
-# stays Material()'s 1), an unknown material (all defaults)
+# stays Material()'s 1), an unknown material (all defaults).  Each model keeps
+# one face form: the reference's build_vertices (ObjLoader.cpp:102-105) reads
+# a texcoord index for every vertex once any face of the model had one, so a
+# model mixing v/vt/vn and v//vn faces makes it read past its index vector
+# (undefined behaviour, an occasional crash).
 OBJ = """mtllib box.mtl
 # floor: two quads
 g floor
@@ -52,7 +56,7 @@ vt 0 0
 vt 1 0
 vt 1 1
 f 1/1/1 2/2/1 3/3/1 4/1/1
-f 4//1 3//1 6//1 5//1
+f 4/1/1 3/2/1 6/3/1 5/1/1
 
 g wall
 usemtl red
