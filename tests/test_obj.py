@@ -214,6 +214,31 @@ f 1 2 3 4 5
     assert np.array_equal(sc.tri_nrm, np.broadcast_to(np.float32([0, 0, 1]), (6, 3, 3)))
 
 
+def test_mixed_face_forms_in_one_model(tmp_path):
+    """v/vt/vn and v//vn faces in one model (the reference's loader reads past
+    its texture-index vector here): positions and normals as indexed."""
+    obj = """mtllib box.mtl
+g light
+usemtl lamp
+v 0 0 0
+v 1 0 0
+v 1 1 0
+v 0 1 0
+vt 0 0
+vt 1 0
+vn 0 0 1
+vn 0 0.6 0.8
+f 1/1/1 2/2/1 3/1/2
+f 1//2 3//1 4//2
+"""
+    sc = photonmap.load_obj(_write(tmp_path, obj=obj))
+    assert sc.ntri == 2 and sc.nmodel == 1
+    v = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32)
+    n = np.array([[0, 0, 1], [0, 0.6, 0.8]], np.float32)
+    assert np.array_equal(sc.tri_pos, np.array([v[[0, 1, 2]], v[[0, 2, 3]]]))
+    assert np.array_equal(sc.tri_nrm, np.array([n[[0, 0, 1]], n[[1, 0, 1]]]))
+
+
 @pytest.mark.parametrize("obj, what", [
     ("g light\nf 1 2 3\n", "vertex index out of range"),
     ("v 0 0 0\nv 1 0 0\nf 1 2\n", "at least 3 vertices"),
