@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -53,6 +55,31 @@ void release(DevBuf& b) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
+}
+std::vector<DevBuf*> all_buffers(pm_ctx* ctx) {
+    std::vector<DevBuf*> v = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
+                              &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage,
+                              &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
+                              &ctx->scratch_pow, &ctx->req_a, &ctx->req_b, &ctx->req_c, &ctx->req_counter,
+                              &ctx->px_base, &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws,
+                              &ctx->cache_w32, &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad,
+                              &ctx->cache_loss, &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm,
+                              &ctx->probe_req, &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts,
+                              &ctx->fallback_list, &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order, &ctx->rq_keys,
+                              &ctx->rq_k0, &ctx->rq_k1, &ctx->rq_v0, &ctx->rq_v1, &ctx->rq_hist, &ctx->rq_ws};
+    for (auto& m : ctx->maps)
+        for (DevBuf* b : {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid, &m.keys0,
+                          &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small, &m.key_counts,
+                          &m.key_starts, &m.counts2})
+            v.push_back(b);
+    return v;
+}
+uint64_t buffer_fingerprint(const std::vector<DevBuf*>& bufs) {
+    uint64_t h = 1469598103934665603ull;   // FNV-1a over the buffers' addresses and sizes
+    for (DevBuf* b : bufs)
+        for (uint64_t w : {(uint64_t)(uintptr_t)b->p, (uint64_t)b->bytes})
+            for (int i = 0; i < 8; i++) h = (h ^ ((w >> (8 * i)) & 0xff)) * 1099511628211ull;
+    return h;
 }
 
 
@@ -290,23 +317,7 @@ void pm_destroy(pm_ctx* ctx) {
     if (ctx->frame_done) cudaEventDestroy(ctx->frame_done);
     if (ctx->train_fork) cudaEventDestroy(ctx->train_fork);
     if (ctx->train_done) cudaEventDestroy(ctx->train_done);
-    DevBuf* bufs[] = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
-                      &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->counter, &ctx->stage,
-                      &ctx->cnt_g, &ctx->cnt_c, &ctx->scan_g, &ctx->scan_c, &ctx->totals, &ctx->trace_ws,
-                      &ctx->scratch_pow, &ctx->req_a, &ctx->req_b, &ctx->req_c, &ctx->req_counter, &ctx->px_base,
-                      &ctx->px_count, &ctx->est_g, &ctx->est_c, &ctx->status, &ctx->gws, &ctx->cache_w32,
-                      &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss,
-                      &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm, &ctx->probe_req,
-                      &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts, &ctx->fallback_list,
-                      &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order, &ctx->rq_keys,
-                      &ctx->rq_k0, &ctx->rq_k1, &ctx->rq_v0, &ctx->rq_v1, &ctx->rq_hist, &ctx->rq_ws};
-    for (DevBuf* b : bufs) release(*b);
-    for (auto& m : ctx->maps) {
-        DevBuf* mb[] = {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid,
-                        &m.keys0, &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small,
-                        &m.key_counts, &m.key_starts, &m.counts2};
-        for (DevBuf* b : mb) release(*b);
-    }
+    for (DevBuf* b : all_buffers(ctx)) release(*b);
     for (auto& ev : ctx->ev) if (ev) cudaEventDestroy(ev);
     if (ctx->own_stream && ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
@@ -374,6 +385,7 @@ uint64_t splitmix64(uint64_t& x) {
 
 int pm_cache_init(pm_ctx* ctx, const pm_cache_opts* o) {
     if (!ctx || !o) return PM_ERR_INVALID;
+    ctx->generation++;
     if (!(o->lr >= 0.f) || !(o->beta1 >= 0.f && o->beta1 < 1.f) || !(o->beta2 >= 0.f && o->beta2 < 1.f) ||
         !(o->eps > 0.f) || !(o->out_scale > 0.f) || o->octave0 < 0 || o->octave0 > 8)
         return fail(ctx, PM_ERR_INVALID, "cache options: lr >= 0, 0 <= beta < 1, eps > 0, out_scale > 0, octave0 0..8");
@@ -563,6 +575,7 @@ int pm_stage_times(pm_ctx* ctx, float out_ms[8]) {
 
 int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
     if (!ctx || !sd) return PM_ERR_INVALID;
+    ctx->generation++;
     if (sd->ntri <= 0 || !sd->tri_pos || !sd->tri_nrm || !sd->tri_model || sd->nmodel <= 0 || !sd->materials)
         return fail(ctx, PM_ERR_INVALID, "scene: empty or missing arrays");
     if (sd->light_model < 0 || sd->light_model >= sd->nmodel) return fail(ctx, PM_ERR_INVALID, "scene: light_model out of range");
@@ -763,12 +776,17 @@ static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, Tr
 
 int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     if (!ctx || !o) return PM_ERR_INVALID;
+    ctx->generation++;
     if (o->global_capacity < 0 || o->caustic_capacity < 0) return fail(ctx, PM_ERR_INVALID, "negative capacity");
     CK(cudaSetDevice(ctx->device));
     const int64_t cg = o->global_capacity, cc = o->caustic_capacity;
     const int64_t max_paths = o->max_paths > 0 ? o->max_paths : 64 * std::max<int64_t>(std::max(cg, cc), 1);
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     MapState& C = ctx->maps[PM_MAP_CAUSTIC];
+    // the lists and grids are empty from here on: a failed allocation below
+    // (ensure releases a buffer before growing it) leaves no map in use
+    G.built = C.built = false;
+    G.n = C.n = 0;
     ENSURE(G.pos, std::max<int64_t>(cg, 1) * 12); ENSURE(G.dir, std::max<int64_t>(cg, 1) * 12); ENSURE(G.pow, std::max<int64_t>(cg, 1) * 12);
     ENSURE(C.pos, std::max<int64_t>(cc, 1) * 12); ENSURE(C.dir, std::max<int64_t>(cc, 1) * 12); ENSURE(C.pow, std::max<int64_t>(cc, 1) * 12);
     G.built = C.built = false;
@@ -875,9 +893,12 @@ int pm_trace_paths(pm_ctx* ctx, const pm_trace_opts* o, int64_t p0, int64_t p1, 
 
 int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const float* power, const float* dir) {
     if (!ctx || n < 0 || (n > 0 && (!pos || !power || !dir))) return PM_ERR_INVALID;
+    ctx->generation++;
     if (int rc = valid_map(ctx, map)) return rc;
     CK(cudaSetDevice(ctx->device));
     MapState& m = ctx->maps[map];
+    m.n = 0;            // empty until the new list is in place
+    m.built = false;
     ENSURE(m.pos, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.dir, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.pow, std::max<int64_t>(n, 1) * 12);
@@ -894,6 +915,7 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
 
 int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb) {
     if (!ctx) return PM_ERR_INVALID;
+    ctx->generation++;
     if (int rc = valid_map(ctx, map)) return rc;
     pm_grid_opts d = {1000, 5, 5, 0, 0};
     if (!o) o = &d;
@@ -906,6 +928,7 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     MapState& m = ctx->maps[map];
     const int64_t n = m.n;
     if (n == 0) return fail(ctx, PM_ERR_INVALID, "map has no photons");
+    m.built = false;   // until the new grid is complete (a failed allocation leaves no half grid in use)
     int d1[3], d2[3];
     float c1, c2;
     grid_dims(box, n, o->desired_per_cell, d1, &c1);
@@ -996,49 +1019,68 @@ int pm_save_photons(pm_ctx* ctx, int map, const char* path) {
     if (int rc = valid_map(ctx, map)) return rc;
     MapState& m = ctx->maps[map];
     const int64_t n = m.n;
-    std::vector<float> pos(3 * n), pw(3 * n), dir(3 * n);
-    if (n > 0) {
-        CK(cudaMemcpyAsync(pos.data(), m.pos.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaMemcpyAsync(pw.data(), m.pow.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaMemcpyAsync(dir.data(), m.dir.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
-    }
-    CK(cudaStreamSynchronize(ctx->st));
-    FILE* f = fopen(path, "wb");
-    if (!f) return fail(ctx, PM_ERR_IO, std::string("cannot open ") + path);
-    uint64_t cnt = (uint64_t)n;
-    bool ok = fwrite(&cnt, 8, 1, f) == 1;
-    std::vector<float> rec(9 * 4096);
-    for (int64_t i = 0; ok && i < n; i += 4096) {
-        int64_t k = std::min<int64_t>(4096, n - i);
-        for (int64_t j = 0; j < k; j++) {
-            std::memcpy(&rec[9 * j], &pos[3 * (i + j)], 12);
-            std::memcpy(&rec[9 * j + 3], &pw[3 * (i + j)], 12);
-            std::memcpy(&rec[9 * j + 6], &dir[3 * (i + j)], 12);
+    try {
+        std::vector<float> pos(3 * n), pw(3 * n), dir(3 * n);
+        if (n > 0) {
+            CK(cudaMemcpyAsync(pos.data(), m.pos.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaMemcpyAsync(pw.data(), m.pow.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaMemcpyAsync(dir.data(), m.dir.p, 12 * n, cudaMemcpyDeviceToHost, ctx->st));
         }
-        ok = fwrite(rec.data(), 36, (size_t)k, f) == (size_t)k;
+        CK(cudaStreamSynchronize(ctx->st));
+        FILE* f = fopen(path, "wb");
+        if (!f) return fail(ctx, PM_ERR_IO, std::string("cannot open ") + path);
+        uint64_t cnt = (uint64_t)n;
+        bool ok = fwrite(&cnt, 8, 1, f) == 1;
+        std::vector<float> rec(9 * 4096);
+        for (int64_t i = 0; ok && i < n; i += 4096) {
+            int64_t k = std::min<int64_t>(4096, n - i);
+            for (int64_t j = 0; j < k; j++) {
+                std::memcpy(&rec[9 * j], &pos[3 * (i + j)], 12);
+                std::memcpy(&rec[9 * j + 3], &pw[3 * (i + j)], 12);
+                std::memcpy(&rec[9 * j + 6], &dir[3 * (i + j)], 12);
+            }
+            ok = fwrite(rec.data(), 36, (size_t)k, f) == (size_t)k;
+        }
+        if (fclose(f) != 0) ok = false;
+        return ok ? PM_OK : fail(ctx, PM_ERR_IO, std::string("write failed: ") + path);
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, PM_ERR_OOM, "pm_save_photons: host memory");
     }
-    if (fclose(f) != 0) ok = false;
-    return ok ? PM_OK : fail(ctx, PM_ERR_IO, std::string("write failed: ") + path);
 }
 
+// The file is checked against its header before anything is allocated: the
+// reference's reader (Initializer.cu:102-141) trusts the count, and a corrupt
+// or truncated header must not turn into a huge allocation here.
 int pm_load_photons(pm_ctx* ctx, int map, const char* path) {
     if (!ctx || !path) return PM_ERR_INVALID;
     if (int rc = valid_map(ctx, map)) return rc;
-    FILE* f = fopen(path, "rb");
+    std::unique_ptr<FILE, int (*)(FILE*)> file(fopen(path, "rb"), fclose);
+    FILE* f = file.get();
     if (!f) return fail(ctx, PM_ERR_IO, std::string("cannot open ") + path);
     uint64_t cnt = 0;
-    if (fread(&cnt, 8, 1, f) != 1 || cnt > ((uint64_t)1 << 32)) { fclose(f); return fail(ctx, PM_ERR_IO, "bad photon count"); }
-    std::vector<float> rec(9 * (size_t)cnt);
-    size_t got = cnt ? fread(rec.data(), 36, (size_t)cnt, f) : 0;
-    fclose(f);
-    if (got != cnt) return fail(ctx, PM_ERR_IO, "truncated photon file");
-    std::vector<float> pos(3 * cnt), pw(3 * cnt), dir(3 * cnt);
-    for (size_t i = 0; i < cnt; i++) {
-        std::memcpy(&pos[3 * i], &rec[9 * i], 12);
-        std::memcpy(&pw[3 * i], &rec[9 * i + 3], 12);
-        std::memcpy(&dir[3 * i], &rec[9 * i + 6], 12);
+    long long bytes = -1;
+    if (fseek(f, 0, SEEK_END) == 0) bytes = (long long)ftello(f);
+    if (bytes < 8 || fseek(f, 0, SEEK_SET) != 0 || fread(&cnt, 8, 1, f) != 1)
+        return fail(ctx, PM_ERR_IO, "photon file: no count header");
+    if (cnt > ((uint64_t)1 << 32) || (uint64_t)(bytes - 8) / 36 < cnt)
+        return fail(ctx, PM_ERR_IO, "photon file: the count header needs " + std::to_string(cnt) +
+                                        " records, the file holds " + std::to_string((bytes - 8) / 36));
+    try {
+        std::vector<float> pos(3 * cnt), pw(3 * cnt), dir(3 * cnt), rec(9 * 4096);
+        for (uint64_t i = 0; i < cnt; i += 4096) {
+            const size_t k = (size_t)std::min<uint64_t>(4096, cnt - i);
+            if (fread(rec.data(), 36, k, f) != k) return fail(ctx, PM_ERR_IO, "truncated photon file");
+            for (size_t j = 0; j < k; j++) {
+                std::memcpy(&pos[3 * (i + j)], &rec[9 * j], 12);
+                std::memcpy(&pw[3 * (i + j)], &rec[9 * j + 3], 12);
+                std::memcpy(&dir[3 * (i + j)], &rec[9 * j + 6], 12);
+            }
+        }
+        file.reset();
+        return pm_set_photons(ctx, map, (int64_t)cnt, pos.data(), pw.data(), dir.data());
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, PM_ERR_OOM, "pm_load_photons: host memory");
     }
-    return pm_set_photons(ctx, map, (int64_t)cnt, pos.data(), pw.data(), dir.data());
 }
 
 
@@ -1359,6 +1401,18 @@ int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int i
     CK(scan_u32(in, out, n, inclusive, nullptr, ctx->gws.p, P<unsigned>(ctx->status), ctx->st));
     ctx->launches += 1;
     return check_status(ctx, "scan");
+}
+
+int pm_debug_scan_stall(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int64_t spin_limit,
+                        int32_t silent_tile) {
+    if (!ctx || n <= 0 || !in || !out || spin_limit < 1 || spin_limit > SCAN_SPIN_LIMIT || silent_tile < -1)
+        return PM_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    ENSURE(ctx->gws, scan_workspace_bytes(n));
+    CK(scan_u32(in, out, n, 1, nullptr, ctx->gws.p, P<unsigned>(ctx->status), ctx->st, (long long)spin_limit,
+                silent_tile));
+    ctx->launches += 1;
+    return check_status(ctx, "scan (stall test)");
 }
 
 }  // extern "C"

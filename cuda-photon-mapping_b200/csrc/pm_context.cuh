@@ -70,6 +70,10 @@ struct pm_ctx {
     cudaStream_t train_st = nullptr;
     cudaEvent_t train_fork = nullptr, train_done = nullptr;
     bool train_pending = false;
+    // bumped by every call that rebuilds or re-initialises what a captured
+    // learned graph reads (scene, photon lists, grids, cache): a graph made
+    // before such a call refuses to run
+    uint64_t generation = 0;
     // pm_frame's eye pass runs on its own stream beside the grid build
     cudaStream_t frame_st = nullptr;
     cudaEvent_t frame_fork = nullptr, frame_done = nullptr;
@@ -97,6 +101,10 @@ int cuda_fail(pm_ctx* c, cudaError_t e, const char* what);
 // grow-only device buffer (1/8 headroom on growth)
 cudaError_t ensure(DevBuf& b, size_t bytes);
 void release(DevBuf& b);
+// every device buffer the context owns; a hash of the addresses and sizes of
+// some buffers (changes whenever one of them is allocated, grown or released)
+std::vector<DevBuf*> all_buffers(pm_ctx* ctx);
+uint64_t buffer_fingerprint(const std::vector<DevBuf*>& bufs);
 template <class T> T* P(DevBuf& b) { return (T*)b.p; }
 DevScene dev_scene(pm_ctx* c);
 // reads and clears the device status word; PM_ERR_TIMEOUT / PM_ERR_OVERFLOW

@@ -14,8 +14,13 @@
 // check, with no host round trip inside it.  The graph owns its request and
 // estimate buffers; it reads the context's scene, photon map and cache, and
 // must be created again after any of those is rebuilt or re-initialised
-// (pm_set_scene, pm_build_grid, pm_cache_init): their device addresses and the
-// cache's encoding box are part of the captured launches.
+// (pm_set_scene, pm_set_photons / pm_load_photons, pm_trace_photons,
+// pm_build_grid, pm_frame, pm_cache_init): their device addresses, the grid's
+// dimensions and the cache's encoding box are part of the captured launches.
+// The graph records the context's generation and the addresses and sizes of
+// the context buffers its launches read (scene, both maps, cache, status word)
+// when it is made; pm_learned_graph_run refuses to launch (PM_ERR_INVALID)
+// when either has changed since.
 #include <algorithm>
 #include <cmath>
 #include "pm_context.cuh"
@@ -46,6 +51,8 @@ struct pm_learned_graph {
     DevBuf req_a, req_b, req_c, counter, px_base, px_count, est_mlp, est_fb, est_g;
     DevBuf probe_pos, probe_nrm, probe_req, probe_est, tile_flag, counts, fb_list, state, eye_order;
     int launches_per_frame = 0;
+    // the context as the captured launches saw it
+    uint64_t generation = 0, buffers = 0;
     // training runs on a second stream beside the eye pass and the probe
     // gathers (it needs neither; inference waits for it)
     cudaStream_t side = nullptr;
@@ -71,6 +78,19 @@ Requests requests_of(pm_learned_graph* g) {
     R.px_base = P<uint32_t>(g->px_base);
     R.px_count = P<uint32_t>(g->px_count);
     return R;
+}
+
+// the context buffers the captured launches read
+uint64_t read_set(pm_ctx* ctx) {
+    std::vector<DevBuf*> v = {&ctx->tri, &ctx->tri_pos, &ctx->tri_nrm, &ctx->tri_diffuse, &ctx->nodes, &ctx->prim,
+                              &ctx->maabb, &ctx->mats, &ctx->ca, &ctx->tri_leaf, &ctx->status, &ctx->cache_w32,
+                              &ctx->cache_w16, &ctx->cache_m, &ctx->cache_v, &ctx->cache_grad, &ctx->cache_loss};
+    for (auto& m : ctx->maps)
+        for (DevBuf* b : {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid, &m.keys0,
+                          &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small, &m.key_counts,
+                          &m.key_starts, &m.counts2})
+            v.push_back(b);
+    return buffer_fingerprint(v);
 }
 
 // every launch of one frame, on ctx->st (captured or eager)
@@ -276,6 +296,8 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
     if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph: end capture"));
     if ((e = cudaGraphInstantiate(&g->exec, g->graph, 0)) != cudaSuccess)
         return bail(cuda_fail(ctx, e, "learned graph: instantiate"));
+    g->generation = ctx->generation;
+    g->buffers = read_set(ctx);
     *out = g;
     return PM_OK;
 }
@@ -283,6 +305,9 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
 int pm_learned_graph_run(pm_learned_graph* g, pm_learned_stats* out_stats) {
     if (!g) return PM_ERR_INVALID;
     pm_ctx* ctx = g->ctx;
+    if (g->generation != ctx->generation || g->buffers != read_set(ctx))
+        return fail(ctx, PM_ERR_INVALID, "learned graph: the scene, a photon map or the cache was rebuilt or "
+                                         "re-initialised since the graph was made; make it again");
     CK(cudaSetDevice(ctx->device));
     if (int rc = cache_fence(ctx)) return rc;
     // the step number follows the context's (training calls between frames count too)

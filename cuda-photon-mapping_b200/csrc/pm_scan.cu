@@ -23,7 +23,8 @@ __device__ __forceinline__ unsigned long long poll(const unsigned long long* st)
 
 __global__ void __launch_bounds__(SCAN_THREADS)
 k_scan_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t n, int inclusive,
-           unsigned long long* tile_state, unsigned* tile_counter, uint32_t* total, unsigned* status) {
+           unsigned long long* tile_state, unsigned* tile_counter, uint32_t* total, unsigned* status,
+           long long spin_limit, int silent_tile) {
     __shared__ uint32_t s_items[SCAN_TILE + SCAN_TILE / 32];
     __shared__ uint32_t s_warp[SCAN_THREADS / 32];
     __shared__ uint32_t s_prefix;
@@ -69,10 +70,11 @@ k_scan_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t 
     // decoupled look-back (warp 0)
     if (warp == 0) {
         uint32_t exclusive = 0;
+        const bool speaks = tile != silent_tile;   // silent_tile: the test hook's tile that publishes nothing
         if (tile == 0) {
-            if (lane == 0) publish(tile_state + tile, FLAG_PREFIX, block_total);
+            if (lane == 0 && speaks) publish(tile_state + tile, FLAG_PREFIX, block_total);
         } else {
-            if (lane == 0) publish(tile_state + tile, FLAG_AGG, block_total);
+            if (lane == 0 && speaks) publish(tile_state + tile, FLAG_AGG, block_total);
             int pred = tile - 1;
             long long spins = 0;
             bool timed_out = false;
@@ -82,7 +84,7 @@ k_scan_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t 
                 if (p >= 0) {
                     s = poll(tile_state + p);
                     while ((s >> 32) == 0ull) {
-                        if (++spins > SCAN_SPIN_LIMIT) { timed_out = true; break; }
+                        if (++spins > spin_limit) { timed_out = true; break; }
                         s = poll(tile_state + p);
                     }
                 }
@@ -100,7 +102,7 @@ k_scan_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t 
                 if (prefix_mask) break;
                 pred -= 32;
             }
-            if (lane == 0) publish(tile_state + tile, FLAG_PREFIX, exclusive + block_total);
+            if (lane == 0 && speaks) publish(tile_state + tile, FLAG_PREFIX, exclusive + block_total);
         }
         if (lane == 0) s_prefix = exclusive;
     }
@@ -126,7 +128,7 @@ k_scan_u32(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t 
 }  // namespace
 
 cudaError_t scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive, uint32_t* total, void* ws,
-                     unsigned* status, cudaStream_t st) {
+                     unsigned* status, cudaStream_t st, long long spin_limit, int silent_tile) {
     if (n <= 0) {
         if (total) return cudaMemsetAsync(total, 0, 4, st);
         return cudaSuccess;
@@ -136,7 +138,8 @@ cudaError_t scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive
     unsigned* counter = (unsigned*)(state + tiles);
     cudaError_t e = cudaMemsetAsync(ws, 0, (size_t)tiles * 8 + 8, st);
     if (e != cudaSuccess) return e;
-    k_scan_u32<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, inclusive, state, counter, total, status);
+    k_scan_u32<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, inclusive, state, counter, total, status,
+                                                           spin_limit, silent_tile);
     return cudaGetLastError();
 }
 
@@ -196,7 +199,8 @@ extern "C" int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n,
     // tile states, the tile counter and the status word must start at zero
     if (cudaMemsetAsync(state, 0, (size_t)tiles * 8, st) != cudaSuccess) return PM_ERR_CUDA;
     if (cudaMemsetAsync(counter, 0, 16, st) != cudaSuccess) return PM_ERR_CUDA;
-    k_scan_u32<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, inclusive, state, counter, nullptr, status);
+    k_scan_u32<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, out, n, inclusive, state, counter, nullptr, status,
+                                                           SCAN_SPIN_LIMIT, -1);
     if (cudaGetLastError() != cudaSuccess) return PM_ERR_CUDA;
     unsigned bits = 0;
     if (cudaMemcpyAsync(&bits, status, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PM_ERR_CUDA;

@@ -27,7 +27,11 @@ inline size_t scan_workspace_bytes(int64_t n) {
 
 // exclusive (inclusive = 0) or inclusive scan of n u32 values; *total (device,
 // may be null) receives the sum of all n values.  ws: scan_workspace_bytes(n).
+// spin_limit: polls of one look-back wait before it gives up (ST_TIMEOUT);
+// silent_tile >= 0 (test hook only) makes that tile publish nothing, so every
+// later tile's look-back runs into the limit.
 cudaError_t scan_u32(const uint32_t* in, uint32_t* out, int64_t n, int inclusive, uint32_t* total, void* ws,
-                     unsigned* status, cudaStream_t st);
+                     unsigned* status, cudaStream_t st, long long spin_limit = SCAN_SPIN_LIMIT,
+                     int silent_tile = -1);
 
 }  // namespace pm

@@ -143,6 +143,7 @@ def library():
         "pm_camera_setup": ([vp, vp, vp, f32, i32, i32, C.POINTER(Camera)], C.c_int),
         "pm_render": ([vp, C.POINTER(Camera), C.POINTER(_RenderOpts), vp, vp], C.c_int),
         "pm_scan_u32": ([vp, vp, vp, i64, C.c_int], C.c_int),
+        "pm_debug_scan_stall": ([vp, vp, vp, i64, i64, i32], C.c_int),
         "pm_stage_times": ([vp, vp], C.c_int),
         "pm_status": ([vp, vp], C.c_int),
         "pm_launch_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
@@ -566,6 +567,16 @@ class Context:
         x = x.to(self.device, torch.int32).contiguous()
         out = torch.empty_like(x)
         self._check(self.L.pm_scan_u32(self.h, _ptr(x), _ptr(out), x.numel(), int(inclusive)), "pm_scan_u32")
+        return out
+
+    def debug_scan_stall(self, x, spin_limit, silent_tile):
+        """Test hook: the inclusive scan with each look-back wait limited to
+        spin_limit polls and tile silent_tile publishing nothing (pm_debug_scan_stall)."""
+        torch = self.torch
+        x = x.to(self.device, torch.int32).contiguous()
+        out = torch.empty_like(x)
+        self._check(self.L.pm_debug_scan_stall(self.h, _ptr(x), _ptr(out), x.numel(), int(spin_limit),
+                                               int(silent_tile)), "pm_debug_scan_stall")
         return out
 
     def stage_times(self):

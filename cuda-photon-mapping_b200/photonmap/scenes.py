@@ -213,6 +213,29 @@ def cornell(sphere_level=3, heightfield_n=0, seed=0, light_offset=(0.0, 0.0, 0.0
                  tri_diffuse=tri_diffuse, names=tuple(q[4] for q in parts))
 
 
+def split_model(sc: Scene, model: int) -> Scene:
+    """The same scene with `model` split into one model per triangle, each with
+    the model's material and its triangle's albedo as diffuse.  The reference
+    holds one material per model (CudaPhotonMapping/Model.cuh:24-28), so this is
+    how a per-triangle albedo is written in its terms; the models after `model`
+    (and the light's index) move up by its triangle count minus one."""
+    tri = np.nonzero(sc.tri_model == model)[0]
+    n = tri.size
+    mats = sc.materials
+    split = np.repeat(mats[model:model + 1], n, 0).copy()
+    if sc.tri_diffuse is not None:
+        split[:, 0:3] = sc.tri_diffuse[tri]
+    new_mats = np.concatenate([mats[:model], split, mats[model + 1:]]).astype(np.float32)
+    tm = sc.tri_model.astype(np.int64).copy()
+    tm[sc.tri_model > model] += n - 1
+    tm[tri] = model + np.arange(n)
+    names = tuple(sc.names[:model]) + tuple(f"{sc.names[model]}_{i}" for i in range(n)) + tuple(sc.names[model + 1:]) \
+        if sc.names else ()
+    light = sc.light_model + (n - 1 if sc.light_model > model else 0)
+    return Scene(sc.tri_pos, sc.tri_nrm, tm.astype(np.int32), new_mats, light_model=light,
+                 light_intensity=sc.light_intensity, default_ior=sc.default_ior, tri_diffuse=None, names=names)
+
+
 def default_camera(width, height):
     return CameraSpec((0.0, 0.0, 3.5), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 45.0, width, height)
 

@@ -233,6 +233,18 @@ int pm_write_pfm(const char* path, const float* radiance, int32_t width, int32_t
  * exclusive (inclusive = 0) or inclusive scan of n u32 device values. */
 int pm_scan_u32(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int inclusive);
 
+/* Test hook for the bounded device waits (no counterpart in the reference,
+ * whose grid scan waits on a spin barrier without a limit,
+ * CudaGridSynchronizer.cuh:13-27): the inclusive look-back scan of
+ * pm_scan_u32 with each wait limited to spin_limit polls (1 .. 2^22) and tile
+ * silent_tile (tiles of 4096 values; -1: none) publishing nothing, so the
+ * tiles after it wait on a flag that nothing sets.  Their waits give up, the
+ * kernel ends normally and the call returns PM_ERR_TIMEOUT with the context
+ * still usable (out then holds no valid sums).  With silent_tile = -1 it is
+ * pm_scan_u32 (inclusive). */
+int pm_debug_scan_stall(pm_ctx* ctx, const uint32_t* in, uint32_t* out, int64_t n, int64_t spin_limit,
+                        int32_t silent_tile);
+
 /* Allocation-free scan (no counterpart in the reference).  For callers that
  * may not allocate device memory: hosts that reserve the whole device for their
  * own pool, or frame loops that must not call cudaMalloc / cudaFree (which can

@@ -2,6 +2,7 @@
 
 ``Oracle``     -> oracle/_build/liboracle.so (CPU restatement, pm_oracle.cpp)
 ``RefHost``    -> oracle/_ref/libref_host.so (the reference's own host render code)
+``RefTrace``   -> oracle/_ref/libref_trace.so (the reference's own photon tracer, as host code)
 
 Only tests/, __graft_entry__.smoke() and bench.py's reference / cpu_baseline leg
 import this module.  Build both libraries with ``make -C oracle``.
@@ -17,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_host.so")
+REF_TRACE_SO = os.path.join(HERE, "_ref", "libref_trace.so")
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
@@ -278,6 +280,8 @@ class RefHost:
         L.ref_hdr.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         L.ref_gather.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_float] + [C.c_void_p] * 5 + \
             [C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_int] + [C.c_void_p] * 5
+        L.ref_grid_sizing.restype = C.c_int
+        L.ref_grid_sizing.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_render.argtypes = ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int,
                                   C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_float] +
                                  [C.c_void_p] * 5 + [C.c_int, C.c_void_p, C.c_float] + [C.c_void_p] * 5 +
@@ -316,6 +320,15 @@ class RefHost:
         out = np.empty_like(rgb)
         self.L.ref_hdr(rgb.shape[0], _ptr(rgb), _ptr(out))
         return out
+
+    def grid_sizing(self, pos, aabb, desired=1000):
+        """The reference's grid sizing + density re-grid for these photon positions:
+        (dims, cell, regridded, largest cell count of the first grid)."""
+        pos = _c(pos, np.float32).reshape(-1, 3)
+        dims = np.empty(3, np.int32); cell = np.empty(1, np.float32); mx = np.empty(1, np.uint32)
+        rg = self.L.ref_grid_sizing(pos.shape[0], _ptr(pos), _ptr(_c(aabb, np.float32)), int(desired), _ptr(dims),
+                                    _ptr(cell), _ptr(mx))
+        return dims, float(cell[0]), bool(rg), int(mx[0])
 
     def gather(self, g: GridResult, qpos, qnrm, radius, k):
         qpos = _c(qpos, np.float32).reshape(-1, 3); qnrm = _c(qnrm, np.float32).reshape(-1, 3)
@@ -368,3 +381,73 @@ class _RefScene:
             int(cargs[0]), _ptr(cargs[1]), float(cargs[2]), *[_ptr(x) for x in cargs[3:]],
             int(max_depth), float(def_ior), int(k), int(k_c), _ptr(ldr), _ptr(rgb))
         return dict(ldr=ldr, rgb8=rgb)
+
+
+class RefTrace:
+    """The reference's own photon tracer (CudaPhotonMapping/PhotonTracing.cu and
+    what it calls), compiled as host code and driven one path at a time by
+    oracle/ref_host/ref_trace.cu.  Its bounce limit is the reference's fixed 10."""
+
+    MAX_BOUNCES = 10
+
+    def __init__(self, path: str = REF_TRACE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference is mounted")
+        L = C.CDLL(path)
+        self.L = L
+        L.ref_trace_scene_create.restype = C.c_void_p
+        L.ref_trace_scene_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_int, C.c_void_p]
+        L.ref_trace_scene_destroy.argtypes = [C.c_void_p]
+        L.ref_trace_critical_angles.restype = C.c_int
+        L.ref_trace_critical_angles.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_int]
+        L.ref_trace_paths.argtypes = ([C.c_void_p, C.c_float, C.c_uint64, C.c_uint32, C.c_int64, C.c_int64,
+                                       C.c_int64, C.c_int] + [C.c_void_p] * 12)
+
+    def scene(self, sc):
+        """A reference scene (one Model per model index).  The reference holds one
+        material per model, so a per-triangle diffuse override is not representable."""
+        if sc.tri_diffuse is not None:
+            raise ValueError("the reference's Model has one material per model: no per-triangle diffuse")
+        keep = [_c(sc.tri_pos, np.float32), _c(sc.tri_nrm, np.float32), _c(sc.tri_model, np.int32),
+                _c(sc.materials, np.float32), _c(sc.light_intensity, np.float32)]
+        h = self.L.ref_trace_scene_create(sc.ntri, _ptr(keep[0]), _ptr(keep[1]), _ptr(keep[2]), sc.nmodel,
+                                          _ptr(keep[3]), int(sc.light_model), _ptr(keep[4]))
+        return _RefTraceScene(self, h, float(sc.default_ior))
+
+
+class _RefTraceScene:
+    def __init__(self, ref: RefTrace, h, default_ior):
+        self.ref = ref
+        self.h = h
+        self.default_ior = default_ior
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_trace_scene_destroy(self.h)
+        except Exception:
+            pass
+
+    def critical_angles(self):
+        """(n1, n2, cos) rows of the reference's critical-angle hash table, in slot order."""
+        out = np.empty(3 * 1024, np.float32)
+        n = self.ref.L.ref_trace_critical_angles(self.h, self.default_ior, _ptr(out), 1024)
+        return out[:3 * min(n, 1024)].reshape(-1, 3)
+
+    def trace_paths(self, seed, power_cap, p0, p1, tag=0, threads=None):
+        n = p1 - p0
+        cap = n * RefTrace.MAX_BOUNCES
+        counts = np.empty((n, 2), np.int32)
+        draws = np.empty(n, np.int32)
+        gp = np.empty((cap, 3), np.float32); gw = np.empty_like(gp); gd = np.empty_like(gp)
+        gb = np.empty(cap, np.int32)
+        cp = np.empty((cap, 3), np.float32); cw = np.empty_like(cp); cd = np.empty_like(cp)
+        cb = np.empty(cap, np.int32)
+        ng = np.zeros(1, np.int64); nc = np.zeros(1, np.int64)
+        threads = threads or max(1, os.cpu_count() or 1)
+        self.ref.L.ref_trace_paths(self.h, self.default_ior, seed, tag, power_cap, p0, p1, int(threads),
+                                   _ptr(counts), _ptr(draws), _ptr(gp), _ptr(gw), _ptr(gd), _ptr(gb),
+                                   _ptr(cp), _ptr(cw), _ptr(cd), _ptr(cb), _ptr(ng), _ptr(nc))
+        return dict(counts=counts, draws=draws, g_pos=gp[:ng[0]], g_pow=gw[:ng[0]], g_dir=gd[:ng[0]],
+                    g_bounce=gb[:ng[0]], c_pos=cp[:nc[0]], c_pow=cw[:nc[0]], c_dir=cd[:nc[0]],
+                    c_bounce=cb[:nc[0]])

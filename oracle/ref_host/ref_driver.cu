@@ -53,6 +53,8 @@ PM_REACH(G_size, PhotonGrid, GridSize3D, grid_size)
 PM_REACH(G_cell, PhotonGrid, float, cell_size)
 PM_REACH(G_starts, PhotonGrid, uint*, cell_starts)
 PM_REACH(G_sizes, PhotonGrid, uint*, cell_sizes)
+struct G_sizing { typedef void (PhotonGrid::*type)(int); friend type member(G_sizing); };
+template struct Reach<G_sizing, &PhotonGrid::compute_grid_and_cell_size>;
 }  // namespace
 
 // the reference's check_cuda lives in CudaUtils.cu, whose static CudaSynchronizer
@@ -61,22 +63,9 @@ void check_cuda(cudaError_t result, char const* const func, const char* const fi
     if (result) fprintf(stderr, "cuda error %d at %s:%d %s\n", (int)result, file, line, func);
 }
 
-namespace {
-
-struct HostScene {
-    std::vector<cpm::vec3*> pos, nrm;
-    std::vector<Model> models;
-    LightSource light;
-    Camera camera;
-    ~HostScene() {
-        for (auto p : pos) delete[] p;
-        for (auto p : nrm) delete[] p;
-    }
-};
-
-static cpm::vec3 V(const float* p) { return cpm::vec3(p[0], p[1], p[2]); }
-
-}  // namespace
+#include "ref_scene.h"
+using ref_host::HostScene;
+using ref_host::V;
 
 extern "C" {
 
@@ -85,30 +74,7 @@ extern "C" {
 // model indices, as CPM/Initializer.cu:11-16 assigns them.
 void* ref_scene_create(int ntri, const float* pos, const float* nrm, const int* tri_model,
                        int nmodel, const float* mats, int light_model, const float* light_intensity) {
-    HostScene* s = new HostScene();
-    s->models.reserve(nmodel);
-    for (int m = 0; m < nmodel; m++) {
-        int first = -1, count = 0;
-        for (int t = 0; t < ntri; t++) if (tri_model[t] == m) { if (first < 0) first = t; count++; }
-        cpm::vec3* P = new cpm::vec3[3 * count];
-        cpm::vec3* N = new cpm::vec3[3 * count];
-        for (int i = 0; i < 3 * count; i++) { P[i] = V(pos + 9 * first + 3 * i); N[i] = V(nrm + 9 * first + 3 * i); }
-        s->pos.push_back(P); s->nrm.push_back(N);
-        ModelConstructInfo mci;
-        mci.positions = P; mci.normals = N; mci.texcoords = nullptr;
-        mci.size = 3 * count; mci.primitives_size = count; mci.type = ModelType::Triangle; mci.smooth = false;
-        const float* q = mats + 12 * m;
-        Material mat;
-        mat.diffuse = V(q); mat.specular = V(q + 3); mat.emission = V(q + 6);
-        mat.refr_index = q[9]; mat.opaque = q[10]; mat.shininess = q[11];
-        mci.material = mat;
-        AABB box(P, 3 * count);
-        s->models.push_back(Model(mci, m, box));
-    }
-    s->light = LightSource();
-    s->light.intensity = V(light_intensity);
-    s->light.model_owner = &s->models[light_model];
-    return s;
+    return ref_host::make_scene(ntri, pos, nrm, tri_model, nmodel, mats, light_model, light_intensity);
 }
 void ref_scene_destroy(void* h) { delete (HostScene*)h; }
 
@@ -235,6 +201,39 @@ void ref_gather(int nph, const float* aabb, const int* dims, float cell, const u
                                                     V(qnrm + 3 * i), 0, 1);
         out_rad[3 * i] = c.x; out_rad[3 * i + 1] = c.y; out_rad[3 * i + 2] = c.z;
     }
+}
+
+// The reference's grid sizing for n photons in the scene box aabb (min xyz,
+// max xyz): PhotonGrid(n, aabb) + compute_grid_and_cell_size(desired)
+// (CPM/PhotonGrid.cu:41-56), the per-cell counts of analyze_density's kernel
+// taken on the host with the reference's hash_position (:10-38, :76-90), and
+// analyze_density's re-grid rule (:112-116): a cell above 5 x desired means
+// compute_grid_and_cell_size(desired / 5).  out_dims / out_cell: the final
+// grid; out_max: the largest cell count of the first grid; returns 1 when the
+// re-grid happened.
+int ref_grid_sizing(int n, const float* pos, const float* aabb, int desired, int* out_dims, float* out_cell,
+                    uint32_t* out_max) {
+    AABB box;
+    for (int i = 0; i < 6; i++) box.corners[i] = aabb[i];
+    PhotonGrid g(n, box);
+    (g.*member(G_sizing()))(desired);
+    const GridSize3D gs = g.*member(G_size());
+    const float cell = g.*member(G_cell());
+    std::vector<uint32_t> counts((size_t)gs.x * gs.y * gs.z, 0);
+    const cpm::vec3 mn(aabb[0], aabb[1], aabb[2]);
+    for (int i = 0; i < n; i++) counts[hash_position(mn, V(pos + 3 * (size_t)i), gs, cell)]++;
+    uint32_t mx = 0;
+    for (uint32_t c : counts) mx = std::max(mx, c);
+    *out_max = mx;
+    int regrid = 0;
+    if (mx > 5 * desired) {
+        (g.*member(G_sizing()))(desired / 5);
+        regrid = 1;
+    }
+    const GridSize3D f = g.*member(G_size());
+    out_dims[0] = f.x; out_dims[1] = f.y; out_dims[2] = f.z;
+    *out_cell = g.*member(G_cell());
+    return regrid;
 }
 
 // The reference's CPU mode over pixel rows [y0, y1): per pixel, Camera ray +

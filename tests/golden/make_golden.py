@@ -5,7 +5,11 @@ Run in a container where the reference is mounted (it reads the reference's
 oracle/_ref/libref_host.so, which `make -C oracle ref` compiles from the
 reference sources in place):
 
-    make -C oracle all && python tests/golden/make_golden.py
+    make -C oracle all && python tests/golden/make_golden.py [fixture100] [cornell] [tracer] [grid]
+
+(no argument: all four; `cornell` continues the random stream of `fixture100`,
+so those two are written together).  The reference root is $PM_REFERENCE_ROOT (default
+/root/reference).
 
 Outputs (all small .npz files, committed):
   fixture100.npz  the reference's 100-photon map (CudaPhotonMapping/global_map_test.txt,
@@ -17,6 +21,14 @@ Outputs (all small .npz files, committed):
                   rays, Ray::reflect / refract, HDR, gathers for 512 points and the CPU-mode
                   render (Raytracer::render_trace per pixel) of an 80 x 60 frame over a
                   20k-photon map traced by the oracle (seed 0; its checksum is stored).
+  tracer_ref.npz  the reference's own photon tracer (CudaPhotonMapping/PhotonTracing.cu and the
+                  functions it calls, compiled as host code into oracle/_ref/libref_trace.so) on
+                  the cases of tests/golden/ref_cases.py: per case the checksum of the whole
+                  path range and, for its first paths, the per-path counts and draws and the
+                  photon records.
+  grid_sizing_ref.npz  the reference's grid sizing and density re-grid (PhotonGrid(n, aabb),
+                  compute_grid_and_cell_size, analyze_density's rule; CudaPhotonMapping/PhotonGrid.cu:41-141)
+                  on the seeded photon sets of tests/golden/ref_cases.py GRID_CASES.
 """
 from __future__ import annotations
 
@@ -29,11 +41,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, os.path.join(ROOT, "cuda-photon-mapping_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 from photonmap import scenes  # noqa: E402
-from oracle import Oracle, RefHost  # noqa: E402
+from oracle import Oracle, RefHost, RefTrace  # noqa: E402
+import ref_cases  # noqa: E402
 
-REF_DUMP = "/root/reference/CudaPhotonMapping/global_map_test.txt"
+REF_ROOT = os.environ.get("PM_REFERENCE_ROOT", "/root/reference")
+REF_DUMP = os.path.join(REF_ROOT, "CudaPhotonMapping", "global_map_test.txt")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -49,16 +64,26 @@ def photons_checksum(tr):
     return int(np.bitwise_xor.reduce(h * np.arange(1, h.size + 1, dtype=np.uint32)))
 
 
-def main():
+def main(parts):
     orc, ref = Oracle(), RefHost()
+    rng = np.random.default_rng(7)
+    if "fixture100" in parts:
+        make_fixture100(orc, ref, rng)
+    if "cornell" in parts:
+        make_cornell(orc, ref, rng)
+    if "tracer" in parts:
+        make_tracer()
+    if "grid" in parts:
+        make_grid_sizing(ref)
+    print("wrote", os.listdir(OUT))
 
-    # ---------------------------------------------------------------- fixture100
+
+def make_fixture100(orc, ref, rng):
     pos, powr, dirs = read_dump(REF_DUMP)
     lo = pos.min(0) - 0.05
     hi = pos.max(0) + 0.05
     aabb = np.concatenate([lo, hi]).astype(np.float32)
     g = orc.grid_build(pos, powr, dirs, aabb, desired=10)
-    rng = np.random.default_rng(7)
     q = (pos[rng.integers(0, len(pos), 300)] + rng.normal(scale=0.1, size=(300, 3))).astype(np.float32)
     qn = rng.normal(size=(300, 3)).astype(np.float32)
     qn /= np.linalg.norm(qn, axis=1, keepdims=True)
@@ -69,7 +94,8 @@ def main():
                         dims=g.dims, cell=np.float32(g.cell), starts=g.starts, sizes=g.sizes, q=q, qn=qn, k=k, r=r,
                         ref_ids=ids, ref_dist=dist, ref_cnt=cnt, ref_full=full, ref_rad=rad)
 
-    # ---------------------------------------------------------------- cornell
+
+def make_cornell(orc, ref, rng):
     sc, _, _ = scenes.workload("cornell_small")
     cam = scenes.default_camera(80, 60)
     os_, rs = orc.scene(sc), ref.scene(sc)
@@ -113,8 +139,34 @@ def main():
                         ref_gather_cnt=gcnt, ref_gather_full=gfull, ref_gather_rad=grad,
                         render_w=80, render_h=60, render_k=100, render_r=0.1, render_depth=4,
                         ref_ldr=ren["ldr"], ref_rgb8=ren["rgb8"])
-    print("wrote", os.listdir(OUT))
+
+
+def make_tracer():
+    rt = RefTrace()
+    arrays = {}
+    for name, (build, seed, cap, p0, p1, sub) in ref_cases.CASES.items():
+        rsc = rt.scene(build())
+        full = rsc.trace_paths(seed, cap, p0, p1)
+        part = rsc.trace_paths(seed, cap, p0, sub)
+        arrays[f"{name}__checksum"] = np.uint32(ref_cases.checksum(full))
+        arrays[f"{name}__n"] = np.array([full["g_pos"].shape[0], full["c_pos"].shape[0]], np.int64)
+        arrays[f"{name}__power"] = np.concatenate([full["g_pow"], full["c_pow"]])[:1]
+        for f in ref_cases.FIELDS:
+            arrays[f"{name}__{f}"] = part[f]
+    np.savez_compressed(os.path.join(OUT, "tracer_ref.npz"), **arrays)
+
+
+def make_grid_sizing(ref):
+    arrays = {}
+    for name, (build, desired) in ref_cases.GRID_CASES.items():
+        pos, aabb = build()
+        dims, cell, regrid, mx = ref.grid_sizing(pos, aabb, desired)
+        arrays[f"{name}__dims"] = dims
+        arrays[f"{name}__cell"] = np.float32(cell)
+        arrays[f"{name}__regrid"] = np.int32(regrid)
+        arrays[f"{name}__max"] = np.uint32(mx)
+    np.savez_compressed(os.path.join(OUT, "grid_sizing_ref.npz"), **arrays)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or ["fixture100", "cornell", "tracer", "grid"])

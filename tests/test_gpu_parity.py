@@ -118,6 +118,25 @@ def test_trace_paths_heightfield_subset(ctx, orc):
     assert np.array_equal(_np(out["c_pos"]), ref["c_pos"])
 
 
+@pytest.mark.parametrize("name", ["cornell_small", "stress_glass", "heightfield", "heightfield_albedo"])
+def test_trace_paths_match_reference_tracer(ctx, name):
+    """The CUDA tracer against the reference's own tracer (CudaPhotonMapping/
+    PhotonTracing.cu compiled as host code, records in tests/golden/tracer_ref.npz
+    written by tests/golden/make_golden.py): per-path photon counts, positions
+    and directions of both maps, bit for bit, at the reference's 10 bounces."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import ref_cases
+    f = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tracer_ref.npz"))
+    build, seed, cap, p0, _, sub = ref_cases.CASES[name]
+    ctx.set_scene(build())
+    out = ctx.trace_paths(seed, ref_cases.MAX_BOUNCES, cap, p0, sub)
+    assert np.array_equal(_np(out["counts"]), f[f"{name}__counts"])
+    for key in ("g_pos", "g_dir", "c_pos", "c_dir"):
+        assert np.array_equal(_np(out[key]), f[f"{name}__{key}"]), key
+    assert ctx.status() == 0
+
+
 @pytest.mark.parametrize("which", ["cornell_small", "heightfield", "cornell_stress_4k"])
 def test_device_bvh_gives_the_same_photons_and_image(ctx, which):
     """The device LBVH and the host SAH tree answer every closest-hit query the

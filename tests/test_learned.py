@@ -196,3 +196,29 @@ def test_learned_graph_training_follows_eager_training(setup):
     np.testing.assert_allclose(w_g, ctx.cache_params(), rtol=0, atol=5e-5)
     a, b = rad_g.cpu().numpy(), rad_e.cpu().numpy()
     assert np.abs(a - b).mean() <= 1e-3 * np.abs(b).mean()
+
+
+@pytest.mark.gpu
+def test_learned_graph_refuses_after_rebuild(setup):
+    """A graph holds the scene's, the map's and the cache's device addresses and
+    the grid's dimensions in its launches: after the grid is rebuilt it refuses
+    to run (PM_ERR_INVALID) instead of reading replaced buffers."""
+    import photonmap
+    from photonmap import learned
+    ctx, cam, w = setup
+    S = learned.FRAME_SETTINGS
+    g = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=None, steps=0, **S)
+    try:
+        g.run()
+        ctx.build_grid(photonmap.PM_MAP_GLOBAL)
+        with pytest.raises(photonmap.PMError) as e:
+            g.run()
+        assert e.value.code == photonmap.PM_ERR_INVALID
+        assert ctx.status() == 0
+    finally:
+        g.close()
+    g = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=None, steps=0, **S)   # made again: runs
+    try:
+        g.run()
+    finally:
+        g.close()
