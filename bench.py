@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache frame comparison")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the learned frame's RMSE against the FP64 reference")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched workload")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--bvh", default="host_sah", choices=["host_sah", "device_lbvh"],
@@ -333,20 +334,36 @@ def batched_frames(args, rank):
             "stage_ms_eager": info["stage_ms"]}
 
 
-def learned_frames(ctx, cam, w, rgb, args, world):
+LEARNED = dict(train_per_frame=1 << 20, batch=1 << 17, warm_steps=3000, pool_samples=2_200_000,
+               rmse_pixels=65_536, rmse_maps=10)
+
+
+def learned_frames(ctx, sc, cs, cam, w, rgb, args, world):
     """Frame time of the plain render against the learned render on the same
     photon map (the map stays resident, as in the reference's render loop).
-    Learned frame = online training on TRAIN_PER_FRAME pooled samples + the
-    cache-answered render with its per-tile exact-gather fallback.  The pool
-    (stratified primary hits labelled by the kNN gather) is built once per map."""
+    Learned frame = online training on 2^20 pooled samples (
+    1M seeded surface points per frame) + the cache-answered render with its
+    per-tile exact-gather fallback.  The pool (stratified primary hits
+    labelled by the kNN gather, at least 2^20 of them) is built once per map;
+    the cache's first fit (warm_steps Adam steps) is a one-time cost reported
+    beside the per-frame times.  The frames' images are then compared with an
+    FP64 reference of 10x the photons (learned_rmse)."""
     import torch
     import torch.distributed as dist
     from photonmap import learned
-    TRAIN_PER_FRAME, BATCH, WARM_STEPS = 1 << 18, 1 << 16, 3000
-    pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=1 << 20, seed=1)
+    P = LEARNED
+    TRAIN_PER_FRAME, BATCH, WARM_STEPS = P["train_per_frame"], P["batch"], P["warm_steps"]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=P["pool_samples"], seed=1)
+    ev[1].record()
     ctx.cache_init(seed=0, lr=3e-3, out_scale=pool.scale)
-    learned.cache_fit(ctx, pool, WARM_STEPS, batch=BATCH)
+    learned.cache_fit(ctx, pool, WARM_STEPS, batch=1 << 16)
+    ev[2].record()
+    torch.cuda.synchronize()
+    pool_ms, warm_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
     K = max(args.steps, 3)
+    steps_per_frame = TRAIN_PER_FRAME // BATCH
 
     def plain():
         ctx.render(cam, w["k"], w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb)
@@ -355,8 +372,7 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     stats = {}
 
     def learned_frame():
-        _, off[0] = learned.cache_fit(ctx, pool, TRAIN_PER_FRAME // BATCH, batch=BATCH, offset=off[0],
-                                      want_loss=False)
+        _, off[0] = learned.cache_fit(ctx, pool, steps_per_frame, batch=BATCH, offset=off[0], want_loss=False)
         _, _, st = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb,
                                       **learned.FRAME_SETTINGS)
         stats.update(st)
@@ -379,7 +395,7 @@ def learned_frames(ctx, cam, w, rgb, args, world):
     ms_plain = timed(plain)
     ms_learned = timed(learned_frame)
     # the same frame captured once and replayed as one CUDA graph per frame
-    graph = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=TRAIN_PER_FRAME // BATCH,
+    graph = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=steps_per_frame,
                               batch=BATCH, offset=off[0], out_rgb8=rgb, **learned.FRAME_SETTINGS)
     gstats = {}
 
@@ -397,55 +413,164 @@ def learned_frames(ctx, cam, w, rgb, args, world):
         ctx.cache_infer(pool.pos[:n], pool.nrm[:n])
 
     def train():
-        learned.cache_fit(ctx, pool, 1, batch=min(BATCH * 4, pool.n))
+        learned.cache_fit(ctx, pool, 1, batch=min(1 << 20, pool.n))
 
     ms_inf = timed(infer)
     ms_tr = timed(train)
     peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"] \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
     inf_tf = fwd * n / (ms_inf * 1e-3) / 1e12
-    tr_tf = 3 * fwd * min(BATCH * 4, pool.n) / (ms_tr * 1e-3) / 1e12
-    return {"ms_per_frame_plain": ms_plain, "ms_per_frame_learned": ms_learned, "speedup": ms_plain / ms_learned,
-            "ms_per_frame_learned_graph": ms_graph, "speedup_graph": ms_plain / ms_graph,
-            "graph_fallback_requests_frac": gstats["fallback_requests"] / max(gstats["requests"], 1),
-            "frame": "eye pass + global estimate + resolve, photon map resident",
-            "train_samples_per_frame": TRAIN_PER_FRAME, "pool": pool.n, "warmup_steps": WARM_STEPS,
-            "check": dict(learned.FRAME_SETTINGS), "fallback_tiles_frac": stats["fallback_tiles"] / max(stats["tiles"], 1),
-            "fallback_requests_frac": stats["fallback_requests"] / max(stats["requests"], 1),
-            "mlp": {"infer_tflops": inf_tf, "train_tflops": tr_tf, "peak_bf16_tflops": peak,
-                    "infer_frac": inf_tf / peak, "train_frac": tr_tf / peak, "unit": "TFLOP/s",
-                    "flop_per_sample_forward": fwd}}
+    tr_tf = 3 * fwd * min(1 << 20, pool.n) / (ms_tr * 1e-3) / 1e12
+    block = {"ms_per_frame_plain": ms_plain, "ms_per_frame_learned": ms_learned, "speedup": ms_plain / ms_learned,
+             "ms_per_frame_learned_graph": ms_graph, "speedup_graph": ms_plain / ms_graph,
+             "graph_fallback_requests_frac": gstats["fallback_requests"] / max(gstats["requests"], 1),
+             "frame": "eye pass + global estimate + resolve, photon map resident",
+             "train_samples_per_frame": TRAIN_PER_FRAME, "train_batch": BATCH, "adam_steps_per_frame": steps_per_frame,
+             "pool": pool.n, "one_time": {"pool_labelling_ms": pool_ms, "warmup_steps": WARM_STEPS,
+                                          "warmup_ms": warm_ms},
+             "check": dict(learned.FRAME_SETTINGS), "fallback_tiles_frac": stats["fallback_tiles"] / max(stats["tiles"], 1),
+             "fallback_requests_frac": stats["fallback_requests"] / max(stats["requests"], 1),
+             "mlp": {"infer_tflops": inf_tf, "train_tflops": tr_tf, "peak_bf16_tflops": peak,
+                     "infer_frac": inf_tf / peak, "train_frac": tr_tf / peak, "unit": "TFLOP/s",
+                     "flop_per_sample_forward": fwd, "train_samples_per_launch": min(1 << 20, pool.n)}}
+    if not args.no_rmse and world == 1:
+        block["rmse"] = learned_rmse(ctx, sc, cs, cam, w)
+    elif not args.no_rmse:
+        block["rmse"] = {"skipped": "measured on one GPU (the frames are the same on every replica)"}
+    return block
+
+
+def learned_rmse(ctx, sc, cs, cam, w):
+    """Relative RMSE of the timed plain and learned frames against an FP64
+    reference, on a seeded sample of pixels of the same 10M-photon 1080p frame.
+
+    * eye paths: the oracle's restatement of the reference's render_trace
+      walks the sampled pixels on the host (its hits are also compared with the
+      GPU eye pass's requests for those pixels);
+    * reference radiance: per hit, the mean over 10 independent 10M-photon maps
+      (photon streams 1..10: 10x the frame's photons) of the FP64 estimate over
+      the oracle's kNN selection (k, r of the frame) on the oracle's grid of
+      that map; resolved per pixel in FP64;
+    * frames: the plain render and the learned render (frame settings, cache
+      as trained by the timed frames) of the resident map, radiance before
+      tone mapping.
+    relative RMSE = sqrt(mean((x - ref)^2)) / sqrt(mean(ref^2)) over the
+    sampled pixels' channels."""
+    import torch
+    import photonmap
+    import render64
+    from photonmap import learned
+    from oracle import Oracle
+    P = LEARNED
+    W, H = cs.width, cs.height
+    t0 = time.perf_counter()
+    _, rad_plain = ctx.render(cam, w["k"], w["radius"], w["max_depth"])
+    req = {k: v.cpu().numpy() for k, v in ctx.requests().items()}
+    _, rad_learned, _ = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], **learned.FRAME_SETTINGS)
+    torch.cuda.synchronize()
+    pixels = np.sort(np.random.default_rng(7).choice(W * H, P["rmse_pixels"], replace=False))
+    orc = Oracle()
+    s = orc.scene(sc)
+    hits = s.eye_hits(orc.camera(cs), W, H, pixels, w["max_depth"])
+    # the oracle's eye paths against the GPU eye pass's requests of the same pixels
+    cnt = req["px_count"][pixels].astype(np.int64)
+    same_count = bool(np.array_equal(cnt, hits["counts"]))
+    hits_equal = False
+    if same_count:
+        q = np.repeat(req["px_base"][pixels].astype(np.int64), cnt) + \
+            (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+        ga, gb, gc = req["a"][q], req["b"][q], req["c"][q]
+        fl = lambda x: (x[:, 3].view(np.uint32) & 1)  # noqa: E731
+        hits_equal = bool(np.array_equal(ga, hits["a"]) and np.array_equal(gb[:, :3], hits["b"][:, :3]) and
+                          np.array_equal(fl(gb), fl(hits["b"])) and np.array_equal(gc[:, :3], hits["c"][:, :3]))
+    tables = render64.scene_tables(sc)
+    g_mask = (hits["b"][:, 3].view(np.uint32) & 1) != 0
+    qp, qn = hits["a"][g_mask, :3], hits["b"][g_mask, :3]
+    maps = []
+    for m in range(1, P["rmse_maps"] + 1):
+        ctx.trace_photons(step_seed(w["seed"], 0, 1_000_000 + m), w["max_bounces"], w["photons"])
+        ph = ctx.photons(0, sorted_=False)
+        maps.append(tuple(ph[k].cpu().numpy() for k in ("list_pos", "list_dir", "list_power")))
+
+    def fp64_estimate(mp):   # the oracle's calls release the GIL: maps in parallel host threads
+        pos, dr, pw = mp
+        g = orc.grid_build(pos, pw, dr, s.aabb())
+        ids, c, _, _ = orc.gather(g, qp, qn, w["radius"], w["k"])
+        return render64.estimate_ids(pos, dr, pw, qp, qn, ids, c)
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(maps), max(1, (os.cpu_count() or 2) // 2))) as ex:
+        est = sum(ex.map(fp64_estimate, maps)) / len(maps)
+    full = np.zeros((hits["a"].shape[0], 3))
+    full[g_mask] = est
+    ref = render64.resolve_hits(hits, tables, lambda idx: full[idx])
+    rel = lambda x: float(np.sqrt(np.mean((x - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))  # noqa: E731
+    plain = rad_plain.cpu().numpy().reshape(-1, 3)[pixels]
+    learn = rad_learned.cpu().numpy().reshape(-1, 3)[pixels]
+    return {"rmse_plain": rel(plain), "rmse_learned": rel(learn), "pixels": int(pixels.size),
+            "reference": f"FP64 estimates over the oracle's kNN of {P['rmse_maps']} independent "
+                         f"{w['photons'] // 1_000_000}M-photon maps ({P['rmse_maps']}x the frame's photons), "
+                         f"eye paths walked by the oracle",
+            "oracle_eye_hits": int(hits["a"].shape[0]), "oracle_eye_hits_equal_gpu_requests": hits_equal,
+            "seconds": time.perf_counter() - t0}
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# default workload's kernels, from one ncu capture of the timed step's launches
-# (profiles/dram_traffic_cornell_hf_1080p.md gives the command and the figures)
+# default workload's two large kernels: constants from one ncu capture of the
+# timed step's launches (the line names the capture in "traffic_source")
 DRAM_TRAFFIC = {"k_trace": 161_125_120 + 443_799_552, "k_gather": 451_488_256 + 14_518_272}
+TRAFFIC_SOURCE = ("constant from one ncu capture of the default workload: ncu --metrics "
+                  "dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:'k_trace|k_gather' "
+                  "python bench.py --steps 1 --warmup 1 --no-cpu-baseline --no-learned --no-batched")
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SMs x 128 FP32 lanes x 2 flop (FMA) x 1965 MHz
+FLOP_PER_BOX_TEST = 20      # one child-box slab test (6 FMA, 6 min/max, 4 min/max and compares)
+FLOP_PER_TRI_TEST = 86      # the reference's count for its triangle test (CudaPhotonMapping/Model.cuh:65-67)
+PHOTON_RECORD_BYTES = 28    # position f32x3 + power f32x3 + octahedral direction u16x2 (a photon's answer bytes)
 
 
-def rooflines(w, sc, bvh, nreq, paths, k_trace_ms, k_gather_ms, hbm, src, default_workload):
-    """HBM rooflines of the step's two large kernels, each timed alone with CUDA
+def rooflines(w, sc, bvh, nreq, paths, k_trace_ms, k_gather_ms, work, hbm, src, default_workload):
+    """Rooflines of the step's two large kernels, each timed alone with CUDA
     events on the context stream (k_trace summed over the photon pass's batches).
 
-    k_trace algorithmic bytes: 32 B stage record per stored photon (at least the
-    photon budget) + 8 B per-path photon counts + the scene read once (64 B per
-    BVH node, 80 B leaf-ordered triangle record + 36 B vertex normals per
-    triangle).  k_gather: per kNN query k neighbours x (16 B position + 12 B
-    direction + 12 B power) + 32 B request (point, normal) + 12 B estimate.
+    k_trace: FP32 flops of its traversal work, counted by the tracer's
+    work-counting launch (pm_trace_work, the same photons): 2 child-box tests
+    x 20 flop per BVH node visited + 86 flop per triangle test, against the
+    nominal FP32 peak (MEASURED_PEAKS.json holds no FP32 figure); rays / s
+    beside it.  Its HBM view: the 32-byte stage record per stored photon, 8 B
+    per-path counts and the scene once, against the measured copy bandwidth.
+    k_gather: per kNN query k photons x 28 B (position and power f32x3, an
+    octahedral u16x2 direction) + 12 B hit point + 12 B radiance out, against
+    the measured copy bandwidth.
     """
+    paths_w, rays, nodes, tris = work
+    flop = 2 * FLOP_PER_BOX_TEST * nodes + FLOP_PER_TRI_TEST * tris
     scene_bytes = bvh["nodes"] * 64 + sc.ntri * (80 + 36)
-    units = {
-        "k_trace": (w["photons"] * 32 + paths * 8 + scene_bytes, k_trace_ms, "BVH traversal: latency / issue bound",
-                    {"paths_per_launch": paths, "photons_per_launch": w["photons"]}),
-        "k_gather": (nreq * (w["k"] * 40 + 44), k_gather_ms, "kNN walk: issue / L1-L2 latency bound",
-                     {"queries_per_launch": nreq}),
-    }
+    trace_bytes = w["photons"] * 32 + paths * 8 + scene_bytes
     out = {}
-    for name, (alg, ms, note, extra) in units.items():
-        achieved = alg / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
-        out[name] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": src, "traffic": DRAM_TRAFFIC.get(name) if default_workload else None,
-                     "algorithmic_bytes_per_launch": int(alg), "ms_per_launch": ms, "note": note, **extra}
+    tf = flop / (k_trace_ms * 1e-3) / 1e12 if k_trace_ms > 0 else 0.0
+    out["k_trace"] = {
+        "bound": "fp32", "achieved": tf, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": tf / FP32_PEAK_TFLOPS,
+        "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 flop x 1965 MHz); no measured FP32 peak",
+        "traffic": DRAM_TRAFFIC["k_trace"] if default_workload else None,
+        "traffic_source": TRAFFIC_SOURCE if default_workload else None,
+        "flop_per_launch": int(flop), "ms_per_launch": k_trace_ms,
+        "work": {"rays": rays, "bvh_node_visits": nodes, "box_tests": 2 * nodes, "triangle_tests": tris,
+                 "flop_per_box_test": FLOP_PER_BOX_TEST, "flop_per_triangle_test": FLOP_PER_TRI_TEST,
+                 "paths": paths_w},
+        "mrays_per_s": rays / (k_trace_ms * 1e-3) / 1e6 if k_trace_ms > 0 else 0.0,
+        "hbm_view": {"algorithmic_bytes_per_launch": int(trace_bytes),
+                     "achieved_gbs": trace_bytes / (k_trace_ms * 1e-3) / 1e9 if k_trace_ms > 0 else 0.0,
+                     "peak_gbs": hbm, "peak_source": src},
+        "note": "BVH traversal: latency / issue bound", "paths_per_launch": paths,
+        "photons_per_launch": w["photons"]}
+    g_bytes = nreq * (w["k"] * PHOTON_RECORD_BYTES + 24)
+    gb = g_bytes / (k_gather_ms * 1e-3) / 1e9 if k_gather_ms > 0 else 0.0
+    out["k_gather"] = {
+        "bound": "hbm", "achieved": gb, "peak": hbm, "unit": "GB/s", "frac": gb / hbm, "peak_source": src,
+        "traffic": DRAM_TRAFFIC["k_gather"] if default_workload else None,
+        "traffic_source": TRAFFIC_SOURCE if default_workload else None,
+        "algorithmic_bytes_per_launch": int(g_bytes), "bytes_per_query": w["k"] * PHOTON_RECORD_BYTES + 24,
+        "ms_per_launch": k_gather_ms, "note": "kNN walk: issue / L1-L2 latency bound", "queries_per_launch": nreq}
     return out
 
 
@@ -524,10 +649,13 @@ def run_ours(args):
     e2e_ms = (time.perf_counter() - t0) * 1000 / args.steps
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], world)
     stages = stage_sum / args.steps
+    # the tracer's work on one step's photon pass (untimed counting launch, same photons as a timed step)
+    work = ctx.trace_work(step_seed(w["seed"], rank, args.warmup), w["max_bounces"], w["photons"])
+    ctx.build_grid(photonmap.PM_MAP_GLOBAL)   # the resident map of the learned-frame comparison
 
     learned_block = None
     if not args.no_learned:
-        learned_block = learned_frames(ctx, cam, w, rgb, args, world)
+        learned_block = learned_frames(ctx, sc, cs, cam, w, rgb, args, world)
     batched_block = None
     if not args.no_batched:
         batched_block = batched_frames(args, rank)
@@ -536,7 +664,7 @@ def run_ours(args):
     line = None
     if rank == 0:
         nreq = ctx.render_requests()   # kNN queries of the frame's gather
-        kernels = rooflines(w, sc, bvh, nreq, paths_timed, stages[5], stages[6], hbm, src,
+        kernels = rooflines(w, sc, bvh, nreq, paths_timed, stages[5], stages[6], work, hbm, src,
                             default_workload=(args.workload == WORKLOAD and not (args.photons or args.width
                                                                                   or args.height)))
         dominant = max(kernels, key=lambda k: kernels[k]["ms_per_launch"])

@@ -49,6 +49,7 @@ cudaError_t ensure(DevBuf& b, size_t bytes) {
     b.bytes = 0;
     cudaError_t e = cudaMalloc(&b.p, bytes);
     if (e == cudaSuccess) b.bytes = bytes;
+    else (void)cudaGetLastError();   // a failed allocation leaves no error behind for the next launch check
     return e;
 }
 void release(DevBuf& b) {
@@ -66,7 +67,8 @@ std::vector<DevBuf*> all_buffers(pm_ctx* ctx) {
                               &ctx->cache_loss, &ctx->est_mlp, &ctx->est_fb, &ctx->probe_pos, &ctx->probe_nrm,
                               &ctx->probe_req, &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts,
                               &ctx->fallback_list, &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order, &ctx->rq_keys,
-                              &ctx->rq_k0, &ctx->rq_k1, &ctx->rq_v0, &ctx->rq_v1, &ctx->rq_hist, &ctx->rq_ws};
+                              &ctx->rq_k0, &ctx->rq_k1, &ctx->rq_v0, &ctx->rq_v1, &ctx->rq_hist, &ctx->rq_ws,
+                              &ctx->work, &ctx->eye_band};
     for (auto& m : ctx->maps)
         for (DevBuf* b : {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid, &m.keys0,
                           &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small, &m.key_counts,
@@ -771,6 +773,7 @@ static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, Tr
     B.status = P<unsigned>(ctx->status);
     B.sm_count = ctx->sm_count;
     B.refill = ctx->trace_refill;
+    B.work = ctx->count_work ? P<unsigned long long>(ctx->work) : nullptr;
     return PM_OK;
 }
 
@@ -860,6 +863,22 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     return PM_OK;
 }
 
+int pm_trace_work(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths, uint64_t out_work[3]) {
+    if (!ctx || !o || !out_work) return PM_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    ENSURE(ctx->work, 32);
+    CK(cudaMemsetAsync(ctx->work.p, 0, 32, ctx->st));
+    ctx->count_work = true;
+    const int rc = pm_trace_photons(ctx, o, out_paths);
+    ctx->count_work = false;
+    if (rc) return rc;
+    unsigned long long w[3] = {0, 0, 0};
+    CK(cudaMemcpyAsync(w, ctx->work.p, 24, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int i = 0; i < 3; i++) out_work[i] = w[i];
+    return PM_OK;
+}
+
 int pm_trace_paths(pm_ctx* ctx, const pm_trace_opts* o, int64_t p0, int64_t p1, int64_t power_capacity,
                    float* g_pos, float* g_dir, float* c_pos, float* c_dir, uint32_t* counts,
                    int64_t* out_ng, int64_t* out_nc) {
@@ -903,9 +922,9 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
     ENSURE(m.dir, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.pow, std::max<int64_t>(n, 1) * 12);
     if (n > 0) {
-        CK(cudaMemcpyAsync(m.pos.p, pos, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaMemcpyAsync(m.dir.p, dir, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaMemcpyAsync(m.pow.p, power, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(m.pos.p, pos, (size_t)n * 12, cudaMemcpyDefault, ctx->st));
+        CK(cudaMemcpyAsync(m.dir.p, dir, (size_t)n * 12, cudaMemcpyDefault, ctx->st));
+        CK(cudaMemcpyAsync(m.pow.p, power, (size_t)n * 12, cudaMemcpyDefault, ctx->st));
     }
     CK(cudaStreamSynchronize(ctx->st));
     m.n = n;
@@ -1143,8 +1162,11 @@ struct FrameSetup {
 };
 
 
-// buffers and the eye pass on stream st (timed into ev[4] .. ev[5])
-int render_eye_launch(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F, cudaStream_t st) {
+// buffers and the eye pass on stream st (timed into ev[4] .. ev[5]); with
+// y0 < y1 only the pixel blocks that meet rows [y0, y1) run, and every other
+// pixel has no requests
+int render_eye_launch(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, FrameSetup& F, cudaStream_t st,
+                      int y0 = 0, int y1 = 0) {
     MapState& C = ctx->maps[PM_MAP_CAUSTIC];
     F.npx = (int64_t)cam->width * cam->height;
     const int64_t per_px = ((int64_t)1 << std::max(o->max_depth, 1)) - 1;
@@ -1171,15 +1193,31 @@ int render_eye_launch(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     R.px_base = P<uint32_t>(ctx->px_base);
     R.px_count = P<uint32_t>(ctx->px_count);
     if (!ctx->eye_order_valid || std::memcmp(&ctx->eye_order_cam, cam, sizeof *cam) != 0) {
-        std::vector<int> order;
+        std::vector<int>& order = ctx->h_eye_order;
+        order.clear();
         eye_block_order(ctx, cam, order);
         ENSURE(ctx->eye_order, order.size() * 4);
         CK(cudaMemcpyAsync(ctx->eye_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st));
         ctx->eye_order_cam = *cam;
         ctx->eye_order_valid = true;
     }
+    const int* order = P<int>(ctx->eye_order);
+    int64_t nblocks = -1;
+    if (y0 < y1) {
+        // the band's blocks, in the full order's (slow blocks first)
+        const int64_t T = eye_threads(), lo = (int64_t)y0 * cam->width, hi = (int64_t)y1 * cam->width;
+        std::vector<int> band;
+        for (int b : ctx->h_eye_order)
+            if ((int64_t)b * T < hi && ((int64_t)b + 1) * T > lo) band.push_back(b);
+        ENSURE(ctx->eye_band, std::max<size_t>(band.size(), 1) * 4);
+        if (!band.empty())
+            CK(cudaMemcpyAsync(ctx->eye_band.p, band.data(), band.size() * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(ctx->px_count.p, 0, (size_t)F.npx * 4, st));
+        order = P<int>(ctx->eye_band);
+        nblocks = (int64_t)band.size();
+    }
     CK(cudaEventRecord(ctx->ev[4], st));
-    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), st, P<int>(ctx->eye_order)));
+    CK(eye_pass(F.S, F.cd, o->max_depth, R, P<unsigned>(ctx->status), st, order, nblocks));
     CK(cudaEventRecord(ctx->ev[5], st));
     ctx->launches += 1;
     return PM_OK;
@@ -1311,6 +1349,18 @@ int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_
     CK(cudaSetDevice(ctx->device));
     FrameSetup F;
     if (int rc = render_eye(ctx, cam, o, F)) return rc;
+    return render_rest(ctx, o, F, out_rgb8, out_radiance);
+}
+
+int pm_render_rows(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, int32_t y0, int32_t y1,
+                   uint8_t* out_rgb8, float* out_radiance) {
+    if (!ctx || !cam || !o || !out_rgb8) return PM_ERR_INVALID;
+    if (int rc = render_checks(ctx, cam, o)) return rc;
+    if (y0 < 0 || y1 > cam->height || y0 >= y1) return fail(ctx, PM_ERR_INVALID, "rows: 0 <= y0 < y1 <= height");
+    CK(cudaSetDevice(ctx->device));
+    FrameSetup F;
+    if (int rc = render_eye_launch(ctx, cam, o, F, ctx->st, y0, y1)) return rc;
+    if (int rc = render_eye_count(ctx, F)) return rc;
     return render_rest(ctx, o, F, out_rgb8, out_radiance);
 }
 

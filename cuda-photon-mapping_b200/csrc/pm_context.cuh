@@ -50,6 +50,9 @@ struct pm_ctx {
     pm::MapState maps[2];
     // photon-pass scratch
     pm::DevBuf counter, stage, cnt_g, cnt_c, scan_g, scan_c, totals, trace_ws, scratch_pow;
+    // the tracer's work-counting launch (pm_trace_work): rays, node visits, triangle tests
+    pm::DevBuf work;
+    bool count_work = false;
     // render scratch
     pm::DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, est_c;
     pm::DevBuf status, gws;
@@ -79,6 +82,8 @@ struct pm_ctx {
     cudaEvent_t frame_fork = nullptr, frame_done = nullptr;
     bool eye_order_valid = false;   // eye_order holds the order for eye_order_cam on this scene
     pm_camera eye_order_cam = {};
+    std::vector<int> h_eye_order;   // host copy of eye_order
+    pm::DevBuf eye_band;            // the blocks of a row band (pm_render_rows), in eye_order's order
     pm::DevBuf est_mlp, est_fb, probe_pos, probe_nrm, probe_req, probe_est, tile_flag, learned_counts, fallback_list;
     pm_cache_opts cache_opts = {};
     float cache_lo[3] = {0, 0, 0}, cache_inv[3] = {1, 1, 1};

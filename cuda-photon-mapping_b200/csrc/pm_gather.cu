@@ -830,6 +830,11 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
     const int64_t n = (int64_t)min(*n_req, (unsigned long long)Q.n);
+    // the instance of the last request and its pixel range: consecutive
+    // requests mostly belong to one instance (the eye pass writes them in
+    // instance order), so the search runs only when the pixel leaves the range
+    int inst = -1;
+    int64_t px_lo = 0, px_hi = 0;
     while (true) {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(queue, (unsigned long long)MULTI_CHUNK);
@@ -837,7 +842,12 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
         if (q0 >= n) break;
         const int64_t q1 = min(q0 + (int64_t)MULTI_CHUNK, n);
         for (int64_t i = q0; i < q1; i++) {
-            const int inst = find_instance_px(px_off, ninst, (int64_t)__float_as_uint(rec_c[i].w));
+            const int64_t px = (int64_t)__float_as_uint(rec_c[i].w);
+            if (px < px_lo || px >= px_hi) {
+                inst = find_instance_px(px_off, ninst, px);
+                px_lo = __ldg(px_off + inst);
+                px_hi = __ldg(px_off + inst + 1);
+            }
             const GatherInstDev& T = tab[inst];
             if (T.cls != cls) continue;
             const float4 a = Q.pos4[i], b = Q.nrm4[i];

@@ -18,12 +18,18 @@
 // weight gradient (MN-major B), and weights [out][in] feed the forward product
 // (K-major B) and the input gradient (MN-major B) without any copy.
 //
-// Per 128-sample tile (one thread per sample row, 4 warps):
+// Per 128-sample tile (one thread per sample row, one warpgroup):
 //   forward   D[128 x out] = X_l[128 x 64] W_l^T               M=128, 4 MMAs (K=16)
 //   backward  dW_l += X_l^T[64 x 128] dY_l[128 x out]         M=64,  8 MMAs, accumulated in TMEM over tiles
 //             dX   = dY_l[128 x out] W_l[out x 64]             M=128, out/16 MMAs
-// TMEM columns: [0, 64) forward / input-gradient tile, [64 + 64 l, ...) the
-// weight-gradient accumulator of layer l (M=64: rows 16 w + i in lanes 32 w + i).
+// Training runs TRAIN_GROUPS such tile pipelines per CTA (one warpgroup each,
+// its own activation and gradient tiles, mbarrier and 64 TMEM columns), which
+// all accumulate into the CTA's one set of weight-gradient columns: the chain
+// of one tile is a series of small dependent products, so a second chain keeps
+// the tensor pipe busy while the first one's epilogue runs.
+// TMEM columns (training): [64 l, 64 l + out_l) the weight-gradient
+// accumulator of layer l (M=64: rows 16 w + i in lanes 32 w + i), zeroed at
+// the start; [TRAIN_FWD_COL + 64 g, +64) group g's forward / input-gradient tile.
 #include <cmath>
 #include <algorithm>
 #include "pm_mlp.cuh"
@@ -38,14 +44,22 @@ constexpr int THREADS = 128;
 constexpr int WAIT_LIMIT = 1 << 24;        // polls of an mbarrier before giving up
 constexpr uint32_t TMEM_COLS_TRAIN = 512;
 constexpr uint32_t TMEM_COLS_INFER = 256;   // 64 per warpgroup
+constexpr uint32_t TRAIN_DW_COLS = 4 * 64 + MLP_OUT;   // weight-gradient accumulators of the five layers
+constexpr uint32_t TRAIN_FWD_COL = 320;                // first per-group tile column
 
 // shared-memory carve-up (bytes)
 constexpr uint32_t W_BYTES = 4 * 8192 + 2048;       // layers 0-3: 64x64, layer 4: 16x64
 constexpr uint32_t X_BYTES = TILE * MLP_DIM * 2;    // one [128][64] activation / gradient tile
-constexpr uint32_t TRAIN_OFF_X = W_BYTES;                       // X_0 .. X_4
-constexpr uint32_t TRAIN_OFF_G = TRAIN_OFF_X + 5 * X_BYTES;     // two gradient tiles
-constexpr uint32_t TRAIN_OFF_BAR = TRAIN_OFF_G + 2 * X_BYTES;
+// training: per group X_0 .. X_4 and one gradient tile (dY_l, replaced in
+// place by dY_{l-1} once the products reading it have landed)
+constexpr int TRAIN_GROUPS = 2;
+constexpr int TRAIN_THREADS = 128 * TRAIN_GROUPS;
+constexpr uint32_t TRAIN_GROUP_BYTES = 6 * X_BYTES;
+constexpr uint32_t TRAIN_OFF_X = W_BYTES;
+constexpr uint32_t TRAIN_OFF_BAR = TRAIN_OFF_X + TRAIN_GROUPS * TRAIN_GROUP_BYTES;
 constexpr uint32_t TRAIN_SMEM = TRAIN_OFF_BAR + 64;
+static_assert(TRAIN_SMEM <= 232448, "training tiles exceed the shared memory of a CTA");
+static_assert(TRAIN_FWD_COL >= TRAIN_DW_COLS && TRAIN_FWD_COL + 64 * TRAIN_GROUPS <= TMEM_COLS_TRAIN, "TMEM layout");
 // inference: INFER_GROUPS independent 128-row pipelines (one warpgroup each)
 // share the weights; each owns one activation tile (the layers run in place),
 // one mbarrier and 64 TMEM columns
@@ -134,6 +148,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// 64 consecutive 32-bit columns of this thread's TMEM lane, one wait
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
+    uint32_t r[64];
+#define PM_R8(b) "=r"(r[b]), "=r"(r[b + 1]), "=r"(r[b + 2]), "=r"(r[b + 3]), "=r"(r[b + 4]), "=r"(r[b + 5]), \
+                 "=r"(r[b + 6]), "=r"(r[b + 7])
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
+        "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+        : PM_R8(0), PM_R8(8), PM_R8(16), PM_R8(24), PM_R8(32), PM_R8(40), PM_R8(48), PM_R8(56)
+        : "r"(taddr));
+#undef PM_R8
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
+}
+// zeros into 16 consecutive 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_zero16(uint32_t taddr) {
+    const uint32_t z = 0u;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};"
+        :: "r"(taddr), "r"(z) : "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -231,67 +269,112 @@ __device__ __forceinline__ void issue_forward(int l, uint32_t tm, uint32_t xa, u
     for (int s = 0; s < 4; s++) umma(tm, sdesc(xa + 4096u * s, 2048u, 128u), sdesc(wa + 2u * lbo_w * s, lbo_w, 128u), id, s > 0);
 }
 
-// ReLU of a [128 x 64] TMEM tile row (this thread's) -> bf16 row of the next activation tile
+// ReLU of a [128 x 64] TMEM tile row (this thread's) -> bf16 row of the next
+// activation tile.  COLS columns per TMEM load (64: one wait per row, for
+// kernels with the registers; 16: four loads, for the 64-register inference).
+template <int COLS>
 __device__ __forceinline__ void relu_row_to_smem(uint32_t taddr, unsigned char* dst, int row) {
 #pragma unroll
-    for (int c0 = 0; c0 < 64; c0 += 16) {
-        float v[16];
-        tmem_ld16(taddr + c0, v);
+    for (int c0 = 0; c0 < 64; c0 += COLS) {
+        float v[COLS];
+        if constexpr (COLS == 64) tmem_ld64(taddr + c0, v);
+        else tmem_ld16(taddr + c0, v);
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
+        for (int b = 0; b < COLS / 8; b++) {
             uint4 q;
-            q.x = pack_bf16(fmaxf(v[8 * h + 0], 0.f), fmaxf(v[8 * h + 1], 0.f));
-            q.y = pack_bf16(fmaxf(v[8 * h + 2], 0.f), fmaxf(v[8 * h + 3], 0.f));
-            q.z = pack_bf16(fmaxf(v[8 * h + 4], 0.f), fmaxf(v[8 * h + 5], 0.f));
-            q.w = pack_bf16(fmaxf(v[8 * h + 6], 0.f), fmaxf(v[8 * h + 7], 0.f));
-            *reinterpret_cast<uint4*>(dst + cm_off(row, c0 + 8 * h, TILE)) = q;
+            q.x = pack_bf16(fmaxf(v[8 * b + 0], 0.f), fmaxf(v[8 * b + 1], 0.f));
+            q.y = pack_bf16(fmaxf(v[8 * b + 2], 0.f), fmaxf(v[8 * b + 3], 0.f));
+            q.z = pack_bf16(fmaxf(v[8 * b + 4], 0.f), fmaxf(v[8 * b + 5], 0.f));
+            q.w = pack_bf16(fmaxf(v[8 * b + 6], 0.f), fmaxf(v[8 * b + 7], 0.f));
+            *reinterpret_cast<uint4*>(dst + cm_off(row, c0 + 8 * b, TILE)) = q;
         }
     }
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+// dY_{l-1} = dX * [X_l > 0] for this thread's row: dX from its TMEM lane, the
+// mask from row `row` of X_l, the result (bf16) over the same row of g
+__device__ __forceinline__ void masked_grad_row(uint32_t taddr, const unsigned char* xrow, unsigned char* g, int row) {
+    float v[64];
+    tmem_ld64(taddr, v);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const uint4 xq = *reinterpret_cast<const uint4*>(xrow + cm_off(row, 8 * b, TILE));
+        const uint32_t xs[4] = {xq.x, xq.y, xq.z, xq.w};
+        uint32_t o[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            float x0, x1;
+            unpack_bf16(xs[e], x0, x1);
+            o[e] = pack_bf16(x0 > 0.f ? v[8 * b + 2 * e] : 0.f, x1 > 0.f ? v[8 * b + 2 * e + 1] : 0.f);
+        }
+        *reinterpret_cast<uint4*>(g + cm_off(row, 8 * b, TILE)) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+// Training: warpgroup g of the CTA runs its own tiles (g + G * CTA, then
+// strided by G * grid): features, five forward products, the output gradient,
+// then per layer (last first) the weight-gradient product into the CTA's
+// shared accumulator and the input-gradient product, each waited on through
+// the group's mbarrier.  Thread 0 of the group issues its products.  The
+// accumulators are zeroed before any product; at the end the CTA adds them to
+// the global gradient once.
+__global__ void __launch_bounds__(TRAIN_THREADS, 1)
 k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const float* __restrict__ weight,
             float grad_scale, float* __restrict__ grad, float* __restrict__ loss_sum, unsigned* status) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = tid >> 7, row = tid & 127;
     unsigned char* sW = smem;
-    unsigned char* sX = smem + TRAIN_OFF_X;
-    unsigned char* sG = smem + TRAIN_OFF_G;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + TRAIN_OFF_BAR);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TRAIN_OFF_BAR + 8);
+    unsigned char* sX = smem + TRAIN_OFF_X + g * TRAIN_GROUP_BYTES;   // X_0 .. X_4
+    unsigned char* sG = sX + 5 * X_BYTES;                             // the gradient tile
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TRAIN_OFF_BAR);
+    uint64_t* bar = bars + g;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + TRAIN_OFF_BAR + 8 * TRAIN_GROUPS);
     load_weights(net.w, sW);
-    if (tid == 0) mbar_init(bar);
+    if (tid < TRAIN_GROUPS) mbar_init(bars + tid);
     if (warp == 0) tmem_alloc(tslot, TMEM_COLS_TRAIN);
     fence_async_smem();
     tc_before();
     __syncthreads();
     tc_after();
-    const uint32_t tm = *tslot;
-    const uint32_t my_lanes = (uint32_t)(32 * warp) << 16;
+    const uint32_t tbase = *tslot;
+    const uint32_t my_lanes = (uint32_t)(32 * (warp & 3)) << 16;
+    // zero the weight-gradient accumulators (group 0's four warps cover the 128 lanes)
+    if (g == 0) {
+#pragma unroll 1
+        for (uint32_t c = 0; c < TRAIN_DW_COLS; c += 16) tmem_zero16(tbase + my_lanes + c);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tm = tbase + TRAIN_FWD_COL + 64u * (uint32_t)g;   // this group's tile columns
     const uint32_t sW_a = (uint32_t)__cvta_generic_to_shared(sW);
     const uint32_t sX_a = (uint32_t)__cvta_generic_to_shared(sX);
     const uint32_t sG_a = (uint32_t)__cvta_generic_to_shared(sG);
+    const bool leader = row == 0;
+    const int bar_id = 1 + g;
     const float inv_scale = 1.f / net.out_scale;
     uint32_t phase = 0;
-    bool ok = true, any = false;
+    bool ok = true;
     float loss = 0.f;
     const int64_t tiles = (in.n + TILE - 1) / TILE;
     const int64_t base = in.base_dev ? *in.base_dev : 0;
-    int iter = 0;
-    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, iter++) {
-        const int64_t i = tile * TILE + tid;
+    const int64_t stride = (int64_t)gridDim.x * TRAIN_GROUPS;
+    for (int64_t tile = (int64_t)blockIdx.x * TRAIN_GROUPS + g; tile < tiles && ok; tile += stride) {
+        const int64_t i = tile * TILE + row;
         V3 p, n;
         const bool use = load_sample(in, in.n, base, i, p, n);
         const float wgt = use ? (weight ? weight[base + i] : 1.f) : 0.f;
         const V3 t = use ? ld3(target + 3 * (base + i)) : v3(0.f, 0.f, 0.f);
-        write_features(sX, tid, net, p, n);
+        write_features(sX, row, net, p, n);
         fence_async_smem();
         tc_before();
-        __syncthreads();
+        wg_sync_and(bar_id, true);
         tc_after();
         float y[3] = {0.f, 0.f, 0.f};
         for (int l = 0; l < MLP_LAYERS && ok; l++) {
-            if (tid == 0) {
+            if (leader) {
                 issue_forward(l, tm, sX_a + l * X_BYTES, sW_a + w_off(l));
                 umma_commit(bar);
             }
@@ -300,7 +383,7 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
             tc_after();
             if (done) {
                 if (l < MLP_LAYERS - 1) {
-                    relu_row_to_smem(tm + my_lanes, sX + (l + 1) * X_BYTES, tid);
+                    relu_row_to_smem<64>(tm + my_lanes, sX + (l + 1) * X_BYTES, row);
                 } else {
                     float v[16];
                     tmem_ld16(tm + my_lanes, v);
@@ -309,35 +392,33 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
             }
             tc_before();
             fence_async_smem();
-            ok = __syncthreads_and(done) != 0;
+            ok = wg_sync_and(bar_id, done);
             tc_after();
         }
         if (!ok) break;
         // d(loss)/dy for the MSE against target / out_scale
         const float d0 = y[0] - t.x * inv_scale, d1 = y[1] - t.y * inv_scale, d2 = y[2] - t.z * inv_scale;
         loss += wgt * (d0 * d0 + d1 * d1 + d2 * d2);
-        const float g = grad_scale * wgt;
-        *reinterpret_cast<uint4*>(sG + cm_off(tid, 0, TILE)) =
-            make_uint4(pack_bf16(g * d0, g * d1), pack_bf16(g * d2, 0.f), 0u, 0u);
-        *reinterpret_cast<uint4*>(sG + cm_off(tid, 8, TILE)) = make_uint4(0u, 0u, 0u, 0u);
+        const float gs = grad_scale * wgt;
+        *reinterpret_cast<uint4*>(sG + cm_off(row, 0, TILE)) =
+            make_uint4(pack_bf16(gs * d0, gs * d1), pack_bf16(gs * d2, 0.f), 0u, 0u);
+        *reinterpret_cast<uint4*>(sG + cm_off(row, 8, TILE)) = make_uint4(0u, 0u, 0u, 0u);
         fence_async_smem();
         tc_before();
-        __syncthreads();
+        wg_sync_and(bar_id, true);
         tc_after();
-        int cur = 0;
         for (int l = MLP_LAYERS - 1; l >= 0; l--) {
             const int out = mlp_out_dim(l);
-            const uint32_t xa = sX_a + l * X_BYTES, ga = sG_a + cur * X_BYTES, wa = sW_a + w_off(l);
-            if (tid == 0) {
+            const uint32_t xa = sX_a + l * X_BYTES, wa = sW_a + w_off(l);
+            if (leader) {
                 const uint32_t idw = idesc_bf16(64, out, 1, 1);
 #pragma unroll
                 for (int s = 0; s < TILE / 16; s++)
-                    umma(tm + 64u + 64u * l, sdesc(xa + 256u * s, 128u, 2048u), sdesc(ga + 256u * s, 128u, 2048u),
-                         idw, (iter > 0 || s > 0) ? 1u : 0u);
+                    umma(tbase + 64u * l, sdesc(xa + 256u * s, 128u, 2048u), sdesc(sG_a + 256u * s, 128u, 2048u), idw, 1u);
                 if (l > 0) {
                     const uint32_t idx = idesc_bf16(TILE, 64, 0, 1);
                     for (int s = 0; s < out / 16; s++)
-                        umma(tm, sdesc(ga + 4096u * s, 2048u, 128u), sdesc(wa + 256u * s, 128u, 16u * (uint32_t)out),
+                        umma(tm, sdesc(sG_a + 4096u * s, 2048u, 128u), sdesc(wa + 256u * s, 128u, 16u * (uint32_t)out),
                              idx, s > 0);
                 }
                 umma_commit(bar);
@@ -345,51 +426,32 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
             const bool done = mbar_wait(bar, phase);
             phase ^= 1u;
             tc_after();
-            if (done && l > 0) {
-                // dY_{l-1} = dX * [X_l > 0], bf16, into the other gradient tile
-                unsigned char* xrow = sX + l * X_BYTES;
-                unsigned char* dst = sG + (cur ^ 1) * X_BYTES;
-#pragma unroll
-                for (int c0 = 0; c0 < 64; c0 += 16) {
-                    float v[16];
-                    tmem_ld16(tm + my_lanes + c0, v);
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const uint4 xq = *reinterpret_cast<const uint4*>(xrow + cm_off(tid, c0 + 8 * h, TILE));
-                        const uint32_t xs[4] = {xq.x, xq.y, xq.z, xq.w};
-                        uint32_t o[4];
-#pragma unroll
-                        for (int e = 0; e < 4; e++) {
-                            float xa0, xa1;
-                            unpack_bf16(xs[e], xa0, xa1);
-                            o[e] = pack_bf16(xa0 > 0.f ? v[8 * h + 2 * e] : 0.f, xa1 > 0.f ? v[8 * h + 2 * e + 1] : 0.f);
-                        }
-                        *reinterpret_cast<uint4*>(dst + cm_off(tid, c0 + 8 * h, TILE)) = make_uint4(o[0], o[1], o[2], o[3]);
-                    }
-                }
-            }
+            // both products have read dY_l: dY_{l-1} replaces it
+            if (done && l > 0) masked_grad_row(tm + my_lanes, sX + l * X_BYTES, sG, row);
             tc_before();
             fence_async_smem();
-            ok = __syncthreads_and(done) != 0;
+            ok = wg_sync_and(bar_id, done);
             tc_after();
             if (!ok) break;
-            cur ^= 1;
         }
-        if (!ok) break;
-        any = true;
     }
     if (!ok) {
-        if (tid == 0) raise_status(status, ST_TIMEOUT);
+        if (leader) raise_status(status, ST_TIMEOUT);
         (void)mbar_wait(bar, phase ^ 1u);   // let the late product land before the columns are freed
-    } else if (any) {
-        // weight gradients: lanes 0-15 of each warp hold rows 16 w + lane (input index)
-        for (int l = 0; l < MLP_LAYERS; l++) {
+    }
+    tc_before();
+    const bool all_ok = __syncthreads_and(ok) != 0;
+    tc_after();
+    if (all_ok && (int64_t)blockIdx.x * TRAIN_GROUPS < tiles) {
+        // weight gradients: lanes 0-15 of each warp hold rows 16 (warp % 4) + lane
+        // (input index); group g drains the layers l with l % TRAIN_GROUPS == g
+        for (int l = g; l < MLP_LAYERS; l += TRAIN_GROUPS) {
             const int out = mlp_out_dim(l);
             for (int c0 = 0; c0 < out; c0 += 16) {
                 float v[16];
-                tmem_ld16(tm + my_lanes + 64u + 64u * l + c0, v);
+                tmem_ld16(tbase + my_lanes + 64u * l + c0, v);
                 if (lane < 16) {
-                    const int m = 16 * warp + lane;
+                    const int m = 16 * (warp & 3) + lane;
 #pragma unroll
                     for (int e = 0; e < 16; e++) atomicAdd(grad + (size_t)l * MLP_LAYER_STRIDE + (c0 + e) * MLP_DIM + m, v[e]);
                 }
@@ -402,7 +464,7 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
     tc_before();
     __syncthreads();
     tc_after();
-    if (warp == 0) tmem_dealloc(tm, TMEM_COLS_TRAIN);
+    if (warp == 0) tmem_dealloc(tbase, TMEM_COLS_TRAIN);
 }
 
 // Inference: warpgroup g of the CTA runs its own tiles (g + G * CTA, then
@@ -462,7 +524,7 @@ k_mlp_infer(MlpNet net, MlpInputs in, float* __restrict__ out, unsigned* status)
             tc_after();
             if (done) {
                 if (l < MLP_LAYERS - 1) {
-                    relu_row_to_smem(tm + my_lanes, sX, row);
+                    relu_row_to_smem<16>(tm + my_lanes, sX, row);
                 } else {
                     float v[16];
                     tmem_ld16(tm + my_lanes, v);
@@ -541,8 +603,9 @@ cudaError_t mlp_train(const MlpNet& net, const MlpInputs& in, const float* targe
     cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM);
     if (e != cudaSuccess) return e;
     const int64_t tiles = (in.n + TILE - 1) / TILE;
-    const int grid = (int)std::min<int64_t>(tiles, std::max(sm_count, 1));   // one CTA per SM: 512 TMEM columns each
-    k_mlp_train<<<grid, THREADS, TRAIN_SMEM, st>>>(net, in, target, weight, grad_scale, grad, loss_sum, status);
+    const int64_t ctas = (tiles + TRAIN_GROUPS - 1) / TRAIN_GROUPS;
+    const int grid = (int)std::min<int64_t>(ctas, std::max(sm_count, 1));   // one CTA per SM: 512 TMEM columns each
+    k_mlp_train<<<grid, TRAIN_THREADS, TRAIN_SMEM, st>>>(net, in, target, weight, grad_scale, grad, loss_sum, status);
     return cudaGetLastError();
 }
 

@@ -422,12 +422,15 @@ int64_t eye_blocks(int64_t npx) { return (npx + EYE_THREADS - 1) / EYE_THREADS; 
 int eye_threads() { return EYE_THREADS; }
 
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
-                     cudaStream_t st, const int* block_order) {
+                     cudaStream_t st, const int* block_order, int64_t nblocks) {
     if (max_depth < 0 || max_depth > RENDER_MAX_DEPTH) return cudaErrorInvalidValue;
     const int64_t npx = (int64_t)cam.W * cam.H;
+    const int64_t all = eye_blocks(npx);
+    if (nblocks < 0) nblocks = all;
+    if (nblocks > all || (nblocks < all && !block_order)) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(R.counter, 0, 8, st);
-    if (e != cudaSuccess) return e;
-    k_eye<<<(unsigned)eye_blocks(npx), EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status, block_order);
+    if (e != cudaSuccess || nblocks == 0) return e;
+    k_eye<<<(unsigned)nblocks, EYE_THREADS, 0, st>>>(S, cam, max_depth, R, status, block_order);
     return cudaGetLastError();
 }
 

@@ -30,8 +30,10 @@ struct Requests {
 
 // block_order (optional, eye_blocks(cam) entries): the pixel block each thread
 // block of the launch takes (a permutation), e.g. the slow ones first.
+// nblocks >= 0: only the first nblocks entries of block_order run (a subset of
+// the pixel blocks); pixels of the other blocks get no requests written.
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
-                     cudaStream_t st, const int* block_order = nullptr);
+                     cudaStream_t st, const int* block_order = nullptr, int64_t nblocks = -1);
 // 30-bit Morton code of each request's hit point in the box aabb (10 bits per axis)
 cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32_t* keys, cudaStream_t st);
 // pixel blocks of the eye pass (EYE_THREADS consecutive pixels each)

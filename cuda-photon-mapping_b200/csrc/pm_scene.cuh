@@ -208,10 +208,23 @@ __device__ __forceinline__ void trav_init(Trav& T, V3 o, V3 d, Stk& stack) {
     trav_pass(T, 0, stack);
 }
 
+// Work counters of a traversal (the tracer's work-counting launch): interior
+// nodes visited (each visit tests both children's boxes) and triangle tests.
+// NoWork compiles to nothing.
+struct NoWork {
+    __device__ __forceinline__ void node() {}
+    __device__ __forceinline__ void tris(int) {}
+};
+struct Work {
+    unsigned nodes = 0, tri_tests = 0;
+    __device__ __forceinline__ void node() { nodes++; }
+    __device__ __forceinline__ void tris(int c) { tri_tests += (unsigned)c; }
+};
+
 // One round: descend until this lane holds a leaf (or every active lane does),
 // then test the held leaves.  Returns true when the pass is complete.
-template <class Stk>
-__device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, Stk& stack) {
+template <class Stk, class W = NoWork>
+__device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, Stk& stack, W&& work = W()) {
     int node = T.node, leaf = T.leaf, sp = T.sp;
     // Box slabs as fused multiply-adds: the boxes are padded far beyond the
     // rounding of either form, so culling stays conservative and the answer
@@ -219,6 +232,7 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
     // half the instructions of the node test.
     const float ix = T.ix, iy = T.iy, iz = T.iz, nox = -T.ox, noy = -T.oy, noz = -T.oz;
     while ((unsigned)node < (unsigned)TRAV_SENTINEL) {
+        work.node();
         const float4* N = S.nodes + 4 * (size_t)node;
         const float4 a0 = __ldg(N), b0 = __ldg(N + 1), a1 = __ldg(N + 2), b1 = __ldg(N + 3);
         const float best_t = T.best_t;
@@ -253,6 +267,7 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
     while (leaf < 0) {
         const int packed = ~leaf;
         const int first = packed >> 8, count = packed & 255;
+        work.tris(count);
         for (int i = 0; i < count; i++) {
             const float4* Q = S.tri_leaf + 5 * (size_t)(first + i);
             float t; V3 uvw; int tri, m;

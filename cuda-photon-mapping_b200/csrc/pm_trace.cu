@@ -22,6 +22,7 @@
 // A path that misses all geometry ends there and stores nothing (the reference
 // returns an undefined value from trace() in that case); a refraction that
 // yields no ray also ends the path.
+#include <type_traits>
 #include <vector>
 #include "pm_trace.cuh"
 #include "pm_scan.cuh"
@@ -71,6 +72,7 @@ struct KParams {
     uint32_t* cnt_c;
     unsigned* status;
     int refill;             // lanes with a finished query that end a warp's traversal loop
+    unsigned long long* work;   // work-counting launch: rays, BVH node visits, triangle tests (else null)
 };
 
 // light point + cosine-weighted direction by rejection (PhotonTracing.cu:345-369)
@@ -234,11 +236,16 @@ enum { L_IDLE = 0, L_RAY = 1, L_TRACE = 2, L_HIT = 3, L_DONE = 4 };
 // long (rays grazing the heightfield cross hundreds of leaves) keep their
 // traversal state while the others get new rays, instead of holding the whole
 // warp until the longest ray of a bounce is done.
+// COUNT: the work-counting variant (the same photons; each thread adds its
+// rays, node visits and triangle tests to P.work at the end).
+template <bool COUNT>
 __global__ void __launch_bounds__(TRACE_THREADS, TRACE_MIN_BLOCKS)
 k_trace(KParams P) {
     const int lane = threadIdx.x & 31;
     Lane L;
     Trav T;
+    std::conditional_t<COUNT, Work, NoWork> work;
+    unsigned rays = 0;
     __shared__ int stack_cols[TRACE_SMEM_STACK * TRACE_THREADS];
     TraceStack stack;
     stack.col = stack_cols + threadIdx.x;
@@ -268,13 +275,14 @@ k_trace(KParams P) {
         if (__all_sync(0xffffffffu, state == L_DONE)) break;
         if (state == L_RAY) {
             trav_init(T, L.ray.o, L.ray.d, stack);
+            if (COUNT) rays++;
             state = L_TRACE;
         }
         while (true) {
             const bool tr = state == L_TRACE;
             if (!__any_sync(0xffffffffu, tr)) break;
             if (__popc(__ballot_sync(0xffffffffu, state == L_HIT)) >= P.refill) break;
-            if (tr && trav_step(P.S, T, L.ray.o, L.ray.d, stack)) state = L_HIT;
+            if (tr && trav_step(P.S, T, L.ray.o, L.ray.d, stack, work)) state = L_HIT;
         }
         if (state == L_HIT) {
             Hit h;
@@ -293,6 +301,15 @@ k_trace(KParams P) {
                     state = L_RAY;
                 }
             }
+        }
+    }
+    if constexpr (COUNT) {
+        unsigned long long v[3] = {rays, work.nodes, work.tri_tests};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+            if (lane == 0) atomicAdd(P.work + c, v[c]);
         }
     }
 }
@@ -462,6 +479,7 @@ cudaError_t trace_multi_tables(const TraceMulti& M, const TraceInst* insts, cuda
         P.cnt_g = M.cnt_g; P.cnt_c = M.cnt_c;
         P.status = M.status;
         P.refill = M.refill > 0 ? std::min(M.refill, 32) : TRACE_REFILL;
+        P.work = nullptr;
     }
     cudaError_t e = cudaMemcpyAsync(M.table, tab.data(), tab.size() * sizeof(KParams), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
@@ -502,12 +520,15 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
     P.cnt_g = B.cnt_g; P.cnt_c = B.cnt_c;
     P.status = B.status;
     P.refill = B.refill > 0 ? std::min(B.refill, 32) : TRACE_REFILL;
+    P.work = B.work;
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace, TRACE_THREADS, 0)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<false>, TRACE_THREADS, 0)) != cudaSuccess)
+        return e;
     int64_t want = (B.npaths + TRACE_THREADS - 1) / TRACE_THREADS;
     int64_t grid = std::min<int64_t>(want, (int64_t)std::max(per_sm, 1) * B.sm_count);
     if (B.k_begin && (e = cudaEventRecord(B.k_begin, st)) != cudaSuccess) return e;
-    k_trace<<<(unsigned)grid, TRACE_THREADS, 0, st>>>(P);
+    if (B.work) k_trace<true><<<(unsigned)grid, TRACE_THREADS, 0, st>>>(P);
+    else k_trace<false><<<(unsigned)grid, TRACE_THREADS, 0, st>>>(P);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (B.k_end && (e = cudaEventRecord(B.k_end, st)) != cudaSuccess) return e;
     if ((e = scan_u32(B.cnt_g, B.scan_g, B.npaths, 0, B.totals, B.scan_ws, B.status, st)) != cudaSuccess) return e;

@@ -26,6 +26,7 @@ struct TraceBatch {
     int sm_count;
     int refill;               // k_trace refill threshold in lanes (1..32); 0: the default
     cudaEvent_t k_begin = nullptr, k_end = nullptr;   // when set: recorded around the k_trace launch
+    unsigned long long* work = nullptr;   // when set: the work-counting launch adds rays, node visits, triangle tests
 };
 
 struct PhotonList {

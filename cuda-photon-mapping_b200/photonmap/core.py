@@ -142,8 +142,10 @@ def library():
         "pm_gather": ([vp, C.c_int, i64, vp, vp, C.c_int, f32, vp, vp, vp], C.c_int),
         "pm_camera_setup": ([vp, vp, vp, f32, i32, i32, C.POINTER(Camera)], C.c_int),
         "pm_render": ([vp, C.POINTER(Camera), C.POINTER(_RenderOpts), vp, vp], C.c_int),
+        "pm_render_rows": ([vp, C.POINTER(Camera), C.POINTER(_RenderOpts), i32, i32, vp, vp], C.c_int),
         "pm_scan_u32": ([vp, vp, vp, i64, C.c_int], C.c_int),
         "pm_debug_scan_stall": ([vp, vp, vp, i64, i64, i32], C.c_int),
+        "pm_trace_work": ([vp, vp, vp, vp], C.c_int),
         "pm_stage_times": ([vp, vp], C.c_int),
         "pm_status": ([vp, vp], C.c_int),
         "pm_launch_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
@@ -333,6 +335,11 @@ class Context:
         self._check(self.L.pm_set_scene(self.h, C.byref(d)), "pm_set_scene")
         self._scene = sc
 
+    @property
+    def light_intensity(self):
+        """The current scene's light intensity (3 floats)."""
+        return np.asarray(self._scene.light_intensity, np.float32)
+
     def scene_aabb(self):
         out = np.empty(6, np.float32)
         self._check(self.L.pm_scene_aabb(self.h, out.ctypes.data), "pm_scene_aabb")
@@ -344,6 +351,14 @@ class Context:
         paths = C.c_int64()
         self._check(self.L.pm_trace_photons(self.h, C.byref(o), C.byref(paths)), "pm_trace_photons")
         return paths.value
+
+    def trace_work(self, seed, max_bounces, global_capacity, caustic_capacity=0, tag=0, max_paths=0):
+        """trace_photons with the tracer's work counted: (paths, rays, BVH node visits, triangle tests)."""
+        o = _TraceOpts(seed, tag, max_bounces, global_capacity, caustic_capacity, max_paths)
+        paths = C.c_int64()
+        w = (C.c_uint64 * 3)()
+        self._check(self.L.pm_trace_work(self.h, C.byref(o), C.byref(paths), w), "pm_trace_work")
+        return paths.value, int(w[0]), int(w[1]), int(w[2])
 
     def trace_paths(self, seed, max_bounces, power_capacity, p0, p1, tag=0):
         torch = self.torch
@@ -359,11 +374,16 @@ class Context:
         return dict(counts=counts, g_pos=gp[:ng.value], g_dir=gd[:ng.value], c_pos=cp[:nc.value], c_dir=cd[:nc.value])
 
     def set_photons(self, map_id, pos, power, direction):
-        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
-        pw = np.ascontiguousarray(power, np.float32).reshape(-1, 3)
-        dr = np.ascontiguousarray(direction, np.float32).reshape(-1, 3)
-        self._check(self.L.pm_set_photons(self.h, map_id, pos.shape[0], pos.ctypes.data, pw.ctypes.data,
-                                          dr.ctypes.data), "pm_set_photons")
+        """A map's photon list from host arrays or device tensors (3 floats per photon)."""
+        torch = self.torch
+        if all(isinstance(a, torch.Tensor) and a.is_cuda for a in (pos, power, direction)):
+            arrs = [a.to(self.device, torch.float32).contiguous().reshape(-1, 3) for a in (pos, power, direction)]
+            ptrs = [a.data_ptr() for a in arrs]
+        else:
+            arrs = [np.ascontiguousarray(a.cpu().numpy() if isinstance(a, torch.Tensor) else a, np.float32)
+                    .reshape(-1, 3) for a in (pos, power, direction)]
+            ptrs = [a.ctypes.data for a in arrs]
+        self._check(self.L.pm_set_photons(self.h, map_id, arrs[0].shape[0], *ptrs), "pm_set_photons")
 
     def build_grid(self, map_id=PM_MAP_GLOBAL, desired=1000, regrid_mult=5, regrid_div=5, aabb=None, sub_div=0,
                    k_hint=0):
@@ -560,6 +580,20 @@ class Context:
             rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
         o = _RenderOpts(max_depth, k_global, r_global, k_caustic, r_caustic, int(faithful_caustic))
         self._check(self.L.pm_render(self.h, C.byref(cam), C.byref(o), _ptr(rgb), _ptr(rad)), "pm_render")
+        return rgb, rad
+
+    def render_rows(self, cam: Camera, k_global, r_global, max_depth, y0, y1, k_caustic=0, r_caustic=0.2,
+                    faithful_caustic=True, radiance=True, out_rgb8=None, out_radiance=None):
+        """Rows [y0, y1) of render()'s frame (pm_render_rows)."""
+        torch = self.torch
+        W, H = cam.width, cam.height
+        rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
+        rad = out_radiance
+        if rad is None and radiance:
+            rad = torch.empty((H * W, 3), dtype=torch.float32, device=self.device)
+        o = _RenderOpts(max_depth, k_global, r_global, k_caustic, r_caustic, int(faithful_caustic))
+        self._check(self.L.pm_render_rows(self.h, C.byref(cam), C.byref(o), int(y0), int(y1), _ptr(rgb), _ptr(rad)),
+                    "pm_render_rows")
         return rgb, rad
 
     def scan_u32(self, x, inclusive):

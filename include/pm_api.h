@@ -162,6 +162,16 @@ int pm_bvh_info(pm_ctx* ctx, int32_t* out_builder, int64_t* out_nodes, float* ou
  * receives the number of paths traced. */
 int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* opts, int64_t* out_paths);
 
+/* The photon pass of pm_trace_photons (the same photons, lists and grids
+ * untouched otherwise) with the tracer's work counted, for the flop roofline
+ * of the photon tracer (no counterpart in the reference, which estimates 86
+ * flop per triangle test, Model.cuh:65-67): out_work[0] = rays traced (a ray
+ * whose nearest hit sits at t = 0 in an earlier model counts once),
+ * [1] BVH interior nodes visited (each visit tests both children's boxes),
+ * [2] triangle tests.  The counting launch runs slower than pm_trace_photons;
+ * time the latter. */
+int pm_trace_work(pm_ctx* ctx, const pm_trace_opts* opts, int64_t* out_paths, uint64_t out_work[3]);
+
 /* Photon output of paths [p0, p1) without a capacity cut (parity testing and
  * path-range sharding).  Writes device arrays of capacity (p1-p0)*max_bounces
  * photons per map: pos/dir (3 floats), and per path counts[2] (global,
@@ -170,9 +180,9 @@ int pm_trace_paths(pm_ctx* ctx, const pm_trace_opts* opts, int64_t p0, int64_t p
                    float* g_pos, float* g_dir, float* c_pos, float* c_dir, uint32_t* counts,
                    int64_t* out_ng, int64_t* out_nc);
 
-/* Replace a map's photon list with caller data (host arrays, 3 floats per
- * photon) -- the input side of PhotonGrid::build and of the photon-map
- * reader load() (Initializer.cu:102-141). */
+/* Replace a map's photon list with caller data (host or device arrays, 3
+ * floats per photon) -- the input side of PhotonGrid::build and of the
+ * photon-map reader load() (Initializer.cu:102-141). */
 int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const float* power, const float* dir);
 
 /* Grid build.  Replaces PhotonGrid(num_photons, aabb).build(photons, 1000,
@@ -205,6 +215,15 @@ int pm_camera_setup(const float position[3], const float direction[3], const flo
  * out_radiance (optional) 3 floats per pixel, before tone mapping.
  * The global map must be built; the caustic map is used when built. */
 int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, uint8_t* out_rgb8, float* out_radiance);
+
+/* The rows [y0, y1) of pm_render's frame (a pixel-row band; no counterpart in
+ * the reference, whose frame is one launch): the eye pass runs only the pixel
+ * blocks that meet those rows, so the band costs about its share of the
+ * frame.  Pixels of the band are pm_render's bit for bit; every other pixel
+ * of out_rgb8 / out_radiance holds 0 or, in the pixel blocks that straddle
+ * the band's edges, pm_render's value.  For frames split over GPUs. */
+int pm_render_rows(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, int32_t y0, int32_t y1,
+                   uint8_t* out_rgb8, float* out_radiance);
 
 /* A whole frame in one call: pm_trace_photons(trace), pm_build_grid of the
  * global map (and of the caustic map when trace fills one and k_caustic > 0)

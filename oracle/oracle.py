@@ -239,6 +239,22 @@ class OracleScene:
         return dict(counts=counts, draws=draws, g_pos=gp[:ng[0]], g_dir=gd[:ng[0]], g_bounce=gb[:ng[0]],
                     c_pos=cp[:nc[0]], c_dir=cd[:nc[0]], c_bounce=cb[:nc[0]])
 
+    def eye_hits(self, cam_vec, width, height, pixels, max_depth=4):
+        """The eye paths of `pixels` (y * width + x) as the reference's render_trace
+        walks them: dict of a, b, c (hits, 4 floats each; the product's request
+        layout), counts per pixel."""
+        px = _c(pixels, np.int64)
+        counts = np.empty(px.size, np.int32)
+        cap = int(px.size) * (2 ** max(max_depth, 1))
+        a = np.empty((cap, 4), np.float32); b = np.empty_like(a); c = np.empty_like(a)
+        self.orc.L.orc_eye_hits.restype = C.c_int64
+        n = self.orc.L.orc_eye_hits(self.h, _ptr(_c(cam_vec, np.float32)), C.c_int(width), C.c_int(height),
+                                    C.c_int64(px.size), _ptr(px), C.c_int(max_depth), _ptr(counts), _ptr(a), _ptr(b),
+                                    _ptr(c), C.c_int64(cap))
+        if n < 0:
+            raise RuntimeError("orc_eye_hits: record capacity exceeded")
+        return dict(a=a[:n], b=b[:n], c=c[:n], counts=counts)
+
     def render(self, cam_vec, width, height, g: GridResult, k, radius, max_depth=4, y0=0, y1=None,
                c: GridResult = None, k_c=0, r_c=0.2, heap_mode=False, faithful_caustic=True):
         y1 = height if y1 is None else y1
@@ -403,6 +419,9 @@ class RefTrace:
         L.ref_trace_critical_angles.argtypes = [C.c_void_p, C.c_float, C.c_void_p, C.c_int]
         L.ref_trace_paths.argtypes = ([C.c_void_p, C.c_float, C.c_uint64, C.c_uint32, C.c_int64, C.c_int64,
                                        C.c_int64, C.c_int] + [C.c_void_p] * 12)
+        L.ref_gpu_trace_paths.restype = C.c_int
+        L.ref_gpu_trace_paths.argtypes = ([C.c_void_p, C.c_float, C.c_uint64, C.c_uint32, C.c_int64, C.c_int64,
+                                           C.c_int64] + [C.c_void_p] * 10)
 
     def scene(self, sc):
         """A reference scene (one Model per model index).  The reference holds one
@@ -451,3 +470,21 @@ class _RefTraceScene:
         return dict(counts=counts, draws=draws, g_pos=gp[:ng[0]], g_pow=gw[:ng[0]], g_dir=gd[:ng[0]],
                     g_bounce=gb[:ng[0]], c_pos=cp[:nc[0]], c_pow=cw[:nc[0]], c_dir=cd[:nc[0]],
                     c_bounce=cb[:nc[0]])
+
+    def gpu_trace_paths(self, seed, power_cap, p0, p1, tag=0):
+        """The same paths through the reference's device build on the current GPU
+        (its GPU numerics: vec3 rounded toward zero), one path per thread."""
+        n = p1 - p0
+        cap = n * RefTrace.MAX_BOUNCES
+        counts = np.empty((n, 2), np.int32)
+        draws = np.empty(n, np.int32)
+        gp = np.empty((cap, 3), np.float32); gd = np.empty_like(gp); gb = np.empty(cap, np.int32)
+        cp = np.empty((cap, 3), np.float32); cd = np.empty_like(cp); cb = np.empty(cap, np.int32)
+        ng = np.zeros(1, np.int64); nc = np.zeros(1, np.int64)
+        rc = self.ref.L.ref_gpu_trace_paths(self.h, self.default_ior, seed, tag, power_cap, p0, p1, _ptr(counts),
+                                            _ptr(draws), _ptr(gp), _ptr(gd), _ptr(gb), _ptr(cp), _ptr(cd), _ptr(cb),
+                                            _ptr(ng), _ptr(nc))
+        if rc != 0:
+            raise RuntimeError(f"ref_gpu_trace_paths: CUDA error {rc}")
+        return dict(counts=counts, draws=draws, g_pos=gp[:ng[0]], g_dir=gd[:ng[0]], g_bounce=gb[:ng[0]],
+                    c_pos=cp[:nc[0]], c_dir=cd[:nc[0]], c_bounce=cb[:nc[0]])

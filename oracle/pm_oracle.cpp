@@ -639,7 +639,13 @@ struct RenderOpts {
     int k_global, k_caustic;
     int knn_heap_mode;      // 1: reference max-heap selection, 0: canonical (distance, id)
     int faithful_caustic;   // 1: caustic estimate reads the global map's dir/power (CPM/Raytracer.cuh:203-204)
+    int hits_only = 0;      // 1: record the eye path's hits, skip the estimates (they do not steer the path)
 };
+
+// One hit of an eye path: where the reference's render_trace would gather
+// (point, triangle, shading normal), whether it takes the global estimate
+// (flags bit 0), and the path weight `coef` its colour is multiplied by.
+struct HitRec { V3 p; int tri; V3 n; uint32_t flags; V3 coef; };
 
 // Per-pixel state of RaytracePlanner + MediumManager with the reference's index
 // arithmetic (CPM/MediumManager.cuh:17-79, MMInnerStack.cuh:131, MMOuterStack.cuh:269).
@@ -738,7 +744,8 @@ struct Maps {
 };
 
 // render_trace (CPM/Raytracer.cuh:140-241); returns the pre-tone-map radiance
-static V3 render_trace(const Scene& s, const Maps& maps, const RenderOpts& o, Ray ray, int* nhits, bool* overflow) {
+static V3 render_trace(const Scene& s, const Maps& maps, const RenderOpts& o, Ray ray, int* nhits, bool* overflow,
+                       std::vector<HitRec>* rec = nullptr) {
     PixelState ps(o.max_depth);
     int new_depth = 0, cur = -1;
     V3 acc = v3(0.f, 0.f, 0.f), coef = v3(1.f, 1.f, 1.f);
@@ -757,7 +764,10 @@ static V3 render_trace(const Scene& s, const Maps& maps, const RenderOpts& o, Ra
         if (in_obj && vdot(ray.d, n) > 0) n = vscale(n, -1.f);
         V3 color = v3(0.f, 0.f, 0.f);
         V3 mdiff = tri_diffuse(s, h);
-        if (!in_obj && !vnull(mdiff)) {
+        if (rec) rec->push_back(HitRec{ip, h.tri, n, (!in_obj && !vnull(mdiff)) ? 1u : 0u, coef});
+        if (o.hits_only) {
+            // the estimates below only colour the hit; the path goes on the same way
+        } else if (!in_obj && !vnull(mdiff)) {
             V3 di_op = vscale(mdiff, m.opaque);
             if (o.knn_heap_mode) knn_heap(maps.g, ip, o.r_global, o.k_global, nb);
             else knn_canonical(maps.g, ip, o.r_global, o.k_global, nb);
@@ -765,7 +775,7 @@ static V3 render_trace(const Scene& s, const Maps& maps, const RenderOpts& o, Ra
             color = vadd(color, vscale(vmul(re, di_op), 4.f));
         }
         color = vadd(color, m.emission);
-        if (maps.has_c) {
+        if (maps.has_c && !o.hits_only) {
             if (o.knn_heap_mode) knn_heap(maps.c, ip, o.r_caustic, o.k_caustic, nb);
             else knn_canonical(maps.c, ip, o.r_caustic, o.k_caustic, nb);
             if ((int)nb.size() == o.k_caustic) {
@@ -1078,6 +1088,45 @@ int orc_render(void* h, const float* cam, int W, int H, int y0, int y1,
         if (out_hits) out_hits[i] = hits;
     }
     return overflow_px;
+}
+
+// The eye paths of the given pixels (px[i] = y * W + x) as the reference's
+// render_trace walks them (CPM/Raytracer.cuh:140-241), without the estimates:
+// per hit, a = (point, triangle bits), b = (shading normal, flags bits: 1 when
+// the hit takes the global estimate), c = (path weight, pixel bits), in the
+// order the path meets them.  counts[i] = hits of pixel i; the records hold
+// `cap` entries.  Returns the number of hits written (-1: cap too small).
+int64_t orc_eye_hits(void* h, const float* cam, int W, int H, int64_t npx, const int64_t* px, int max_depth,
+                     int* counts, float* out_a, float* out_b, float* out_c, int64_t cap) {
+    Scene* s = (Scene*)h;
+    Camera c;
+    c.pos = ld3(cam); c.fwd = ld3(cam + 3); c.right = ld3(cam + 6); c.up = ld3(cam + 9);
+    c.vw = cam[12]; c.vh = cam[13]; c.focal = cam[14]; c.W = W; c.H = H;
+    Maps maps{};
+    maps.has_c = false;
+    RenderOpts o{max_depth, 0.f, 0.f, 0, 0, 0, 0, 1};
+    std::vector<std::vector<HitRec>> recs((size_t)npx);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < npx; i++) {
+        const int x = (int)(px[i] % W), y = (int)(px[i] / W);
+        Ray r;
+        r.o = c.pos;
+        r.d = vnormalize_static(camera_dir(c, x, y));
+        (void)render_trace(*s, maps, o, r, nullptr, nullptr, &recs[i]);
+    }
+    int64_t k = 0;
+    for (int64_t i = 0; i < npx; i++) {
+        counts[i] = (int)recs[i].size();
+        for (const HitRec& q : recs[i]) {
+            if (k >= cap) return -1;
+            const uint32_t pix = (uint32_t)px[i];
+            st3(out_a + 4 * k, q.p); std::memcpy(out_a + 4 * k + 3, &q.tri, 4);
+            st3(out_b + 4 * k, q.n); std::memcpy(out_b + 4 * k + 3, &q.flags, 4);
+            st3(out_c + 4 * k, q.coef); std::memcpy(out_c + 4 * k + 3, &pix, 4);
+            k++;
+        }
+    }
+    return k;
 }
 
 // normalised eye-ray directions for pixels (xs[i], ys[i]); cam as from orc_camera

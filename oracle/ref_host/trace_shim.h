@@ -21,6 +21,14 @@
 //    memory (and cudaGetLastError reports success), and the device atomics the included headers name act on plain
 //    host integers (they run on one host thread per slot).
 // Kernels (__global__) keep their qualifier: their bodies are never run here.
+//
+// In the device pass the reference stays device code (its vec3 rounds toward
+// zero, CPM/vec3.cuh:18-20: the reference's GPU numerics), with two changes
+// for the harness kernel of ref_trace.cu that runs it on the GPU, one path per
+// thread: curand_uniform(state) draws the calling thread's injected path
+// stream, and __constant__ globals become __device__ globals, so that the
+// harness's set-up kernel can give them their values (the reference sets them
+// with cudaMemcpyToSymbol from its host code).
 #include "shim.h"
 #include <device_launch_parameters.h>
 #include <cstdint>
@@ -75,4 +83,9 @@ inline int pm_ref_atomic_exch(int* a, int v) { int o = *a; *a = v; return o; }
 #define atomicAdd pm_ref_atomic_add
 #define atomicCAS pm_ref_atomic_cas
 #define atomicExch pm_ref_atomic_exch
+#else
+__device__ float pm_ref_dev_uniform();
+#define curand_uniform(state) pm_ref_dev_uniform()
+#undef __constant__
+#define __constant__ __device__
 #endif

@@ -53,6 +53,40 @@ class PhotonMap64:
         return acc * norm[:, None]
 
 
+def estimate_ids(pos, direction, power, qpos, qnrm, ids, cnt):
+    """FP64 estimate of get_color_from_photon_grid (CudaPhotonMapping/Raytracer.cuh:110-138)
+    over given neighbour sets: ids[i, :cnt[i]] index the photon arrays (the
+    oracle's kNN selection); r_k is the largest neighbour distance, in FP64."""
+    qpos = np.asarray(qpos, np.float64).reshape(-1, 3)
+    qnrm = np.asarray(qnrm, np.float64).reshape(-1, 3)
+    ids = np.asarray(ids)
+    k = ids.shape[1]
+    valid = np.arange(k)[None, :] < np.asarray(cnt)[:, None]
+    safe = np.where(valid, ids, 0).astype(np.int64)
+    p = np.asarray(pos, np.float32)[safe].astype(np.float64)
+    d = np.sqrt(((p - qpos[:, None, :]) ** 2).sum(-1))
+    d = np.where(valid, d, 0.0)
+    rk = d.max(axis=1)
+    cos = -np.einsum("qkc,qc->qk", np.asarray(direction, np.float32)[safe].astype(np.float64), qnrm)
+    use = valid & (cos > 0)
+    fr = np.where(rk > 0, rk * rk, 1.0)[:, None]
+    filt = ALPHA * (1 - (1 - np.exp(-BETA * d * d / (2 * fr))) / (1 - np.exp(-BETA)))
+    filt = np.where(use, filt, 0.0)
+    acc = np.einsum("qk,qkc->qc", filt, np.asarray(power, np.float32)[safe].astype(np.float64))
+    norm = np.where(rk > 0, 1.0 / (np.pi * rk * rk), 0.0)
+    return acc * norm[:, None]
+
+
+def resolve_hits(hits, tables, est_global):
+    """FP64 radiance per pixel from its eye-path hits (records a, b, c and
+    counts per pixel, as Oracle scene eye_hits returns them); est_global(hit
+    indices) -> (m, 3) FP64 estimates of those hits."""
+    counts = np.asarray(hits["counts"], np.int64)
+    base = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int32)
+    req = dict(a=hits["a"], b=hits["b"], c=hits["c"], px_base=base, px_count=counts.astype(np.int32))
+    return resolve64(req, np.arange(counts.size), tables, est_global)
+
+
 def scene_tables(scene):
     """Per-triangle albedo, opaque and emission arrays of a photonmap.scenes.Scene."""
     mats = np.asarray(scene.materials, np.float64)

@@ -87,3 +87,29 @@ def test_batch_autotuned(gpu):
         assert int((a - ref).abs().max()) <= 1, i
         assert float((a != ref).float().mean()) < 0.01, i
     b.close()
+
+
+@pytest.mark.gpu
+def test_batch_instances_against_the_oracle(gpu, orc):
+    """Two batch instances (jittered light, random sphere radii) against the
+    oracle's own photon pass, grid and render of them: 8-bit pixels at most
+    one level apart (the estimates differ only by CUDA's expf / powf)."""
+    import numpy as np
+    import photonmap
+    from photonmap import scenes
+    insts = _instances(2, seed=21, photons_range=(20_000, 60_000), res_range=(64, 96))
+    b = photonmap.Batch(insts, autotune=False, use_graph=True)
+    b.frame(3)
+    for i, inst in enumerate(insts):
+        s = orc.scene(inst["scene"])
+        tr = s.trace_photons(inst["seed"] + 3, inst["max_bounces"], inst["photons"])
+        g = orc.grid_build(tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
+        c = inst["camera"]
+        cs = scenes.default_camera(c.width, c.height)
+        out = s.render(orc.camera(cs), c.width, c.height, g, inst["k"], inst["radius"], inst["max_depth"])
+        img = b.image(i).cpu().numpy().reshape(-1, 3).astype(int)
+        d = np.abs(img - out["rgb8"].astype(int))
+        assert d.max() <= 1, i
+        assert (d != 0).mean() < 0.01, i
+        assert img.max() > 0
+    b.close()

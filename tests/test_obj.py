@@ -12,7 +12,10 @@ import photonmap
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
-REF_OBJ = "/root/reference/CudaPhotonMapping/Models/cornell_box_sphere"
+# the reference's Cornell-sphere scene, where the reference is mounted
+# ($PM_REFERENCE_ROOT, default /root/reference; the test skips without it)
+REF_OBJ = os.path.join(os.environ.get("PM_REFERENCE_ROOT", "/root/reference"), "CudaPhotonMapping", "Models",
+                       "cornell_box_sphere")
 
 MTL = """# materials
 newmtl white
