@@ -394,17 +394,21 @@ def learned_frames(ctx, sc, cs, cam, w, rgb, args, world):
 
     ms_plain = timed(plain)
     ms_learned = timed(learned_frame)
-    # the same frame captured once and replayed as one CUDA graph per frame
-    graph = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=steps_per_frame,
-                              batch=BATCH, offset=off[0], out_rgb8=rgb, **learned.FRAME_SETTINGS)
+    # the same frame captured once and replayed as one CUDA graph per frame: the
+    # training first, then the render with the trained cache (serial), or the
+    # render with the cache the previous frames trained while this frame's
+    # training runs beside it (overlapped; the timed learned form)
     gstats = {}
-
-    def graph_frame():
-        graph.run()
-
-    ms_graph = timed(graph_frame)
-    gstats.update(graph.run(stats=True)[2])
-    graph.close()
+    ms_graphs = {}
+    for overlap in (False, True):
+        graph = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=steps_per_frame,
+                                  batch=BATCH, offset=off[0], out_rgb8=rgb, overlap_training=overlap,
+                                  **learned.FRAME_SETTINGS)
+        ms_graphs[overlap] = timed(graph.run)
+        gstats[overlap] = graph.run(stats=True)[2]
+        off[0] = graph.offset()
+        graph.close()
+    ms_graph = ms_graphs[True]
     # tensor-core throughput of the cache kernels (forward 32,640 flop per sample, backward ~2x)
     fwd = 2 * (60 * 64 + 3 * 64 * 64 + 64 * 3)
     n = min(pool.n, 1 << 20)
@@ -423,8 +427,13 @@ def learned_frames(ctx, sc, cs, cam, w, rgb, args, world):
     tr_tf = 3 * fwd * min(1 << 20, pool.n) / (ms_tr * 1e-3) / 1e12
     block = {"ms_per_frame_plain": ms_plain, "ms_per_frame_learned": ms_learned, "speedup": ms_plain / ms_learned,
              "ms_per_frame_learned_graph": ms_graph, "speedup_graph": ms_plain / ms_graph,
-             "graph_fallback_requests_frac": gstats["fallback_requests"] / max(gstats["requests"], 1),
+             "ms_per_frame_learned_graph_serial": ms_graphs[False],
+             "speedup_graph_serial": ms_plain / ms_graphs[False],
+             "graph_fallback_requests_frac": gstats[True]["fallback_requests"] / max(gstats[True]["requests"], 1),
              "frame": "eye pass + global estimate + resolve, photon map resident",
+             "graph": "overlapped: the render reads the cache as the previous frames trained it (a copy at the "
+                      "frame's start) while the frame's 2^20-sample training runs beside it; serial: training, "
+                      "then the render",
              "train_samples_per_frame": TRAIN_PER_FRAME, "train_batch": BATCH, "adam_steps_per_frame": steps_per_frame,
              "pool": pool.n, "one_time": {"pool_labelling_ms": pool_ms, "warmup_steps": WARM_STEPS,
                                           "warmup_ms": warm_ms},
@@ -472,17 +481,23 @@ def learned_rmse(ctx, sc, cs, cam, w):
     orc = Oracle()
     s = orc.scene(sc)
     hits = s.eye_hits(orc.camera(cs), W, H, pixels, w["max_depth"])
-    # the oracle's eye paths against the GPU eye pass's requests of the same pixels
+    # the oracle's eye paths against the GPU eye pass's requests of the same
+    # pixels: per pixel the same number of hits, and per hit the same point,
+    # triangle, normal, global-estimate flag and path weight (bit for bit)
     cnt = req["px_count"][pixels].astype(np.int64)
-    same_count = bool(np.array_equal(cnt, hits["counts"]))
-    hits_equal = False
-    if same_count:
-        q = np.repeat(req["px_base"][pixels].astype(np.int64), cnt) + \
-            (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
-        ga, gb, gc = req["a"][q], req["b"][q], req["c"][q]
-        fl = lambda x: (x[:, 3].view(np.uint32) & 1)  # noqa: E731
-        hits_equal = bool(np.array_equal(ga, hits["a"]) and np.array_equal(gb[:, :3], hits["b"][:, :3]) and
-                          np.array_equal(fl(gb), fl(hits["b"])) and np.array_equal(gc[:, :3], hits["c"][:, :3]))
+    same_px = cnt == hits["counts"]
+    q = np.repeat(req["px_base"][pixels].astype(np.int64), cnt) + \
+        (np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt))
+    hb = np.concatenate([[0], np.cumsum(hits["counts"])]).astype(np.int64)
+    gb_ = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+    ok_px = np.zeros(pixels.size, bool)
+    fl = lambda x: (x[:, 3].view(np.uint32) & 1)  # noqa: E731
+    for i in np.nonzero(same_px)[0]:
+        o, g0 = slice(hb[i], hb[i + 1]), slice(gb_[i], gb_[i + 1])
+        ga, gbb, gc = req["a"][q[g0]], req["b"][q[g0]], req["c"][q[g0]]
+        ok_px[i] = (np.array_equal(ga, hits["a"][o]) and np.array_equal(gbb[:, :3], hits["b"][o, :3]) and
+                    np.array_equal(fl(gbb), fl(hits["b"][o])) and np.array_equal(gc[:, :3], hits["c"][o, :3]))
+    hits_equal = bool(ok_px.all())
     tables = render64.scene_tables(sc)
     g_mask = (hits["b"][:, 3].view(np.uint32) & 1) != 0
     qp, qn = hits["a"][g_mask, :3], hits["b"][g_mask, :3]
@@ -512,6 +527,7 @@ def learned_rmse(ctx, sc, cs, cam, w):
                          f"{w['photons'] // 1_000_000}M-photon maps ({P['rmse_maps']}x the frame's photons), "
                          f"eye paths walked by the oracle",
             "oracle_eye_hits": int(hits["a"].shape[0]), "oracle_eye_hits_equal_gpu_requests": hits_equal,
+            "pixels_same_hit_count": float(same_px.mean()), "pixels_hits_bit_equal": float(ok_px.mean()),
             "seconds": time.perf_counter() - t0}
 
 

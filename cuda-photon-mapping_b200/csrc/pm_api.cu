@@ -470,7 +470,10 @@ int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const 
     cudaStream_t st = ctx->st;
     if (!out_loss && steps > 0) {
         if (!ctx->train_st) {
-            CK(cudaStreamCreateWithFlags(&ctx->train_st, cudaStreamNonBlocking));
+            // the lowest priority: queued training fills the SMs the frame's launches leave idle
+            int prio_low = 0, prio_high = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+            CK(cudaStreamCreateWithPriority(&ctx->train_st, cudaStreamNonBlocking, prio_low));
             CK(cudaEventCreateWithFlags(&ctx->train_fork, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&ctx->train_done, cudaEventDisableTiming));
         }

@@ -47,16 +47,17 @@ struct pm_learned_graph {
     const float* pool_target = nullptr;
     int64_t pool_n = 0, batch = 0;
     int steps = 0;
+    bool overlap = false;       // inference reads w16_snap (the cache before this frame's training)
     // device buffers owned by the graph
     DevBuf req_a, req_b, req_c, counter, px_base, px_count, est_mlp, est_fb, est_g;
-    DevBuf probe_pos, probe_nrm, probe_req, probe_est, tile_flag, counts, fb_list, state, eye_order;
+    DevBuf probe_pos, probe_nrm, probe_req, probe_est, tile_flag, counts, fb_list, state, eye_order, w16_snap;
     int launches_per_frame = 0;
     // the context as the captured launches saw it
     uint64_t generation = 0, buffers = 0;
     // training runs on a second stream beside the eye pass and the probe
     // gathers (it needs neither; inference waits for it)
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr;
+    cudaStream_t side = nullptr, inf = nullptr, hi = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr, inf_done = nullptr, hi_done = nullptr;
 };
 
 namespace {
@@ -99,8 +100,14 @@ int enqueue_frame(pm_learned_graph* g) {
     const cudaStream_t main_st = ctx->st;
     unsigned* status = P<unsigned>(ctx->status);
     const MlpNet net = cache_net(ctx);
+    MlpNet net_infer = net;
     const pm_cache_opts& co = ctx->cache_opts;
     int launches = 0;
+    if (g->overlap) {   // the cache as the previous frames trained it, for this frame's inference
+        CK(cudaMemcpyAsync(g->w16_snap.p, ctx->cache_w16.p, (size_t)PM_CACHE_PARAMS * 2, cudaMemcpyDeviceToDevice,
+                           main_st));
+        net_infer.w = P<__nv_bfloat16>(g->w16_snap);
+    }
     // online training on the pool, on the side stream: the eye pass leaves
     // most SMs idle while its slowest pixels finish, and training fills them
     CK(cudaEventRecord(g->fork, main_st));
@@ -125,23 +132,32 @@ int enqueue_frame(pm_learned_graph* g) {
         CK(cudaGetLastError());
         launches += 5;
     }
-    st = main_st;
     // the learned render: eye pass, then the probe gathers here while the side
     // stream (after its training) answers every request with the cache
+    // (overlapped: the render on the high-priority stream, inference beside it)
+    st = main_st;
+    if (g->overlap) {
+        CK(cudaStreamWaitEvent(g->hi, g->fork, 0));
+        st = g->hi;
+    }
     const DevScene S = dev_scene(ctx);
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     const Requests R = requests_of(g);
     CK(eye_pass(S, g->cd, g->ro.max_depth, R, status, st, P<int>(g->eye_order)));
     CK(cudaEventRecord(g->eye_done, st));
-    CK(cudaStreamWaitEvent(g->side, g->eye_done, 0));
+    // inference: after the training on the side stream, or (overlap) on its
+    // own stream with the frame-start copy while the training goes on
+    const cudaStream_t ist = g->overlap ? g->inf : g->side;
+    CK(cudaStreamWaitEvent(ist, g->eye_done, 0));
     MlpInputs in{};
     in.n = g->cap;
     in.rec_pos = R.a;
     in.rec_nrm = R.b;
     in.flag_mask = 1u;
     in.n_dev = R.counter;
-    CK(mlp_infer(net, in, P<float>(g->est_mlp), status, ctx->sm_count, g->side));
-    CK(cudaEventRecord(g->join, g->side));
+    CK(mlp_infer(net_infer, in, P<float>(g->est_mlp), status, ctx->sm_count, ist));
+    CK(cudaEventRecord(g->overlap ? g->inf_done : g->join, ist));
+    if (g->overlap) CK(cudaEventRecord(g->join, g->side));   // the training, joined at the frame's end
     const int T = g->lo.tile, Pn = g->lo.probes;
     CK(learned_probes(g->cd, R, T, Pn, P<float4>(g->probe_pos), P<float4>(g->probe_nrm), P<uint32_t>(g->probe_req), st));
     GatherQueries PQ{};
@@ -151,7 +167,7 @@ int enqueue_frame(pm_learned_graph* g) {
     PQ.flag_mask = 1u;
     GatherOut PO{P<float>(g->probe_est), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), PQ, g->ro.r_global, g->ro.k_global, 0, PO, status, st));
-    CK(cudaStreamWaitEvent(st, g->join, 0));   // the cache's answers
+    CK(cudaStreamWaitEvent(st, g->overlap ? g->inf_done : g->join, 0));   // the cache's answers
     unsigned long long* counts = P<unsigned long long>(g->counts);
     CK(cudaMemsetAsync(counts, 0, 32, st));
     CK(learned_select(g->cd, R, g->cap, R.counter, T, Pn, P<uint32_t>(g->probe_req), P<float>(g->probe_est),
@@ -169,6 +185,11 @@ int enqueue_frame(pm_learned_graph* g) {
                      st));
     const float tone_t = (float)std::pow((double)0.6f, -1);
     CK(resolve(S, g->cd, R, P<float>(g->est_g), nullptr, tone_t, g->out_rgb8, g->out_radiance, st));
+    if (g->overlap) {   // back to the context's stream; the next frame's copy sees this frame's training
+        CK(cudaEventRecord(g->hi_done, st));
+        CK(cudaStreamWaitEvent(main_st, g->hi_done, 0));
+        CK(cudaStreamWaitEvent(main_st, g->join, 0));
+    }
     launches += 10;
     g->launches_per_frame = launches;
     return PM_OK;
@@ -180,10 +201,14 @@ void free_graph(pm_learned_graph* g) {
     if (g->fork) cudaEventDestroy(g->fork);
     if (g->join) cudaEventDestroy(g->join);
     if (g->eye_done) cudaEventDestroy(g->eye_done);
+    if (g->inf_done) cudaEventDestroy(g->inf_done);
+    if (g->hi_done) cudaEventDestroy(g->hi_done);
     if (g->side) cudaStreamDestroy(g->side);
+    if (g->inf) cudaStreamDestroy(g->inf);
+    if (g->hi) cudaStreamDestroy(g->hi);
     DevBuf* bufs[] = {&g->req_a, &g->req_b, &g->req_c, &g->counter, &g->px_base, &g->px_count, &g->est_mlp, &g->est_fb,
                       &g->est_g, &g->probe_pos, &g->probe_nrm, &g->probe_req, &g->probe_est, &g->tile_flag,
-                      &g->counts, &g->fb_list, &g->state, &g->eye_order};
+                      &g->counts, &g->fb_list, &g->state, &g->eye_order, &g->w16_snap};
     for (DevBuf* b : bufs) release(*b);
     delete g;
 }
@@ -199,8 +224,8 @@ extern "C" {
 
 int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, const pm_learned_opts* lo,
                             const float* pool_pos, const float* pool_nrm, const float* pool_target, int64_t pool_n,
-                            int64_t batch, int32_t steps, int64_t pool_offset, uint8_t* out_rgb8, float* out_radiance,
-                            pm_learned_graph** out) {
+                            int64_t batch, int32_t steps, int64_t pool_offset, int32_t overlap_training,
+                            uint8_t* out_rgb8, float* out_radiance, pm_learned_graph** out) {
     if (!ctx || !cam || !o || !lo || !out_rgb8 || !out) return PM_ERR_INVALID;
     *out = nullptr;
     if (int rc = learned_checks(ctx, lo)) return rc;
@@ -231,6 +256,7 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
     g->pool_n = pool_n;
     g->batch = std::min(batch, std::max<int64_t>(pool_n, 1));
     g->steps = steps;
+    g->overlap = overlap_training != 0;
     auto bail = [&](int rc) { free_graph(g); return rc; };
     auto need = [&](DevBuf& b, size_t bytes) { return ensure(b, std::max<size_t>(bytes, 16)); };
     cudaError_t e = cudaSuccess;
@@ -240,10 +266,21 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
         {&g->est_mlp, (size_t)g->cap * 12}, {&g->est_fb, (size_t)g->cap * 12}, {&g->est_g, (size_t)g->cap * 12},
         {&g->probe_pos, (size_t)g->nprobe * 16}, {&g->probe_nrm, (size_t)g->nprobe * 16},
         {&g->probe_req, (size_t)g->nprobe * 4}, {&g->probe_est, (size_t)g->nprobe * 12},
-        {&g->tile_flag, (size_t)g->ntiles}, {&g->counts, 32}, {&g->fb_list, (size_t)g->cap * 4}, {&g->state, 16}};
+        {&g->tile_flag, (size_t)g->ntiles}, {&g->counts, 32}, {&g->fb_list, (size_t)g->cap * 4}, {&g->state, 16},
+        {&g->w16_snap, (size_t)PM_CACHE_PARAMS * 2}};
     for (const auto& a : allocs)
         if ((e = need(*a.b, a.bytes)) != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph buffers"));
-    if ((e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking)) != cudaSuccess ||
+    // overlapped frames: the render's launches at the highest stream priority,
+    // the training at the lowest, so the training takes the SMs the render
+    // leaves idle (the graph keeps the priorities of the capturing streams)
+    int prio_low = 0, prio_high = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)) != cudaSuccess)
+        return bail(cuda_fail(ctx, e, "learned graph streams"));
+    if ((e = cudaStreamCreateWithPriority(&g->side, cudaStreamNonBlocking, g->overlap ? prio_low : 0)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&g->inf, cudaStreamNonBlocking, prio_high)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&g->hi, cudaStreamNonBlocking, prio_high)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g->inf_done, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g->hi_done, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->eye_done, cudaEventDisableTiming)) != cudaSuccess)
@@ -294,7 +331,7 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
     g->graph = graph;
     if (rc != PM_OK) return bail(rc);
     if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph: end capture"));
-    if ((e = cudaGraphInstantiate(&g->exec, g->graph, 0)) != cudaSuccess)
+    if ((e = cudaGraphInstantiate(&g->exec, g->graph, cudaGraphInstantiateFlagUseNodePriority)) != cudaSuccess)
         return bail(cuda_fail(ctx, e, "learned graph: instantiate"));
     g->generation = ctx->generation;
     g->buffers = read_set(ctx);

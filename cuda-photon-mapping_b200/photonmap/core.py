@@ -170,7 +170,7 @@ def library():
         "pm_cache_sample_points": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
         "pm_render_learned": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "pm_frame": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
-        "pm_learned_graph_create": ([vp, vp, vp, vp, vp, vp, vp, i64, i64, i32, i64, vp, vp, vp], C.c_int),
+        "pm_learned_graph_create": ([vp, vp, vp, vp, vp, vp, vp, i64, i64, i32, i64, i32, vp, vp, vp], C.c_int),
         "pm_learned_graph_run": ([vp, vp], C.c_int),
         "pm_learned_graph_offset": ([vp, vp], C.c_int),
         "pm_learned_graph_destroy": ([vp], None),
@@ -526,10 +526,12 @@ class Context:
 
     def learned_graph(self, cam: Camera, k_global, r_global, max_depth=4, pool=None, steps=4, batch=65536, offset=0,
                       tile=16, probes=16, max_rel_err=0.05, noise_z=0.0, radiance=False, out_rgb8=None,
-                      out_radiance=None):
+                      out_radiance=None, overlap_training=False):
         """The learned frame (`steps` Adam steps on the pool + render_learned) as one
         replayable CUDA graph (pm_learned_graph_create); `pool` a photonmap.learned.Pool
-        (or None with steps=0).  Returns a LearnedGraph: .run(stats=False) -> (rgb, radiance, stats)."""
+        (or None with steps=0).  overlap_training: the render reads the cache as the
+        previous frames trained it while this frame's training runs beside it.
+        Returns a LearnedGraph: .run(stats=False) -> (rgb, radiance, stats)."""
         torch = self.torch
         W, H = cam.width, cam.height
         rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
@@ -546,8 +548,9 @@ class Context:
             n = 0
         h = C.c_void_p()
         self._check(self.L.pm_learned_graph_create(self.h, C.byref(cam), C.byref(o), C.byref(lo), _ptr(pos), _ptr(nrm),
-                                                   _ptr(tgt), int(n), int(batch), int(steps), int(offset), _ptr(rgb),
-                                                   _ptr(rad), C.byref(h)), "pm_learned_graph_create")
+                                                   _ptr(tgt), int(n), int(batch), int(steps), int(offset),
+                                                   int(bool(overlap_training)), _ptr(rgb), _ptr(rad), C.byref(h)),
+                    "pm_learned_graph_create")
         return LearnedGraph(self, h, rgb, rad, (pos, nrm, tgt))
 
     def frame(self, seed, max_bounces, global_capacity, cam: Camera, k_global, r_global, max_depth=4,

@@ -122,8 +122,8 @@ class SplitFrame:
     # ---------------------------------------------------------------- frame
     def render(self, cam, k_global, r_global, max_depth=4, k_caustic=0, r_caustic=0.2, gather_to=0):
         """Step 4: this rank's band, then the frame on rank gather_to (None:
-        on every rank).  Returns (rgb8 (H * W * 3,) uint8, radiance (H * W, 3))
-        on the ranks that hold the frame, else (band rgb8, band radiance)."""
+        on every rank).  Returns host tensors: (rgb8 (H * W * 3,) uint8,
+        radiance (H * W, 3)) on the ranks that hold the frame, else the band's."""
         torch = self.torch
         W, H = cam.width, cam.height
         y0, y1 = band(H, self.rank, self.world)
@@ -134,5 +134,5 @@ class SplitFrame:
         rgbs = self._all_gather(rgb)
         rads = self._all_gather(rad)
         if gather_to is not None and self.rank != gather_to:
-            return rgb.reshape(-1), rad.reshape(-1, 3)
+            return rgb.reshape(-1).cpu(), rad.reshape(-1, 3).cpu()
         return (torch.cat([x.cpu() for x in rgbs]).reshape(-1), torch.cat([x.cpu() for x in rads]).reshape(-1, 3))

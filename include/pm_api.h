@@ -381,13 +381,20 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
  * one frame eagerly to load its kernels and puts the cache back as it was,
  * then captures on the context's stream (which must not be the legacy default
  * stream).  The graph reads the context's scene, photon map and cache: create
- * it again after pm_set_scene, pm_build_grid or pm_cache_init.  Each run is
- * one graph launch and one status check; out_stats optional. */
+ * it again after pm_set_scene, pm_build_grid or pm_cache_init (a run refuses
+ * with PM_ERR_INVALID otherwise).  Each run is one graph launch and one
+ * status check; out_stats optional.
+ * overlap_training = 0: the frame's training, then its render with the
+ * trained cache (pm_cache_train_steps + pm_render_learned).
+ * overlap_training = 1: the render reads the cache as the previous frames
+ * trained it (a copy taken at the frame's start) and the frame's training runs
+ * beside the whole render, for the frames that follow (pm_render_learned +
+ * pm_cache_train_steps, in that order). */
 typedef struct pm_learned_graph pm_learned_graph;
 int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts, const pm_learned_opts* lopts,
                             const float* pool_pos, const float* pool_nrm, const float* pool_target, int64_t pool_n,
-                            int64_t batch, int32_t steps, int64_t pool_offset, uint8_t* out_rgb8, float* out_radiance,
-                            pm_learned_graph** out);
+                            int64_t batch, int32_t steps, int64_t pool_offset, int32_t overlap_training,
+                            uint8_t* out_rgb8, float* out_radiance, pm_learned_graph** out);
 int pm_learned_graph_run(pm_learned_graph* graph, pm_learned_stats* out_stats);
 /* The pool offset the next frame's training starts at. */
 int pm_learned_graph_offset(pm_learned_graph* graph, int64_t* out_offset);

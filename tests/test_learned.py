@@ -213,7 +213,7 @@ def test_learned_graph_refuses_after_rebuild(setup):
         ctx.build_grid(photonmap.PM_MAP_GLOBAL)
         with pytest.raises(photonmap.PMError) as e:
             g.run()
-        assert e.value.code == photonmap.PM_ERR_INVALID
+        assert e.value.code == -1   # PM_ERR_INVALID
         assert ctx.status() == 0
     finally:
         g.close()
@@ -222,3 +222,39 @@ def test_learned_graph_refuses_after_rebuild(setup):
         g.run()
     finally:
         g.close()
+
+
+@pytest.mark.gpu
+def test_learned_graph_overlapped_training(setup):
+    """overlap_training: a frame renders with the cache as the previous frames
+    trained it while its own training runs beside it, i.e. render_learned, then
+    cache_train_steps: the same pool slices and weights, images as the eager
+    sequence's."""
+    from photonmap import learned
+    ctx, cam, w = setup
+    pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=1 << 16, seed=4)
+    S = learned.FRAME_SETTINGS
+    frames, steps, batch = 3, 2, 16384
+    ctx.cache_init(seed=5, lr=1e-3, out_scale=pool.scale)
+    w0 = ctx.cache_params()
+    g = ctx.learned_graph(cam, w["k"], w["radius"], w["max_depth"], pool=pool, steps=steps, batch=batch, offset=0,
+                          radiance=True, overlap_training=True, **S)
+    try:
+        rads = []
+        for _ in range(frames):
+            _, rad_g, _ = g.run()
+            rads.append(rad_g.clone())
+        w_g = ctx.cache_params()
+        off_g = g.offset()
+    finally:
+        g.close()
+    ctx.cache_init(seed=5, lr=1e-3, out_scale=pool.scale)   # the same start: weights, Adam state, step
+    assert np.array_equal(ctx.cache_params(), w0)
+    off = 0
+    for f in range(frames):
+        _, rad_e, _ = ctx.render_learned(cam, w["k"], w["radius"], w["max_depth"], **S)
+        a, b = rads[f].cpu().numpy(), rad_e.cpu().numpy()
+        assert np.abs(a - b).mean() <= 1e-3 * np.abs(b).mean(), f
+        _, off = learned.cache_fit(ctx, pool, steps, batch=batch, offset=off, want_loss=False)
+    assert off_g == off
+    np.testing.assert_allclose(w_g, ctx.cache_params(), rtol=0, atol=5e-5)
