@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache frame comparison")
     ap.add_argument("--no-rmse", action="store_true", help="skip the learned frame's RMSE against the FP64 reference")
+    ap.add_argument("--train-batch", type=int, default=LEARNED["batch"],
+                    help="samples per Adam step of the learned frame's 2^20 training samples")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batched workload")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--bvh", default="host_sah", choices=["host_sah", "device_lbvh"],
@@ -329,12 +331,13 @@ def batched_frames(args, rank):
             "speedup_vs_sequential": ms_seq / ms_wall, "launches_per_frame": info["launches_per_frame"],
             "graph": bool(info["graph"]), "autotuned": {"desired_per_cell": info["desired_per_cell"],
                                                         "gather_warps": info["gather_warps"],
+                                                        "gather_guess": info["gather_guess"],
                                                         "trace_refill": info["trace_refill"]},
             "underfilled_instances": info["underfilled"], "create_s": t_create,
             "stage_ms_eager": info["stage_ms"]}
 
 
-LEARNED = dict(train_per_frame=1 << 20, batch=1 << 17, warm_steps=3000, pool_samples=2_200_000,
+LEARNED = dict(train_per_frame=1 << 20, batch=1 << 18, warm_steps=3000, pool_samples=2_200_000,
                rmse_pixels=65_536, rmse_maps=10)
 
 
@@ -352,7 +355,7 @@ def learned_frames(ctx, sc, cs, cam, w, rgb, args, world):
     import torch.distributed as dist
     from photonmap import learned
     P = LEARNED
-    TRAIN_PER_FRAME, BATCH, WARM_STEPS = P["train_per_frame"], P["batch"], P["warm_steps"]
+    TRAIN_PER_FRAME, BATCH, WARM_STEPS = P["train_per_frame"], args.train_batch, P["warm_steps"]
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     ev[0].record()
     pool = learned.training_pool(ctx, cam, w["k"], w["radius"], n=P["pool_samples"], seed=1)

@@ -155,6 +155,7 @@ GatherGrid grid_of(MapState& m, MapState& est_src) {
     G.gx = m.dims[0]; G.gy = m.dims[1]; G.gz = m.dims[2];
     G.cell = m.cell;
     G.S = m.S;
+    G.guess = GATHER_GUESS;
     return G;
 }
 
@@ -470,10 +471,7 @@ int pm_cache_train_steps(pm_ctx* ctx, const float* pos, const float* nrm, const 
     cudaStream_t st = ctx->st;
     if (!out_loss && steps > 0) {
         if (!ctx->train_st) {
-            // the lowest priority: queued training fills the SMs the frame's launches leave idle
-            int prio_low = 0, prio_high = 0;
-            CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
-            CK(cudaStreamCreateWithPriority(&ctx->train_st, cudaStreamNonBlocking, prio_low));
+            CK(cudaStreamCreateWithFlags(&ctx->train_st, cudaStreamNonBlocking));
             CK(cudaEventCreateWithFlags(&ctx->train_fork, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&ctx->train_done, cudaEventDisableTiming));
         }

@@ -62,6 +62,7 @@ struct pm_batch {
     DevBuf req_a, req_b, req_c, req_counter, px_base, px_count, est_g, queues, rgb8, status;
     // choices
     int desired = 1000, gather_warps = 8, refill = 8;
+    float guess = GATHER_GUESS;   // the gather walk's first-ring guess (photons within it, in units of k)
     // graph
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
@@ -159,6 +160,7 @@ int plan_grids(pm_batch* b, int desired) {
         t.G.gx = q.gx; t.G.gy = q.gy; t.G.gz = q.gz;
         t.G.cell = q.cell;
         t.G.S = q.S;
+        t.G.guess = b->guess;
         t.r = b->inst[(size_t)i].radius;
         t.k = b->inst[(size_t)i].k;
         t.cls = gather_class(t.k);
@@ -296,7 +298,9 @@ int time_stage(pm_batch* b, int stage, int reps, float* ms) {
 
 // Times each stage's candidates on frame 0 and keeps the fastest: the
 // tracer's refill threshold; the grid sizing together with the gather block
-// shape (grid build + eye pass + gather of that grid).
+// shape (grid build + eye pass + gather of that grid); then the gather walk's
+// first-ring guess (no guess, or a bound expected to hold 1.5, 2 or 3 x k
+// photons) on the chosen grid.  No candidate changes an answer.
 int autotune(pm_batch* b) {
     if (int rc = launch_stages(b, -1, nullptr)) return rc;   // one full frame fills every stage's inputs
     BCK(cudaStreamSynchronize(b->st));
@@ -323,6 +327,18 @@ int autotune(pm_batch* b) {
         }
     }
     b->gather_warps = best_warps;
+    float best_guess = b->guess;
+    best = 1e30f;
+    for (float guess : {0.f, 1.5f, 2.f, 3.f}) {
+        b->guess = guess;
+        if (int rc = plan_grids(b, best_desired)) return rc;
+        float tg = 0.f, te = 0.f, tq = 0.f;
+        if (int rc = time_stage(b, 1, 1, &tg)) return rc;
+        if (int rc = time_stage(b, 2, 1, &te)) return rc;
+        if (int rc = time_stage(b, 3, 2, &tq)) return rc;
+        if (tq < best) { best = tq; best_guess = guess; }
+    }
+    b->guess = best_guess;
     return plan_grids(b, best_desired);
 }
 
@@ -554,6 +570,7 @@ int pm_batch_get_info(pm_batch* b, pm_batch_info* o) {
     o->request_capacity = b->req_cap;
     o->desired_per_cell = b->desired;
     o->gather_warps = b->gather_warps;
+    o->gather_guess = b->guess;
     o->trace_refill = b->refill;
     o->graph = b->exec ? 1 : 0;
     o->launches_per_frame = b->launches;

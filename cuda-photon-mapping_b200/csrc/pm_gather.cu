@@ -269,15 +269,16 @@ struct WarpWalk {
     // Density guess of the bound before the first ring's photons are scanned:
     // its N photons lie in the 3 x 3 x 3 block of sub-cells of edge sc around
     // the query; spread over a plane through the block (area 9 sc^2) they give
-    // about 2k photons within g = 3 sc sqrt(2k / (pi N)).  The guess only
+    // about G.guess x k photons within g = 3 sc sqrt(G.guess k / (pi N)).  The guess only
     // filters which candidates enter the store; when fewer than k lie within
     // it, the walk starts again with the bound r, so the answer is unchanged.
     __device__ void guess_bound(float sc) {
+        if (!(G.guess > 0.f)) return;
         uint32_t c = lane < qn ? U.qc[lane] : 0u;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
         if (c <= (uint32_t)k) return;   // too few photons in the block to gain anything
-        const float g = 3.f * sc * sqrtf((float)(2 * k) / (3.14159265f * (float)c));
+        const float g = 3.f * sc * sqrtf(G.guess * (float)k / (3.14159265f * (float)c));
         if (g < lim) {
             lim = g;
             lim2 = g * g * 1.000001f;

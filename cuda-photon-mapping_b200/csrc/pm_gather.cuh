@@ -14,7 +14,10 @@ struct GatherGrid {
     int gx, gy, gz;
     float cell;
     int S;                     // sub-cells per cell axis
+    float guess;               // the walk's first-ring bound is guessed to hold about guess x k photons
+                               // (GATHER_GUESS by default; 0: no guess).  Speed only: answers do not change
 };
+constexpr float GATHER_GUESS = 2.f;
 
 struct GatherQueries {
     int64_t n;

@@ -56,17 +56,21 @@ struct pm_learned_graph {
     uint64_t generation = 0, buffers = 0;
     // training runs on a second stream beside the eye pass and the probe
     // gathers (it needs neither; inference waits for it)
-    cudaStream_t side = nullptr, inf = nullptr, hi = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr, inf_done = nullptr, hi_done = nullptr;
+    cudaStream_t side = nullptr, inf = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr, inf_done = nullptr;
 };
 
 namespace {
 
-// the pool offset of the next batch: wrap to 0 where the batch would run past n
-__global__ void k_pool_wrap(int64_t* off, int64_t n, int64_t b) {
-    if (*off + b > n) *off = 0;
+// after a training step: the pool offset past the batch it read (which
+// started at 0 where the stored offset would have run past n: the wrap the
+// training kernel applies) and the Adam step number the step's update uses
+__global__ void k_pool_step(int64_t* off, int64_t n, int64_t b, int* step) {
+    int64_t o = *off;
+    if (o + b > n) o = 0;
+    *off = o + b;
+    *step += 1;
 }
-__global__ void k_pool_advance(int64_t* off, int64_t b) { *off += b; }
 
 int64_t* state_offset(pm_learned_graph* g) { return P<int64_t>(g->state); }
 int* state_step(pm_learned_graph* g) { return reinterpret_cast<int*>(P<int64_t>(g->state) + 1); }
@@ -113,33 +117,31 @@ int enqueue_frame(pm_learned_graph* g) {
     CK(cudaEventRecord(g->fork, main_st));
     CK(cudaStreamWaitEvent(g->side, g->fork, 0));
     cudaStream_t st = g->side;
-    for (int s = 0; s < g->steps; s++) {
-        k_pool_wrap<<<1, 1, 0, st>>>(state_offset(g), g->pool_n, g->batch);
-        CK(cudaGetLastError());
+    if (g->steps > 0) {
+        // the gradient starts at zero (each Adam step zeroes it after use); the
+        // loss is not read back by a replayed frame
         CK(cudaMemsetAsync(ctx->cache_grad.p, 0, (size_t)PM_CACHE_PARAMS * 4, st));
         CK(cudaMemsetAsync(ctx->cache_loss.p, 0, 4, st));
+    }
+    for (int s = 0; s < g->steps; s++) {
         MlpInputs in{};
         in.n = g->batch;
         in.pos3 = g->pool_pos;
         in.nrm3 = g->pool_nrm;
         in.base_dev = state_offset(g);
+        in.base_wrap = g->pool_n;
         CK(mlp_train(net, in, g->pool_target, nullptr, 2.f / (3.f * (float)g->batch), P<float>(ctx->cache_grad),
                      P<float>(ctx->cache_loss), status, ctx->sm_count, st));
+        k_pool_step<<<1, 1, 0, st>>>(state_offset(g), g->pool_n, g->batch, state_step(g));
+        CK(cudaGetLastError());
         CK(mlp_adam_dev(P<float>(ctx->cache_w32), P<__nv_bfloat16>(ctx->cache_w16), P<float>(ctx->cache_grad),
                         P<float>(ctx->cache_m), P<float>(ctx->cache_v), state_step(g), co.lr, co.beta1, co.beta2,
-                        co.eps, st));
-        k_pool_advance<<<1, 1, 0, st>>>(state_offset(g), g->batch);
-        CK(cudaGetLastError());
-        launches += 5;
+                        co.eps, st, false));
+        launches += 3;
     }
     // the learned render: eye pass, then the probe gathers here while the side
     // stream (after its training) answers every request with the cache
-    // (overlapped: the render on the high-priority stream, inference beside it)
     st = main_st;
-    if (g->overlap) {
-        CK(cudaStreamWaitEvent(g->hi, g->fork, 0));
-        st = g->hi;
-    }
     const DevScene S = dev_scene(ctx);
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     const Requests R = requests_of(g);
@@ -185,11 +187,7 @@ int enqueue_frame(pm_learned_graph* g) {
                      st));
     const float tone_t = (float)std::pow((double)0.6f, -1);
     CK(resolve(S, g->cd, R, P<float>(g->est_g), nullptr, tone_t, g->out_rgb8, g->out_radiance, st));
-    if (g->overlap) {   // back to the context's stream; the next frame's copy sees this frame's training
-        CK(cudaEventRecord(g->hi_done, st));
-        CK(cudaStreamWaitEvent(main_st, g->hi_done, 0));
-        CK(cudaStreamWaitEvent(main_st, g->join, 0));
-    }
+    if (g->overlap) CK(cudaStreamWaitEvent(st, g->join, 0));   // the next frame's copy sees this frame's training
     launches += 10;
     g->launches_per_frame = launches;
     return PM_OK;
@@ -202,10 +200,8 @@ void free_graph(pm_learned_graph* g) {
     if (g->join) cudaEventDestroy(g->join);
     if (g->eye_done) cudaEventDestroy(g->eye_done);
     if (g->inf_done) cudaEventDestroy(g->inf_done);
-    if (g->hi_done) cudaEventDestroy(g->hi_done);
     if (g->side) cudaStreamDestroy(g->side);
     if (g->inf) cudaStreamDestroy(g->inf);
-    if (g->hi) cudaStreamDestroy(g->hi);
     DevBuf* bufs[] = {&g->req_a, &g->req_b, &g->req_c, &g->counter, &g->px_base, &g->px_count, &g->est_mlp, &g->est_fb,
                       &g->est_g, &g->probe_pos, &g->probe_nrm, &g->probe_req, &g->probe_est, &g->tile_flag,
                       &g->counts, &g->fb_list, &g->state, &g->eye_order, &g->w16_snap};
@@ -270,17 +266,9 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
         {&g->w16_snap, (size_t)PM_CACHE_PARAMS * 2}};
     for (const auto& a : allocs)
         if ((e = need(*a.b, a.bytes)) != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph buffers"));
-    // overlapped frames: the render's launches at the highest stream priority,
-    // the training at the lowest, so the training takes the SMs the render
-    // leaves idle (the graph keeps the priorities of the capturing streams)
-    int prio_low = 0, prio_high = 0;
-    if ((e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)) != cudaSuccess)
-        return bail(cuda_fail(ctx, e, "learned graph streams"));
-    if ((e = cudaStreamCreateWithPriority(&g->side, cudaStreamNonBlocking, g->overlap ? prio_low : 0)) != cudaSuccess ||
-        (e = cudaStreamCreateWithPriority(&g->inf, cudaStreamNonBlocking, prio_high)) != cudaSuccess ||
-        (e = cudaStreamCreateWithPriority(&g->hi, cudaStreamNonBlocking, prio_high)) != cudaSuccess ||
+    if ((e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&g->inf, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->inf_done, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&g->hi_done, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->eye_done, cudaEventDisableTiming)) != cudaSuccess)
@@ -331,7 +319,7 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
     g->graph = graph;
     if (rc != PM_OK) return bail(rc);
     if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph: end capture"));
-    if ((e = cudaGraphInstantiate(&g->exec, g->graph, cudaGraphInstantiateFlagUseNodePriority)) != cudaSuccess)
+    if ((e = cudaGraphInstantiate(&g->exec, g->graph, 0)) != cudaSuccess)
         return bail(cuda_fail(ctx, e, "learned graph: instantiate"));
     g->generation = ctx->generation;
     g->buffers = read_set(ctx);

@@ -359,7 +359,8 @@ k_mlp_train(MlpNet net, MlpInputs in, const float* __restrict__ target, const fl
     bool ok = true;
     float loss = 0.f;
     const int64_t tiles = (in.n + TILE - 1) / TILE;
-    const int64_t base = in.base_dev ? *in.base_dev : 0;
+    int64_t base = in.base_dev ? *in.base_dev : 0;
+    if (in.base_wrap > 0 && base + in.n > in.base_wrap) base = 0;
     const int64_t stride = (int64_t)gridDim.x * TRAIN_GROUPS;
     for (int64_t tile = (int64_t)blockIdx.x * TRAIN_GROUPS + g; tile < tiles && ok; tile += stride) {
         const int64_t i = tile * TILE + row;
@@ -634,8 +635,8 @@ cudaError_t mlp_adam(float* w32, __nv_bfloat16* w16, float* grad, float* m, floa
 }
 
 cudaError_t mlp_adam_dev(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int* step_dev, float lr,
-                         float beta1, float beta2, float eps, cudaStream_t st) {
-    k_step_inc<<<1, 1, 0, st>>>(step_dev);
+                         float beta1, float beta2, float eps, cudaStream_t st, bool increment) {
+    if (increment) k_step_inc<<<1, 1, 0, st>>>(step_dev);
     k_adam_dev<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(w32, w16, grad, m, v, lr, beta1, beta2, eps, step_dev);
     return cudaGetLastError();
 }

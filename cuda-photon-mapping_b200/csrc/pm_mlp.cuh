@@ -44,6 +44,7 @@ struct MlpInputs {
     // optional, for launches whose sizes live on the device (graph replay):
     const unsigned long long* n_dev;   // inference: min(*n_dev, n) samples (n a capacity)
     const int64_t* base_dev;           // training on pos3 / nrm3: sample i is array entry *base_dev + i
+    int64_t base_wrap;                 // > 0: a base with base + n > base_wrap reads from entry 0 instead
 };
 
 // One training pass over n samples: accumulates d(loss)/d(weights) into grad
@@ -63,10 +64,11 @@ cudaError_t mlp_infer(const MlpNet& net, const MlpInputs& in, float* out, unsign
 cudaError_t mlp_adam(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int step, float lr,
                      float beta1, float beta2, float eps, cudaStream_t st);
 
-// The same with the step number on the device: *step_dev += 1, then the step
-// uses it for the bias corrections (a replayed graph advances it itself).
+// The same with the step number on the device: *step_dev += 1 (unless
+// increment is false: the caller advanced it), then the step uses it for the
+// bias corrections (a replayed graph advances it itself).
 cudaError_t mlp_adam_dev(float* w32, __nv_bfloat16* w16, float* grad, float* m, float* v, int* step_dev, float lr,
-                         float beta1, float beta2, float eps, cudaStream_t st);
+                         float beta1, float beta2, float eps, cudaStream_t st, bool increment = true);
 
 // BF16 copies of FP32 weights.
 cudaError_t mlp_to_bf16(const float* w32, __nv_bfloat16* w16, cudaStream_t st);

@@ -29,6 +29,7 @@ struct TraceBatch {
     unsigned long long* work = nullptr;   // when set: the work-counting launch adds rays, node visits, triangle tests
 };
 
+
 struct PhotonList {
     float* pos;               // 3 floats per photon
     float* dir;

@@ -153,6 +153,7 @@ int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]);
 #define PM_BVH_HOST_SAH 0     /* binned SAH on the host (default): the faster tree to trace */
 #define PM_BVH_DEVICE_LBVH 1  /* linear BVH over Morton codes, built on the device in ~1 ms */
 int pm_set_bvh_builder(pm_ctx* ctx, int builder);
+
 /* The current scene's BVH: its builder, interior nodes, build time in ms. */
 int pm_bvh_info(pm_ctx* ctx, int32_t* out_builder, int64_t* out_nodes, float* out_build_ms);
 
@@ -466,6 +467,7 @@ typedef struct pm_batch_info {
     int64_t requests_last_frame;
     int32_t underfilled;          /* instances whose last frame produced fewer photons than their capacity */
     float stage_ms[5];            /* trace, grid, eye, gather, resolve of one eager frame timed at creation */
+    float gather_guess;           /* chosen first-ring guess of the gather walk (photons in units of k; 0: none) */
 } pm_batch_info;
 
 /* Creation traces each instance once (calibration), builds the grids, runs

@@ -79,6 +79,7 @@ def test_batch_autotuned(gpu):
     info = b.info()
     assert info["desired_per_cell"] in (250, 500, 1000, 2000)
     assert info["gather_warps"] in (4, 8) and info["trace_refill"] in (4, 8, 16)
+    assert info["gather_guess"] in (0.0, 1.5, 2.0, 3.0)
     b.frame(0)
     for i, inst in enumerate(insts):
         a = b.image(i).to(torch.int32)
