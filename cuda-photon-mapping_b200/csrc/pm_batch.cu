@@ -72,6 +72,7 @@ struct pm_batch {
     uint64_t seeded_frame = 0;
     float ms_last = 0.f;
     int64_t photons_last = 0, requests_last = 0;
+    std::vector<int64_t> stored_last;   // photons each instance stored in the last frame
     int underfilled = 0;
     float stage_ms[5] = {0, 0, 0, 0, 0};
 };
@@ -542,9 +543,11 @@ int pm_batch_frame(pm_batch* b, uint64_t frame) {
     b->ms_last = elapsed(b->ev0, b->ev1);
     b->photons_last = 0;
     b->underfilled = 0;
+    b->stored_last.assign((size_t)b->n, 0);
     for (int i = 0; i < b->n; i++) {
         const int64_t cap = b->inst[(size_t)i].photons;
-        b->photons_last += std::min(cap, tot[(size_t)i]);
+        b->stored_last[(size_t)i] = std::min(cap, tot[(size_t)i]);
+        b->photons_last += b->stored_last[(size_t)i];
         if (tot[(size_t)i] < cap) b->underfilled++;
     }
     b->requests_last = (int64_t)(nreq_cls[0] + nreq_cls[1]);
@@ -556,6 +559,17 @@ int pm_batch_image(pm_batch* b, int32_t i, const uint8_t** out, int32_t* w, int3
     *out = P<uint8_t>(b->rgb8) + 3 * b->px_off[(size_t)i];
     if (w) *w = b->inst[(size_t)i].camera.width;
     if (h) *h = b->inst[(size_t)i].camera.height;
+    return PM_OK;
+}
+
+int pm_batch_photons(pm_batch* b, int32_t i, const float** pos, const float** power, const float** dir,
+                     int64_t* count) {
+    if (!b || i < 0 || i >= b->n || b->stored_last.size() != (size_t)b->n) return PM_ERR_INVALID;
+    const int64_t o = 3 * b->ph_off[(size_t)i];
+    if (pos) *pos = P<float>(b->pos) + o;
+    if (power) *power = P<float>(b->pow) + o;
+    if (dir) *dir = P<float>(b->dir) + o;
+    if (count) *count = b->stored_last[(size_t)i];
     return PM_OK;
 }
 

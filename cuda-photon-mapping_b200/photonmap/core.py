@@ -182,6 +182,8 @@ def library():
         "pm_batch_frame": ([vp, C.c_uint64], C.c_int),
         "pm_batch_image": ([vp, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
         "pm_batch_get_info": ([vp, C.POINTER(_BatchInfo)], C.c_int),
+        "pm_batch_photons": ([vp, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                              C.POINTER(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -736,6 +738,17 @@ class Batch:
         self._check(self.L.pm_batch_image(self.h, int(i), C.byref(p), C.byref(w), C.byref(h)), "pm_batch_image")
         return self.torch.as_tensor(_DeviceArray(p.value, (h.value, w.value, 3), self.torch.uint8),
                                     device=self.device).clone()
+
+    def photons(self, i):
+        """Copies of the photon list instance i stored in the last frame (canonical
+        order): dict of (count, 3) float32 CUDA tensors pos, power, dir."""
+        ptr = [C.c_void_p() for _ in range(3)]
+        n = C.c_int64()
+        self._check(self.L.pm_batch_photons(self.h, int(i), *(C.byref(x) for x in ptr), C.byref(n)),
+                    "pm_batch_photons")
+        return {k: self.torch.as_tensor(_DeviceArray(x.value, (n.value, 3), self.torch.float32),
+                                        device=self.device).clone()
+                for k, x in zip(("pos", "power", "dir"), ptr)}
 
     def info(self):
         o = _BatchInfo()

@@ -481,6 +481,14 @@ int pm_batch_frame(pm_batch* b, uint64_t frame);
 /* Device pointer to instance i's last image (uchar3, width x height, rows as pm_render). */
 int pm_batch_image(pm_batch* b, int32_t i, const uint8_t** out_rgb8, int32_t* width, int32_t* height);
 int pm_batch_get_info(pm_batch* b, pm_batch_info* out);
+/* The photon list instance i stored in the last pm_batch_frame (its global
+ * map before the grid's cell sort, canonical order: path, then bounce), as
+ * device pointers into the batch (3 floats per photon each), valid until the
+ * next pm_batch_frame or pm_batch_destroy; *count photons.  The same list as
+ * pm_trace_photons of the instance with seed + frame.  PM_ERR_INVALID before
+ * the first frame. */
+int pm_batch_photons(pm_batch* b, int32_t i, const float** pos, const float** power, const float** dir,
+                     int64_t* count);
 
 /* Gather requests (eye-path hits that query the global map) of the last
  * pm_render call: the number of kNN queries its gather stage answered. */

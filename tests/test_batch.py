@@ -93,8 +93,9 @@ def test_batch_autotuned(gpu):
 @pytest.mark.gpu
 def test_batch_instances_against_the_oracle(gpu, orc):
     """Two batch instances (jittered light, random sphere radii) against the
-    oracle's own photon pass, grid and render of them: 8-bit pixels at most
-    one level apart (the estimates differ only by CUDA's expf / powf)."""
+    oracle's own photon pass, grid and render of them: the photon lists bit
+    for bit, 8-bit pixels at most one level apart (the estimates differ only
+    by CUDA's expf / powf)."""
     import numpy as np
     import photonmap
     from photonmap import scenes
@@ -104,6 +105,10 @@ def test_batch_instances_against_the_oracle(gpu, orc):
     for i, inst in enumerate(insts):
         s = orc.scene(inst["scene"])
         tr = s.trace_photons(inst["seed"] + 3, inst["max_bounces"], inst["photons"])
+        ph = {k: v.cpu().numpy() for k, v in b.photons(i).items()}
+        assert ph["pos"].shape[0] == inst["photons"] == tr["g_pos"].shape[0]
+        for k, o in (("pos", "g_pos"), ("power", "g_pow"), ("dir", "g_dir")):
+            assert np.array_equal(ph[k].view(np.uint32), np.ascontiguousarray(tr[o], np.float32).view(np.uint32)), (i, k)
         g = orc.grid_build(tr["g_pos"], tr["g_pow"], tr["g_dir"], s.aabb())
         c = inst["camera"]
         cs = scenes.default_camera(c.width, c.height)
