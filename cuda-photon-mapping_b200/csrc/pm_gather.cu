@@ -269,12 +269,16 @@ struct WarpWalk {
     // Density guess of the bound before the first ring's photons are scanned:
     // its N photons lie in the 3 x 3 x 3 block of sub-cells of edge sc around
     // the query; spread over a plane through the block (area 9 sc^2) they give
-    // about G.guess x k photons within g = 3 sc sqrt(G.guess k / (pi N)).  The guess only
-    // filters which candidates enter the store; when fewer than k lie within
-    // it, the walk starts again with the bound r, so the answer is unchanged.
-    __device__ void guess_bound(float sc) {
+    // about G.guess x k photons within g = 3 sc sqrt(G.guess k / (pi N)).  The
+    // guess filters which candidates enter the store, and a ring-1 sub-cell
+    // whose padded box lies farther than g is not scanned at all; when fewer
+    // than k photons lie within g, the walk starts again with the bound r, so
+    // the answer is unchanged.  One lane per ring-1 sub-cell (all 27 in one
+    // round): (a, b) its photon range (empty when it is out of reach), gap2 its
+    // squared box distance.
+    __device__ void guess_ring1(uint32_t a, uint32_t& b, float gap2, float sc, float m) {
         if (!(G.guess > 0.f)) return;
-        uint32_t c = lane < qn ? U.qc[lane] : 0u;
+        uint32_t c = b - a;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
         if (c <= (uint32_t)k) return;   // too few photons in the block to gain anything
@@ -283,6 +287,8 @@ struct WarpWalk {
             lim = g;
             lim2 = g * g * 1.000001f;
             guessed = true;
+            const float L = g * m;
+            if (gap2 > L * L) b = a;
         }
     }
 
@@ -520,7 +526,6 @@ struct WarpWalk {
     // together.  After each shell the distance histogram tightens the bound; a
     // shell whose nearest possible point is farther than the bound ends the walk.
     __device__ void walk(int X0, int Y0, int Z0, int lx, int ly, int lz, int hx, int hy, int hz, bool use_guess) {
-        constexpr int NM = 1;
         const int S = G.S, sh = __ffs(S) - 1;
         const float sc = G.cell / (float)S, pad = G.cell * 1e-4f;
         const float m = 1.f + 1e-5f;
@@ -552,33 +557,30 @@ struct WarpWalk {
             const int total = shell + (R == 1 ? 1 : 0);   // ring 1 also carries the query's own sub-cell
             const float inv_side = 1.0f / (float)side, inv_per = 1.0f / (float)(4 * (side - 1));
             const float L = lim * m;
-            for (int base = 0; base < total; base += 32 * NM) {
-                uint32_t a[NM], b[NM];
-#pragma unroll
-                for (int u = 0; u < NM; u++) {
-                    const int t = base + 32 * u + lane;
-                    a[u] = 0u; b[u] = 0u;
-                    if (t < total) {
-                        int dx = 0, dy = 0, dz = 0;
-                        if (t < shell) shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
-                        const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
-                        if (X >= lx && X <= hx && Y >= ly && Y <= hy && Z >= lz && Z <= hz) {
-                            float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
-                            float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
-                            float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
-                            if (ax * ax + ay * ay + az * az <= L * L) {
-                                const uint32_t key = key_of(X, Y, Z);
-                                a[u] = __ldg(G.key_starts + key);
-                                b[u] = __ldg(G.key_starts + key + 1);
-                            }
+            for (int base = 0; base < total; base += 32) {
+                const int t = base + lane;
+                uint32_t a = 0u, b = 0u;
+                float gap2 = 0.f;
+                if (t < total) {
+                    int dx = 0, dy = 0, dz = 0;
+                    if (t < shell) shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
+                    const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
+                    if (X >= lx && X <= hx && Y >= ly && Y <= hy && Z >= lz && Z <= hz) {
+                        float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
+                        float ay = axis_gap(q.y, G.mn[1] + Y * sc - pad, G.mn[1] + (Y + 1) * sc + pad, Y == 0, Y == GY);
+                        float az = axis_gap(q.z, G.mn[2] + Z * sc - pad, G.mn[2] + (Z + 1) * sc + pad, Z == 0, Z == GZ);
+                        gap2 = ax * ax + ay * ay + az * az;
+                        if (gap2 <= L * L) {
+                            const uint32_t key = key_of(X, Y, Z);
+                            a = __ldg(G.key_starts + key);
+                            b = __ldg(G.key_starts + key + 1);
                         }
                     }
                 }
-#pragma unroll
-                for (int u = 0; u < NM; u++)
-                    if (base + 32 * u < total) enqueue(b[u] > a[u], a[u], b[u] - a[u]);
+                // ring 1 (27 sub-cells) is this one round
+                if (R == 1 && use_guess) guess_ring1(a, b, gap2, sc, m);
+                enqueue(b > a, a, b - a);
             }
-            if (R == 1 && use_guess) guess_bound(sc);   // ring 1 (27 sub-cells) is all still queued
             flush();
             if (R == 1 && guessed && n < k) {
                 failed = true;
