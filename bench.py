@@ -332,6 +332,7 @@ def batched_frames(args, rank):
             "graph": bool(info["graph"]), "autotuned": {"desired_per_cell": info["desired_per_cell"],
                                                         "gather_warps": info["gather_warps"],
                                                         "gather_guess": info["gather_guess"],
+                                                        "subcell_khint": info["subcell_khint"],
                                                         "trace_refill": info["trace_refill"]},
             "underfilled_instances": info["underfilled"], "create_s": t_create,
             "stage_ms_eager": info["stage_ms"]}

@@ -63,6 +63,8 @@ struct pm_batch {
     // choices
     int desired = 1000, gather_warps = 8, refill = 8;
     float guess = GATHER_GUESS;   // the gather walk's first-ring guess (photons within it, in units of k)
+    float khint = 0.f;            // sub-cell split: 0 = the library default (sized for k 64), else the
+                                  // automatic rule for khint x the instance's k
     // graph
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
@@ -115,7 +117,8 @@ int plan_grids(pm_batch* b, int desired) {
     std::vector<int64_t> keys((size_t)b->n), cells((size_t)b->n);
     for (int i = 0; i < b->n; i++) {
         pm_ctx* c = b->ctx[(size_t)i];
-        pm_grid_opts go = {desired, 5, 5, 0, 0};
+        const int kh = b->khint > 0.f ? std::max(1, (int)std::lround(b->khint * (float)b->inst[(size_t)i].k)) : 0;
+        pm_grid_opts go = {desired, 5, 5, 0, kh};
         if (int rc = pm_build_grid(c, PM_MAP_GLOBAL, &go, nullptr)) return bfail(b, rc, pm_last_error(c));
         const MapState& m = c->maps[PM_MAP_GLOBAL];
         GridInstDev& t = g[(size_t)i];
@@ -299,9 +302,11 @@ int time_stage(pm_batch* b, int stage, int reps, float* ms) {
 
 // Times each stage's candidates on frame 0 and keeps the fastest: the
 // tracer's refill threshold; the grid sizing together with the gather block
-// shape (grid build + eye pass + gather of that grid); then the gather walk's
-// first-ring guess (no guess, or a bound expected to hold 1.5, 2 or 3 x k
-// photons) on the chosen grid.  No candidate changes an answer.
+// shape (grid build + eye pass + gather of that grid); the sub-cell split (the
+// library default, or the automatic rule for 1/4, 1 or 4 x each instance's
+// own k: one power of two finer, the rule's, one coarser); then the gather
+// walk's first-ring guess (no guess, or a bound expected to hold 1.5, 2 or
+// 3 x k photons) on the chosen grid.  No candidate changes an answer.
 int autotune(pm_batch* b) {
     if (int rc = launch_stages(b, -1, nullptr)) return rc;   // one full frame fills every stage's inputs
     BCK(cudaStreamSynchronize(b->st));
@@ -316,7 +321,7 @@ int autotune(pm_batch* b) {
     if (int rc = launch_stages(b, 0, nullptr)) return rc;   // frame 0's photons for the grid candidates
     best = 1e30f;
     int best_desired = b->desired, best_warps = b->gather_warps;
-    for (int desired : {250, 500, 1000, 2000}) {
+    for (int desired : {125, 250, 500, 1000, 2000}) {
         if (int rc = plan_grids(b, desired)) return rc;
         for (int warps : {4, 8}) {
             b->gather_warps = warps;
@@ -328,6 +333,18 @@ int autotune(pm_batch* b) {
         }
     }
     b->gather_warps = best_warps;
+    float best_khint = b->khint;
+    best = 1e30f;
+    for (float kh : {0.f, 0.25f, 1.f, 4.f}) {
+        b->khint = kh;
+        if (int rc = plan_grids(b, best_desired)) return rc;
+        float tg = 0.f, te = 0.f, tq = 0.f;
+        if (int rc = time_stage(b, 1, 1, &tg)) return rc;
+        if (int rc = time_stage(b, 2, 1, &te)) return rc;
+        if (int rc = time_stage(b, 3, 2, &tq)) return rc;
+        if (tg + tq < best) { best = tg + tq; best_khint = kh; }
+    }
+    b->khint = best_khint;
     float best_guess = b->guess;
     best = 1e30f;
     for (float guess : {0.f, 1.5f, 2.f, 3.f}) {
@@ -585,6 +602,7 @@ int pm_batch_get_info(pm_batch* b, pm_batch_info* o) {
     o->desired_per_cell = b->desired;
     o->gather_warps = b->gather_warps;
     o->gather_guess = b->guess;
+    o->subcell_khint = b->khint;
     o->trace_refill = b->refill;
     o->graph = b->exec ? 1 : 0;
     o->launches_per_frame = b->launches;

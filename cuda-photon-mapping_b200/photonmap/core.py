@@ -88,7 +88,7 @@ class _BatchInfo(C.Structure):
                 ("gather_warps", C.c_int32), ("trace_refill", C.c_int32), ("graph", C.c_int32),
                 ("launches_per_frame", C.c_int32), ("ms_last_frame", C.c_float), ("photons_last_frame", C.c_int64),
                 ("requests_last_frame", C.c_int64), ("underfilled", C.c_int32), ("stage_ms", C.c_float * 5),
-                ("gather_guess", C.c_float)]
+                ("gather_guess", C.c_float), ("subcell_khint", C.c_float)]
 
 
 class _LearnedOpts(C.Structure):

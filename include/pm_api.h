@@ -468,6 +468,8 @@ typedef struct pm_batch_info {
     int32_t underfilled;          /* instances whose last frame produced fewer photons than their capacity */
     float stage_ms[5];            /* trace, grid, eye, gather, resolve of one eager frame timed at creation */
     float gather_guess;           /* chosen first-ring guess of the gather walk (photons in units of k; 0: none) */
+    float subcell_khint;          /* chosen sub-cell split: 0 = pm_grid_opts' default, else the automatic
+                                     split for subcell_khint x each instance's k */
 } pm_batch_info;
 
 /* Creation traces each instance once (calibration), builds the grids, runs

@@ -77,7 +77,8 @@ def test_batch_autotuned(gpu):
     insts = _instances(4, seed=3, photons_range=(20_000, 100_000), res_range=(64, 128))
     b = photonmap.Batch(insts, autotune=True, use_graph=True)
     info = b.info()
-    assert info["desired_per_cell"] in (250, 500, 1000, 2000)
+    assert info["desired_per_cell"] in (125, 250, 500, 1000, 2000)
+    assert info["subcell_khint"] in (0.0, 0.25, 1.0, 4.0)
     assert info["gather_warps"] in (4, 8) and info["trace_refill"] in (4, 8, 16)
     assert info["gather_guess"] in (0.0, 1.5, 2.0, 3.0)
     b.frame(0)
