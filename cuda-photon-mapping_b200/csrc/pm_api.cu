@@ -791,6 +791,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     // (ensure releases a buffer before growing it) leaves no map in use
     G.built = C.built = false;
     G.n = C.n = 0;
+    G.uniform_pow = C.uniform_pow = false;
     ENSURE(G.pos, std::max<int64_t>(cg, 1) * 12); ENSURE(G.dir, std::max<int64_t>(cg, 1) * 12); ENSURE(G.pow, std::max<int64_t>(cg, 1) * 12);
     ENSURE(C.pos, std::max<int64_t>(cc, 1) * 12); ENSURE(C.dir, std::max<int64_t>(cc, 1) * 12); ENSURE(C.pow, std::max<int64_t>(cc, 1) * 12);
     G.built = C.built = false;
@@ -836,6 +837,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         uint32_t tot[2] = {0, 0};
         CK(cudaMemcpyAsync(tot, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
+        if (cc == 0) tot[1] = 0;   // no caustic map: its total was not scanned
         k_trace_ms += elapsed(ctx->ev[12], ctx->ev[13]);
         got_g += tot[0];
         got_c += tot[1];
@@ -857,6 +859,10 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     ctx->stage_ms[5] = k_trace_ms;
     G.n = fg;
     C.n = fc;
+    for (MapState* m : {&G, &C}) {   // every photon of a traced map has power intensity / global capacity
+        m->uniform_pow = true;
+        for (int a = 0; a < 3; a++) m->pow_value[a] = power[a];
+    }
     if (out_paths) *out_paths = p0;
     int rc = check_status(ctx, "trace");
     if (rc) return rc;
@@ -919,6 +925,7 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
     MapState& m = ctx->maps[map];
     m.n = 0;            // empty until the new list is in place
     m.built = false;
+    m.uniform_pow = false;
     ENSURE(m.pos, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.dir, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.pow, std::max<int64_t>(n, 1) * 12);
@@ -933,8 +940,21 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
     return PM_OK;
 }
 
-int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb) {
-    if (!ctx) return PM_ERR_INVALID;
+namespace {
+
+// A grid build issued on the context stream (grid_issue) and not yet
+// recorded in its map (grid_commit).
+struct GridIssued {
+    GridPlan plan;
+    int S = 1;
+    float box[6] = {0, 0, 0, 0, 0, 0};
+};
+
+// Every launch of a grid build on the context stream (the counting pass's
+// read of the fullest cell, which decides the re-grid and the sub-cell split,
+// is the one host wait); the map stays unbuilt until grid_commit.  The global
+// map's build is timed into ev[2] .. ev[3].
+int grid_issue(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb, GridIssued& gi) {
     ctx->generation++;
     if (int rc = valid_map(ctx, map)) return rc;
     pm_grid_opts d = {1000, 5, 5, 0, 0};
@@ -969,6 +989,8 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     ENSURE(m.counts2, (size_t)((int64_t)d2[0] * d2[1] * d2[2]) * 4);
     GridBuffers B;
     B.pos = P<float>(m.pos); B.dir = P<float>(m.dir); B.pow = P<float>(m.pow); B.n = n;
+    B.uniform_pow = m.uniform_pow;
+    for (int a = 0; a < 3; a++) B.pow_value[a] = m.pow_value[a];
     B.cell_starts = P<uint32_t>(m.starts); B.cell_sizes = P<uint32_t>(m.sizes);
     B.gpos = P<float4>(m.gpos); B.gdir = P<float>(m.gdir); B.gpow = P<float>(m.gpow);
     B.cid = P<uint32_t>(m.cid);
@@ -977,10 +999,10 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     B.small = P<uint32_t>(m.small);
     B.counts2 = P<uint32_t>(m.counts2);
     B.status = P<unsigned>(ctx->status);
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
-    GridPlan plan;
+    if (map == PM_MAP_GLOBAL) CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    GridPlan& plan = gi.plan;
     CK(grid_count(B, box, o->desired_per_cell, o->regrid_mult, o->regrid_div, &plan, ctx->st));
-    const int S = o->sub_div > 0 ? o->sub_div : grid_auto_subdiv(plan.max_count, o->k_hint > 0 ? o->k_hint : 64);
+    const int S = gi.S = o->sub_div > 0 ? o->sub_div : grid_auto_subdiv(plan.max_count, o->k_hint > 0 ? o->k_hint : 64);
     const int64_t keys = plan.cells * S * S * S;
     if (keys > ((int64_t)1 << 31)) return fail(ctx, PM_ERR_INVALID, "grid: too many sub-cells");
     size_t hist_elems = 0, scan_ws = 0;
@@ -995,17 +1017,31 @@ int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb
     B.key_starts = P<uint32_t>(m.key_starts);
     CK(grid_sort(B, box, plan, S, ctx->st));
     ctx->launches += plan.launches;
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
-    CK(cudaEventSynchronize(ctx->ev[3]));
-    if (map == PM_MAP_GLOBAL) ctx->stage_ms[1] = elapsed(ctx->ev[2], ctx->ev[3]);
-    for (int a = 0; a < 3; a++) m.dims[a] = plan.dims[a];
-    m.cell = plan.cell;
-    m.cells = plan.cells;
-    m.S = S;
-    std::memcpy(m.aabb, box, 24);
-    int rc = check_status(ctx, "grid build");
-    if (rc) return rc;
+    if (map == PM_MAP_GLOBAL) CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    std::memcpy(gi.box, box, 24);
+    return PM_OK;
+}
+
+void grid_commit(pm_ctx* ctx, int map, const GridIssued& gi) {
+    MapState& m = ctx->maps[map];
+    for (int a = 0; a < 3; a++) m.dims[a] = gi.plan.dims[a];
+    m.cell = gi.plan.cell;
+    m.cells = gi.plan.cells;
+    m.S = gi.S;
+    std::memcpy(m.aabb, gi.box, 24);
     m.built = true;
+}
+
+}  // namespace
+
+int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb) {
+    if (!ctx) return PM_ERR_INVALID;
+    GridIssued gi;
+    if (int rc = grid_issue(ctx, map, o, aabb, gi)) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    if (map == PM_MAP_GLOBAL) ctx->stage_ms[1] = elapsed(ctx->ev[2], ctx->ev[3]);
+    if (int rc = check_status(ctx, "grid build")) return rc;
+    grid_commit(ctx, map, gi);
     return PM_OK;
 }
 
@@ -1160,6 +1196,8 @@ struct FrameSetup {
     DevScene S;
     int64_t npx = 0, cap = 0, nreq = 0;
     bool caustic = false;
+    bool ordered = false;              // the requests' Morton order is already issued (pm_frame)
+    const uint32_t* order = nullptr;
 };
 
 
@@ -1225,10 +1263,11 @@ int render_eye_launch(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
 }
 
 // the request count of the eye pass (ordered on ctx->st)
-int render_eye_count(pm_ctx* ctx, FrameSetup& F) {
+int render_eye_count(pm_ctx* ctx, FrameSetup& F, cudaStream_t st = nullptr) {
+    if (!st) st = ctx->st;
     unsigned long long nreq = 0;
-    CK(cudaMemcpyAsync(&nreq, F.R.counter, 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpyAsync(&nreq, F.R.counter, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     F.nreq = (int64_t)std::min<unsigned long long>(nreq, (unsigned long long)F.cap);
     ctx->last_requests = F.nreq;
     ctx->last_pixels = F.npx;
@@ -1271,30 +1310,36 @@ int render_finish(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* 
 namespace {
 
 // global gather, caustic gather, resolve and the status check of a frame whose requests are counted
+// The gather visits the requests in Morton order of their hit points: 30-bit
+// keys in the scene box, sorted by the library's stable radix sort on stream st.
+int request_order(pm_ctx* ctx, FrameSetup& F, cudaStream_t st) {
+    F.ordered = true;
+    F.order = nullptr;
+    if (F.nreq <= 0) return PM_OK;
+    const int64_t n = F.nreq;
+    ENSURE(ctx->rq_keys, (size_t)n * 4);
+    ENSURE(ctx->rq_k0, (size_t)n * 4); ENSURE(ctx->rq_k1, (size_t)n * 4);
+    ENSURE(ctx->rq_v0, (size_t)n * 4); ENSURE(ctx->rq_v1, (size_t)n * 4);
+    ENSURE(ctx->rq_hist, radix_hist_elems(n) * 4);
+    ENSURE(ctx->rq_ws, scan_workspace_bytes((int64_t)radix_hist_elems(n)));
+    CK(request_keys(F.R.a, n, ctx->aabb, P<uint32_t>(ctx->rq_keys), st));
+    RadixBuffers RB{{P<uint32_t>(ctx->rq_k0), P<uint32_t>(ctx->rq_k1)}, {P<uint32_t>(ctx->rq_v0), P<uint32_t>(ctx->rq_v1)},
+                    P<uint32_t>(ctx->rq_hist), ctx->rq_ws.p, P<unsigned>(ctx->status)};
+    int launches = 0;
+    CK(radix_sort_u32(RB, P<uint32_t>(ctx->rq_keys), nullptr, n, 30, false, nullptr, &F.order, &launches, st));
+    ctx->launches += launches + 1;
+    return PM_OK;
+}
+
 int render_rest(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* out_rgb8, float* out_radiance) {
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     GatherQueries Q{};
     Q.n = F.nreq; Q.pos4 = F.R.a; Q.nrm4 = F.R.b; Q.flag_mask = 1u;
-    // the gather visits the requests in Morton order of their hit points
-    const uint32_t* order = nullptr;
-    if (F.nreq > 0) {
-        const int64_t n = F.nreq;
-        ENSURE(ctx->rq_keys, (size_t)n * 4);
-        ENSURE(ctx->rq_k0, (size_t)n * 4); ENSURE(ctx->rq_k1, (size_t)n * 4);
-        ENSURE(ctx->rq_v0, (size_t)n * 4); ENSURE(ctx->rq_v1, (size_t)n * 4);
-        ENSURE(ctx->rq_hist, radix_hist_elems(n) * 4);
-        ENSURE(ctx->rq_ws, scan_workspace_bytes((int64_t)radix_hist_elems(n)));
-        CK(cudaEventRecord(ctx->ev[6], ctx->st));
-        CK(request_keys(F.R.a, n, ctx->aabb, P<uint32_t>(ctx->rq_keys), ctx->st));
-        RadixBuffers RB{{P<uint32_t>(ctx->rq_k0), P<uint32_t>(ctx->rq_k1)}, {P<uint32_t>(ctx->rq_v0), P<uint32_t>(ctx->rq_v1)},
-                        P<uint32_t>(ctx->rq_hist), ctx->rq_ws.p, P<unsigned>(ctx->status)};
-        int launches = 0;
-        CK(radix_sort_u32(RB, P<uint32_t>(ctx->rq_keys), nullptr, n, 30, false, nullptr, &order, &launches, ctx->st));
-        ctx->launches += launches + 1;
-        Q.idx = order;
-    }
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    if (!F.ordered)
+        if (int rc = request_order(ctx, F, ctx->st)) return rc;
+    Q.idx = F.order;
     GatherOut OG{P<float>(ctx->est_g), nullptr, nullptr, nullptr};
-    if (F.nreq <= 0) CK(cudaEventRecord(ctx->ev[6], ctx->st));
     CK(cudaEventRecord(ctx->ev[11], ctx->st));
     CK(gather(grid_of(G, G), Q, o->r_global, o->k_global, 0, OG, P<unsigned>(ctx->status), ctx->st));
     CK(cudaEventRecord(ctx->ev[12], ctx->st));
@@ -1316,32 +1361,45 @@ int pm_frame(pm_ctx* ctx, const pm_trace_opts* to, const pm_grid_opts* go, const
     if (cam->width <= 0 || cam->height <= 0) return fail(ctx, PM_ERR_INVALID, "bad camera size");
     CK(cudaSetDevice(ctx->device));
     if (int rc = pm_trace_photons(ctx, to, out_paths)) return rc;
-    // the eye pass needs neither the photons nor the grid: it runs on the
-    // frame stream beside the grid build
+    // The eye pass needs neither the photons nor the grid: it runs on the frame
+    // stream beside the grid build, followed there by the request count and
+    // the requests' Morton order; the gather waits for both streams.
     if (!ctx->frame_st) {
         CK(cudaStreamCreateWithFlags(&ctx->frame_st, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&ctx->frame_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ctx->frame_done, cudaEventDisableTiming));
     }
+    const bool caustic = to->caustic_capacity > 0 && o->k_caustic > 0;
     FrameSetup F;
+    GridIssued gg, gc;
     CK(cudaEventRecord(ctx->frame_fork, ctx->st));
     CK(cudaStreamWaitEvent(ctx->frame_st, ctx->frame_fork, 0));
     int rc = render_eye_launch(ctx, cam, o, F, ctx->frame_st);
-    if (rc == PM_OK) {
-        if (cudaEventRecord(ctx->frame_done, ctx->frame_st) != cudaSuccess) rc = cuda_fail(ctx, cudaErrorUnknown, "frame event");
-    }
-    if (rc == PM_OK) rc = pm_build_grid(ctx, PM_MAP_GLOBAL, go, nullptr);
-    if (rc == PM_OK && to->caustic_capacity > 0 && o->k_caustic > 0) rc = pm_build_grid(ctx, PM_MAP_CAUSTIC, go, nullptr);
+    if (rc == PM_OK) rc = grid_issue(ctx, PM_MAP_GLOBAL, go, nullptr, gg);
+    if (rc == PM_OK && caustic) rc = grid_issue(ctx, PM_MAP_CAUSTIC, go, nullptr, gc);
+    if (rc == PM_OK) rc = render_eye_count(ctx, F, ctx->frame_st);
+    if (rc == PM_OK) rc = request_order(ctx, F, ctx->frame_st);
+    if (rc == PM_OK && cudaEventRecord(ctx->frame_done, ctx->frame_st) != cudaSuccess)
+        rc = cuda_fail(ctx, cudaErrorUnknown, "frame event");
+    if (rc == PM_OK && cudaStreamWaitEvent(ctx->st, ctx->frame_done, 0) != cudaSuccess)
+        rc = cuda_fail(ctx, cudaErrorUnknown, "frame join");
     if (rc != PM_OK) {
-        cudaStreamSynchronize(ctx->frame_st);   // the eye pass's buffers stay in use until it ends
+        // the frame stream's buffers stay in use until it ends
+        cudaStreamSynchronize(ctx->frame_st);
+        cudaStreamSynchronize(ctx->st);
         return rc;
     }
-    CK(cudaStreamWaitEvent(ctx->st, ctx->frame_done, 0));
+    // the grids are complete in stream order before the gather reads them;
+    // their device status is checked with the frame's
+    grid_commit(ctx, PM_MAP_GLOBAL, gg);
+    if (caustic) grid_commit(ctx, PM_MAP_CAUSTIC, gc);
     if (int rc2 = render_checks(ctx, cam, o)) return rc2;
     F.caustic = ctx->maps[PM_MAP_CAUSTIC].built;
     if (F.caustic) ENSURE(ctx->est_c, (size_t)F.cap * 12);
-    if (int rc2 = render_eye_count(ctx, F)) return rc2;
-    return render_rest(ctx, o, F, out_rgb8, out_radiance);
+    rc = render_rest(ctx, o, F, out_rgb8, out_radiance);
+    if (rc == PM_OK) ctx->stage_ms[1] = elapsed(ctx->ev[2], ctx->ev[3]);
+    else ctx->maps[PM_MAP_GLOBAL].built = ctx->maps[PM_MAP_CAUSTIC].built = false;
+    return rc;
 }
 
 int pm_render(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o, uint8_t* out_rgb8, float* out_radiance) {

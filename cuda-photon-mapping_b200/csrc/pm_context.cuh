@@ -20,6 +20,8 @@ struct DevBuf {
 struct MapState {
     int64_t n = 0;                       // photons in the list
     DevBuf pos, dir, pow;                // traced-order list (3 floats per photon)
+    bool uniform_pow = false;            // every photon of the list has power pow_value (a traced map)
+    float pow_value[3] = {0, 0, 0};
     bool built = false;
     int dims[3] = {0, 0, 0};
     float cell = 0.f;

@@ -350,9 +350,12 @@ k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restri
     }
 }
 
+// pw == nullptr: every photon has power pw0 (a traced map), so the power is
+// written without a random read of the source list
 __global__ void k_grid_gather(const uint32_t* __restrict__ order, int64_t n, const float* __restrict__ pos,
-                              const float* __restrict__ dir, const float* __restrict__ pw, float4* __restrict__ gpos,
-                              float* __restrict__ gdir, float* __restrict__ gpow, unsigned* status) {
+                              const float* __restrict__ dir, const float* __restrict__ pw, float3 pw0,
+                              float4* __restrict__ gpos, float* __restrict__ gdir, float* __restrict__ gpow,
+                              unsigned* status) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t s = order[j];
@@ -361,8 +364,12 @@ __global__ void k_grid_gather(const uint32_t* __restrict__ order, int64_t n, con
     gpos[j] = make_float4(p[0], p[1], p[2], __uint_as_float(s));
     const float* d = dir + 3 * (int64_t)s;
     gdir[3 * j] = d[0]; gdir[3 * j + 1] = d[1]; gdir[3 * j + 2] = d[2];
-    const float* w = pw + 3 * (int64_t)s;
-    gpow[3 * j] = w[0]; gpow[3 * j + 1] = w[1]; gpow[3 * j + 2] = w[2];
+    float3 w = pw0;
+    if (pw) {
+        const float* q = pw + 3 * (int64_t)s;
+        w = make_float3(q[0], q[1], q[2]);
+    }
+    gpow[3 * j] = w.x; gpow[3 * j + 1] = w.y; gpow[3 * j + 2] = w.z;
 }
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -527,7 +534,9 @@ cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* 
     const uint32_t* order = nullptr;
     cudaError_t e = radix_sort_u32(RB, B.cid, nullptr, n, bits, false, nullptr, &order, launches, st);
     if (e != cudaSuccess) return e;
-    k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(order, n, B.pos, B.dir, B.pow, B.gpos, B.gdir, B.gpow, B.status);
+    k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(
+        order, n, B.pos, B.dir, B.uniform_pow ? nullptr : B.pow,
+        make_float3(B.pow_value[0], B.pow_value[1], B.pow_value[2]), B.gpos, B.gdir, B.gpow, B.status);
     *launches += 1;
     return cudaGetLastError();
 }

@@ -14,6 +14,8 @@ struct GridBuffers {
     const float* pos;
     const float* dir;
     const float* pow;
+    bool uniform_pow = false;   // every photon has power pow_value: the sorted power is written, not gathered
+    float pow_value[3] = {0.f, 0.f, 0.f};
     int64_t n;
     // outputs (sized by grid_build_sizes)
     uint32_t* cell_starts;

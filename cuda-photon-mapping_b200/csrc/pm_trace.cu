@@ -441,7 +441,7 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= npaths) return;
     int ng = (int)cnt_g[j], nc = (int)cnt_c[j];
-    int64_t og = gfilled + scan_g[j], oc = cfilled + scan_c[j];
+    int64_t og = gfilled + scan_g[j], oc = ccap > 0 ? cfilled + scan_c[j] : 0;
     for (int k = 0; k < ng + nc; k++) {
         size_t o = (size_t)k * (size_t)npaths + (size_t)j;
         float4 p = stage[2 * o];
@@ -532,7 +532,9 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (B.k_end && (e = cudaEventRecord(B.k_end, st)) != cudaSuccess) return e;
     if ((e = scan_u32(B.cnt_g, B.scan_g, B.npaths, 0, B.totals, B.scan_ws, B.status, st)) != cudaSuccess) return e;
-    if ((e = scan_u32(B.cnt_c, B.scan_c, B.npaths, 0, B.totals + 1, B.scan_ws, B.status, st)) != cudaSuccess) return e;
+    // no caustic map: its counts still steer the loop below, its offsets are not needed
+    if (C.cap > 0 && (e = scan_u32(B.cnt_c, B.scan_c, B.npaths, 0, B.totals + 1, B.scan_ws, B.status, st)) != cudaSuccess)
+        return e;
     k_compact<<<(unsigned)((B.npaths + 255) / 256), 256, 0, st>>>(
         B.npaths, B.stage, B.cnt_g, B.cnt_c, B.scan_g, B.scan_c, P.power,
         G.pos, G.dir, G.pow, G.cap, G.filled, C.pos, C.dir, C.pow, C.cap, C.filled);

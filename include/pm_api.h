@@ -230,7 +230,8 @@ int pm_render_rows(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts
  * global map (and of the caustic map when trace fills one and k_caustic > 0)
  * with grid, then pm_render's frame.  The eye pass needs neither the photons
  * nor the grid, so it runs on a second stream of the context beside the grid
- * build.  Results are pm_trace_photons + pm_build_grid + pm_render's
+ * build, followed there by the ordering of its requests for the gather.
+ * Results are pm_trace_photons + pm_build_grid + pm_render's
  * (Initializer.cu:142-177 followed by Drawer::draw_in_gpu, Drawer.cu:22-41). */
 int pm_frame(pm_ctx* ctx, const pm_trace_opts* trace, const pm_grid_opts* grid, const pm_camera* cam,
              const pm_render_opts* opts, uint8_t* out_rgb8, float* out_radiance, int64_t* out_paths);
@@ -285,7 +286,8 @@ int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclus
 /* Per-stage device times of the last pm_trace_photons / pm_build_grid /
  * pm_render calls in milliseconds (CUDA events on the context stream):
  * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather (request
- * ordering + global gather + caustic gather), [4] resolve, [5] the k_trace
+ * ordering + global gather + caustic gather; in pm_frame the ordering runs
+ * beside the grid build and is not counted here), [4] resolve, [5] the k_trace
  * kernels alone, [6] the global gather kernel alone. */
 int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
 
