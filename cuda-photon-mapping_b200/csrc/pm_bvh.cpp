@@ -3,8 +3,9 @@
 // The reference has no acceleration structure: every ray tests every triangle
 // of every model whose box it meets (CudaPhotonMapping/Model.cuh:366-446); its
 // kd-tree code only reduces a model's triangles to one AABB
-// (KdTree.cu:395-464).  This is a binary BVH built with binned SAH (16 bins on
-// the widest centroid axis, leaves of <= 4 triangles, depth <= 60), stored as
+// (KdTree.cu:395-464).  This is a binary BVH built with binned SAH (32 bins on
+// each centroid axis; a range of <= 4 triangles becomes a leaf when testing
+// them costs no more than the best split; depth <= 60), stored as
 // interior nodes that carry both children's boxes, so one 64-byte fetch tests
 // both children.  Boxes are padded so that culling is conservative with
 // respect to the exact triangle test; the traversal (pm_scene.cuh) keeps the
@@ -44,6 +45,11 @@ struct Node {
 
 struct Task { int node, b, e, depth; };
 
+constexpr int BINS = 32;        // SAH bins per axis
+constexpr int LEAF_MAX = 4;     // larger ranges are always split
+constexpr float SAH_CT = 1.0f;  // cost of an interior visit (one 64-byte node, two slab tests) ...
+constexpr float SAH_CI = 1.2f;  // ... and of one triangle test (one 80-byte record)
+
 }  // namespace
 
 // nodes_out: 16 floats per interior node (both children's boxes and refs, see below);
@@ -60,7 +66,6 @@ void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& no
     std::vector<Node> nodes(1);
     std::vector<Task> stack;
     stack.push_back(Task{0, 0, ntri, 0});
-    const int BINS = 16;
     while (!stack.empty()) {
         Task tk = stack.back();
         stack.pop_back();
@@ -69,25 +74,23 @@ void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& no
         nodes[tk.node].box = nb;
         const int n = tk.e - tk.b;
         auto make_leaf = [&]() { nodes[tk.node].first = tk.b; nodes[tk.node].count = n; };
-        if (n <= 4 || (tk.depth >= 60 && n <= 255)) { make_leaf(); continue; }
-        int axis = 0;
+        if (n <= 1 || (tk.depth >= 60 && n <= 255)) { make_leaf(); continue; }
+        // binned SAH over all three axes; cost = CT + CI (A_l n_l + A_r n_r) / A
         float ext[3];
         for (int a = 0; a < 3; a++) ext[a] = cb.hi[a] - cb.lo[a];
-        if (ext[1] > ext[axis]) axis = 1;
-        if (ext[2] > ext[axis]) axis = 2;
-        int mid;
-        if (!(ext[axis] > 0.f)) {
-            mid = tk.b + n / 2;
-        } else {
+        float best = FLT_MAX;
+        int baxis = -1, bsplit = -1;
+        for (int axis = 0; axis < 3; axis++) {
+            if (!(ext[axis] > 0.f)) continue;
             Box bb[BINS];
             int bc[BINS] = {0};
-            auto bin_of = [&](int t) {
+            for (int i = tk.b; i < tk.e; i++) {
+                const int t = prim[i];
                 int k = (int)((cen[3 * (size_t)t + axis] - cb.lo[axis]) / ext[axis] * BINS);
-                return std::min(std::max(k, 0), BINS - 1);
-            };
-            for (int i = tk.b; i < tk.e; i++) { int k = bin_of(prim[i]); bc[k]++; bb[k].grow(pb[prim[i]]); }
-            float best = FLT_MAX;
-            int bsplit = -1;
+                k = std::min(std::max(k, 0), BINS - 1);
+                bc[k]++;
+                bb[k].grow(pb[t]);
+            }
             Box left[BINS];
             int lc[BINS];
             Box acc; int ac = 0;
@@ -97,23 +100,30 @@ void build_bvh(const float* tri_pos, int ntri, float pad, std::vector<float>& no
                 racc.grow(bb[k]); rc += bc[k];
                 if (lc[k - 1] == 0 || rc == 0) continue;
                 float c = left[k - 1].area() * lc[k - 1] + racc.area() * rc;
-                if (c < best) { best = c; bsplit = k; }
-            }
-            if (bsplit < 0) {
-                mid = tk.b + n / 2;
-            } else {
-                int* it = std::partition(prim.data() + tk.b, prim.data() + tk.e,
-                                         [&](int t) { return bin_of(t) < bsplit; });
-                mid = (int)(it - prim.data());
-                if (mid == tk.b || mid == tk.e) mid = tk.b + n / 2;
+                if (c < best) { best = c; baxis = axis; bsplit = k; }
             }
         }
-        if (mid == tk.b + n / 2 && !(ext[axis] > 0.f)) {
+        const float A = nb.area();
+        const float split_cost = A > 0.f && baxis >= 0 ? SAH_CT + SAH_CI * best / A : FLT_MAX;
+        if (n <= LEAF_MAX && SAH_CI * (float)n <= split_cost) { make_leaf(); continue; }
+        int mid;
+        if (baxis < 0) {
             // all centroids coincide: keep order, split by count
-        } else if (mid == tk.b + n / 2) {
-            std::nth_element(prim.data() + tk.b, prim.data() + mid, prim.data() + tk.e, [&](int x, int y) {
-                return cen[3 * (size_t)x + axis] < cen[3 * (size_t)y + axis];
-            });
+            mid = tk.b + n / 2;
+        } else {
+            const int axis = baxis;
+            auto bin_of = [&](int t) {
+                int k = (int)((cen[3 * (size_t)t + axis] - cb.lo[axis]) / ext[axis] * BINS);
+                return std::min(std::max(k, 0), BINS - 1);
+            };
+            int* it = std::partition(prim.data() + tk.b, prim.data() + tk.e, [&](int t) { return bin_of(t) < bsplit; });
+            mid = (int)(it - prim.data());
+            if (mid == tk.b || mid == tk.e) {
+                mid = tk.b + n / 2;
+                std::nth_element(prim.data() + tk.b, prim.data() + mid, prim.data() + tk.e, [&](int x, int y) {
+                    return cen[3 * (size_t)x + axis] < cen[3 * (size_t)y + axis];
+                });
+            }
         }
         int left_idx = (int)nodes.size();
         nodes.resize(nodes.size() + 2);
