@@ -68,8 +68,7 @@ std::vector<DevBuf*> all_buffers(pm_ctx* ctx) {
                               &ctx->probe_req, &ctx->probe_est, &ctx->tile_flag, &ctx->learned_counts,
                               &ctx->fallback_list, &ctx->bvh_scratch, &ctx->tri_leaf, &ctx->eye_order, &ctx->rq_keys,
                               &ctx->rq_k0, &ctx->rq_k1, &ctx->rq_v0, &ctx->rq_v1, &ctx->rq_hist, &ctx->rq_ws,
-                              &ctx->work, &ctx->eye_band, &ctx->tr_start, &ctx->tr_keys, &ctx->tr_order,
-                              &ctx->tr_buckets};
+                              &ctx->work, &ctx->eye_band};
     for (auto& m : ctx->maps)
         for (DevBuf* b : {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid, &m.keys0,
                           &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small, &m.key_counts,
@@ -748,9 +747,6 @@ int pm_scene_aabb(pm_ctx* ctx, float out_aabb[6]) {
     return PM_OK;
 }
 
-// batches of at least this many paths take their paths in first-direction order
-constexpr int64_t TRACE_ORDER_MIN = 1 << 16;
-
 static int prepare_trace(pm_ctx* ctx, const pm_trace_opts* o, int64_t npaths, TraceBatch& B) {
     if (!ctx->has_scene) return fail(ctx, PM_ERR_INVALID, "pm_set_scene first");
     if (o->max_bounces < 1 || o->max_bounces > 32) return fail(ctx, PM_ERR_INVALID, "max_bounces must be 1..32");
@@ -834,21 +830,6 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         for (int a = 0; a < 3; a++) B.power[a] = power[a];
         B.k_begin = ctx->ev[12];
         B.k_end = ctx->ev[13];
-        if (nb >= TRACE_ORDER_MIN) {
-            // emission ahead of the tracer, and paths in the order of their first
-            // ray's direction: a warp's first rays leave the light the same way
-            // and traverse the same subtrees
-            ENSURE(ctx->tr_start, (size_t)nb * 32);
-            ENSURE(ctx->tr_keys, (size_t)nb * 4);
-            ENSURE(ctx->tr_order, (size_t)nb * 4);
-            ENSURE(ctx->tr_buckets, 512 * 4);
-            CK(trace_start_paths(B, P<float4>(ctx->tr_start), P<uint32_t>(ctx->tr_keys), ctx->st));
-            CK(trace_path_order(P<uint32_t>(ctx->tr_keys), nb, P<uint32_t>(ctx->tr_buckets), P<uint32_t>(ctx->tr_order),
-                                ctx->st));
-            B.starts = P<float4>(ctx->tr_start);
-            B.order = P<uint32_t>(ctx->tr_order);
-            ctx->launches += 4;
-        }
         PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg};
         PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc};
         CK(trace_batch(B, LG, LC, ctx->st));

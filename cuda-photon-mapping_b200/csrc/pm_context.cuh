@@ -70,7 +70,6 @@ struct pm_ctx {
     std::vector<float> h_maabb, h_mats;
     pm::DevBuf eye_order;
     pm::DevBuf rq_keys, rq_k0, rq_k1, rq_v0, rq_v1, rq_hist, rq_ws;   // the gather's request order
-    pm::DevBuf tr_start, tr_keys, tr_order, tr_buckets;   // the photon pass's emission records and path order
     // training steps queued without a loss run on their own stream; whatever
     // reads or writes the cache (or synchronises the context) waits for them
     cudaStream_t train_st = nullptr;

@@ -11,11 +11,6 @@
 //  * a persistent grid traces the paths [p0, p0 + npaths) of one batch.  Lanes
 //    whose path ended take the next path indices together (one atomic per
 //    warp, ballot ranks), so SIMD lanes stay busy however long paths are;
-//  * for large batches the emission (light point, rejection-sampled first
-//    direction) runs ahead in k_start_paths, which records each path's first
-//    ray and stream position, and the paths are queued grouped by an 8-bit
-//    code of that direction (k_order_*): the lanes of a warp then start with
-//    rays that leave the light the same way and traverse the same subtrees;
 //  * the k-th photon a path stores goes to stage slot [k][path], a 32-byte
 //    record written as two 16-byte vector stores: (position, map flag) and
 //    (direction, 0); one record fills one DRAM sector, so no sector is left
@@ -78,8 +73,6 @@ struct KParams {
     unsigned* status;
     int refill;             // lanes with a finished query that end a warp's traversal loop
     unsigned long long* work;   // work-counting launch: rays, BVH node visits, triangle tests (else null)
-    const uint32_t* order;      // batch-local path taken at each queue position (null: the position itself)
-    const float4* starts;       // each path's first ray and stream position (null: emitted in the tracer)
 };
 
 // light point + cosine-weighted direction by rejection (PhotonTracing.cu:345-369)
@@ -114,22 +107,6 @@ __device__ __forceinline__ void start_path(const KParams& P, Lane& L, int64_t pa
         if (dt < 0) { dt = -dt; d = vscale(d, -1.f); }
     } while (prob > dt);
     if (tries <= REJECT_LIMIT) L.ray.d = d;
-    L.bounce = 0;
-    L.ng = L.nc = 0;
-    L.diffuse_surfs = 0;
-    L.last = NONE;
-    L.sn = 0;
-}
-
-// the state start_path leaves, from the record k_start_paths wrote
-__device__ __forceinline__ void resume_path(const KParams& P, Lane& L, int64_t j) {
-    const float4 a = __ldg(P.starts + 2 * j), b = __ldg(P.starts + 2 * j + 1);
-    L.st.init(P.seed, (uint64_t)(P.p0 + j), P.tag);
-    L.st.n = __float_as_uint(a.w);
-    if ((L.st.n & 3u) != 0u)
-        L.st.buf = philox10(make_uint4(L.st.n >> 2, L.st.plo, L.st.phi, L.st.tag), L.st.k0, L.st.k1);
-    L.ray.o = v3(a.x, a.y, a.z);
-    L.ray.d = v3(b.x, b.y, b.z);
     L.bounce = 0;
     L.ng = L.nc = 0;
     L.diffuse_surfs = 0;
@@ -287,16 +264,9 @@ k_trace(KParams P) {
             if (need) {
                 const unsigned long long mine = base + (unsigned long long)__popc(m & lanemask_lt());
                 if ((int64_t)mine < P.npaths) {
-                    j = P.order ? (int64_t)__ldg(P.order + mine) : (int64_t)mine;
-                    if (j >= P.npaths) {   // not a permutation of the batch: stop this lane
-                        raise_status(P.status, ST_BAD_INPUT);
-                        j = -1;
-                        state = L_DONE;
-                    } else {
-                        if (P.starts) resume_path(P, L, j);
-                        else start_path(P, L, P.p0 + j);
-                        state = L_RAY;
-                    }
+                    j = (int64_t)mine;
+                    start_path(P, L, P.p0 + j);
+                    state = L_RAY;
                 } else {
                     state = L_DONE;
                 }
@@ -492,111 +462,9 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
     }
 }
 
-// Morton interleave of two 8-bit values
-__device__ __forceinline__ uint32_t spread8(uint32_t v) {
-    v = (v | (v << 4)) & 0x0f0fu;
-    v = (v | (v << 2)) & 0x3333u;
-    v = (v | (v << 1)) & 0x5555u;
-    return v;
-}
-
-// each batch path's emission -> start record + 8-bit direction key
-// (octahedral coordinates, Morton interleaved, top 8 of 16 bits)
-__global__ void k_start_paths(KParams P, float4* __restrict__ starts, uint32_t* __restrict__ keys) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.npaths) return;
-    Lane L;
-    start_path(P, L, P.p0 + i);
-    starts[2 * i] = make_float4(L.ray.o.x, L.ray.o.y, L.ray.o.z, __uint_as_float(L.st.n));
-    starts[2 * i + 1] = make_float4(L.ray.d.x, L.ray.d.y, L.ray.d.z, 0.f);
-    const V3 d = L.ray.d;
-    const float s = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
-    float u = s > 0.f ? d.x / s : 0.f, v = s > 0.f ? d.y / s : 0.f;
-    if (d.z < 0.f) {
-        const float fu = (1.f - fabsf(v)) * (u >= 0.f ? 1.f : -1.f);
-        const float fv = (1.f - fabsf(u)) * (v >= 0.f ? 1.f : -1.f);
-        u = fu;
-        v = fv;
-    }
-    const uint32_t qu = (uint32_t)fminf(fmaxf((u * 0.5f + 0.5f) * 256.f, 0.f), 255.f);
-    const uint32_t qv = (uint32_t)fminf(fmaxf((v * 0.5f + 0.5f) * 256.f, 0.f), 255.f);
-    keys[i] = (spread8(qu) | (spread8(qv) << 1)) >> 8;
-}
-
-constexpr int ORDER_THREADS = 256;
-constexpr int ORDER_ITEMS = 16;   // keys per thread: 4096 per block, one global atomic per bucket per block
-
-__global__ void __launch_bounds__(ORDER_THREADS) k_order_count(const uint32_t* __restrict__ keys, int64_t n,
-                                                              uint32_t* __restrict__ counts) {
-    __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0u;
-    __syncthreads();
-    const int64_t b0 = (int64_t)blockIdx.x * ORDER_THREADS * ORDER_ITEMS;
-#pragma unroll
-    for (int e = 0; e < ORDER_ITEMS; e++) {
-        const int64_t i = b0 + (int64_t)e * ORDER_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&h[__ldg(keys + i) & 255u], 1u);
-    }
-    __syncthreads();
-    if (h[threadIdx.x]) atomicAdd(counts + threadIdx.x, h[threadIdx.x]);
-}
-
-// counts[0..256) -> cursors[0..256): exclusive scan (one block of 256)
-__global__ void k_order_starts(const uint32_t* __restrict__ counts, uint32_t* __restrict__ cursors) {
-    __shared__ uint32_t s[256];
-    const int t = threadIdx.x;
-    s[t] = counts[t];
-    __syncthreads();
-    for (int o = 1; o < 256; o <<= 1) {
-        const uint32_t v = t >= o ? s[t - o] : 0u;
-        __syncthreads();
-        s[t] += v;
-        __syncthreads();
-    }
-    cursors[t] = s[t] - counts[t];
-}
-
-__global__ void __launch_bounds__(ORDER_THREADS) k_order_scatter(const uint32_t* __restrict__ keys, int64_t n,
-                                                                uint32_t* __restrict__ cursors,
-                                                                uint32_t* __restrict__ order) {
-    __shared__ uint32_t h[256];
-    __shared__ uint32_t base[256];
-    h[threadIdx.x] = 0u;
-    __syncthreads();
-    const int64_t b0 = (int64_t)blockIdx.x * ORDER_THREADS * ORDER_ITEMS;
-    uint32_t rank[ORDER_ITEMS];
-#pragma unroll
-    for (int e = 0; e < ORDER_ITEMS; e++) {
-        const int64_t i = b0 + (int64_t)e * ORDER_THREADS + threadIdx.x;
-        rank[e] = i < n ? atomicAdd(&h[__ldg(keys + i) & 255u], 1u) : 0u;
-    }
-    __syncthreads();
-    base[threadIdx.x] = h[threadIdx.x] ? atomicAdd(cursors + threadIdx.x, h[threadIdx.x]) : 0u;
-    __syncthreads();
-#pragma unroll
-    for (int e = 0; e < ORDER_ITEMS; e++) {
-        const int64_t i = b0 + (int64_t)e * ORDER_THREADS + threadIdx.x;
-        if (i < n) {
-            const uint32_t pos = base[__ldg(keys + i) & 255u] + rank[e];
-            if ((int64_t)pos < n) order[pos] = (uint32_t)i;
-        }
-    }
-}
-
 }  // namespace
 
 size_t trace_multi_table_bytes(int ninst) { return (size_t)ninst * sizeof(KParams); }
-
-cudaError_t trace_path_order(const uint32_t* keys, int64_t n, uint32_t* buckets, uint32_t* order, cudaStream_t st) {
-    if (n <= 0) return cudaSuccess;
-    cudaError_t e;
-    if ((e = cudaMemsetAsync(buckets, 0, 256 * 4, st)) != cudaSuccess) return e;
-    const unsigned blocks = (unsigned)((n + ORDER_THREADS * ORDER_ITEMS - 1) / (ORDER_THREADS * ORDER_ITEMS));
-    k_order_count<<<blocks, ORDER_THREADS, 0, st>>>(keys, n, buckets);
-    k_order_starts<<<1, 256, 0, st>>>(buckets, buckets + 256);
-    k_order_scatter<<<blocks, ORDER_THREADS, 0, st>>>(keys, n, buckets + 256, order);
-    return cudaGetLastError();
-}
 
 cudaError_t trace_multi_tables(const TraceMulti& M, const TraceInst* insts, cudaStream_t st) {
     std::vector<KParams> tab((size_t)M.ninst);
@@ -639,16 +507,6 @@ cudaError_t trace_multi(const TraceMulti& M, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t trace_start_paths(const TraceBatch& B, float4* starts, uint32_t* keys, cudaStream_t st) {
-    if (B.npaths <= 0) return cudaSuccess;
-    KParams P{};
-    P.S = B.S; P.seed = B.seed; P.tag = B.tag; P.max_bounces = B.max_bounces;
-    P.p0 = B.p0; P.npaths = B.npaths;
-    P.status = B.status;
-    k_start_paths<<<(unsigned)((B.npaths + 255) / 256), 256, 0, st>>>(P, starts, keys);
-    return cudaGetLastError();
-}
-
 cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_t st) {
     cudaError_t e;
     if (B.npaths <= 0) return cudaSuccess;
@@ -663,8 +521,6 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
     P.status = B.status;
     P.refill = B.refill > 0 ? std::min(B.refill, 32) : TRACE_REFILL;
     P.work = B.work;
-    P.order = B.order;
-    P.starts = B.starts;
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<false>, TRACE_THREADS, 0)) != cudaSuccess)
         return e;

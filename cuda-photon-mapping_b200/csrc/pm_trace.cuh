@@ -27,8 +27,6 @@ struct TraceBatch {
     int refill;               // k_trace refill threshold in lanes (1..32); 0: the default
     cudaEvent_t k_begin = nullptr, k_end = nullptr;   // when set: recorded around the k_trace launch
     unsigned long long* work = nullptr;   // when set: the work-counting launch adds rays, node visits, triangle tests
-    const uint32_t* order = nullptr;      // when set: lanes take the batch-local paths order[0], order[1], ...
-    const float4* starts = nullptr;       // when set: each path's first ray and stream position (trace_start_paths)
 };
 
 
@@ -83,18 +81,5 @@ cudaError_t trace_multi(const TraceMulti& M, cudaStream_t st);
 // trace one batch and append its photons (canonical order) to the two lists;
 // totals[0..1] receive the batch's photon counts before the capacity cut
 cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_t st);
-
-// Every batch path's emission (light point, first direction; the same draws
-// as in k_trace) done ahead of the tracer: starts[2 i], starts[2 i + 1] =
-// (origin, draws taken), (direction, 0) of batch path i, and keys[i] an 8-bit
-// code of the direction (octahedral coordinates, Morton interleaved, top
-// bits).  Sorted by key, the paths give the tracer's lanes first rays that
-// leave the light the same way (TraceBatch::order, TraceBatch::starts).
-cudaError_t trace_start_paths(const TraceBatch& B, float4* starts, uint32_t* keys, cudaStream_t st);
-
-// A permutation of [0, n) grouped by key (8-bit keys; the order inside a key
-// is whatever the atomics give: it only schedules the tracer's lanes, whose
-// results are indexed by path).  buckets: 512 u32 of scratch.
-cudaError_t trace_path_order(const uint32_t* keys, int64_t n, uint32_t* buckets, uint32_t* order, cudaStream_t st);
 
 }  // namespace pm
