@@ -402,3 +402,24 @@ def test_frame_call_equals_the_three_calls(ctx):
         st = ctx.stage_times()
         assert 0 < st["k_trace_ms"] <= st["trace_ms"]
         assert 0 < st["k_gather_ms"] <= st["gather_ms"]
+
+
+def test_photon_pass_batches_equal_the_path_range(ctx):
+    """pm_trace_photons (a pilot batch, then batches sized by the measured
+    yield, cut at the capacity) gives the first 150,000 global photons of
+    pm_trace_paths over the same paths in canonical order (heightfield room)."""
+    sc, cam, w = scenes.workload("cornell_hf_1080p")
+    ctx.set_scene(sc)
+    seed, nb = 11, 10
+    n_paths = ctx.trace_photons(seed, nb, 150_000)
+    assert n_paths >= 1 << 16
+    lst = ctx.photons(0, sorted_=False)
+    part = ctx.trace_paths(seed, nb, 150_000, 0, n_paths)
+    cnt = _np(part["counts"])
+    g = int(cnt[:, 0].sum())
+    assert g >= 150_000
+    # canonical order (path, then bounce) cut at the capacity: the list is the
+    # first 150,000 global photons of the path-ordered records
+    assert np.array_equal(_np(part["g_pos"])[:150_000], _np(lst["list_pos"]))
+    assert np.array_equal(_np(part["g_dir"])[:150_000], _np(lst["list_dir"]))
+    assert ctx.status() == 0
