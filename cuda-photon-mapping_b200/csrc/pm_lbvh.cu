@@ -19,8 +19,11 @@
 //                     triangles and split from the common-prefix lengths of
 //                     the keys (code, sorted position)
 //   k_lbvh_boxes      bottom-up from each triangle: the second thread to reach
-//                     an interior node unions its children's boxes and writes
-//                     the node (children of <= 4 triangles become leaves)
+//                     an interior node unions its children's boxes, computes
+//                     the subtree's SAH cost and writes the node; a child of
+//                     <= 4 triangles becomes a leaf when testing them costs
+//                     no more than its best split (the host builder's cost
+//                     model: 1 per interior visit, 1.2 per triangle test)
 #include <algorithm>
 #include "pm_lbvh.cuh"
 #include "pm_grid.cuh"
@@ -32,6 +35,8 @@ namespace pm {
 namespace {
 
 constexpr int LEAF_MAX = 4;
+constexpr float SAH_CT = 1.0f;   // cost of an interior visit (one node, two slab tests) ...
+constexpr float SAH_CI = 1.2f;   // ... and of one triangle test
 constexpr int MAX_CLIMB = 256;   // levels a bottom-up thread may climb (tree depth is < 70)
 
 // float <-> unsigned with the same order (for atomicMin / atomicMax)
@@ -172,18 +177,24 @@ __device__ __forceinline__ void put_child(float4* o, const Box6& b, int ref, flo
 }
 
 // the traversal's ref of child c: interior node index, or a leaf ~(first << 8 | count)
-__device__ __forceinline__ int child_ref(int c, const int* __restrict__ range) {
+// (a single triangle, or an interior node whose subtree is cheaper as a leaf)
+__device__ __forceinline__ int child_ref(int c, const int* __restrict__ range, const int* isleaf) {
     if (c < 0) return ~(((~c) << 8) | 1);
     const int lo = range[2 * c], hi = range[2 * c + 1];
-    if (hi - lo + 1 <= LEAF_MAX) return ~((lo << 8) | (hi - lo + 1));
+    if (__ldcg(isleaf + c)) return ~((lo << 8) | (hi - lo + 1));
     return c;
+}
+
+__device__ __forceinline__ float half_area(const Box6& b) {
+    const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    return dx * dy + dy * dz + dz * dx;
 }
 
 __global__ void k_lbvh_boxes(const float* __restrict__ tp, int n, const uint32_t* __restrict__ order,
                              const int* __restrict__ child, const int* __restrict__ range,
                              const int* __restrict__ parent_int, const int* __restrict__ parent_leaf,
-                             uint32_t* __restrict__ arrived, float* ibox, float* lbox, float4* __restrict__ nodes,
-                             int* __restrict__ prim, float pad, unsigned* status) {
+                             uint32_t* __restrict__ arrived, float* ibox, float* lbox, float* cost, int* isleaf,
+                             float4* __restrict__ nodes, int* __restrict__ prim, float pad, unsigned* status) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int tri = (int)order[p];
@@ -203,8 +214,17 @@ __global__ void k_lbvh_boxes(const float* __restrict__ tp, int n, const uint32_t
 #pragma unroll
         for (int a = 0; a < 3; a++) { u.lo[a] = fminf(b0.lo[a], b1.lo[a]); u.hi[a] = fmaxf(b0.hi[a], b1.hi[a]); }
         store_box(ibox, x, u);
-        put_child(nodes + 4 * (size_t)x, b0, child_ref(c0, range), pad);
-        put_child(nodes + 4 * (size_t)x + 2, b1, child_ref(c1, range), pad);
+        // SAH cost of the subtree: CT + (A0 C0 + A1 C1) / A as an interior node,
+        // CI n as a leaf of n <= LEAF_MAX triangles; the cheaper one is kept
+        const float C0 = c0 < 0 ? SAH_CI : __ldcg(cost + c0), C1 = c1 < 0 ? SAH_CI : __ldcg(cost + c1);
+        const float A = half_area(u);
+        const float split = SAH_CT + (A > 0.f ? (half_area(b0) * C0 + half_area(b1) * C1) / A : C0 + C1);
+        const int cnt = range[2 * x + 1] - range[2 * x] + 1;
+        const bool leaf = x != 0 && cnt <= LEAF_MAX && SAH_CI * (float)cnt <= split;
+        __stcg(cost + x, leaf ? SAH_CI * (float)cnt : split);
+        __stcg(isleaf + x, leaf ? 1 : 0);
+        put_child(nodes + 4 * (size_t)x, b0, child_ref(c0, range, isleaf), pad);
+        put_child(nodes + 4 * (size_t)x + 2, b1, child_ref(c1, range, isleaf), pad);
         x = parent_int[x];
     }
 }
@@ -222,7 +242,8 @@ inline unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t)
 
 // scratch carve-up (byte offsets, 256-aligned)
 struct Layout {
-    size_t cb, codes, keys0, keys1, vals0, vals1, hist, scan, child, range, pint, pleaf, arrived, ibox, lbox, total;
+    size_t cb, codes, keys0, keys1, vals0, vals1, hist, scan, child, range, pint, pleaf, arrived, ibox, lbox, cost,
+        isleaf, total;
 };
 inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 Layout layout(int n) {
@@ -246,6 +267,8 @@ Layout layout(int n) {
     L.arrived = take(N * 4);
     L.ibox = take(6 * N * 4);
     L.lbox = take(6 * N * 4);
+    L.cost = take(N * 4);
+    L.isleaf = take(N * 4);
     L.total = o;
     return L;
 }
@@ -294,6 +317,8 @@ cudaError_t lbvh_build(const float* tri_pos, int ntri, float pad, float4* nodes,
     uint32_t* arrived = reinterpret_cast<uint32_t*>(base + L.arrived);
     float* ibox = reinterpret_cast<float*>(base + L.ibox);
     float* lbox = reinterpret_cast<float*>(base + L.lbox);
+    float* cost = reinterpret_cast<float*>(base + L.cost);
+    int* isleaf = reinterpret_cast<int*>(base + L.isleaf);
     if ((e = cudaMemsetAsync(cb, 0xff, 12, st)) != cudaSuccess) return e;   // minima start at the largest key
     if ((e = cudaMemsetAsync(cb + 3, 0, 12, st)) != cudaSuccess) return e;  // maxima at the smallest
     if ((e = cudaMemsetAsync(arrived, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
@@ -308,7 +333,7 @@ cudaError_t lbvh_build(const float* tri_pos, int ntri, float pad, float4* nodes,
     if ((e = radix_sort_u32(RB, codes, nullptr, n, 30, true, &skeys, &order, launches, st)) != cudaSuccess) return e;
     k_lbvh_hierarchy<<<blocks_of(n - 1, 256), 256, 0, st>>>(skeys, n, child, range, pint, pleaf);
     k_lbvh_boxes<<<blocks_of(n, 256), 256, 0, st>>>(tri_pos, n, order, child, range, pint, pleaf, arrived, ibox, lbox,
-                                                    nodes, prim, pad, status);
+                                                    cost, isleaf, nodes, prim, pad, status);
     *launches += 4;
     return cudaGetLastError();
 }
