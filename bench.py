@@ -185,36 +185,45 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- CPU leg
-def cpu_reference_estimate(sc, w, rows=8, trace_photons=5000, threads=None):
+def cpu_reference_estimate(sc, w, rows=8, trace_paths=16384, threads=None):
     """The reference's CPU path on the host cores, on a bounded sample, scaled
     to one full frame of the workload.
 
-    * photon pass: the reference has no CPU tracer (emit is __device__); its
-      algorithm (brute-force closest hit) is timed as the oracle's restatement,
-      OpenMP over the host cores, on ``trace_photons`` photons, scaled to the
-      workload's photon count;
+    * photon pass: the reference's tracer is device code (emit is __global__,
+      trace / destiny __device__); its algorithm (brute-force closest hit) is
+      timed as the oracle's restatement, which tests/test_tracer_pin.py pins
+      bit for bit to the reference's own tracer compiled as host code,
+      OpenMP over the host cores, on the exact path range [0, trace_paths);
+      scaled by the paths the workload needs (its photon count over the
+      sample's global photons per path);
     * grid: the oracle's grid build over a map of the workload's size (the
       traced sample replicated with a 1e-4 jitter);
     * frame: the reference's own Raytracer::render_trace (oracle/_ref, its CPU
       mode, single-threaded by design) on ``rows`` image rows spread over the
       frame, one process per host core, over that map; the mean row time is
       scaled to all rows and divided over the cores.
+    Returns the scaled times and wall_s, the sample's own wall time.
     """
     import multiprocessing as mp
     import tempfile
     from oracle import Oracle
+    w0 = time.perf_counter()
     orc = Oracle()
     s = orc.scene(sc)
     threads = threads or os.cpu_count() or 1
-    t0 = time.perf_counter()
-    tr = s.trace_photons(w["seed"], w["max_bounces"], trace_photons)
-    t_trace = (time.perf_counter() - t0) * (w["photons"] / trace_photons)
     n = w["photons"]
-    rep = int(np.ceil(n / trace_photons))
+    t0 = time.perf_counter()
+    tr = s.trace_paths(w["seed"], w["max_bounces"], n, 0, trace_paths)
+    t_sample = time.perf_counter() - t0
+    got = int(tr["g_pos"].shape[0])
+    per_path = got / trace_paths
+    paths_needed = n / max(per_path, 1e-9)
+    t_trace = t_sample * paths_needed / trace_paths
+    rep = int(np.ceil(n / max(got, 1)))
     rng = np.random.default_rng(1)
     pos = (np.tile(tr["g_pos"], (rep, 1))[:n] + rng.normal(scale=1e-4, size=(n, 3)).astype(np.float32)).astype(np.float32)
     dirs = np.tile(tr["g_dir"], (rep, 1))[:n]
-    pw = np.tile(tr["g_pow"], (rep, 1))[:n]
+    pw = np.tile(np.asarray(sc.light_intensity, np.float32) / np.float32(n), (n, 1))
     t0 = time.perf_counter()
     g = orc.grid_build(pos, pw, dirs, s.aabb())
     t_grid = time.perf_counter() - t0
@@ -226,17 +235,17 @@ def cpu_reference_estimate(sc, w, rows=8, trace_photons=5000, threads=None):
         np.save(os.path.join(tmp, "cell.npy"), np.float32(g.cell))
         ctx = mp.get_context("spawn")
         args = [(w, tmp, int(y), sc) for y in ys]
-        t0 = time.perf_counter()
         with ctx.Pool(min(threads, rows)) as pool:
             per_row = pool.map(_ref_row, args)
-        wall = time.perf_counter() - t0
     t_row = float(np.mean(per_row))
     t_frame = t_row * H / threads
     total = t_trace + t_grid + t_frame
     return dict(step_s=total, trace_s=t_trace, grid_s=t_grid, frame_s=t_frame, row_s=t_row, cores=threads,
-                sample=f"{trace_photons} photons traced by the oracle (scaled to {n}); grid of {n} photons "
-                       f"(sample replicated); {rows} of {H} rows rendered by the reference's render_trace, "
-                       f"{threads} processes", wall_s=wall)
+                sample=f"photon pass: paths [0, {trace_paths}) traced by the oracle's restatement of the "
+                       f"reference's tracer ({got} global photons, scaled to the {paths_needed:.0f} paths of "
+                       f"{n} photons); grid of {n} photons (sample replicated); {rows} of {H} rows rendered by "
+                       f"the reference's own render_trace; {threads} threads / processes",
+                wall_s=time.perf_counter() - w0)
 
 
 def _ref_row(arg):
@@ -725,27 +734,34 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU path (cpu_reference_estimate) on
+    a bounded sample per step; ms_per_step is the sample step's own wall
+    time, value the workload's Mphotons/s scaled from it."""
     from photonmap import scenes
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
     sc, cs, w = scenes.workload(args.workload)
-    times = []
+    ests = []
     for i in range(args.warmup + args.steps):
-        est = cpu_reference_estimate(sc, w, rows=8, trace_photons=2000)
+        est = cpu_reference_estimate(sc, w)
         if i >= args.warmup:
-            times.append(est["step_s"])
-    step_s = float(np.mean(times))
+            ests.append(est)
+    step_s = float(np.mean([e["step_s"] for e in ests]))
+    wall_ms = float(np.mean([e["wall_s"] for e in ests])) * 1000
     v = w["photons"] / step_s / 1e6
     return {"metric": METRIC, "value": v, "unit": "Mphotons/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1000, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "ms_per_frame_estimated": step_s * 1000,
             "config": {"workload": args.workload, "photons": w["photons"], "max_bounces": w["max_bounces"],
                        "image": f"{w['width']}x{w['height']}", "k": w["k"], "radius": w["radius"],
                        "eye_depth": w["max_depth"], "triangles": sc.ntri, "parallelism": "replicas1",
-                       "api": "the reference's CPU mode (render_cpu) + the oracle's CPU photon pass and grid"},
-            "cpu_baseline": {"value": v, "unit": "Mphotons/s", "cores": est["cores"], "kind": "reference",
-                             "sample": est["sample"]},
+                       "api": "the reference's CPU mode (render_cpu) + the oracle's CPU photon pass and grid",
+                       "step": "one bounded sample (cpu_baseline.sample) scaled to the workload; ms_per_step is "
+                               "the sample's wall time, ms_per_frame_estimated the scaled full frame"},
+            "cpu_baseline": {"value": v, "unit": "Mphotons/s", "cores": ests[-1]["cores"], "kind": "reference",
+                             "sample": ests[-1]["sample"]},
             "e2e": {"value": v, "unit": "Mphotons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

@@ -59,3 +59,24 @@ def test_zero_time_gives_zero_rate():
     w, sc, bvh = _inputs()
     out = bench.rooflines(w, sc, bvh, 0, 0, 0.0, 0.0, (0, 0, 0, 0), 6000.0, "fallback", default_workload=False)
     assert out["k_trace"]["achieved"] == 0.0 and out["k_gather"]["achieved"] == 0.0
+
+
+def test_reference_arm_times_its_sample(monkeypatch):
+    """The reference arm (CPU, no GPU): one step is a bounded sample whose own
+    wall time is ms_per_step; value is the workload's Mphotons/s scaled from
+    it, and the photon pass is scaled by the sample's exact path count."""
+    import bench
+    from oracle import REF_SO
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference host harness not built")
+    from photonmap import scenes
+    sc, cs, w = scenes.workload("cornell_small")
+    monkeypatch.setattr(scenes, "workload", lambda name: (sc, cs, w))
+    monkeypatch.setenv("RANK", "0")
+    args = types.SimpleNamespace(workload="cornell_small", steps=1, warmup=0, gpus=1)
+    line = bench.run_reference(args)
+    assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "reference"
+    assert line["value"] == pytest.approx(w["photons"] / (line["ms_per_frame_estimated"] / 1e3) / 1e6)
+    assert 0 < line["ms_per_step"] < 600_000
+    assert "paths [0, 16384)" in line["cpu_baseline"]["sample"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
