@@ -68,6 +68,7 @@ constexpr int INFER_THREADS = 128 * INFER_GROUPS;
 constexpr uint32_t INFER_OFF_X = W_BYTES;
 constexpr uint32_t INFER_OFF_BAR = INFER_OFF_X + INFER_GROUPS * X_BYTES;
 constexpr uint32_t INFER_SMEM = INFER_OFF_BAR + 8 * INFER_GROUPS + 16;
+static_assert(2 * (INFER_SMEM + 1024) <= 233472, "two inference CTAs per SM must fit in shared memory");
 
 __host__ __device__ constexpr uint32_t w_off(int l) { return (uint32_t)l * 8192u; }
 
@@ -119,13 +120,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// barrier `id` over the 128 threads of one warpgroup; true iff v on all of them
-__device__ __forceinline__ bool wg_sync_and(int id, bool v) {
+// barrier `id` (1..4) over the 128 threads of one warpgroup; true iff v on all
+// of them.  The id is an immediate in each branch, so the kernel reserves only
+// the barriers it names (a register id reserves all 16 of the CTA).
+template <int ID>
+__device__ __forceinline__ uint32_t wg_red_and(uint32_t v) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
         "bar.red.and.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(r) : "r"((uint32_t)v), "r"(id) : "memory");
+        : "=r"(r) : "r"(v), "n"(ID) : "memory");
+    return r;
+}
+__device__ __forceinline__ bool wg_sync_and(int id, bool v) {
+    const uint32_t u = (uint32_t)v;
+    uint32_t r;
+    switch (id) {
+        case 1: r = wg_red_and<1>(u); break;
+        case 2: r = wg_red_and<2>(u); break;
+        case 3: r = wg_red_and<3>(u); break;
+        default: r = wg_red_and<4>(u); break;
+    }
     return r != 0;
 }
 
@@ -615,10 +630,16 @@ cudaError_t mlp_infer(const MlpNet& net, const MlpInputs& in, float* out, unsign
     if (in.n <= 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INFER_SMEM);
     if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_infer, INFER_THREADS, INFER_SMEM)) != cudaSuccess)
-        return e;
-    per_sm = std::min(std::max(per_sm, 1), 512 / (int)TMEM_COLS_INFER);
+    // Two CTAs per SM (8 tile pipelines): each holds 256 of the SM's 512 TMEM
+    // columns, 64 registers x 512 threads (half the register file, the launch
+    // bounds) and under half the shared memory, with the largest carve-out.
+    // The occupancy calculator reports one CTA per SM for any kernel that
+    // allocates TMEM, so the grid is sized from these limits instead; the
+    // tile loop is strided over the whole grid either way.
+    e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    const int per_sm = 512 / (int)TMEM_COLS_INFER;
     const int64_t tiles = (in.n + TILE - 1) / TILE;
     const int64_t ctas = (tiles + INFER_GROUPS - 1) / INFER_GROUPS;
     const int grid = (int)std::min<int64_t>(ctas, (int64_t)per_sm * std::max(sm_count, 1));
