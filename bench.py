@@ -4,9 +4,14 @@ One step = one full frame of the plain method on the ``cornell_hf_1080p``
 workload: trace 10M global photons (max 10 bounces), build the photon grid,
 render 1920x1080 (kNN k = 64, r = 0.05, eye depth 4).  ``value`` is Mphotons/s
 of the whole frame pipeline (photons / step time) summed over ranks;
-``ms_per_step`` is ms/frame.  Inputs (scene, photon maps ~0.5 GB) are larger
-than L2.  Multi-GPU: independent replicas (weak scaling, no collective on the
-data path; the photon maps do not exchange).
+``ms_per_step`` is ms/frame, from CUDA events on the stream the context
+launches on.  Inputs (scene, photon maps ~0.5 GB) are larger than L2.
+``e2e``: the same frames through the public API with every frame read back
+to pinned host memory (6.2 MB at 1080p), the read-back of frame i on a copy
+stream beside frame i + 1 (two frame buffers); host-to-device bytes are 0,
+since a step's only input is its seed (the scene stays resident).
+Multi-GPU: independent replicas (weak scaling, no collective on the data
+path; the photon maps do not exchange).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -624,14 +629,23 @@ def run_ours(args):
 
     sc, cs, w = scenes.workload(args.workload)
     w, cs = override(w, cs, args)
-    ctx = photonmap.Context(local)
+    # the context launches on this stream, and the timing events below are
+    # recorded on it (it is the thread's current torch stream from here on)
+    ctx_st = torch.cuda.Stream()
+    torch.cuda.set_stream(ctx_st)
+    ctx = photonmap.Context(local, stream=ctx_st)
     ctx.set_bvh_builder(args.bvh)
     ctx.set_scene(sc)
     bvh = ctx.bvh_info()
     cam = photonmap.camera_setup(cs.position, cs.direction, cs.up, cs.fov_deg, cs.width, cs.height)
     W, H = cs.width, cs.height
     rgb = torch.empty(W * H * 3, dtype=torch.uint8, device="cuda")
-    host_rgb = torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True)
+    # end to end: two frame buffers, each frame read back to pinned host memory
+    # on a copy stream while the next frame (into the other buffer) runs
+    rgbs = [rgb, torch.empty_like(rgb)]
+    hosts = [torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    copy_st = torch.cuda.Stream()
+    copied = [None, None]
 
     paths = [0]
 
@@ -639,10 +653,18 @@ def run_ours(args):
         # pm_frame: photon pass, grid build and frame in one call (the eye pass
         # runs beside the grid build); same photons and image as
         # trace_photons + build_grid + render
+        b = i % 2 if e2e else 0
+        if e2e and copied[b] is not None:
+            copied[b].synchronize()   # the read-back of this buffer's previous frame has ended
         _, _, paths[0] = ctx.frame(step_seed(w["seed"], rank, i), w["max_bounces"], w["photons"], cam, w["k"],
-                                   w["radius"], w["max_depth"], radiance=False, out_rgb8=rgb)
+                                   w["radius"], w["max_depth"], radiance=False, out_rgb8=rgbs[b])
         if e2e:
-            host_rgb.copy_(rgb, non_blocking=True)
+            copy_st.wait_stream(ctx_st)
+            with torch.cuda.stream(copy_st):
+                hosts[b].copy_(rgbs[b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy_st)
+            copied[b] = ev
 
     for i in range(args.warmup):
         step(i)
