@@ -72,7 +72,7 @@ std::vector<DevBuf*> all_buffers(pm_ctx* ctx) {
     for (auto& m : ctx->maps)
         for (DevBuf* b : {&m.pos, &m.dir, &m.pow, &m.starts, &m.sizes, &m.gpos, &m.gdir, &m.gpow, &m.cid, &m.keys0,
                           &m.keys1, &m.vals0, &m.vals1, &m.hist, &m.scan_ws, &m.small, &m.key_counts,
-                          &m.key_starts, &m.counts2})
+                          &m.key_starts, &m.counts2, &m.rec})
             v.push_back(b);
     return v;
 }
@@ -792,6 +792,8 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     G.built = C.built = false;
     G.n = C.n = 0;
     G.uniform_pow = C.uniform_pow = false;
+    G.has_rec = C.has_rec = false;
+    ENSURE(G.rec, std::max<int64_t>(cg, 1) * 32); ENSURE(C.rec, std::max<int64_t>(cc, 1) * 32);
     ENSURE(G.pos, std::max<int64_t>(cg, 1) * 12); ENSURE(G.dir, std::max<int64_t>(cg, 1) * 12); ENSURE(G.pow, std::max<int64_t>(cg, 1) * 12);
     ENSURE(C.pos, std::max<int64_t>(cc, 1) * 12); ENSURE(C.dir, std::max<int64_t>(cc, 1) * 12); ENSURE(C.pow, std::max<int64_t>(cc, 1) * 12);
     G.built = C.built = false;
@@ -830,8 +832,8 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         for (int a = 0; a < 3; a++) B.power[a] = power[a];
         B.k_begin = ctx->ev[12];
         B.k_end = ctx->ev[13];
-        PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg};
-        PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc};
+        PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg, P<float4>(G.rec)};
+        PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc, P<float4>(C.rec)};
         CK(trace_batch(B, LG, LC, ctx->st));
         ctx->launches += 4;
         uint32_t tot[2] = {0, 0};
@@ -861,6 +863,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     C.n = fc;
     for (MapState* m : {&G, &C}) {   // every photon of a traced map has power intensity / global capacity
         m->uniform_pow = true;
+        m->has_rec = true;
         for (int a = 0; a < 3; a++) m->pow_value[a] = power[a];
     }
     if (out_paths) *out_paths = p0;
@@ -926,6 +929,7 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
     m.n = 0;            // empty until the new list is in place
     m.built = false;
     m.uniform_pow = false;
+    m.has_rec = false;
     ENSURE(m.pos, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.dir, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.pow, std::max<int64_t>(n, 1) * 12);
@@ -990,6 +994,7 @@ int grid_issue(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb, G
     GridBuffers B;
     B.pos = P<float>(m.pos); B.dir = P<float>(m.dir); B.pow = P<float>(m.pow); B.n = n;
     B.uniform_pow = m.uniform_pow;
+    B.rec = m.has_rec ? P<float4>(m.rec) : nullptr;
     for (int a = 0; a < 3; a++) B.pow_value[a] = m.pow_value[a];
     B.cell_starts = P<uint32_t>(m.starts); B.cell_sizes = P<uint32_t>(m.sizes);
     B.gpos = P<float4>(m.gpos); B.gdir = P<float>(m.gdir); B.gpow = P<float>(m.gpow);

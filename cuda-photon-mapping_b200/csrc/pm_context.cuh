@@ -20,6 +20,8 @@ struct DevBuf {
 struct MapState {
     int64_t n = 0;                       // photons in the list
     DevBuf pos, dir, pow;                // traced-order list (3 floats per photon)
+    DevBuf rec;                          // a traced list's (position, direction) records, 32 B per photon
+    bool has_rec = false;                // rec holds the current list
     bool uniform_pow = false;            // every photon of the list has power pow_value (a traced map)
     float pow_value[3] = {0, 0, 0};
     bool built = false;

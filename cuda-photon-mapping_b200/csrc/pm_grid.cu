@@ -351,19 +351,30 @@ k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restri
 }
 
 // pw == nullptr: every photon has power pw0 (a traced map), so the power is
-// written without a random read of the source list
+// written without a random read of the source list.  rec != nullptr: the
+// photon's position and direction are read as one 32-byte record (one DRAM
+// sector) instead of two 12-byte pieces of the position and direction arrays.
 __global__ void k_grid_gather(const uint32_t* __restrict__ order, int64_t n, const float* __restrict__ pos,
-                              const float* __restrict__ dir, const float* __restrict__ pw, float3 pw0,
-                              float4* __restrict__ gpos, float* __restrict__ gdir, float* __restrict__ gpow,
-                              unsigned* status) {
+                              const float* __restrict__ dir, const float4* __restrict__ rec,
+                              const float* __restrict__ pw, float3 pw0, float4* __restrict__ gpos,
+                              float* __restrict__ gdir, float* __restrict__ gpow, unsigned* status) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t s = order[j];
     if ((int64_t)s >= n) { raise_status(status, ST_BAD_INPUT); return; }
-    const float* p = pos + 3 * (int64_t)s;
-    gpos[j] = make_float4(p[0], p[1], p[2], __uint_as_float(s));
-    const float* d = dir + 3 * (int64_t)s;
-    gdir[3 * j] = d[0]; gdir[3 * j + 1] = d[1]; gdir[3 * j + 2] = d[2];
+    float3 pp, dd;
+    if (rec) {
+        const float4 a = __ldg(rec + 2 * (int64_t)s), b = __ldg(rec + 2 * (int64_t)s + 1);
+        pp = make_float3(a.x, a.y, a.z);
+        dd = make_float3(b.x, b.y, b.z);
+    } else {
+        const float* p = pos + 3 * (int64_t)s;
+        const float* d = dir + 3 * (int64_t)s;
+        pp = make_float3(p[0], p[1], p[2]);
+        dd = make_float3(d[0], d[1], d[2]);
+    }
+    gpos[j] = make_float4(pp.x, pp.y, pp.z, __uint_as_float(s));
+    gdir[3 * j] = dd.x; gdir[3 * j + 1] = dd.y; gdir[3 * j + 2] = dd.z;
     float3 w = pw0;
     if (pw) {
         const float* q = pw + 3 * (int64_t)s;
@@ -535,7 +546,7 @@ cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* 
     cudaError_t e = radix_sort_u32(RB, B.cid, nullptr, n, bits, false, nullptr, &order, launches, st);
     if (e != cudaSuccess) return e;
     k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(
-        order, n, B.pos, B.dir, B.uniform_pow ? nullptr : B.pow,
+        order, n, B.pos, B.dir, B.rec, B.uniform_pow ? nullptr : B.pow,
         make_float3(B.pow_value[0], B.pow_value[1], B.pow_value[2]), B.gpos, B.gdir, B.gpow, B.status);
     *launches += 1;
     return cudaGetLastError();

@@ -14,6 +14,7 @@ struct GridBuffers {
     const float* pos;
     const float* dir;
     const float* pow;
+    const float4* rec = nullptr;   // when set: (position, 0), (direction, 0) per photon, gathered as one record
     bool uniform_pow = false;   // every photon has power pow_value: the sorted power is written, not gathered
     float pow_value[3] = {0.f, 0.f, 0.f};
     int64_t n;

@@ -433,11 +433,13 @@ __global__ void k_compact_multi(int64_t total, const int64_t* __restrict__ off, 
 }
 
 // canonical-order append of one batch into the two photon lists
+// (rec lists, when set: each photon's position and direction also as one
+// 32-byte record, which the grid build gathers with one sector read)
 __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
                           const uint32_t* __restrict__ cnt_g, const uint32_t* __restrict__ cnt_c,
                           const uint32_t* __restrict__ scan_g, const uint32_t* __restrict__ scan_c, V3 power,
-                          float* gpos, float* gdir, float* gpow, int64_t gcap, int64_t gfilled,
-                          float* cpos, float* cdir, float* cpow, int64_t ccap, int64_t cfilled) {
+                          float* gpos, float* gdir, float* gpow, int64_t gcap, int64_t gfilled, float4* grec,
+                          float* cpos, float* cdir, float* cpow, int64_t ccap, int64_t cfilled, float4* crec) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= npaths) return;
     int ng = (int)cnt_g[j], nc = (int)cnt_c[j];
@@ -448,17 +450,22 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
         float4 d = stage[2 * o + 1];
         bool caustic = __float_as_int(p.w) == 2;
         float *dp, *dd, *dw;
+        float4* dr;
         int64_t idx;
         if (caustic) {
             if (oc >= ccap) { oc++; continue; }
-            idx = oc++; dp = cpos; dd = cdir; dw = cpow;
+            idx = oc++; dp = cpos; dd = cdir; dw = cpow; dr = crec;
         } else {
             if (og >= gcap) { og++; continue; }
-            idx = og++; dp = gpos; dd = gdir; dw = gpow;
+            idx = og++; dp = gpos; dd = gdir; dw = gpow; dr = grec;
         }
         dp[3 * idx] = p.x; dp[3 * idx + 1] = p.y; dp[3 * idx + 2] = p.z;
         dd[3 * idx] = d.x; dd[3 * idx + 1] = d.y; dd[3 * idx + 2] = d.z;
         dw[3 * idx] = power.x; dw[3 * idx + 1] = power.y; dw[3 * idx + 2] = power.z;
+        if (dr) {
+            dr[2 * idx] = make_float4(p.x, p.y, p.z, 0.f);
+            dr[2 * idx + 1] = make_float4(d.x, d.y, d.z, 0.f);
+        }
     }
 }
 
@@ -537,7 +544,7 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
         return e;
     k_compact<<<(unsigned)((B.npaths + 255) / 256), 256, 0, st>>>(
         B.npaths, B.stage, B.cnt_g, B.cnt_c, B.scan_g, B.scan_c, P.power,
-        G.pos, G.dir, G.pow, G.cap, G.filled, C.pos, C.dir, C.pow, C.cap, C.filled);
+        G.pos, G.dir, G.pow, G.cap, G.filled, G.rec, C.pos, C.dir, C.pow, C.cap, C.filled, C.rec);
     return cudaGetLastError();
 }
 

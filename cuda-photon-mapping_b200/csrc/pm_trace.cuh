@@ -36,6 +36,7 @@ struct PhotonList {
     float* pow;
     int64_t cap;
     int64_t filled;           // photons already in the list before this batch
+    float4* rec = nullptr;    // when set: also (position, 0), (direction, 0) per photon, 32-byte aligned
 };
 
 // ---- several scene instances in one launch (global map only) ----
