@@ -1314,8 +1314,7 @@ int render_finish(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* 
 
 namespace {
 
-// global gather, caustic gather, resolve and the status check of a frame whose requests are counted
-// The gather visits the requests in Morton order of their hit points: 30-bit
+// The gather visits the requests in Morton order of their hit points: 27-bit
 // keys in the scene box, sorted by the library's stable radix sort on stream st.
 int request_order(pm_ctx* ctx, FrameSetup& F, cudaStream_t st) {
     F.ordered = true;
@@ -1331,11 +1330,13 @@ int request_order(pm_ctx* ctx, FrameSetup& F, cudaStream_t st) {
     RadixBuffers RB{{P<uint32_t>(ctx->rq_k0), P<uint32_t>(ctx->rq_k1)}, {P<uint32_t>(ctx->rq_v0), P<uint32_t>(ctx->rq_v1)},
                     P<uint32_t>(ctx->rq_hist), ctx->rq_ws.p, P<unsigned>(ctx->status)};
     int launches = 0;
-    CK(radix_sort_u32(RB, P<uint32_t>(ctx->rq_keys), nullptr, n, 30, false, nullptr, &F.order, &launches, st));
+    CK(radix_sort_u32(RB, P<uint32_t>(ctx->rq_keys), nullptr, n, REQUEST_KEY_BITS, false, nullptr, &F.order, &launches,
+                      st));
     ctx->launches += launches + 1;
     return PM_OK;
 }
 
+// global gather, caustic gather, resolve and the status check of a frame whose requests are counted
 int render_rest(pm_ctx* ctx, const pm_render_opts* o, FrameSetup& F, uint8_t* out_rgb8, float* out_radiance) {
     MapState& G = ctx->maps[PM_MAP_GLOBAL];
     GatherQueries Q{};

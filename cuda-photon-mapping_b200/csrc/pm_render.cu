@@ -399,9 +399,9 @@ __global__ void k_request_keys(const float4* __restrict__ a, int64_t n, float lx
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = a[i];
-    const uint32_t x = (uint32_t)min(max((int)((p.x - lx) * sx), 0), 1023);
-    const uint32_t y = (uint32_t)min(max((int)((p.y - ly) * sy), 0), 1023);
-    const uint32_t z = (uint32_t)min(max((int)((p.z - lz) * sz), 0), 1023);
+    const uint32_t x = (uint32_t)min(max((int)((p.x - lx) * sx), 0), 511);
+    const uint32_t y = (uint32_t)min(max((int)((p.y - ly) * sy), 0), 511);
+    const uint32_t z = (uint32_t)min(max((int)((p.z - lz) * sz), 0), 511);
     keys[i] = (spread10r(x) << 2) | (spread10r(y) << 1) | spread10r(z);
 }
 }  // namespace
@@ -411,7 +411,7 @@ cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32
     float sc[3];
     for (int k = 0; k < 3; k++) {
         const float ext = aabb[3 + k] - aabb[k];
-        sc[k] = ext > 0.f ? 1024.f / ext : 0.f;
+        sc[k] = ext > 0.f ? 512.f / ext : 0.f;
     }
     k_request_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, n, aabb[0], aabb[1], aabb[2], sc[0], sc[1], sc[2],
                                                                  keys);

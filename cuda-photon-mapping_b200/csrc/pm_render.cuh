@@ -34,7 +34,9 @@ struct Requests {
 // the pixel blocks); pixels of the other blocks get no requests written.
 cudaError_t eye_pass(const DevScene& S, const CameraDev& cam, int max_depth, Requests R, unsigned* status,
                      cudaStream_t st, const int* block_order = nullptr, int64_t nblocks = -1);
-// 30-bit Morton code of each request's hit point in the box aabb (10 bits per axis)
+// 27-bit Morton code of each request's hit point in the box aabb (9 bits per
+// axis: three radix passes of 9 bits)
+constexpr int REQUEST_KEY_BITS = 27;
 cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32_t* keys, cudaStream_t st);
 // pixel blocks of the eye pass (EYE_THREADS consecutive pixels each)
 int64_t eye_blocks(int64_t npx);
