@@ -691,7 +691,7 @@ int pm_set_scene(pm_ctx* ctx, const pm_scene_desc* sd) {
         release(ctx->bvh_scratch);
         if (int rc = check_status(ctx, "device BVH build")) return rc;
     }
-    ENSURE(ctx->tri_leaf, 80 * (size_t)T);
+    ENSURE(ctx->tri_leaf, 64 * (size_t)T);
     CK(bvh_leaf_records(P<float4>(ctx->tri), P<int>(ctx->prim), T, P<float4>(ctx->tri_leaf), ctx->st));
     ctx->launches += 1;
     CK(cudaMemcpyAsync(ctx->maabb.p, maabb.data(), maabb.size() * 4, cudaMemcpyHostToDevice, ctx->st));

@@ -280,10 +280,10 @@ __global__ void k_leaf_records(const float4* __restrict__ tri, const int* __rest
     const int t = prim[j];
     if (t < 0 || t >= n) return;
     const float4* src = tri + 5 * (size_t)t;
-    float4* dst = out + 5 * (size_t)j;
-    dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; dst[3] = src[3];
+    float4* dst = out + 4 * (size_t)j;
+    dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2];
     const float4 q4 = src[4];
-    dst[4] = make_float4(q4.x, q4.y, q4.z, __int_as_float(t));
+    dst[3] = make_float4(q4.x, q4.y, q4.z, __int_as_float(t));
 }
 
 }  // namespace

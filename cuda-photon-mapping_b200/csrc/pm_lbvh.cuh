@@ -19,8 +19,9 @@ inline int64_t lbvh_node_count(int ntri) { return ntri > 1 ? (int64_t)ntri - 1 :
 cudaError_t lbvh_build(const float* tri_pos, int ntri, float pad, float4* nodes, int* prim, void* scratch,
                        unsigned* status, int* launches, cudaStream_t st);
 
-// Triangle records (5 float4 each) in leaf order: out[j] = tri[prim[j]] with
-// the triangle's index in the w of its fifth float4.
+// Triangle records in leaf order, 4 float4 each: out[j] = the first three
+// float4 of tri[prim[j]] and its fifth (the normal) with the triangle's index
+// in w (the fourth, v0 - v2, is formed by the test).
 cudaError_t bvh_leaf_records(const float4* tri, const int* prim, int ntri, float4* out, cudaStream_t st);
 
 }  // namespace pm

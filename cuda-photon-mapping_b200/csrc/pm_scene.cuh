@@ -24,7 +24,10 @@ namespace pm {
 
 // Triangle record: 5 float4 = 80 bytes
 //   q0 = (v0, n.v0)   q1 = (v1 - v0, 1/(n.n))   q2 = (v2, model bits)
-//   q3 = (v0 - v2, 0) q4 = (n, 0 / in tri_leaf: the triangle index bits)   n = cross(v1 - v0, v2 - v0)
+//   q3 = (v0 - v2, 0) q4 = (n, 0)   n = cross(v1 - v0, v2 - v0)
+// Leaf-ordered record (tri_leaf): 4 float4 = 64 bytes, one aligned line:
+//   q0, q1, q2 as above, (n, the triangle index bits); the test forms v0 - v2
+//   from q0 and q2 (the same float subtraction that made q3)
 struct DevScene {
     const float4* tri;        // 5 per triangle
     const float* tri_pos;     // 9 per triangle (vertex positions, as given)
@@ -32,8 +35,8 @@ struct DevScene {
     const float* tri_diffuse; // 3 per triangle or null
     const float4* nodes;      // 4 per interior node: both children's (lo, ref), (hi, -)
     const int* prim;          // leaf triangle indices
-    const float4* tri_leaf;   // the triangle records again in leaf order (record j = triangle prim[j],
-                              // its index in q4.w), so a leaf's triangles are contiguous
+    const float4* tri_leaf;   // 4 per triangle in leaf order (record j = triangle prim[j], its index
+                              // in the last float4's w), so a leaf's triangles are contiguous
     const float* maabb;       // 6 per model (min xyz, max xyz)
     const float* mats;        // 12 per model
     const float* ca;          // critical angle table: (n1, n2, cos) triples
@@ -96,14 +99,14 @@ struct Hit {
 };
 
 // edge-function test with precomputed terms on a leaf-ordered triangle record
-// (q4.w its triangle index, q2.w its model); returns false when the triangle
+// (T[3].w its triangle index, q2.w its model); returns false when the triangle
 // belongs to a model below min_model or cannot be a better (t, index)
 // candidate than (best_t, best_tri).  The record's index and model come with
 // the 16-byte loads the test makes anyway, the model only once the plane test
 // has passed.
 __device__ __forceinline__ bool tri_test(const float4* __restrict__ T, V3 o, V3 d, float best_t, int best_tri,
                                          int min_model, float& t_out, V3& uvw, int& tri_out, int& m_out) {
-    const float4 q0 = __ldg(T), q4 = __ldg(T + 4);
+    const float4 q0 = __ldg(T), q4 = __ldg(T + 3);
     const int tri = __float_as_int(q4.w);
     V3 n = xyz(q4);
     float ndd = vdot(n, d);
@@ -111,14 +114,14 @@ __device__ __forceinline__ bool tri_test(const float4* __restrict__ T, V3 o, V3 
     float t = (q0.w - vdot(n, o)) / ndd;
     if (t < 0) return false;
     if (t > best_t || (t == best_t && tri > best_tri)) return false;
-    const float4 q1 = __ldg(T + 1), q2 = __ldg(T + 2), q3 = __ldg(T + 3);
+    const float4 q1 = __ldg(T + 1), q2 = __ldg(T + 2);
     const int m = __float_as_int(q2.w);
     if (m < min_model) return false;
     V3 v0 = xyz(q0);
     V3 P = vadd(o, vscale(d, t));
     float w = vdot(n, vcross(xyz(q1), vsub(P, v0)));
     if (w < 0) return false;
-    float v = vdot(n, vcross(xyz(q3), vsub(P, xyz(q2))));
+    float v = vdot(n, vcross(vsub(v0, xyz(q2)), vsub(P, xyz(q2))));
     if (v < 0) return false;
     w = w * q1.w;
     v = v * q1.w;
@@ -269,7 +272,7 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
         const int first = packed >> 8, count = packed & 255;
         work.tris(count);
         for (int i = 0; i < count; i++) {
-            const float4* Q = S.tri_leaf + 5 * (size_t)(first + i);
+            const float4* Q = S.tri_leaf + 4 * (size_t)(first + i);
             float t; V3 uvw; int tri, m;
             if (!tri_test(Q, o, d, T.best_t, T.best_tri, T.min_model, t, uvw, tri, m)) continue;
             const bool zero = t == 0.0f;
