@@ -23,7 +23,8 @@
 // append the survivors' 64-bit keys (distance bits << 32 | source id;
 // non-negative float bits order like the floats, so integer order is the
 // lexicographic order) to a per-warp shared-memory store by ballot, counting
-// each in a 256-bin histogram of distance over [0, r].  After each shell the
+// each in a 64-bin histogram of distance over [0, r] (over [0, g] once the
+// first ring's density guess g bounds the stored distances).  After each shell the
 // histogram bounds the k-th distance (the upper edge of the bin where the
 // running count reaches k).  When the store fills, and at the end, the exact
 // k-th key is found from the histogram: the keys of its bin (a handful) are
@@ -42,14 +43,19 @@ constexpr int WARPS = 8;   // queries per block
 
 constexpr int QCAP = 64;   // queued sub-cells per warp
 
-constexpr int DBINS = 256;   // distance histogram bins over [0, r]
+// distance histogram bins over [0, r], or over [0, g] once the first ring's
+// guess g is set: 64 for the frame's gather (its queries nearly all take the
+// guess), 256 for the batch's (many of its queries take none, and 64 bins
+// over [0, r] leave too many keys in the k-th bin)
+constexpr int GATHER_BINS = 64;
+constexpr int MULTI_BINS = 256;
 
-template <int UCAP>
+template <int UCAP, int NB>
 struct WarpStore {
     unsigned long long key[UCAP];
     uint32_t slot[UCAP];
     uint32_t hist[256];   // radix-select histogram; doubles as 32 x u64 scratch
-    uint32_t dh[DBINS];   // distance histogram of the keys in the store
+    uint32_t dh[NB];      // distance histogram of the keys in the store
     unsigned long long sel[32];
     uint32_t qa[QCAP];    // queued sub-cells: first photon, photon count
     uint32_t qc[QCAP];
@@ -83,8 +89,8 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, 
 // differ are skipped, each round histograms the next (up to) 8 bits of the keys
 // still in play (lanes with equal digits add once, __match_any_sync), and the
 // round that leaves <= 32 keys finishes with a 32-lane bitonic sort.
-template <int UCAP>
-__device__ unsigned long long select_kth(WarpStore<UCAP>& U, int n, int need, int lane) {
+template <int UCAP, int NB>
+__device__ unsigned long long select_kth(WarpStore<UCAP, NB>& U, int n, int need, int lane) {
     unsigned long long* scratch = reinterpret_cast<unsigned long long*>(U.hist);
     const unsigned long long k0 = U.key[0];
     unsigned long long diff = 0ull;
@@ -163,8 +169,8 @@ __device__ unsigned long long select_kth(WarpStore<UCAP>& U, int n, int need, in
     }
 }
 
-template <int UCAP>
-__device__ __forceinline__ unsigned long long warp_max_key(const WarpStore<UCAP>& U, int n, int lane) {
+template <int UCAP, int NB>
+__device__ __forceinline__ unsigned long long warp_max_key(const WarpStore<UCAP, NB>& U, int n, int lane) {
     unsigned long long m = 0ull;
     for (int i = lane; i < n; i += 32) m = U.key[i] > m ? U.key[i] : m;
 #pragma unroll
@@ -229,10 +235,10 @@ __device__ __forceinline__ void shell_member(int t, int R, int side, float inv_s
     dy = y - R;
 }
 
-template <int UCAP>
+template <int UCAP, int NB>
 struct WarpWalk {
     const GatherGrid& G;
-    WarpStore<UCAP>& U;
+    WarpStore<UCAP, NB>& U;
     V3 q;
     float r;
     int k, lane;
@@ -240,15 +246,15 @@ struct WarpWalk {
     int qn;                   // queued sub-cells
     unsigned long long T;     // a candidate enters when its key < T
     float lim, lim2;          // distance bound for pruning; squared pre-filter bound
-    float bscale;             // DBINS / r: distance histogram bin of d = min(DBINS - 1, (int)(d * bscale))
+    float bscale;             // NB / (r or g): distance histogram bin of d = min(NB - 1, (int)(d * bscale))
     bool guessed;             // the first ring ran with a density guess of the bound
     bool failed;              // ... and found fewer than k photons within it: walk again without
 
-    __device__ WarpWalk(const GatherGrid& g, WarpStore<UCAP>& u, V3 qq, float rr, int kk, int ln)
+    __device__ WarpWalk(const GatherGrid& g, WarpStore<UCAP, NB>& u, V3 qq, float rr, int kk, int ln)
         : G(g), U(u), q(qq), r(rr), k(kk), lane(ln), n(0), qn(0), T(~0ull), lim(rr), lim2(rr * rr * 1.000001f),
-          bscale((float)DBINS / rr), guessed(false), failed(false) {
+          bscale((float)NB / rr), guessed(false), failed(false) {
 #pragma unroll
-        for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+        for (int b = 0; b < NB / 32; b++) U.dh[b * 32 + lane] = 0u;
         __syncwarp();
     }
 
@@ -259,10 +265,11 @@ struct WarpWalk {
         T = ~0ull;
         lim = r;
         lim2 = r * r * 1.000001f;
+        bscale = (float)NB / r;
         guessed = failed = false;
         __syncwarp();
 #pragma unroll
-        for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+        for (int b = 0; b < NB / 32; b++) U.dh[b * 32 + lane] = 0u;
         __syncwarp();
     }
 
@@ -287,22 +294,23 @@ struct WarpWalk {
             lim = g;
             lim2 = g * g * 1.000001f;
             guessed = true;
+            bscale = (float)NB / g;   // no candidate is stored yet: the histogram spans [0, g] from here on
             const float L = g * m;
             if (gap2 > L * L) b = a;
         }
     }
 
     __device__ __forceinline__ uint32_t bin_of(float d) const {
-        return (uint32_t)min((int)(d * bscale), DBINS - 1);   // non-decreasing in d
+        return (uint32_t)min((int)(d * bscale), NB - 1);   // non-decreasing in d
     }
 
     // The k-th smallest key of the store (n > k).  The distance histogram
     // locates the bin holding it; the keys of that bin (normally a handful)
     // are sorted by one warp, else the radix select runs over the store.
     __device__ unsigned long long kth_key() {
-        uint32_t c[DBINS / 32], sum = 0;
+        uint32_t c[NB / 32], sum = 0;
 #pragma unroll
-        for (int b = 0; b < DBINS / 32; b++) { c[b] = U.dh[(DBINS / 32) * lane + b]; sum += c[b]; }
+        for (int b = 0; b < NB / 32; b++) { c[b] = U.dh[(NB / 32) * lane + b]; sum += c[b]; }
         uint32_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -316,8 +324,8 @@ struct WarpWalk {
         if (lane == owner) {
             uint32_t run = excl;
 #pragma unroll
-            for (int b = 0; b < DBINS / 32; b++) {
-                if (cnt == 0 && (uint32_t)k <= run + c[b]) { bin = (DBINS / 32) * lane + b; before = run; cnt = c[b]; }
+            for (int b = 0; b < NB / 32; b++) {
+                if (cnt == 0 && (uint32_t)k <= run + c[b]) { bin = (NB / 32) * lane + b; before = run; cnt = c[b]; }
                 run += c[b];
             }
         }
@@ -349,9 +357,9 @@ struct WarpWalk {
     // smallest distance lies in the bin where the running count reaches k, so
     // the bin's upper edge (with a margin over the rounding of d * bscale) bounds it.
     __device__ void bound() {
-        uint32_t c[DBINS / 32], sum = 0;
+        uint32_t c[NB / 32], sum = 0;
 #pragma unroll
-        for (int b = 0; b < DBINS / 32; b++) { c[b] = U.dh[(DBINS / 32) * lane + b]; sum += c[b]; }
+        for (int b = 0; b < NB / 32; b++) { c[b] = U.dh[(NB / 32) * lane + b]; sum += c[b]; }
         uint32_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -367,13 +375,13 @@ struct WarpWalk {
             uint32_t run = excl;
             bool found = false;
 #pragma unroll
-            for (int b = 0; b < DBINS / 32; b++) {
-                if (!found && (uint32_t)k <= run + c[b]) { bin = (DBINS / 32) * lane + b; found = true; }
+            for (int b = 0; b < NB / 32; b++) {
+                if (!found && (uint32_t)k <= run + c[b]) { bin = (NB / 32) * lane + b; found = true; }
                 run += c[b];
             }
         }
         bin = __shfl_sync(0xffffffffu, bin, owner);
-        const float edge = (float)(bin + 1) * (r / (float)DBINS) * (1.f + 1e-5f);
+        const float edge = (float)(bin + 1) / bscale * (1.f + 1e-5f);
         if (edge < lim) {
             lim = edge;
             lim2 = lim * lim * 1.000001f;
@@ -406,7 +414,7 @@ struct WarpWalk {
             if (!last) {
                 // the histogram counts the store's keys again
 #pragma unroll
-                for (int b = 0; b < DBINS / 32; b++) U.dh[b * 32 + lane] = 0u;
+                for (int b = 0; b < NB / 32; b++) U.dh[b * 32 + lane] = 0u;
                 __syncwarp();
                 for (int i = lane; i < n; i += 32) atomicAdd(&U.dh[bin_of(__uint_as_float((uint32_t)(U.key[i] >> 32)))], 1u);
             }
@@ -639,10 +647,10 @@ struct WarpWalk {
 };
 
 // one query (one warp): the k nearest photons within r of q and the estimate
-template <int UCAP>
-__device__ __forceinline__ void gather_query(const GatherGrid& G, WarpStore<UCAP>& U, int64_t i, V3 q, V3 nrm,
+template <int UCAP, int NB>
+__device__ __forceinline__ void gather_query(const GatherGrid& G, WarpStore<UCAP, NB>& U, int64_t i, V3 q, V3 nrm,
                                              float r, int k, int require_full, const GatherOut& O, int lane) {
-    WarpWalk<UCAP> W(G, U, q, r, k, lane);
+    WarpWalk<UCAP, NB> W(G, U, q, r, k, lane);
     int hx, hy, hz, sx, sy, sz;
     locate(q.x, G.mn[0], G.cell, G.gx, G.S, hx, sx);
     locate(q.y, G.mn[1], G.cell, G.gy, G.S, hy, sy);
@@ -743,7 +751,7 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
     const int64_t qi = (int64_t)blockIdx.x * WARPS + warp;
     if (qi >= Q.n) return;
     const int64_t i = Q.idx ? (int64_t)Q.idx[qi] : qi;
-    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
+    WarpStore<UCAP, GATHER_BINS>& U = reinterpret_cast<WarpStore<UCAP, GATHER_BINS>*>(smem_raw)[warp];
     V3 q, nrm;
     bool active = true;
     if (Q.pos3) {
@@ -759,7 +767,7 @@ k_gather(GatherGrid G, GatherQueries Q, float r, int k, int require_full, Gather
         gather_zero(i, k, O, lane);
         return;
     }
-    gather_query<UCAP>(G, U, i, q, nrm, r, k, require_full, O, lane);
+    gather_query<UCAP, GATHER_BINS>(G, U, i, q, nrm, r, k, require_full, O, lane);
 }
 
 // Listed queries, persistent: warps take list positions from *queue until
@@ -772,7 +780,7 @@ k_gather_listed(GatherGrid G, GatherQueries Q, const unsigned long long* __restr
                 unsigned long long* __restrict__ queue, float r, int k, GatherOut O) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
+    WarpStore<UCAP, GATHER_BINS>& U = reinterpret_cast<WarpStore<UCAP, GATHER_BINS>*>(smem_raw)[warp];
     const int64_t n = (int64_t)min(*n_dev, (unsigned long long)Q.n);
     while (true) {
         unsigned long long t = 0;
@@ -785,7 +793,7 @@ k_gather_listed(GatherGrid G, GatherQueries Q, const unsigned long long* __restr
             gather_zero(i, k, O, lane);
             continue;
         }
-        gather_query<UCAP>(G, U, i, xyz(a), xyz(b), r, k, 0, O, lane);
+        gather_query<UCAP, GATHER_BINS>(G, U, i, xyz(a), xyz(b), r, k, 0, O, lane);
         __syncwarp();
     }
 }
@@ -794,7 +802,7 @@ template <int UCAP>
 cudaError_t launch_listed(const GatherGrid& G, const GatherQueries& Q, const unsigned long long* n_dev,
                           unsigned long long* queue, float r, int k, const GatherOut& O, int sm_count,
                           cudaStream_t st) {
-    const size_t smem = sizeof(WarpStore<UCAP>) * WARPS;
+    const size_t smem = sizeof(WarpStore<UCAP, GATHER_BINS>) * WARPS;
     cudaError_t e = cudaFuncSetAttribute(k_gather_listed<UCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -831,7 +839,7 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
                unsigned long long* __restrict__ queue, int cls, GatherOut O) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpStore<UCAP>& U = reinterpret_cast<WarpStore<UCAP>*>(smem_raw)[warp];
+    WarpStore<UCAP, MULTI_BINS>& U = reinterpret_cast<WarpStore<UCAP, MULTI_BINS>*>(smem_raw)[warp];
     const int64_t n = (int64_t)min(*n_req, (unsigned long long)Q.n);
     // the instance of the last request and its pixel range: consecutive
     // requests mostly belong to one instance (the eye pass writes them in
@@ -859,7 +867,7 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
                 continue;
             }
             const GatherGrid G = T.G;
-            gather_query<UCAP>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
+            gather_query<UCAP, MULTI_BINS>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
             __syncwarp();
         }
     }
@@ -868,7 +876,7 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
 template <int UCAP>
 cudaError_t launch(const GatherGrid& G, const GatherQueries& Q, float r, int k, int require_full, const GatherOut& O,
                    cudaStream_t st) {
-    const size_t smem = sizeof(WarpStore<UCAP>) * WARPS;
+    const size_t smem = sizeof(WarpStore<UCAP, GATHER_BINS>) * WARPS;
     cudaError_t e = cudaFuncSetAttribute(k_gather<UCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     unsigned blocks = (unsigned)((Q.n + WARPS - 1) / WARPS);
@@ -882,7 +890,7 @@ template <int UCAP, int NW>
 cudaError_t launch_multi(const GatherInstDev* tab, const int64_t* px_off, int ninst, const GatherQueries& Q,
                          const float4* rec_c, const unsigned long long* n_req, unsigned long long* queue, int cls,
                          const GatherOut& O, int sm_count, cudaStream_t st) {
-    const size_t smem = sizeof(WarpStore<UCAP>) * NW;
+    const size_t smem = sizeof(WarpStore<UCAP, MULTI_BINS>) * NW;
     cudaError_t e = cudaFuncSetAttribute(k_gather_multi<UCAP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
