@@ -479,13 +479,17 @@ struct WarpWalk {
             float4 p[NL];
 #pragma unroll
             for (int u = 0; u < NL; u++) {
-                const uint32_t o = base + 32 * u + lane;
-                int mm = 0;   // the last queued sub-cell whose first list entry is <= o
-#pragma unroll
-                for (int st = 16; st > 0; st >>= 1) {
-                    const uint32_t e = __shfl_sync(0xffffffffu, excl, mm + st);
-                    if (e <= o) mm += st;
-                }
+                const uint32_t b0 = base + 32 * u, o = b0 + lane;
+                // the last queued sub-cell whose first list entry is <= o: the
+                // sub-cells that start before this round, plus those starting in
+                // it at or before this lane (starts are distinct: queued
+                // sub-cells are non-empty)
+                const bool valid = lane < cnt;
+                const uint32_t starts =
+                    __reduce_or_sync(0xffffffffu, valid && excl >= b0 && excl - b0 < 32u ? 1u << (excl - b0) : 0u);
+                const int before = __popc(__ballot_sync(0xffffffffu, valid && excl < b0));
+                const uint32_t upto = lane == 31 ? 0xffffffffu : (2u << lane) - 1u;
+                const int mm = before + __popc(starts & upto) - 1;
                 j[u] = __shfl_sync(0xffffffffu, a, mm) + (o - __shfl_sync(0xffffffffu, excl, mm));
                 v[u] = o < total;
             }
