@@ -320,20 +320,26 @@ def batched_frames(args, rank):
         c.set_scene(d["scene"])
         ctxs.append(c)
 
+    dev_ms = [0.0]
+
     def sequential(f):
         for c, d in zip(ctxs, insts):
             c.trace_photons(d["seed"] + f, d["max_bounces"], d["photons"])
             c.build_grid(photonmap.PM_MAP_GLOBAL)
             c.render(d["camera"], d["k"], d["radius"], d["max_depth"], radiance=False)
+            st = c.stage_times()
+            dev_ms[0] += st["trace_ms"] + st["grid_ms"] + st["eye_ms"] + st["gather_ms"] + st["resolve_ms"]
         for c in ctxs:
             c.sync()
 
     sequential(0)
     torch.cuda.synchronize()
+    dev_ms[0] = 0.0
     t0 = time.perf_counter()
     for f in range(K):
         sequential(2 + f)
     ms_seq = (time.perf_counter() - t0) * 1000 / K
+    ms_seq_dev = dev_ms[0] / K
     for c in ctxs:
         c.close()
     photons = sum(d["photons"] for d in insts)
@@ -342,7 +348,12 @@ def batched_frames(args, rank):
     return {"instances": len(insts), "photons_per_frame": photons, "pixels_per_frame": pixels,
             "ms_per_frame": ms, "mphotons_per_s": photons / (ms * 1e-3) / 1e6,
             "ms_per_frame_wall": ms_wall, "ms_per_frame_sequential_api": ms_seq,
-            "speedup_vs_sequential": ms_seq / ms_wall, "launches_per_frame": info["launches_per_frame"],
+            "speedup_vs_sequential": ms_seq / ms_wall,
+            "ms_per_frame_sequential_device": ms_seq_dev, "speedup_vs_sequential_device": ms_seq_dev / ms,
+            "sequential": "the instances one after another through the single-instance API, 64 contexts, host "
+                          "clock (host-synchronous calls: depends on the host); _device: the sum of their stage "
+                          "times (CUDA events), against the batch's device time",
+            "launches_per_frame": info["launches_per_frame"],
             "graph": bool(info["graph"]), "autotuned": {"desired_per_cell": info["desired_per_cell"],
                                                         "gather_warps": info["gather_warps"],
                                                         "gather_guess": info["gather_guess"],

@@ -575,7 +575,14 @@ struct WarpWalk {
                 float gap2 = 0.f;
                 if (t < total) {
                     int dx = 0, dy = 0, dz = 0;
-                    if (t < shell) shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
+                    if (R == 1) {   // ring 1 with the query's own sub-cell: the 3x3x3 block
+                        const int t3 = t / 3, t9 = t3 / 3;
+                        dx = t - 3 * t3 - 1;
+                        dy = t3 - 3 * t9 - 1;
+                        dz = t9 - 1;
+                    } else if (t < shell) {
+                        shell_member(t, R, side, inv_side, inv_per, dx, dy, dz);
+                    }
                     const int X = X0 + dx, Y = Y0 + dy, Z = Z0 + dz;
                     if (X >= lx && X <= hx && Y >= ly && Y <= hy && Z >= lz && Z <= hz) {
                         float ax = axis_gap(q.x, G.mn[0] + X * sc - pad, G.mn[0] + (X + 1) * sc + pad, X == 0, X == GX);
