@@ -40,7 +40,6 @@ namespace pm {
 namespace {
 
 constexpr int TILE = 128;
-constexpr int THREADS = 128;
 constexpr int WAIT_LIMIT = 1 << 24;        // polls of an mbarrier before giving up
 constexpr uint32_t TMEM_COLS_TRAIN = 512;
 constexpr uint32_t TMEM_COLS_INFER = 256;   // 64 per warpgroup
