@@ -1456,13 +1456,15 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     MlpInputs in{};
     in.n = F.nreq; in.rec_pos = F.R.a; in.rec_nrm = F.R.b; in.flag_mask = 1u;
     CK(mlp_infer(cache_net(ctx), in, P<float>(ctx->est_mlp), P<unsigned>(ctx->status), ctx->sm_count, ctx->st));
-    // exact gathers at the probes; tiles whose cache error is too large fall back
-    CK(learned_probes(F.cd, F.R, T, Pn, P<float4>(ctx->probe_pos), P<float4>(ctx->probe_nrm), P<uint32_t>(ctx->probe_req),
-                      ctx->st));
+    // exact gathers at the probes (their pixels' primary hits, traced from the
+    // camera); tiles whose cache error is too large fall back
+    CK(probe_hits(dev_scene(ctx), F.cd, T, Pn, P<float4>(ctx->probe_pos), P<float4>(ctx->probe_nrm), ctx->st));
     GatherQueries PQ{};
     PQ.n = nprobe; PQ.pos4 = P<float4>(ctx->probe_pos); PQ.nrm4 = P<float4>(ctx->probe_nrm); PQ.flag_mask = 1u;
     GatherOut PO{P<float>(ctx->probe_est), nullptr, nullptr, nullptr};
     CK(gather(grid_of(G, G), PQ, o->r_global, o->k_global, 0, PO, P<unsigned>(ctx->status), ctx->st));
+    CK(learned_probe_req(F.cd, F.R, T, Pn, P<float4>(ctx->probe_pos), P<float4>(ctx->probe_nrm),
+                         P<uint32_t>(ctx->probe_req), P<unsigned>(ctx->status), ctx->st));
     CK(cudaMemsetAsync(ctx->learned_counts.p, 0, 32, ctx->st));
     CK(learned_select(F.cd, F.R, F.nreq, nullptr, T, Pn, P<uint32_t>(ctx->probe_req), P<float>(ctx->probe_est),
                       P<float>(ctx->est_mlp), lo->max_rel_err, lo->noise_z, P<uint8_t>(ctx->tile_flag),
@@ -1477,7 +1479,7 @@ int pm_render_learned(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
     CK(gather_listed(grid_of(G, G), Q, counts + 1, counts + 2, o->r_global, o->k_global, OF, ctx->sm_count, ctx->st));
     CK(learned_merge(F.R, F.nreq, nullptr, P<float>(ctx->est_mlp), P<float>(ctx->est_fb), P<float>(ctx->est_g),
                      ctx->sm_count, ctx->st));
-    ctx->launches += (F.nreq > 0 ? 1 : 0) + 1 + 1 + 1 + (F.nreq > 0 ? 1 : 0) + 1 + (F.nreq > 0 ? 1 : 0);
+    ctx->launches += (F.nreq > 0 ? 1 : 0) + 1 + 1 + 1 + 1 + (F.nreq > 0 ? 1 : 0) + 1 + (F.nreq > 0 ? 1 : 0);
     if (int rc = render_finish(ctx, o, F, out_rgb8, out_radiance)) return rc;
     if (out_stats) {
         unsigned long long cnt[2] = {0, 0};

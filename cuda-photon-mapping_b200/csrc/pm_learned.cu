@@ -16,15 +16,13 @@ namespace pm {
 namespace {
 
 // probe position k of P inside a tile of edge T: a ceil(sqrt(P)) grid of cell centres
-__device__ __forceinline__ void probe_xy(int k, int P, int T, int& dx, int& dy) {
-    int g = 1;
-    while (g * g < P) g++;
-    dx = ((k % g) * 2 + 1) * T / (2 * g);
-    dy = ((k / g) * 2 + 1) * T / (2 * g);
-}
-
-__global__ void k_probe_select(CameraDev cam, Requests R, int tile, int P, int tiles_x, int64_t ntiles,
-                               float4* __restrict__ ppos, float4* __restrict__ pnrm, uint32_t* __restrict__ preq) {
+// Each probe's request: the first request of its pixel, which the probe pass
+// (probe_hits) traced from the camera with the eye pass's own device code;
+// the two records must agree bit for bit, and a probe whose record differs
+// from its request raises ST_BAD_INPUT (its request index is then dropped).
+__global__ void k_probe_req(CameraDev cam, Requests R, int tile, int P, int tiles_x, int64_t ntiles,
+                            const float4* __restrict__ ppos, const float4* __restrict__ pnrm,
+                            uint32_t* __restrict__ preq, unsigned* status) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= ntiles * P) return;
     const int64_t t = s / P;
@@ -32,22 +30,28 @@ __global__ void k_probe_select(CameraDev cam, Requests R, int tile, int P, int t
     int dx, dy;
     probe_xy(k, P, tile, dx, dy);
     const int x = (int)(t % tiles_x) * tile + dx, y = (int)(t / tiles_x) * tile + dy;
-    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = make_float4(0.f, 0.f, 1.f, 0.f);
     uint32_t q = 0xffffffffu;
     if (x < cam.W && y < cam.H) {
         const int64_t px = (int64_t)y * cam.W + x;
         if (R.px_count[px] > 0) {
             const uint32_t r = R.px_base[px];
-            const float4 rb = R.b[r];
-            if (__float_as_uint(rb.w) & 1u) {
-                a = R.a[r];
-                b = make_float4(rb.x, rb.y, rb.z, __uint_as_float(1u));
-                q = r;
-            }
+            if (__float_as_uint(R.b[r].w) & 1u) q = r;
         }
     }
-    ppos[s] = a;
-    pnrm[s] = b;
+    const float4 pa = ppos[s], pb = pnrm[s];
+    const bool probe = (__float_as_uint(pb.w) & 1u) != 0u;
+    bool same = probe == (q != 0xffffffffu);
+    if (same && probe) {
+        const float4 ra = R.a[q], rb = R.b[q];
+        same = __float_as_uint(pa.x) == __float_as_uint(ra.x) && __float_as_uint(pa.y) == __float_as_uint(ra.y) &&
+               __float_as_uint(pa.z) == __float_as_uint(ra.z) && __float_as_uint(pa.w) == __float_as_uint(ra.w) &&
+               __float_as_uint(pb.x) == __float_as_uint(rb.x) && __float_as_uint(pb.y) == __float_as_uint(rb.y) &&
+               __float_as_uint(pb.z) == __float_as_uint(rb.z);
+    }
+    if (!same) {
+        raise_status(status, ST_BAD_INPUT);
+        q = 0xffffffffu;
+    }
     preq[s] = q;
 }
 
@@ -151,11 +155,11 @@ inline unsigned req_blocks(int64_t cap, bool on_device, int sm_count) {
 
 }  // namespace
 
-cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, int P, float4* ppos, float4* pnrm,
-                           uint32_t* preq, cudaStream_t st) {
+cudaError_t learned_probe_req(const CameraDev& cam, const Requests& R, int tile, int P, const float4* ppos,
+                              const float4* pnrm, uint32_t* preq, unsigned* status, cudaStream_t st) {
     const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
     const int64_t ntiles = (int64_t)tx * ty;
-    k_probe_select<<<blocks(ntiles * P, 256), 256, 0, st>>>(cam, R, tile, P, tx, ntiles, ppos, pnrm, preq);
+    k_probe_req<<<blocks(ntiles * P, 256), 256, 0, st>>>(cam, R, tile, P, tx, ntiles, ppos, pnrm, preq, status);
     return cudaGetLastError();
 }
 

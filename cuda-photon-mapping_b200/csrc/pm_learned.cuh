@@ -8,11 +8,13 @@ namespace pm {
 
 constexpr uint32_t LEARNED_FALLBACK = 4u;   // request flag: answered by the exact gather
 
-// P probe records per tile of edge `tile` (float4 position / normal records with
-// flag 1 when the probe pixel's first request needs the global estimate, else 0)
-// and the request each probe stands for (UINT32_MAX: none).
-cudaError_t learned_probes(const CameraDev& cam, const Requests& R, int tile, int P, float4* ppos, float4* pnrm,
-                           uint32_t* preq, cudaStream_t st);
+// The request each of the P probes per tile of edge `tile` stands for (its
+// pixel's first request when that needs the global estimate, else
+// UINT32_MAX), after the eye pass; ppos / pnrm are the probe records of
+// probe_hits (pm_render.cuh), checked against the requests bit for bit
+// (a mismatch raises ST_BAD_INPUT in status).
+cudaError_t learned_probe_req(const CameraDev& cam, const Requests& R, int tile, int P, const float4* ppos,
+                              const float4* pnrm, uint32_t* preq, unsigned* status, cudaStream_t st);
 
 // Tile flags from the probes' exact and cached estimates (bias above
 // max_rel_err plus noise_z standard errors), then flag bit

@@ -54,10 +54,11 @@ struct pm_learned_graph {
     int launches_per_frame = 0;
     // the context as the captured launches saw it
     uint64_t generation = 0, buffers = 0;
-    // training runs on a second stream beside the eye pass and the probe
-    // gathers (it needs neither; inference waits for it)
-    cudaStream_t side = nullptr, inf = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr, inf_done = nullptr;
+    // training runs on a second stream beside the eye pass (it needs neither;
+    // inference waits for it); the probes' own primary hits and exact gathers
+    // run on a third, beside the eye pass's tail
+    cudaStream_t side = nullptr, inf = nullptr, probe = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, eye_done = nullptr, inf_done = nullptr, probe_done = nullptr;
 };
 
 namespace {
@@ -116,6 +117,23 @@ int enqueue_frame(pm_learned_graph* g) {
     // most SMs idle while its slowest pixels finish, and training fills them
     CK(cudaEventRecord(g->fork, main_st));
     CK(cudaStreamWaitEvent(g->side, g->fork, 0));
+    // the probes: their pixels' primary hits traced from the camera and
+    // gathered exactly, on their own stream beside the eye pass
+    {
+        const DevScene S = dev_scene(ctx);
+        MapState& G = ctx->maps[PM_MAP_GLOBAL];
+        CK(cudaStreamWaitEvent(g->probe, g->fork, 0));
+        CK(probe_hits(S, g->cd, g->lo.tile, g->lo.probes, P<float4>(g->probe_pos), P<float4>(g->probe_nrm), g->probe));
+        GatherQueries PQ{};
+        PQ.n = g->nprobe;
+        PQ.pos4 = P<float4>(g->probe_pos);
+        PQ.nrm4 = P<float4>(g->probe_nrm);
+        PQ.flag_mask = 1u;
+        GatherOut PO{P<float>(g->probe_est), nullptr, nullptr, nullptr};
+        CK(gather(grid_of(G, G), PQ, g->ro.r_global, g->ro.k_global, 0, PO, status, g->probe));
+        CK(cudaEventRecord(g->probe_done, g->probe));
+        launches += 2;
+    }
     cudaStream_t st = g->side;
     if (g->steps > 0) {
         // the gradient starts at zero (each Adam step zeroes it after use); the
@@ -161,14 +179,9 @@ int enqueue_frame(pm_learned_graph* g) {
     CK(cudaEventRecord(g->overlap ? g->inf_done : g->join, ist));
     if (g->overlap) CK(cudaEventRecord(g->join, g->side));   // the training, joined at the frame's end
     const int T = g->lo.tile, Pn = g->lo.probes;
-    CK(learned_probes(g->cd, R, T, Pn, P<float4>(g->probe_pos), P<float4>(g->probe_nrm), P<uint32_t>(g->probe_req), st));
-    GatherQueries PQ{};
-    PQ.n = g->nprobe;
-    PQ.pos4 = P<float4>(g->probe_pos);
-    PQ.nrm4 = P<float4>(g->probe_nrm);
-    PQ.flag_mask = 1u;
-    GatherOut PO{P<float>(g->probe_est), nullptr, nullptr, nullptr};
-    CK(gather(grid_of(G, G), PQ, g->ro.r_global, g->ro.k_global, 0, PO, status, st));
+    CK(cudaStreamWaitEvent(st, g->probe_done, 0));   // the probes' records and exact estimates
+    CK(learned_probe_req(g->cd, R, T, Pn, P<float4>(g->probe_pos), P<float4>(g->probe_nrm), P<uint32_t>(g->probe_req),
+                         status, st));
     CK(cudaStreamWaitEvent(st, g->overlap ? g->inf_done : g->join, 0));   // the cache's answers
     unsigned long long* counts = P<unsigned long long>(g->counts);
     CK(cudaMemsetAsync(counts, 0, 32, st));
@@ -188,7 +201,7 @@ int enqueue_frame(pm_learned_graph* g) {
     const float tone_t = (float)std::pow((double)0.6f, -1);
     CK(resolve(S, g->cd, R, P<float>(g->est_g), nullptr, tone_t, g->out_rgb8, g->out_radiance, st));
     if (g->overlap) CK(cudaStreamWaitEvent(st, g->join, 0));   // the next frame's copy sees this frame's training
-    launches += 10;
+    launches += 9;   // eye, inference, probe requests, counts reset, tile flags, marks, fallback gather, merge, resolve
     g->launches_per_frame = launches;
     return PM_OK;
 }
@@ -200,6 +213,8 @@ void free_graph(pm_learned_graph* g) {
     if (g->join) cudaEventDestroy(g->join);
     if (g->eye_done) cudaEventDestroy(g->eye_done);
     if (g->inf_done) cudaEventDestroy(g->inf_done);
+    if (g->probe_done) cudaEventDestroy(g->probe_done);
+    if (g->probe) cudaStreamDestroy(g->probe);
     if (g->side) cudaStreamDestroy(g->side);
     if (g->inf) cudaStreamDestroy(g->inf);
     DevBuf* bufs[] = {&g->req_a, &g->req_b, &g->req_c, &g->counter, &g->px_base, &g->px_count, &g->est_mlp, &g->est_fb,
@@ -268,6 +283,8 @@ int pm_learned_graph_create(pm_ctx* ctx, const pm_camera* cam, const pm_render_o
         if ((e = need(*a.b, a.bytes)) != cudaSuccess) return bail(cuda_fail(ctx, e, "learned graph buffers"));
     if ((e = cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&g->inf, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&g->probe, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&g->probe_done, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->inf_done, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&g->join, cudaEventDisableTiming)) != cudaSuccess ||

@@ -168,6 +168,28 @@ __global__ void k_sample_hits(DevScene S, CameraDev cam, int64_t n, uint64_t see
     weight[i] = w;
 }
 
+// The record of one eye-path hit: (hit point, triangle), (shading normal,
+// flags); the model and material of the hit for the path's next step.
+__device__ __forceinline__ void hit_record(const DevScene& S, const Ray& ray, const Hit& h, bool in_obj, float4& a,
+                                          float4& b, int& model, Material& m, V3& n, V3& ip) {
+    model = hit_model(S, h.tri);
+    m = load_mat(S, model);
+    n = shading_normal(S, h);
+    ip = vadd(vscale(ray.d, h.t), ray.o);
+    if (in_obj && vdot(ray.d, n) > 0) n = vscale(n, -1.f);
+    V3 mdiff = tri_albedo(S, h.tri, m);
+    uint32_t flags = 2u | ((!in_obj && !vnull(mdiff)) ? 1u : 0u);
+    a = make_float4(ip.x, ip.y, ip.z, __int_as_float(h.tri));
+    b = make_float4(n.x, n.y, n.z, __uint_as_float(flags));
+}
+
+__device__ __forceinline__ Ray primary_ray(const CameraDev& cam, int x, int y) {
+    Ray ray;
+    ray.o = ld3(cam.pos);
+    ray.d = vnorm_div(camera_dir(cam, x, y));
+    return ray;
+}
+
 // the eye path of local pixel `li` (image of `cam`): its gather requests in hit
 // order (c.w = pixel bits `px`); returns the number of hits
 __device__ __forceinline__ int eye_hits(const DevScene& S, const CameraDev& cam, int D, int64_t li, uint32_t px,
@@ -176,9 +198,7 @@ __device__ __forceinline__ int eye_hits(const DevScene& S, const CameraDev& cam,
     const int64_t i = li;
     {
         const int x = (int)(i % cam.W), y = (int)(i / cam.W);
-        Ray ray;
-        ray.o = ld3(cam.pos);
-        ray.d = vnorm_div(camera_dir(cam, x, y));
+        Ray ray = primary_ray(cam, x, y);
         MediumState M;
         M.init(D);
         int new_depth = 0, cur = -1;
@@ -188,16 +208,14 @@ __device__ __forceinline__ int eye_hits(const DevScene& S, const CameraDev& cam,
             cur = new_depth;
             Hit h;
             if (!intersect(S, ray.o, ray.d, h)) continue;
-            const int model = hit_model(S, h.tri);
-            const Material m = load_mat(S, model);
-            V3 n = shading_normal(S, h);
-            V3 ip = vadd(vscale(ray.d, h.t), ray.o);
-            if (in_obj && vdot(ray.d, n) > 0) n = vscale(n, -1.f);
-            V3 mdiff = tri_albedo(S, h.tri, m);
-            uint32_t flags = 2u | ((!in_obj && !vnull(mdiff)) ? 1u : 0u);
+            int model;
+            Material m;
+            V3 n, ip;
+            float4 ra, rb;
+            hit_record(S, ray, h, in_obj, ra, rb, model, m, n, ip);
             if (nh < RENDER_MAX_HITS) {
-                ha[nh] = make_float4(ip.x, ip.y, ip.z, __int_as_float(h.tri));
-                hb[nh] = make_float4(n.x, n.y, n.z, __uint_as_float(flags));
+                ha[nh] = ra;
+                hb[nh] = rb;
                 hc[nh] = make_float4(coef.x, coef.y, coef.z, __uint_as_float(px));
                 nh++;
             } else {
@@ -415,6 +433,45 @@ cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32
     }
     k_request_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, n, aabb[0], aabb[1], aabb[2], sc[0], sc[1], sc[2],
                                                                  keys);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void k_probe_hits(DevScene S, CameraDev cam, int tile, int P, int tiles_x, int64_t nprobe,
+                             float4* __restrict__ ppos, float4* __restrict__ pnrm) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nprobe) return;
+    const int64_t t = s / P;
+    int dx, dy;
+    probe_xy((int)(s % P), P, tile, dx, dy);
+    const int x = (int)(t % tiles_x) * tile + dx, y = (int)(t / tiles_x) * tile + dy;
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = make_float4(0.f, 0.f, 1.f, 0.f);
+    if (x < cam.W && y < cam.H) {
+        const Ray ray = primary_ray(cam, x, y);
+        Hit h;
+        if (intersect(S, ray.o, ray.d, h)) {
+            int model;
+            Material m;
+            V3 n, ip;
+            float4 ra, rb;
+            hit_record(S, ray, h, false, ra, rb, model, m, n, ip);
+            if (__float_as_uint(rb.w) & 1u) {
+                a = ra;
+                b = make_float4(rb.x, rb.y, rb.z, __uint_as_float(1u));
+            }
+        }
+    }
+    ppos[s] = a;
+    pnrm[s] = b;
+}
+}  // namespace
+
+cudaError_t probe_hits(const DevScene& S, const CameraDev& cam, int tile, int P, float4* ppos, float4* pnrm,
+                       cudaStream_t st) {
+    const int tx = (cam.W + tile - 1) / tile, ty = (cam.H + tile - 1) / tile;
+    const int64_t n = (int64_t)tx * ty * P;
+    if (n <= 0) return cudaSuccess;
+    k_probe_hits<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, cam, tile, P, tx, n, ppos, pnrm);
     return cudaGetLastError();
 }
 

@@ -42,6 +42,24 @@ cudaError_t request_keys(const float4* a, int64_t n, const float aabb[6], uint32
 int64_t eye_blocks(int64_t npx);
 int eye_threads();
 
+// The k-th of P probe pixels of a tile x tile block: a g x g lattice
+// (g = ceil(sqrt(P))) of cell centres, row by row.
+__host__ __device__ inline void probe_xy(int k, int P, int T, int& dx, int& dy) {
+    int g = 1;
+    while (g * g < P) g++;
+    dx = ((k % g) * 2 + 1) * T / (2 * g);
+    dy = ((k / g) * 2 + 1) * T / (2 * g);
+}
+// The first gather request of P probe pixels per tile x tile block of the
+// image (probe s = tile s / P, lattice point s % P), traced directly from the
+// camera: where the pixel's primary ray hits a surface that needs the global
+// estimate, ppos = (hit point, triangle bits), pnrm = (shading normal, 1);
+// else (0, 0, 0, 0), (0, 0, 1, 0).  The same values (by the same device code)
+// as the eye pass's first request of those pixels, so the probes' exact
+// gathers can run before or beside the eye pass.
+cudaError_t probe_hits(const DevScene& S, const CameraDev& cam, int tile, int P, float4* ppos, float4* pnrm,
+                       cudaStream_t st);
+
 // ---- several instances in one launch: global pixel g of instance i lies in
 // [px_off[i], px_off[i+1]); requests and outputs are indexed by global pixel ----
 struct RenderInstDev {
