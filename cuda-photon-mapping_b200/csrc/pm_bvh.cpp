@@ -48,7 +48,7 @@ struct Task { int node, b, e, depth; };
 constexpr int BINS = 32;        // SAH bins per axis
 constexpr int LEAF_MAX = 4;     // larger ranges are always split
 constexpr float SAH_CT = 1.0f;  // cost of an interior visit (one 64-byte node, two slab tests) ...
-constexpr float SAH_CI = 1.2f;  // ... and of one triangle test (one 80-byte record)
+constexpr float SAH_CI = 1.2f;  // ... and of one triangle test (one 64-byte leaf-ordered record)
 
 }  // namespace
 
