@@ -38,10 +38,18 @@ struct MediumState {
     int nplans;
     Plan plans[MD];
     bool overflow;
+    bool zeroed;   // cont / dior / did hold their zeros (written on the first refraction)
     __device__ void init(int d) {
-        D = d; DC = (d + 1) / 2; outer_size = 0; nplans = 0; overflow = false;
+        D = d; DC = (d + 1) / 2; outer_size = 0; nplans = 0; overflow = false; zeroed = false;
+    }
+    // The storage starts zeroed; most eye paths never refract, so the zeros are
+    // written only when a path first reads or writes it (plans are always
+    // written before they are read).
+    __device__ void touch() {
+        if (zeroed) return;
         for (int i = 0; i < SLOTS; i++) cont[i] = 0;
         for (int i = 0; i < SLOTS * DCMAX; i++) { dior[i] = 0.f; did[i] = 0; }
+        zeroed = true;
     }
     __device__ int idx(int slot, int depth) {
         if (slot < 0 || slot > D + 1 || depth < 0 || depth >= DC) { overflow = true; return -1; }
@@ -60,6 +68,7 @@ struct Rgi { float n1, n2; bool in_obj; };
 __device__ Rgi get_refractive_indices(MediumState& M, float def, int model_id, float ior) {
     int L = M.outer_size;
     if (L == 0) return Rgi{def, ior, true};
+    M.touch();
     int s = M.cont[L - 1];
     if (s == 0) return Rgi{def, ior, true};
     if (M.id_at(L, s - 1) == model_id) {
@@ -69,6 +78,7 @@ __device__ Rgi get_refractive_indices(MediumState& M, float def, int model_id, f
     return Rgi{M.ior_at(L, s - 1), ior, true};
 }
 __device__ void increase_depth(MediumState& M, bool& max_level) {
+    M.touch();
     int L = M.outer_size;
     if (L == 0) { M.outer_size = 1; L = 1; }
     if (L < M.D) {
@@ -91,6 +101,7 @@ __device__ void reduce_depth(MediumState& M, bool& max_level) {
     max_level = false;
 }
 __device__ void inform(MediumState& M, int model_id, float ior, bool max_level) {
+    M.touch();
     int pos = M.outer_size - 1 - (max_level ? 0 : 1);
     if (pos < 0 || pos >= SLOTS) { M.overflow = true; return; }
     int s = M.cont[pos];
