@@ -156,6 +156,8 @@ GatherGrid grid_of(MapState& m, MapState& est_src) {
     G.cell = m.cell;
     G.S = m.S;
     G.guess = GATHER_GUESS;
+    G.pow_uniform = est_src.uniform_pow;
+    for (int c = 0; c < 3; c++) G.pw[c] = est_src.pow_value[c];
     return G;
 }
 

@@ -53,6 +53,18 @@ __device__ __forceinline__ V3 vnorm_div(V3 a) {
     return v3(a.x / l, a.y / l, a.z / l);
 }
 __device__ __forceinline__ float vmax3(V3 a) { return fmaxf(fmaxf(a.x, a.y), a.z); }
+// three-source float min / max (PTX min.f32 / max.f32 with three inputs,
+// sm_100 and later): one instruction for two fminf / fmaxf, the same value
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
 __device__ __forceinline__ V3 vmin1(V3 a, float m) { return v3(fminf(a.x, m), fminf(a.y, m), fminf(a.z, m)); }
 __device__ __forceinline__ bool vnear(V3 a, V3 b) {   // |a - b| < 1e-3 per component
     return fabsf(a.x - b.x) < 0.001f && fabsf(a.y - b.y) < 0.001f && fabsf(a.z - b.z) < 0.001f;

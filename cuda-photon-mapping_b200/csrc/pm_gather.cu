@@ -195,7 +195,7 @@ __device__ __forceinline__ void locate(float p, float mn, float cell, int g, int
 __device__ __forceinline__ float axis_gap(float q, float lo, float hi, bool open_lo, bool open_hi) {
     float a = open_lo ? 0.f : lo - q;
     float b = open_hi ? 0.f : q - hi;
-    return fmaxf(fmaxf(a, b), 0.f);
+    return fmax3(a, b, 0.f);
 }
 
 // u / d for 0 <= u < 2^22, d > 0: float estimate, one correction step
@@ -658,7 +658,9 @@ struct WarpWalk {
 };
 
 // one query (one warp): the k nearest photons within r of q and the estimate
-template <int UCAP, int NB>
+// (UNI: G.pow_uniform is honoured; the batch kernel, whose instance table is
+// copied per query, reads the power array instead and keeps its registers)
+template <int UCAP, int NB, bool UNI = true>
 __device__ __forceinline__ void gather_query(const GatherGrid& G, WarpStore<UCAP, NB>& U, int64_t i, V3 q, V3 nrm,
                                              float r, int k, int require_full, const GatherOut& O, int lane) {
     WarpWalk<UCAP, NB> W(G, U, q, r, k, lane);
@@ -684,27 +686,42 @@ __device__ __forceinline__ void gather_query(const GatherGrid& G, WarpStore<UCAP
     const unsigned long long kmax = cnt >= k ? W.T : (cnt ? warp_max_key(U, cnt, lane) : 0ull);
     const float rk = cnt ? __uint_as_float((uint32_t)(kmax >> 32)) : 0.f;
 
-    // estimate (Raytracer.cuh:110-138): lanes take entries, then a fixed-order reduction
+    // estimate (Raytracer.cuh:110-138): lanes take entries, then a fixed-order
+    // reduction.  The filter's two divisions (by 2 r_k^2 and by its norm) are
+    // multiplications by reciprocals taken once per query (the estimate
+    // changes by float rounding only); a map of uniform power takes each
+    // photon's power from the grid parameters instead of loading it (the same
+    // products and sums, so a traced map and the same photons given as a list
+    // give the same bits).
     V3 res = v3(0.f, 0.f, 0.f);
     if (cnt > 0 && !(require_full && cnt != k)) {
         const float alpha = 1.818f, beta = 1.953f;
         const float fr = rk * rk;
-        const float norm = 1.f - expf(-beta);
+        const float inv_2fr = 1.f / (2.f * fr);
+        const float inv_norm = 1.f / (1.f - expf(-beta));
+        const bool uni = UNI && G.pow_uniform;
+        const V3 pwu = UNI ? v3(G.pw[0], G.pw[1], G.pw[2]) : v3(0.f, 0.f, 0.f);
         for (int e0 = 0; e0 < cnt; e0 += 64) {
             const int ea = e0 + lane, eb = ea + 32;
             const bool va = ea < cnt, vb = eb < cnt;
             const uint32_t sa = va ? U.slot[ea] : 0u, sb = vb ? U.slot[eb] : 0u;
-            V3 pda = v3(0.f, 0.f, 0.f), pdb = pda, pwa = pda, pwb = pda;
-            if (va) { pda = ld3(G.gdir + 3 * (size_t)sa); pwa = ld3(G.gpow + 3 * (size_t)sa); }
-            if (vb) { pdb = ld3(G.gdir + 3 * (size_t)sb); pwb = ld3(G.gpow + 3 * (size_t)sb); }
+            V3 pda = v3(0.f, 0.f, 0.f), pdb = pda, pwa = pwu, pwb = pwu;
+            if (va) {
+                pda = ld3(G.gdir + 3 * (size_t)sa);
+                if (!uni) pwa = ld3(G.gpow + 3 * (size_t)sa);
+            }
+            if (vb) {
+                pdb = ld3(G.gdir + 3 * (size_t)sb);
+                if (!uni) pwb = ld3(G.gpow + 3 * (size_t)sb);
+            }
             if (va && vdot(nrm, vneg(pda)) > 0) {
-                float d = __uint_as_float((uint32_t)(U.key[ea] >> 32));
-                float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / norm);
+                const float d = __uint_as_float((uint32_t)(U.key[ea] >> 32));
+                const float filter = alpha * (1.f - (1.f - expf(-beta * d * d * inv_2fr)) * inv_norm);
                 res = vadd(res, vscale(pwa, filter));
             }
             if (vb && vdot(nrm, vneg(pdb)) > 0) {
-                float d = __uint_as_float((uint32_t)(U.key[eb] >> 32));
-                float filter = alpha * (1.f - (1.f - expf(-beta * d * d / (2 * fr))) / norm);
+                const float d = __uint_as_float((uint32_t)(U.key[eb] >> 32));
+                const float filter = alpha * (1.f - (1.f - expf(-beta * d * d * inv_2fr)) * inv_norm);
                 res = vadd(res, vscale(pwb, filter));
             }
         }
@@ -878,7 +895,7 @@ k_gather_multi(const GatherInstDev* __restrict__ tab, const int64_t* __restrict_
                 continue;
             }
             const GatherGrid G = T.G;
-            gather_query<UCAP, MULTI_BINS>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
+            gather_query<UCAP, MULTI_BINS, false>(G, U, i, xyz(a), xyz(b), T.r, T.k, 0, O, lane);
             __syncwarp();
         }
     }

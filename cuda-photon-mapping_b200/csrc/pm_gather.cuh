@@ -16,6 +16,8 @@ struct GatherGrid {
     int S;                     // sub-cells per cell axis
     float guess;               // the walk's first-ring bound is guessed to hold about guess x k photons
                                // (GATHER_GUESS by default; 0: no guess).  Speed only: answers do not change
+    bool pow_uniform;          // every photon has power pw (a traced map): the estimate reads no power array
+    float pw[3];
 };
 constexpr float GATHER_GUESS = 2.f;
 

@@ -224,9 +224,11 @@ struct Work {
     __device__ __forceinline__ void tris(int c) { tri_tests += (unsigned)c; }
 };
 
-// One round: descend until this lane holds a leaf (or every active lane does),
-// then test the held leaves.  Returns true when the pass is complete.
-template <class Stk, class W = NoWork>
+// One round: descend until this lane holds a leaf (or every active lane does,
+// or, CUT > 0, no more than CUT lanes still descend), then test the held
+// leaves.  Returns true when the pass is complete; a lane stopped before its
+// leaf keeps its place (node, stack) for the next round.
+template <int CUT = 0, class Stk, class W = NoWork>
 __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d, Stk& stack, W&& work = W()) {
     int node = T.node, leaf = T.leaf, sp = T.sp;
     // Box slabs as fused multiply-adds: the boxes are padded far beyond the
@@ -242,13 +244,13 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
         float t0x = __fmaf_rn(a0.x, ix, nox), t1x = __fmaf_rn(b0.x, ix, nox);
         float t0y = __fmaf_rn(a0.y, iy, noy), t1y = __fmaf_rn(b0.y, iy, noy);
         float t0z = __fmaf_rn(a0.z, iz, noz), t1z = __fmaf_rn(b0.z, iz, noz);
-        const float c0min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
-        const float c0max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
+        const float c0min = fmax3(fminf(t0x, t1x), fminf(t0y, t1y), fmaxf(fminf(t0z, t1z), 0.0f));
+        const float c0max = fmin3(fmaxf(t0x, t1x), fmaxf(t0y, t1y), fminf(fmaxf(t0z, t1z), best_t));
         t0x = __fmaf_rn(a1.x, ix, nox); t1x = __fmaf_rn(b1.x, ix, nox);
         t0y = __fmaf_rn(a1.y, iy, noy); t1y = __fmaf_rn(b1.y, iy, noy);
         t0z = __fmaf_rn(a1.z, iz, noz); t1z = __fmaf_rn(b1.z, iz, noz);
-        const float c1min = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
-        const float c1max = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), best_t));
+        const float c1min = fmax3(fminf(t0x, t1x), fminf(t0y, t1y), fmaxf(fminf(t0z, t1z), 0.0f));
+        const float c1max = fmin3(fmaxf(t0x, t1x), fmaxf(t0y, t1y), fminf(fmaxf(t0z, t1z), best_t));
         const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
         if (!h0 && !h1) {
             node = stack.get(sp--);
@@ -266,6 +268,7 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, Trav& T, V3 o, V3 d
             node = stack.get(sp--);
         }
         if (!__any_sync(__activemask(), leaf >= 0)) break;   // every lane holds a leaf
+        if (CUT > 0 && __popc(__activemask()) <= CUT) break;
     }
     while (leaf < 0) {
         const int packed = ~leaf;
