@@ -233,6 +233,25 @@ def test_grid_regrid_path_and_multi_pass_radix(ctx, orc):
     assert g.sizes.size > 256 * 256   # re-gridded; cell ids need three 8-bit passes
 
 
+@pytest.mark.parametrize("cluster,sub_div", [(5_000, 1), (5_000, 8), (20_000, 2), (40_000, 1)])
+def test_grid_dense_keys_and_radix_fallback(ctx, orc, cluster, sub_div):
+    # a tight cluster puts `cluster` photons into one cell and one sub-cell
+    # (its key's run in every radix pass is thousands of photons long), the
+    # rest are spread over the box
+    rng = np.random.default_rng(9)
+    n = cluster + 50_000
+    pos = np.concatenate([rng.normal(0.25, 1e-4, (cluster, 3)), rng.uniform(-1, 1, (n - cluster, 3))]).astype(np.float32)
+    pos = rng.permutation(np.clip(pos, -1, 1))
+    dr = rng.normal(size=(n, 3)).astype(np.float32)
+    pw = rng.uniform(1e-6, 1e-5, (n, 3)).astype(np.float32)
+    aabb = np.array([-1, -1, -1, 1, 1, 1], np.float32)
+    ctx.set_photons(0, pos, pw, dr)
+    ctx.build_grid(0, aabb=aabb, sub_div=sub_div)
+    g = _check_grid(ctx, orc, pos, pw, dr, aabb)
+    assert g.sizes.max() >= cluster
+    assert ctx.status() == 0
+
+
 def test_grid_fixture100(ctx, orc, golden_dir):
     f = np.load(os.path.join(golden_dir, "fixture100.npz"))
     ctx.set_photons(0, f["pos"], f["power"], f["dir"])
