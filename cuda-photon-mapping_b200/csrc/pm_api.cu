@@ -795,6 +795,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     G.n = C.n = 0;
     G.uniform_pow = C.uniform_pow = false;
     G.has_rec = C.has_rec = false;
+    G.lists_pending = C.lists_pending = G.spow_pending = C.spow_pending = false;
     ENSURE(G.rec, std::max<int64_t>(cg, 1) * 32); ENSURE(C.rec, std::max<int64_t>(cc, 1) * 32);
     ENSURE(G.pos, std::max<int64_t>(cg, 1) * 12); ENSURE(G.dir, std::max<int64_t>(cg, 1) * 12); ENSURE(G.pow, std::max<int64_t>(cg, 1) * 12);
     ENSURE(C.pos, std::max<int64_t>(cc, 1) * 12); ENSURE(C.dir, std::max<int64_t>(cc, 1) * 12); ENSURE(C.pow, std::max<int64_t>(cc, 1) * 12);
@@ -812,7 +813,9 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         double need = 0.0;
         if (need_g > 0) need = std::max(need, yg > 0 ? (double)need_g / yg : (double)MAX_BATCH);
         if (need_c > 0) need = std::max(need, yc > 0 ? (double)need_c / yc : (double)MAX_BATCH);
-        return std::min<int64_t>(MAX_BATCH, std::max<int64_t>(4096, (int64_t)(need * 1.01) + 1024));
+        // margin: the yield of 10M photons' worth of paths varies by about 3e-4
+        // between seeds; a short batch is followed by another one
+        return std::min<int64_t>(MAX_BATCH, std::max<int64_t>(4096, (int64_t)(need * 1.002) + 4096));
     };
     int64_t nb;
     if (ctx->yield_bounces == o->max_bounces && (ctx->yield_g > 0 || cg == 0) && (ctx->yield_c > 0 || cc == 0))
@@ -836,6 +839,9 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
         B.k_end = ctx->ev[13];
         PhotonList LG{P<float>(G.pos), P<float>(G.dir), P<float>(G.pow), cg, fg, P<float4>(G.rec)};
         PhotonList LC{P<float>(C.pos), P<float>(C.dir), P<float>(C.pow), cc, fc, P<float4>(C.rec)};
+        // the direction and power lists are left to fill_pending: the grid
+        // reads the records, and a traced map's power is uniform
+        LG.lists = LC.lists = false;
         CK(trace_batch(B, LG, LC, ctx->st));
         ctx->launches += 4;
         uint32_t tot[2] = {0, 0};
@@ -866,6 +872,7 @@ int pm_trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths) {
     for (MapState* m : {&G, &C}) {   // every photon of a traced map has power intensity / global capacity
         m->uniform_pow = true;
         m->has_rec = true;
+        m->lists_pending = true;
         for (int a = 0; a < 3; a++) m->pow_value[a] = power[a];
     }
     if (out_paths) *out_paths = p0;
@@ -932,6 +939,7 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
     m.built = false;
     m.uniform_pow = false;
     m.has_rec = false;
+    m.lists_pending = m.spow_pending = false;
     ENSURE(m.pos, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.dir, std::max<int64_t>(n, 1) * 12);
     ENSURE(m.pow, std::max<int64_t>(n, 1) * 12);
@@ -996,6 +1004,7 @@ int grid_issue(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb, G
     GridBuffers B;
     B.pos = P<float>(m.pos); B.dir = P<float>(m.dir); B.pow = P<float>(m.pow); B.n = n;
     B.uniform_pow = m.uniform_pow;
+    B.defer_pow = true;   // a uniform sorted power is written by fill_pending when asked for
     B.rec = m.has_rec ? P<float4>(m.rec) : nullptr;
     for (int a = 0; a < 3; a++) B.pow_value[a] = m.pow_value[a];
     B.cell_starts = P<uint32_t>(m.starts); B.cell_sizes = P<uint32_t>(m.sizes);
@@ -1037,6 +1046,22 @@ void grid_commit(pm_ctx* ctx, int map, const GridIssued& gi) {
     m.S = gi.S;
     std::memcpy(m.aabb, gi.box, 24);
     m.built = true;
+    m.spow_pending = m.uniform_pow;
+}
+
+// A traced map's direction and power lists, and its grid's sorted power, are
+// not written by the photon pass and the grid build (the grid reads the
+// 32-byte records, the estimate the uniform power): they are written here,
+// on the context stream, for the calls that hand them out.
+int fill_pending(pm_ctx* ctx, MapState& m) {
+    if (!m.lists_pending && !m.spow_pending) return PM_OK;
+    if (m.lists_pending)
+        CK(photon_lists_from_rec(P<float4>(m.rec), m.n, m.pow_value, P<float>(m.dir), P<float>(m.pow), ctx->st));
+    if (m.spow_pending && m.built)
+        CK(photon_lists_from_rec(nullptr, m.n, m.pow_value, nullptr, P<float>(m.gpow), ctx->st));
+    m.lists_pending = m.spow_pending = false;
+    CK(cudaStreamSynchronize(ctx->st));
+    return PM_OK;
 }
 
 }  // namespace
@@ -1056,6 +1081,8 @@ int pm_get_photons(pm_ctx* ctx, int map, pm_photon_view* out) {
     if (!ctx || !out) return PM_ERR_INVALID;
     if (int rc = valid_map(ctx, map)) return rc;
     MapState& m = ctx->maps[map];
+    CK(cudaSetDevice(ctx->device));
+    if (int rc = fill_pending(ctx, m)) return rc;
     std::memset(out, 0, sizeof *out);
     out->count = m.n;
     out->list_pos = P<float>(m.pos);
@@ -1081,6 +1108,8 @@ int pm_save_photons(pm_ctx* ctx, int map, const char* path) {
     if (!ctx || !path) return PM_ERR_INVALID;
     if (int rc = valid_map(ctx, map)) return rc;
     MapState& m = ctx->maps[map];
+    CK(cudaSetDevice(ctx->device));
+    if (int rc = fill_pending(ctx, m)) return rc;
     const int64_t n = m.n;
     try {
         std::vector<float> pos(3 * n), pw(3 * n), dir(3 * n);

@@ -23,6 +23,9 @@ struct MapState {
     DevBuf rec;                          // a traced list's (position, direction) records, 32 B per photon
     bool has_rec = false;                // rec holds the current list
     bool uniform_pow = false;            // every photon of the list has power pow_value (a traced map)
+    bool lists_pending = false;          // dir / pow lists not written yet (a traced map: rec and pow_value
+                                         // hold them; written by the first pm_get_photons / pm_save_photons)
+    bool spow_pending = false;           // the grid's sorted power not written yet (uniform: pow_value)
     float pow_value[3] = {0, 0, 0};
     bool built = false;
     int dims[3] = {0, 0, 0};

@@ -362,7 +362,8 @@ k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restri
 }
 
 // pw == nullptr: every photon has power pw0 (a traced map), so the power is
-// written without a random read of the source list.  rec != nullptr: the
+// written without a random read of the source list (gpow == nullptr: not
+// written at all).  rec != nullptr: the
 // photon's position and direction are read as one 32-byte record (one DRAM
 // sector) instead of two 12-byte pieces of the position and direction arrays.
 __global__ void k_grid_gather(const uint32_t* __restrict__ order, int64_t n, const float* __restrict__ pos,
@@ -386,6 +387,7 @@ __global__ void k_grid_gather(const uint32_t* __restrict__ order, int64_t n, con
     }
     gpos[j] = make_float4(pp.x, pp.y, pp.z, __uint_as_float(s));
     gdir[3 * j] = dd.x; gdir[3 * j + 1] = dd.y; gdir[3 * j + 2] = dd.z;
+    if (!gpow) return;
     float3 w = pw0;
     if (pw) {
         const float* q = pw + 3 * (int64_t)s;
@@ -558,7 +560,8 @@ cudaError_t radix_and_gather(GridBuffers& B, int64_t n, int64_t key_space, int* 
     if (e != cudaSuccess) return e;
     k_grid_gather<<<blocks_for(n, 256), 256, 0, st>>>(
         order, n, B.pos, B.dir, B.rec, B.uniform_pow ? nullptr : B.pow,
-        make_float3(B.pow_value[0], B.pow_value[1], B.pow_value[2]), B.gpos, B.gdir, B.gpow, B.status);
+        make_float3(B.pow_value[0], B.pow_value[1], B.pow_value[2]), B.gpos, B.gdir,
+        B.uniform_pow && B.defer_pow ? nullptr : B.gpow, B.status);
     *launches += 1;
     return cudaGetLastError();
 }

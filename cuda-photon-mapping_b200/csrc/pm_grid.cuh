@@ -16,6 +16,8 @@ struct GridBuffers {
     const float* pow;
     const float4* rec = nullptr;   // when set: (position, 0), (direction, 0) per photon, gathered as one record
     bool uniform_pow = false;   // every photon has power pow_value: the sorted power is written, not gathered
+    bool defer_pow = false;     // with uniform_pow: the sorted power is not written at all (the caller fills
+                                // it with pow_value when it is asked for)
     float pow_value[3] = {0.f, 0.f, 0.f};
     int64_t n;
     // outputs (sized by grid_build_sizes)

@@ -495,6 +495,16 @@ __global__ void k_compact_multi(int64_t total, const int64_t* __restrict__ off, 
     }
 }
 
+__global__ void k_lists_from_rec(const float4* __restrict__ rec, int64_t n, V3 pw, float* dir, float* pow) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (dir) {
+        const float4 d = rec[2 * i + 1];
+        dir[3 * i] = d.x; dir[3 * i + 1] = d.y; dir[3 * i + 2] = d.z;
+    }
+    pow[3 * i] = pw.x; pow[3 * i + 1] = pw.y; pow[3 * i + 2] = pw.z;
+}
+
 // canonical-order append of one batch into the two photon lists
 // (rec lists, when set: each photon's position and direction also as one
 // 32-byte record, which the grid build gathers with one sector read)
@@ -502,7 +512,8 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
                           const uint32_t* __restrict__ cnt_g, const uint32_t* __restrict__ cnt_c,
                           const uint32_t* __restrict__ scan_g, const uint32_t* __restrict__ scan_c, V3 power,
                           float* gpos, float* gdir, float* gpow, int64_t gcap, int64_t gfilled, float4* grec,
-                          float* cpos, float* cdir, float* cpow, int64_t ccap, int64_t cfilled, float4* crec) {
+                          bool glists, float* cpos, float* cdir, float* cpow, int64_t ccap, int64_t cfilled,
+                          float4* crec, bool clists) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= npaths) return;
     int ng = (int)cnt_g[j], nc = (int)cnt_c[j];
@@ -514,17 +525,20 @@ __global__ void k_compact(int64_t npaths, const float4* __restrict__ stage,
         bool caustic = __float_as_int(p.w) == 2;
         float *dp, *dd, *dw;
         float4* dr;
+        bool lists;
         int64_t idx;
         if (caustic) {
             if (oc >= ccap) { oc++; continue; }
-            idx = oc++; dp = cpos; dd = cdir; dw = cpow; dr = crec;
+            idx = oc++; dp = cpos; dd = cdir; dw = cpow; dr = crec; lists = clists;
         } else {
             if (og >= gcap) { og++; continue; }
-            idx = og++; dp = gpos; dd = gdir; dw = gpow; dr = grec;
+            idx = og++; dp = gpos; dd = gdir; dw = gpow; dr = grec; lists = glists;
         }
         dp[3 * idx] = p.x; dp[3 * idx + 1] = p.y; dp[3 * idx + 2] = p.z;
-        dd[3 * idx] = d.x; dd[3 * idx + 1] = d.y; dd[3 * idx + 2] = d.z;
-        dw[3 * idx] = power.x; dw[3 * idx + 1] = power.y; dw[3 * idx + 2] = power.z;
+        if (lists) {   // else rec carries the direction and the power is the batch's
+            dd[3 * idx] = d.x; dd[3 * idx + 1] = d.y; dd[3 * idx + 2] = d.z;
+            dw[3 * idx] = power.x; dw[3 * idx + 1] = power.y; dw[3 * idx + 2] = power.z;
+        }
         if (dr) {
             dr[2 * idx] = make_float4(p.x, p.y, p.z, 0.f);
             dr[2 * idx + 1] = make_float4(d.x, d.y, d.z, 0.f);
@@ -609,7 +623,15 @@ cudaError_t trace_batch(TraceBatch& B, PhotonList& G, PhotonList& C, cudaStream_
         return e;
     k_compact<<<(unsigned)((B.npaths + 255) / 256), 256, 0, st>>>(
         B.npaths, B.stage, B.cnt_g, B.cnt_c, B.scan_g, B.scan_c, P.power,
-        G.pos, G.dir, G.pow, G.cap, G.filled, G.rec, C.pos, C.dir, C.pow, C.cap, C.filled, C.rec);
+        G.pos, G.dir, G.pow, G.cap, G.filled, G.rec, G.lists || !G.rec, C.pos, C.dir, C.pow, C.cap, C.filled, C.rec,
+        C.lists || !C.rec);
+    return cudaGetLastError();
+}
+
+cudaError_t photon_lists_from_rec(const float4* rec, int64_t n, const float pw[3], float* dir, float* pow,
+                                  cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_lists_from_rec<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(rec, n, v3(pw[0], pw[1], pw[2]), dir, pow);
     return cudaGetLastError();
 }
 

@@ -37,7 +37,14 @@ struct PhotonList {
     int64_t cap;
     int64_t filled;           // photons already in the list before this batch
     float4* rec = nullptr;    // when set: also (position, 0), (direction, 0) per photon, 32-byte aligned
+    bool lists = true;        // false (with rec set): dir and pow are not written; photon_lists_from_rec
+                              // fills them later from rec and the batch's power
 };
+
+// dir[i] = rec[2i + 1].xyz and pow[i] = pw for i < n (the lists a batch traced
+// with PhotonList::lists = false left unwritten); pow only when dir is null
+cudaError_t photon_lists_from_rec(const float4* rec, int64_t n, const float pw[3], float* dir, float* pow,
+                                  cudaStream_t st);
 
 // ---- several scene instances in one launch (global map only) ----
 struct TraceInst {

@@ -189,6 +189,13 @@ int pm_set_photons(pm_ctx* ctx, int map, int64_t n, const float* pos, const floa
 /* Grid build.  Replaces PhotonGrid(num_photons, aabb).build(photons, 1000,
  * 5000) (PhotonGrid.cuh:44-66, PhotonGrid.cu:41-218).  aabb: NULL = scene AABB. */
 int pm_build_grid(pm_ctx* ctx, int map, const pm_grid_opts* opts, const float* aabb);
+
+/* Device pointers to a map's photon list and grid (valid until the next call
+ * that replaces them).  A traced map's direction and power lists and its
+ * grid's sorted power are not written by the photon pass and the grid build
+ * (the grid reads 32-byte position + direction records, the gather the
+ * uniform power); the first pm_get_photons or pm_save_photons after them
+ * writes them on the context stream and synchronises it. */
 int pm_get_photons(pm_ctx* ctx, int map, pm_photon_view* out);
 
 /* Photon-map file in the reference's layout: u64 count, then per photon

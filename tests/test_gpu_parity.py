@@ -77,6 +77,29 @@ def test_scene_aabb_and_tracer_matches_oracle(ctx, cornell):
     assert np.array_equal(_np(ph["list_power"]), tr["g_pow"])
 
 
+def test_traced_map_grid_arrays_written_when_asked(ctx, orc, cornell):
+    # a traced map's direction / power lists and its grid's sorted power are
+    # written by the first photons() call after the photon pass / grid build;
+    # the grid itself equals the oracle's grid of the same photons
+    sc, cam, w, s = cornell
+    ctx.set_scene(sc)
+    ctx.trace_photons(4, w["max_bounces"], 40_000, 3_000)
+    ctx.build_grid(0)
+    ctx.build_grid(1)
+    tr = s.trace_photons(4, w["max_bounces"], 40_000, 3_000)
+    for map_id, key in ((0, "g"), (1, "c")):
+        ph = ctx.photons(map_id)
+        g = orc.grid_build(tr[f"{key}_pos"], tr[f"{key}_pow"], tr[f"{key}_dir"], s.aabb(), sub_div=ph["sub_div"])
+        sp = _np(ph["sorted_pos"])
+        assert np.array_equal(sp[:, :3], g.spos) and np.array_equal(sp[:, 3].view(np.uint32), g.sid)
+        assert np.array_equal(_np(ph["sorted_dir"]), g.sdir)
+        assert np.array_equal(_np(ph["sorted_power"]), g.spow)
+        lst = ctx.photons(map_id, sorted_=False)
+        assert np.array_equal(_np(lst["list_dir"]), tr[f"{key}_dir"])
+        assert np.array_equal(_np(lst["list_power"]), tr[f"{key}_pow"])
+    assert ctx.status() == 0
+
+
 def test_trace_with_caustic_map(ctx, cornell):
     sc, cam, w, s = cornell
     paths = ctx.trace_photons(3, 8, 20_000, 2_000)
