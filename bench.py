@@ -563,7 +563,7 @@ def learned_rmse(ctx, sc, cs, cam, w):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # default workload's two large kernels: constants from one ncu capture of the
 # timed step's launches (the line names the capture in "traffic_source")
-DRAM_TRAFFIC = {"k_trace": 164_207_616 + 447_744_000, "k_gather": 452_934_912 + 14_981_888}
+DRAM_TRAFFIC = {"k_trace": 145_125_888 + 425_197_056, "k_gather": 333_065_984 + 13_496_320}
 TRAFFIC_SOURCE = ("constant from one ncu capture of the default workload (the timed step's launches): ncu --metrics "
                   "dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none "
                   "-k regex:'k_trace|k_gather|k_compact|k_grid_gather' -c 12 "
