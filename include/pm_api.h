@@ -295,7 +295,10 @@ int pm_scan_u32_noalloc(const uint32_t* in, uint32_t* out, int64_t n, int inclus
  * [0] trace, [1] grid build (global map), [2] eye pass, [3] gather (request
  * ordering + global gather + caustic gather; in pm_frame the ordering runs
  * beside the grid build and is not counted here), [4] resolve, [5] the k_trace
- * kernels alone, [6] the global gather kernel alone. */
+ * kernels alone, [6] the global gather kernel alone.  In pm_frame the eye pass
+ * is queued beside the photon pass, so [2] spans the photon pass as well and
+ * [0] includes the eye blocks' share of the GPU; [1] runs from the grid
+ * build's start to the gather's start (the join of both streams). */
 int pm_stage_times(pm_ctx* ctx, float out_ms[8]);
 
 /* ---------------------------------------------------------------------------
