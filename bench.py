@@ -662,7 +662,7 @@ def run_ours(args):
 
     def step(i, e2e=False):
         # pm_frame: photon pass, grid build and frame in one call (the eye pass
-        # runs beside the grid build); same photons and image as
+        # runs beside the photon pass); same photons and image as
         # trace_photons + build_grid + render
         b = i % 2 if e2e else 0
         if e2e and copied[b] is not None:
