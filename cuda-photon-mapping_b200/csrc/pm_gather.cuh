@@ -19,7 +19,11 @@ struct GatherGrid {
     bool pow_uniform;          // every photon has power pw (a traced map): the estimate reads no power array
     float pw[3];
 };
-constexpr float GATHER_GUESS = 2.f;
+// 1080p frame of 10M photons, k 64: 2.0 -> 3.07 ms, 1.6 -> 3.03, 1.5 -> 3.02,
+// 1.4 -> 3.01, 1.2 -> 3.21 (more walks restart); k 200 at r 0.02 on 30M
+// photons: 7.03 ms at 2.0 and 1.6, 7.04 at 1.5, 7.07 at 1.4 (and on the
+// 100M-photon 4K frame 1.5 measured 27.9 ms against 27.4 at 2.0)
+constexpr float GATHER_GUESS = 1.6f;
 
 struct GatherQueries {
     int64_t n;
