@@ -109,9 +109,9 @@ DevScene dev_scene(pm_ctx* c) {
 
 int check_status(pm_ctx* ctx, const char* what) {
     if (int rc = cache_fence(ctx)) return rc;
-    uint32_t bits = 0;
-    CK(cudaMemcpyAsync(&bits, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ctx->hbuf, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    const uint32_t bits = ctx->hbuf[0];
     if (bits) {
         CK(cudaMemsetAsync(ctx->status.p, 0, 4, ctx->st));
         char buf[160];
@@ -285,6 +285,9 @@ int pm_create(pm_ctx** out, const pm_device_opts* opts) {
     ctx->device = opts ? opts->device : 0;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) { delete ctx; return PM_ERR_CUDA; }
+    e = cudaHostAlloc((void**)&ctx->hbuf, 64, cudaHostAllocDefault);
+    if (e != cudaSuccess) { ctx->hbuf = nullptr; delete ctx; return PM_ERR_OOM; }
+    std::memset(ctx->hbuf, 0, 64);
     if (opts && opts->stream) {
         ctx->st = (cudaStream_t)opts->stream;
     } else {
@@ -320,6 +323,7 @@ void pm_destroy(pm_ctx* ctx) {
         cudaStreamDestroy(ctx->frame_st);
     }
     if (ctx->frame_fork) cudaEventDestroy(ctx->frame_fork);
+    if (ctx->hbuf) cudaFreeHost(ctx->hbuf);
     if (ctx->frame_done) cudaEventDestroy(ctx->frame_done);
     if (ctx->train_fork) cudaEventDestroy(ctx->train_fork);
     if (ctx->train_done) cudaEventDestroy(ctx->train_done);
@@ -850,9 +854,9 @@ int trace_photons(pm_ctx* ctx, const pm_trace_opts* o, int64_t* out_paths, const
         CK(trace_batch(B, LG, LC, ctx->st));
         if (p0 == 0 && after_launch) after_launch();
         ctx->launches += 4;
-        uint32_t tot[2] = {0, 0};
-        CK(cudaMemcpyAsync(tot, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(ctx->hbuf + 2, B.totals, 8, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
+        uint32_t tot[2] = {ctx->hbuf[2], ctx->hbuf[3]};
         if (cc == 0) tot[1] = 0;   // no caustic map: its total was not scanned
         k_trace_ms += elapsed(ctx->ev[12], ctx->ev[13]);
         got_g += tot[0];
@@ -1023,6 +1027,7 @@ int grid_issue(pm_ctx* ctx, int map, const pm_grid_opts* o, const float* aabb, G
     B.cid = P<uint32_t>(m.cid);
     B.keys[0] = P<uint32_t>(m.keys0); B.keys[1] = P<uint32_t>(m.keys1);
     B.vals[0] = P<uint32_t>(m.vals0); B.vals[1] = P<uint32_t>(m.vals1);
+    B.host_words = ctx->hbuf + 4;
     B.small = P<uint32_t>(m.small);
     B.counts2 = P<uint32_t>(m.counts2);
     B.status = P<unsigned>(ctx->status);
@@ -1312,9 +1317,10 @@ int render_eye_launch(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* o
 // the request count of the eye pass (ordered on ctx->st)
 int render_eye_count(pm_ctx* ctx, FrameSetup& F, cudaStream_t st = nullptr) {
     if (!st) st = ctx->st;
-    unsigned long long nreq = 0;
-    CK(cudaMemcpyAsync(&nreq, F.R.counter, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ctx->hbuf + 6, F.R.counter, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    unsigned long long nreq = 0;
+    std::memcpy(&nreq, ctx->hbuf + 6, 8);
     F.nreq = (int64_t)std::min<unsigned long long>(nreq, (unsigned long long)F.cap);
     ctx->last_requests = F.nreq;
     ctx->last_pixels = F.npx;

@@ -43,6 +43,10 @@ struct pm_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
     bool own_stream = false;
+    // pinned host words the small per-call device reads land in (a read into
+    // pageable memory is staged by the driver): [0] status, [2..3] photon
+    // totals, [4..5] grid count maxima, [6..7] request count
+    uint32_t* hbuf = nullptr;
     std::string err;
     int sm_count = 148;
     int trace_refill = 0;      // k_trace refill threshold; 0: the kernel's default

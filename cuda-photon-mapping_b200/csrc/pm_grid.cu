@@ -472,7 +472,8 @@ cudaError_t grid_count(GridBuffers& B, const float aabb[6], int desired, int reg
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         launches = 1;
     }
-    uint32_t mx[2] = {0u, 0u};
+    uint32_t stack_mx[2] = {0u, 0u};
+    uint32_t* mx = B.host_words ? B.host_words : stack_mx;
     if ((e = cudaMemcpyAsync(mx, B.small, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
     pa.max_count = mx[0];

@@ -36,6 +36,7 @@ struct GridBuffers {
     uint32_t* hist;       // 512 * tiles
     void* scan_ws;
     uint32_t* small;      // 16 u32 of device scratch (max count, totals)
+    uint32_t* host_words = nullptr;   // 2 pinned host words the count maxima are read into (else the stack)
     unsigned* status;
 };
 

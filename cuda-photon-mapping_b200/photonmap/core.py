@@ -560,7 +560,7 @@ class Context:
               caustic_capacity=0, k_caustic=0, r_caustic=0.2, faithful_caustic=True, desired=1000, sub_div=0,
               radiance=True, out_rgb8=None, out_radiance=None):
         """Photon pass + grid build(s) + frame in one call (pm_frame; the eye pass
-        runs beside the grid build).  Returns (rgb8, radiance, paths traced)."""
+        runs beside the photon pass).  Returns (rgb8, radiance, paths traced)."""
         torch = self.torch
         W, H = cam.width, cam.height
         rgb = out_rgb8 if out_rgb8 is not None else torch.empty((H * W * 3,), dtype=torch.uint8, device=self.device)
