@@ -88,7 +88,8 @@ struct pm_ctx {
     // learned graph reads (scene, photon lists, grids, cache): a graph made
     // before such a call refuses to run
     uint64_t generation = 0;
-    // pm_frame's eye pass runs on its own stream beside the grid build
+    // pm_frame's eye pass runs on its own stream beside the photon pass, its
+    // request ordering beside the grid build
     cudaStream_t frame_st = nullptr;
     cudaEvent_t frame_fork = nullptr, frame_done = nullptr;
     bool eye_order_valid = false;   // eye_order holds the order for eye_order_cam on this scene

@@ -236,8 +236,10 @@ int pm_render_rows(pm_ctx* ctx, const pm_camera* cam, const pm_render_opts* opts
 /* A whole frame in one call: pm_trace_photons(trace), pm_build_grid of the
  * global map (and of the caustic map when trace fills one and k_caustic > 0)
  * with grid, then pm_render's frame.  The eye pass needs neither the photons
- * nor the grid, so it runs on a second stream of the context beside the grid
- * build, followed there by the ordering of its requests for the gather.
+ * nor the grid, so it is queued on a second stream of the context right after
+ * the photon pass's kernels (its blocks take the tracer's SMs as its last
+ * paths end), followed there by the ordering of its requests for the gather,
+ * beside the grid build.
  * Results are pm_trace_photons + pm_build_grid + pm_render's
  * (Initializer.cu:142-177 followed by Drawer::draw_in_gpu, Drawer.cu:22-41). */
 int pm_frame(pm_ctx* ctx, const pm_trace_opts* trace, const pm_grid_opts* grid, const pm_camera* cam,
