@@ -563,11 +563,10 @@ def learned_rmse(ctx, sc, cs, cam, w):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # default workload's two large kernels: constants from one ncu capture of the
 # timed step's launches (the line names the capture in "traffic_source")
-DRAM_TRAFFIC = {"k_trace": 145_125_888 + 425_197_056, "k_gather": 333_065_984 + 13_496_320}
+DRAM_TRAFFIC = {"k_trace": 149_363_200 + 429_206_272, "k_gather": 333_646_592 + 13_331_456}
 TRAFFIC_SOURCE = ("constant from one ncu capture of the default workload (the timed step's launches): ncu --metrics "
-                  "dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none "
-                  "-k regex:'k_trace|k_gather|k_compact|k_grid_gather' -c 12 "
-                  "python bench.py --steps 1 --warmup 1 --no-cpu-baseline --no-learned --no-batched")
+                  "gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum --clock-control none "
+                  "-c 400 python bench.py --steps 1 --warmup 1 --no-cpu-baseline --no-learned --no-batched")
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SMs x 128 FP32 lanes x 2 flop (FMA) x 1965 MHz
 FLOP_PER_BOX_TEST = 20      # one child-box slab test (6 FMA, 6 min/max, 4 min/max and compares)
 FLOP_PER_TRI_TEST = 86      # the reference's count for its triangle test (CudaPhotonMapping/Model.cuh:65-67)
