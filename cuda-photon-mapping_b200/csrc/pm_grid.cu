@@ -30,8 +30,13 @@ namespace pm {
 
 namespace {
 
-constexpr int RADIX_THREADS = 256;
-constexpr int RADIX_ITEMS = 16;
+// 512 threads of 8 keys per tile (3 blocks, 48 warps per SM): grid build
+// 1.10 -> 1.03 ms per 10M photons against 256 x 16 (4 blocks, 32 warps) and
+// 256 x 8 (5 or 6 blocks, 1.07 ms); the ranking and staging phases are
+// latency bound, so more resident warps per SM pay.  RADIX_THREADS <=
+// RADIX_MAX_BINS (each thread owns whole bins in the downsweep's prefix).
+constexpr int RADIX_THREADS = 512;
+constexpr int RADIX_ITEMS = 8;
 constexpr int RADIX_TILE = RADIX_THREADS * RADIX_ITEMS;
 constexpr int RADIX_WARPS = RADIX_THREADS / 32;
 constexpr int RADIX_MAX_BITS = 9;
@@ -238,7 +243,7 @@ k_radix_upsweep(const uint32_t* __restrict__ keys, int64_t n, int shift, int bit
     for (int b = tid; b < bins; b += RADIX_THREADS) hist[(int64_t)b * tiles + blockIdx.x] = h[b];
 }
 
-// Stable scatter of one radix pass.  A warp owns 512 consecutive keys and walks
+// Stable scatter of one radix pass.  A warp owns 256 consecutive keys and walks
 // them 32 at a time in order; equal digits inside a step are ranked by lane
 // (the lanes of a digit found by one ballot per digit bit: grid build 1.14 ->
 // 1.10 ms against __match_any_sync), across steps by a per-warp running
@@ -256,7 +261,7 @@ struct RadixSmem {
     uint32_t val[RADIX_TILE];
 };
 
-__global__ void __launch_bounds__(RADIX_THREADS, 4)   // 4 blocks per SM: the shared-memory limit
+__global__ void __launch_bounds__(RADIX_THREADS, 3)   // 3 blocks per SM: the shared-memory limit
 k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, int64_t n, int shift,
                   int bits, const uint32_t* __restrict__ offsets, int tiles, uint32_t* __restrict__ keys_out,
                   uint32_t* __restrict__ vals_out) {
@@ -305,6 +310,7 @@ k_radix_downsweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restri
     __syncthreads();
     // per digit: exclusive prefix over warps; the tile's count of the digit
     constexpr int BPT = RADIX_MAX_BINS / RADIX_THREADS;   // bins per thread
+    static_assert(BPT >= 1, "a thread owns at least one bin");
     uint32_t tot[BPT], part = 0;
 #pragma unroll
     for (int q = 0; q < BPT; q++) {
