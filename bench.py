@@ -370,8 +370,8 @@ LEARNED = dict(train_per_frame=1 << 20, batch=1 << 18, warm_steps=3000, pool_sam
 def learned_frames(ctx, sc, cs, cam, w, rgb, args, world):
     """Frame time of the plain render against the learned render on the same
     photon map (the map stays resident, as in the reference's render loop).
-    Learned frame = online training on 2^20 pooled samples (
-    1M seeded surface points per frame) + the cache-answered render with its
+    Learned frame = online training on 2^20 pooled samples (the learned-cache
+    configuration: 1M seeded surface points per frame) + the cache-answered render with its
     per-tile exact-gather fallback.  The pool (stratified primary hits
     labelled by the kNN gather, at least 2^20 of them) is built once per map;
     the cache's first fit (warm_steps Adam steps) is a one-time cost reported

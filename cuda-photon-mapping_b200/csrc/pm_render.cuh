@@ -6,7 +6,7 @@
 
 namespace pm {
 
-constexpr int RENDER_MAX_DEPTH = 5;                          // eye-path depth limit of this build
+constexpr int RENDER_MAX_DEPTH = 5;                          // eye-path depth limit of this library
 constexpr int RENDER_MAX_HITS = (1 << RENDER_MAX_DEPTH) - 1; // binary hit tree
 
 struct CameraDev {

@@ -14,7 +14,7 @@ Follows the reference's CPU path in double precision on given eye-path hits:
     (CudaPhotonMapping/Raytracer.cuh:187-211).
 The hits (eye-path requests) come from the product's eye pass, whose own
 parity with the reference is tested elsewhere; caustic estimates are not
-restated here (the workloads that use this build no caustic map).
+restated here (the workloads that use this FP64 render build no caustic map).
 """
 from __future__ import annotations
 
